@@ -1,0 +1,163 @@
+"""hydist_c_b200 -- B200 (sm_100a) implementation of the Hydist_C ADI time step.
+
+Python mirror of the reference's entry points for this path, over the C ABI
+of ``libhydist_b200.so`` (include/hydist_capi.h):
+
+=======================================  =====================================
+reference (Hydist_C)                     here
+=======================================  =====================================
+main.cpp:138-304 set-up sequence         ``Simulation(bundle)``
+Hydraulic_Calculation (engine.cpp:41)    ``Simulation.hydraulic_calculation``
+one pass of its time loop                ``Simulation.step`` / ``step_graph``
+synch_and_check (engine.cpp:13)          ``Simulation.sync``
+save_result / save_FS (loader.cpp:397)   ``Simulation.download``
+tridiag / gtsv_spike_partial_diag_pivot  ``gtsv_batched``
+=======================================  =====================================
+
+Errors are raised as :class:`HydistError`; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import capi, scenario
+from .capi import FIELDS, FP32_REFINE, FP64, HydistError
+
+__all__ = ["Simulation", "gtsv_batched", "HydistError", "scenario", "FP64", "FP32_REFINE",
+           "FIELDS", "library"]
+
+
+def library():
+    return capi.load_library()
+
+
+class Simulation:
+    """One scenario resident on a GPU (the reference's Argument_Pointers,
+    Array_Pointers and Constant_Coeffs of one run, engine.h:39-78)."""
+
+    def __init__(self, bundle: dict, device: int = 0, precision: int | None = None):
+        lib = capi.load_library()
+        sc = bundle["scenario"]
+        self.M, self.N = int(sc["M"]), int(sc["N"])
+        self.shape = (self.N + 3, self.M + 3)
+        self._ss = capi.ScenarioStruct(sc)
+        self._p = capi.params_from_dict(bundle.get("params", {}))
+        opts = dict(bundle.get("options", {}))
+        if precision is not None:
+            opts["precision"] = int(precision)
+        self._o = capi.options_from_dict(opts)
+        h = C.c_void_p()
+        st = lib.hydist_create(C.byref(self._ss.struct), C.byref(self._p), C.byref(self._o),
+                               int(device), C.byref(h))
+        capi.check(lib, st, "hydist_create")
+        self._h = h
+        self._lib = lib
+        self.dT = float(self._p.dT)
+
+    # -- lifecycle
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.hydist_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- time stepping
+    def step(self, n: int = 1):
+        capi.check(self._lib, self._lib.hydist_step(self._h, int(n)), "hydist_step")
+
+    def step_graph(self, n: int = 1):
+        capi.check(self._lib, self._lib.hydist_step_graph(self._h, int(n)), "hydist_step_graph")
+
+    def hydraulic_calculation(self, Tmax: float, graph: bool = False):
+        """Advance while t < Tmax, one full step (two half-steps) at a time,
+        as the while-loop of Hydraulic_Calculation (engine.cpp:65)."""
+        n = 0
+        t = self.t
+        while t < int(Tmax):
+            t += self.dT
+            n += 1
+        if n:
+            (self.step_graph if graph else self.step)(n)
+        return n
+
+    def sync(self):
+        capi.check(self._lib, self._lib.hydist_sync(self._h), "hydist_sync")
+
+    @property
+    def t(self) -> float:
+        v = C.c_double()
+        capi.check(self._lib, self._lib.hydist_get_time(self._h, C.byref(v)), "hydist_get_time")
+        return v.value
+
+    @t.setter
+    def t(self, value: float):
+        capi.check(self._lib, self._lib.hydist_set_time(self._h, float(value)), "hydist_set_time")
+
+    @property
+    def stream(self) -> int:
+        return int(self._lib.hydist_stream(self._h) or 0)
+
+    # -- fields
+    def download(self, name: str) -> np.ndarray:
+        f = FIELDS[name]
+        out = np.empty(self.shape, dtype=np.int32 if name == "khouot" else np.float64)
+        capi.check(self._lib, self._lib.hydist_download(self._h, f, out.ctypes.data),
+                   "hydist_download")
+        return out
+
+    def upload(self, name: str, arr):
+        f = FIELDS[name]
+        a = np.ascontiguousarray(arr, dtype=np.int32 if name == "khouot" else np.float64)
+        if a.shape != self.shape:
+            raise ValueError(f"{name}: expected shape {self.shape}, got {a.shape}")
+        capi.check(self._lib, self._lib.hydist_upload(self._h, f, a.ctypes.data), "hydist_upload")
+
+    def mass(self) -> float:
+        v = C.c_double()
+        capi.check(self._lib, self._lib.hydist_mass(self._h, C.byref(v)), "hydist_mass")
+        return v.value
+
+
+def gtsv_batched(dl, d, du, b, offsets, lengths, algo: int = 0, x=None, stream=None):
+    """Solve a packed batch of tridiagonal systems on the GPU.
+
+    Arguments are CUDA tensors (torch) of one dtype (float64 or float32);
+    offsets/lengths are int32 CUDA tensors. Returns x. algo: 0 autotuned,
+    1 Thomas, 2 partitioned Thomas/SPIKE with diagonal pivoting, 3 PCR-Thomas.
+    """
+    import torch
+
+    lib = capi.load_library()
+    if d.dtype == torch.float64:
+        dt = 0
+    elif d.dtype == torch.float32:
+        dt = 1
+    else:
+        raise TypeError("float64 or float32 expected")
+    for t in (dl, d, du, b):
+        if not (t.is_cuda and t.is_contiguous() and t.dtype == d.dtype):
+            raise ValueError("dl, d, du, b must be contiguous CUDA tensors of one dtype")
+    if x is None:
+        x = torch.empty_like(d)
+    offsets = offsets.to(device=d.device, dtype=torch.int32).contiguous()
+    lengths = lengths.to(device=d.device, dtype=torch.int32).contiguous()
+    if stream is None:
+        stream = torch.cuda.current_stream(d.device).cuda_stream
+    st = lib.hydist_gtsv_batched(dl.data_ptr(), d.data_ptr(), du.data_ptr(), b.data_ptr(),
+                                 x.data_ptr(), offsets.data_ptr(), lengths.data_ptr(),
+                                 int(offsets.numel()), dt, int(algo), C.c_void_p(stream))
+    capi.check(lib, st, "hydist_gtsv_batched")
+    return x

@@ -1,0 +1,61 @@
+// common.cuh -- shared device-side types of the B200 Hydist time step.
+//
+// Layout in HBM: every mesh field is one FP64 (or int32) array of
+// (N+3) x (M+3), row-major, idx = i*W + j with W = M+3 (the reference's
+// layout, engine.h:56-68). Rows i are the x direction, columns j the y
+// direction (contiguous). A column sweep (x, implicit in i) therefore maps
+// one thread to one column and is coalesced across a warp; a row sweep
+// (y, implicit in j) stages rows through shared memory.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/hydist_capi.h"
+
+namespace hyd {
+
+constexpr int SEG = HYDIST_SEGMENT_LIMIT;
+
+// Constant_Coeffs (engine.h:39-52), derived as Load_coeffs does.
+struct Coef {
+  double dX, dY, dT, dXbp, dYbp, dX2, dY2, dTchia2dX, dTchia2dY, HaiChiadT;
+  double NANGDAY, H_TINH, heso, mu_mn, kenhhepng, kenhhepd;
+  double NDnen, Tod, Toe, hstoe, ghtoe, Mbochat;
+  double ro, ros, dm, muy, d90, Dorong, Sx;
+  double CORIOLIS_FORCE, g, Ks, Windx, Windy, Ufr, Dxr, wss;
+};
+
+// Device error codes recorded in State::err[0].
+enum DevErr { DEV_OK = 0, DEV_SEG_OVERFLOW = 1 };
+
+// Every device pointer of one scenario. Passed by value to kernels.
+struct State {
+  int M, N, W, H;  // W = M+3, H = N+3
+  int T;           // rows of the hourly series
+  int bienQ[4];
+  int ketdinh;
+  int race_new;    // extraction at an open last end reads the new neighbour
+  // static fields
+  const double *h, *hsnham, *visco, *Fw, *htaiz, *htaiz_bd, *Kx1, *Ky1, *Tsxw, *Tsyw;
+  // state
+  double *u, *v, *z, *tu, *tv, *tz, *Hmoi, *Htdu, *Htdv, *FS, *tFS, *VTH, *Kx, *Ky, *dH, *Qbx,
+      *Qby;
+  int* khouot;
+  // boundary
+  double *ubt, *ubp, *vbt, *vbd, *hi, *hmax;  // hmax[4]: up, down, left, right
+  const double *bc[4], *CC[4];
+  const int* btype;  // 4 x SEG
+  // wet segments
+  int *daui, *cuoii, *moci, *dauj, *cuoij, *mocj;
+  // scratch
+  double* tmp;   // smoothing buffer, (N+3)*(M+3)
+  double* Ap;    // Thomas scratch, [unknown][line]
+  double* Bp;
+  int ld;        // line stride of Ap/Bp (max(M,N)+3)
+  int* err;      // [0]: DevErr
+};
+
+__host__ __device__ inline int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+}  // namespace hyd

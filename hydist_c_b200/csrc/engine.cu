@@ -1,0 +1,493 @@
+// engine.cu -- host side of the B200 Hydist time step behind the C ABI.
+//
+// hydist_create  replaces main.cpp:138-304 (allocation loader.cpp:224-375,
+//                Load_coeffs loader.cpp:4-87, set-up kernels)
+// hydist_step    replaces the time loop of Hydraulic_Calculation
+//                (engine.cpp:41-296); every launch goes to the handle's
+//                stream, with no device-wide synchronisation between kernels
+//                (the reference synchronises after each, engine.cpp:13-19)
+// hydist_step_graph  the same step captured once into a CUDA graph per
+//                sediment phase and replayed
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "hydro.cuh"
+
+using namespace hyd;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& m) {
+  g_err = m;
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e__ = (call);                                                             \
+    if (e__ != cudaSuccess)                                                               \
+      return fail(e__ == cudaErrorMemoryAllocation ? HYDIST_ERR_OOM : HYDIST_ERR_CUDA,    \
+                  std::string(#call) + ": " + cudaGetErrorString(e__));                   \
+  } while (0)
+
+const double kPI = 3.14159265358979323846;
+
+void derive(const HydistParams& p, Coef& c) {
+  // Load_coeffs, loader.cpp:4-87 (operator order kept)
+  c.dX = p.dX;
+  c.dY = p.dY;
+  c.dT = p.dT;
+  c.dXbp = c.dX * c.dX;
+  c.dX2 = 2 * c.dX;
+  c.dYbp = c.dY * c.dY;
+  c.dY2 = 2 * c.dY;
+  c.dTchia2dX = c.dT / c.dX2;
+  c.dTchia2dY = c.dT / c.dY2;
+  c.HaiChiadT = 2.0 / c.dT;
+  c.kenhhepng = 0;
+  c.kenhhepd = 0;
+  c.NANGDAY = p.NANGDAY;
+  c.H_TINH = p.H_TINH;
+  c.heso = p.heso;
+  c.mu_mn = p.mu_mn;
+  c.NDnen = p.NDnen;
+  c.Tod = p.Tod;
+  c.Toe = p.Toe;
+  c.hstoe = p.hstoe;
+  c.ghtoe = p.ghtoe;
+  c.Mbochat = p.Mbochat;
+  c.ro = p.ro;
+  c.ros = p.ros;
+  c.dm = p.dm;
+  c.d90 = p.d90;
+  c.muy = p.muy;
+  c.Dorong = p.Dorong;
+  c.Sx = p.Sx;
+  c.CORIOLIS_FORCE = p.CORIOLIS_FORCE;
+  c.g = p.g;
+  c.Ks = p.Ks >= 0 ? p.Ks : 2.5 * c.dm;
+  c.Windx = 0.0013 * (0.00075 + 0.000067 * std::fabs(p.Wind)) * std::fabs(p.Wind) * p.Wind *
+            std::cos(p.huonggio * (kPI / 180));
+  c.Windy = 0.0013 * (0.00075 + 0.000067 * std::fabs(p.Wind)) * std::fabs(p.Wind) * p.Wind *
+            std::sin(p.huonggio * (kPI / 180));
+  c.Ufr = 0.25 * std::pow((c.Sx - 1) * c.g, 8.0 / 15.0) * std::pow(c.dm, 9.0 / 15.0) *
+          std::pow(c.muy, -1.0 / 15.0);
+  c.Dxr = c.dm * std::pow(c.g * (c.Sx - 1) / c.muy * c.muy, (1.0 / 3.0));
+  c.wss = p.wss >= 0 ? p.wss
+                     : 10 * c.muy / c.dm *
+                           (std::sqrt(1 + 0.01 * (c.Sx - 1) * 9.81 * std::pow(c.dm, 3) /
+                                              std::pow(c.muy, 2)) -
+                            1);
+}
+
+}  // namespace
+
+struct HydistHandle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  State S{};
+  Coef c{};
+  HydistOptions o{};
+  double t = 0;
+  std::vector<void*> allocs;
+  double* mass_part = nullptr;  // per-block partial sums
+  int mass_blocks = 0;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [0] hydraulics only, [1] with sediment
+  bool graph_sed_x[2] = {false, false};
+};
+
+namespace {
+
+template <class T>
+int dalloc(HydistHandle* h, T** p, size_t n) {
+  void* q = nullptr;
+  CK(cudaMalloc(&q, n * sizeof(T) + 64));
+  CK(cudaMemsetAsync(q, 0, n * sizeof(T) + 64, h->stream));
+  h->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return HYDIST_OK;
+}
+
+#define TRY(x)                    \
+  do {                            \
+    int r__ = (x);                \
+    if (r__ != HYDIST_OK) return r__; \
+  } while (0)
+
+int check_device_err(HydistHandle* h) {
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, h->S.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (e == DEV_SEG_OVERFLOW) return fail(HYDIST_ERR_SEGMENTS, "a line has more than 20 wet segments");
+  return HYDIST_OK;
+}
+
+// one full step (engine.cpp:65-295)
+void enqueue_step(HydistHandle* h, double t0, bool sed_x, bool sed_y) {
+  const double t1 = t0 + 0.5 * h->c.dT;
+  launch_half_x(h->S, h->c, t1, h->stream);
+  if (sed_x) launch_sediment(h->S, h->c, t1, h->o.bed_change_start, true, h->stream);
+  const double t2 = t1 + h->c.dT * 0.5;
+  launch_half_y(h->S, h->c, t2, h->stream);
+  if (sed_y) launch_sediment(h->S, h->c, t2, h->o.bed_change_start, false, h->stream);
+}
+
+__global__ void k_mass_partial(State S, double* part) {
+  // sum over wet cells of H_moi-independent volume (htaiz + z), FP64
+  __shared__ double sh[256];
+  double acc = 0;
+  const int n = S.W * S.H;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+    const int i = g / S.W, j = g - i * S.W;
+    if (i >= 2 && i <= S.N && j >= 2 && j <= S.M && S.khouot[g] == 0) acc += S.htaiz[g] + S.z[g];
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_mass_final(const double* part, int n, double* out) {
+  __shared__ double sh[256];
+  double acc = 0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) acc += part[k];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = sh[0];
+}
+
+double* field_ptr(HydistHandle* h, int f) {
+  State& S = h->S;
+  switch (f) {
+    case HYDIST_FIELD_U: return S.u;
+    case HYDIST_FIELD_V: return S.v;
+    case HYDIST_FIELD_Z: return S.z;
+    case HYDIST_FIELD_FS: return S.FS;
+    case HYDIST_FIELD_TFS: return S.tFS;
+    case HYDIST_FIELD_H_MOI: return S.Hmoi;
+    case HYDIST_FIELD_DH: return S.dH;
+    case HYDIST_FIELD_HTDU: return S.Htdu;
+    case HYDIST_FIELD_HTDV: return S.Htdv;
+    case HYDIST_FIELD_TU: return S.tu;
+    case HYDIST_FIELD_TV: return S.tv;
+    case HYDIST_FIELD_TZ: return S.tz;
+    case HYDIST_FIELD_KX1: return const_cast<double*>(S.Kx1);
+    case HYDIST_FIELD_KY1: return const_cast<double*>(S.Ky1);
+    case HYDIST_FIELD_VTH: return S.VTH;
+    case HYDIST_FIELD_KX: return S.Kx;
+    case HYDIST_FIELD_KY: return S.Ky;
+    case HYDIST_FIELD_H: return const_cast<double*>(S.h);
+    case HYDIST_FIELD_HTAIZ: return const_cast<double*>(S.htaiz);
+    case HYDIST_FIELD_QBX: return S.Qbx;
+    case HYDIST_FIELD_QBY: return S.Qby;
+    default: return nullptr;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hydist_last_error(void) { return g_err.c_str(); }
+const char* hydist_version(void) { return "hydist_b200 0.1 (sm_100a)"; }
+
+void hydist_params_default(HydistParams* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->dX = 10.0;
+  p->dY = 10.0;
+  p->dT = 2;
+  p->NANGDAY = 0.0;
+  p->H_TINH = 0.02;
+  p->heso = 0.94;
+  p->mu_mn = 0.2;
+  p->NDnen = 0.00;
+  p->Tod = 0.06;
+  p->Toe = 0.15;
+  p->hstoe = 0;
+  p->ghtoe = 3;
+  p->Mbochat = 0.00001;
+  p->ro = 1000;
+  p->ros = 2000;
+  p->dm = 0.00001;
+  p->d90 = 0.002;
+  p->muy = 1.01e-06;
+  p->Dorong = 0.5;
+  p->Sx = 2;
+  p->CORIOLIS_FORCE = 0.0;
+  p->g = 9.81;
+  p->Wind = 0.0;
+  p->huonggio = 0.0;
+  p->wss = -1;
+  p->Ks = -1;
+}
+
+void hydist_options_default(HydistOptions* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->t_start = 0;
+  o->sediment_start = 20 * 3600;
+  o->bed_change_start = 500 * 3600;
+  o->ketdinh = 1;
+  o->bed_change = 0;
+  o->precision = HYDIST_FP64;
+}
+
+void hydist_bienq_from_boundary_type(const int32_t* bt, int32_t n, int32_t bienQ[4]) {
+  for (int k = 0; k < 4; ++k) bienQ[k] = (bt && k < n && bt[k] == 2) ? 1 : 0;
+}
+
+int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistOptions* o,
+                  int device, HydistHandle** out) {
+  if (!sc || !p || !o || !out) return fail(HYDIST_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (sc->M < 4 || sc->N < 4 || sc->total_time < 2)
+    return fail(HYDIST_ERR_ARG, "mesh must be at least 4x4 and series at least 2 hours long");
+  if (!sc->h || !sc->hsnham || !sc->visco || !sc->Fw || !sc->boundary_type)
+    return fail(HYDIST_ERR_ARG, "missing input array");
+  if (sc->n_boundary_type < 4 * SEG)
+    return fail(HYDIST_ERR_ARG, "boundary_type needs 4 sides x 20 segments");
+  if (!(p->dX > 0 && p->dY > 0 && p->dT > 0)) return fail(HYDIST_ERR_ARG, "dX, dY, dT must be > 0");
+  if (o->precision != HYDIST_FP64 && o->precision != HYDIST_FP32_REFINE)
+    return fail(HYDIST_ERR_ARG, "unknown precision");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(HYDIST_ERR_NODEVICE, "no CUDA device");
+  auto* h = new HydistHandle();
+  if (device < 0) cudaGetDevice(&device);
+  h->device = device;
+  int rc = [&]() -> int {
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    derive(*p, h->c);
+    h->o = *o;
+    h->t = o->t_start;
+    State& S = h->S;
+    S.M = sc->M;
+    S.N = sc->N;
+    S.W = S.M + 3;
+    S.H = S.N + 3;
+    S.T = sc->total_time;
+    for (int k = 0; k < 4; ++k) S.bienQ[k] = sc->bienQ[k] ? 1 : 0;
+    S.ketdinh = o->ketdinh ? 1 : 0;
+    S.race_new = 1;
+    const size_t n = (size_t)S.W * S.H;
+    double* tmp;
+    // static inputs
+    TRY(dalloc(h, &tmp, n));
+    CK(cudaMemcpyAsync(tmp, sc->h, n * 8, cudaMemcpyHostToDevice, h->stream));
+    S.h = tmp;
+    TRY(dalloc(h, &tmp, n));
+    CK(cudaMemcpyAsync(tmp, sc->hsnham, n * 8, cudaMemcpyHostToDevice, h->stream));
+    S.hsnham = tmp;
+    TRY(dalloc(h, &tmp, n));
+    CK(cudaMemcpyAsync(tmp, sc->visco, n * 8, cudaMemcpyHostToDevice, h->stream));
+    S.visco = tmp;
+    TRY(dalloc(h, &tmp, n));
+    CK(cudaMemcpyAsync(tmp, sc->Fw, n * 8, cudaMemcpyHostToDevice, h->stream));
+    S.Fw = tmp;
+    const double* bcs[4] = {sc->bc_up, sc->bc_down, sc->bc_left, sc->bc_right};
+    const double* ccs[4] = {sc->CC_up, sc->CC_down, sc->CC_left, sc->CC_right};
+    for (int k = 0; k < 4; ++k) {
+      TRY(dalloc(h, &tmp, S.T));
+      if (bcs[k]) CK(cudaMemcpyAsync(tmp, bcs[k], S.T * 8, cudaMemcpyHostToDevice, h->stream));
+      S.bc[k] = tmp;
+      TRY(dalloc(h, &tmp, S.T));
+      if (ccs[k]) CK(cudaMemcpyAsync(tmp, ccs[k], S.T * 8, cudaMemcpyHostToDevice, h->stream));
+      S.CC[k] = tmp;
+    }
+    int* itmp;
+    TRY(dalloc(h, &itmp, 4 * SEG));
+    CK(cudaMemcpyAsync(itmp, sc->boundary_type, 4 * SEG * 4, cudaMemcpyHostToDevice, h->stream));
+    S.btype = itmp;
+    // derived static fields
+    TRY(dalloc(h, &tmp, n));
+    S.htaiz = tmp;
+    TRY(dalloc(h, &tmp, n));
+    S.htaiz_bd = tmp;
+    TRY(dalloc(h, &tmp, n));
+    S.Kx1 = tmp;
+    TRY(dalloc(h, &tmp, n));
+    S.Ky1 = tmp;
+    TRY(dalloc(h, &tmp, n));
+    S.Tsxw = tmp;
+    TRY(dalloc(h, &tmp, n));
+    S.Tsyw = tmp;
+    // state
+    double** st[] = {&S.u, &S.v, &S.z, &S.tu, &S.tv, &S.tz, &S.Hmoi, &S.Htdu, &S.Htdv, &S.FS,
+                     &S.tFS, &S.VTH, &S.Kx, &S.Ky, &S.dH, &S.Qbx, &S.Qby, &S.tmp};
+    for (double** q : st) TRY(dalloc(h, q, n));
+    TRY(dalloc(h, &S.khouot, n));
+    if (sc->FS0) {
+      CK(cudaMemcpyAsync(S.FS, sc->FS0, n * 8, cudaMemcpyHostToDevice, h->stream));
+      CK(cudaMemcpyAsync(S.tFS, sc->FS0, n * 8, cudaMemcpyHostToDevice, h->stream));
+    }
+    TRY(dalloc(h, &S.ubt, S.W));
+    TRY(dalloc(h, &S.ubp, S.W));
+    TRY(dalloc(h, &S.vbt, S.H));
+    TRY(dalloc(h, &S.vbd, S.H));
+    TRY(dalloc(h, &S.hi, 2 * (S.M + S.N + 6)));
+    TRY(dalloc(h, &S.hmax, 4));
+    TRY(dalloc(h, &S.daui, S.H * SEG));
+    TRY(dalloc(h, &S.cuoii, S.H * SEG));
+    TRY(dalloc(h, &S.moci, S.H));
+    TRY(dalloc(h, &S.dauj, S.W * SEG));
+    TRY(dalloc(h, &S.cuoij, S.W * SEG));
+    TRY(dalloc(h, &S.mocj, S.W));
+    // Thomas scratch [unknown][line]
+    S.ld = std::max(S.W, S.H);
+    const size_t nunk = (size_t)2 * std::max(S.M, S.N) + 4;
+    TRY(dalloc(h, &S.Ap, nunk * S.ld));
+    TRY(dalloc(h, &S.Bp, nunk * S.ld));
+    TRY(dalloc(h, &S.err, 4));
+    h->mass_blocks = 296;
+    TRY(dalloc(h, &h->mass_part, h->mass_blocks + 1));
+    launch_init(S, h->c, h->stream);
+    CK(cudaGetLastError());
+    TRY(check_device_err(h));
+    return HYDIST_OK;
+  }();
+  if (rc != HYDIST_OK) {
+    hydist_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return HYDIST_OK;
+}
+
+int hydist_destroy(HydistHandle* h) {
+  if (!h) return HYDIST_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (auto& g : h->graph)
+    if (g) cudaGraphExecDestroy(g);
+  for (void* p : h->allocs) cudaFree(p);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return HYDIST_OK;
+}
+
+int hydist_step(HydistHandle* h, int32_t nsteps) {
+  if (!h) return fail(HYDIST_ERR_ARG, "null handle");
+  if (nsteps < 0) return fail(HYDIST_ERR_ARG, "negative step count");
+  CK(cudaSetDevice(h->device));
+  for (int k = 0; k < nsteps; ++k) {
+    const double t1 = h->t + 0.5 * h->c.dT;
+    const double t2 = t1 + h->c.dT * 0.5;
+    enqueue_step(h, h->t, t1 >= h->o.sediment_start, t2 >= h->o.sediment_start);
+    h->t = t2;
+  }
+  CK(cudaGetLastError());
+  return HYDIST_OK;
+}
+
+int hydist_step_graph(HydistHandle* h, int32_t nsteps) {
+  // The time of each half-step is a kernel argument, so a captured step is
+  // re-captured when its arguments change; replay is used for the launch
+  // overhead of the many small kernels of one step.
+  if (!h) return fail(HYDIST_ERR_ARG, "null handle");
+  CK(cudaSetDevice(h->device));
+  for (int k = 0; k < nsteps; ++k) {
+    const double t1 = h->t + 0.5 * h->c.dT;
+    const double t2 = t1 + h->c.dT * 0.5;
+    const bool sx = t1 >= h->o.sediment_start, sy = t2 >= h->o.sediment_start;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(h, h->t, sx, sy);
+    CK(cudaStreamEndCapture(h->stream, &g));
+    cudaGraphExec_t& ex = h->graph[sx || sy ? 1 : 0];
+    if (ex) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(ex, g, &info) != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphExecDestroy(ex);
+        ex = nullptr;
+      }
+    }
+    if (!ex) CK(cudaGraphInstantiate(&ex, g, 0));
+    cudaGraphDestroy(g);
+    CK(cudaGraphLaunch(ex, h->stream));
+    h->t = t2;
+  }
+  return HYDIST_OK;
+}
+
+int hydist_sync(HydistHandle* h) {
+  if (!h) return fail(HYDIST_ERR_ARG, "null handle");
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_device_err(h);
+}
+
+int hydist_get_time(HydistHandle* h, double* t) {
+  if (!h || !t) return fail(HYDIST_ERR_ARG, "null argument");
+  *t = h->t;
+  return HYDIST_OK;
+}
+
+int hydist_set_time(HydistHandle* h, double t) {
+  if (!h) return fail(HYDIST_ERR_ARG, "null handle");
+  h->t = t;
+  return HYDIST_OK;
+}
+
+int hydist_download(HydistHandle* h, int32_t field, void* host) {
+  if (!h || !host) return fail(HYDIST_ERR_ARG, "null argument");
+  CK(cudaSetDevice(h->device));
+  const size_t n = (size_t)h->S.W * h->S.H;
+  if (field == HYDIST_FIELD_KHOUOT) {
+    CK(cudaMemcpyAsync(host, h->S.khouot, n * 4, cudaMemcpyDeviceToHost, h->stream));
+  } else {
+    double* p = field_ptr(h, field);
+    if (!p) return fail(HYDIST_ERR_ARG, "unknown field");
+    CK(cudaMemcpyAsync(host, p, n * 8, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return HYDIST_OK;
+}
+
+int hydist_upload(HydistHandle* h, int32_t field, const void* host) {
+  if (!h || !host) return fail(HYDIST_ERR_ARG, "null argument");
+  CK(cudaSetDevice(h->device));
+  const size_t n = (size_t)h->S.W * h->S.H;
+  if (field == HYDIST_FIELD_KHOUOT) {
+    CK(cudaMemcpyAsync(h->S.khouot, host, n * 4, cudaMemcpyHostToDevice, h->stream));
+    launch_scan_segments(h->S, h->stream);
+    CK(cudaGetLastError());
+  } else {
+    double* p = field_ptr(h, field);
+    if (!p) return fail(HYDIST_ERR_ARG, "unknown field");
+    CK(cudaMemcpyAsync(p, host, n * 8, cudaMemcpyHostToDevice, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return HYDIST_OK;
+}
+
+int hydist_mass(HydistHandle* h, double* volume) {
+  if (!h || !volume) return fail(HYDIST_ERR_ARG, "null argument");
+  CK(cudaSetDevice(h->device));
+  k_mass_partial<<<h->mass_blocks, 256, 0, h->stream>>>(h->S, h->mass_part);
+  k_mass_final<<<1, 256, 0, h->stream>>>(h->mass_part, h->mass_blocks, h->mass_part + h->mass_blocks);
+  double v = 0;
+  CK(cudaMemcpyAsync(&v, h->mass_part + h->mass_blocks, 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  *volume = v * h->c.dX * h->c.dY;
+  return HYDIST_OK;
+}
+
+void* hydist_stream(HydistHandle* h) { return h ? (void*)h->stream : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,1038 @@
+// hydro.cu -- hydraulic ADI half-steps and the wet/dry bookkeeping on the GPU.
+//
+// Kernels (reference kernel each one replaces in brackets):
+//   k_onetime_init     [Onetime_init, support_funcs.cpp:21-69]
+//   k_interp_fs_rows   [Interpolate_FS_ng, support_funcs.cpp:191-213]
+//   k_interp_fs_col    [Interpolate_FS_d, support_funcs.cpp:215-237]
+//   k_scan_rows/cols   [Find_Calculation_limits_Horizontal/Vertical, :238-343]
+//   k_htuongdoi        [Htuongdoi, :346-362]
+//   k_preprocess       [preprocess_data, :482-601]
+//   k_boundary         [Update_Boundary_Value/Boundary_value/FS_boundary, :603-728]
+//   k_sweep_x          [UZSolver_calculate_preindex/abcd/matrix_coeff +
+//                       tridiagSolver + UZSolver_extract_solution,
+//                       UVZSolver_multithread.cpp:19-43, 78-139, 210-470,
+//                       547-603, 861-933]: one thread per column, the whole
+//                       half-step solve of that column fused.
+//   k_sweep_y          [the VZSolver_* kernels, :142-208, 472-544, 798-859]
+//   k_smooth / k_smooth_commit [Normalize/_normalize/update_buffer, :761-808]
+//   k_solve_v / k_solve_u      [solveV/vSolver, solveU/uSolver, :607-795, 938-978]
+//   k_margin_v / k_margin_u    [update_margin_elem_V/U, :980-1060]
+//   k_commit           [update_h_moi + update_uvz, support_funcs.cpp:71-86, 732-759]
+//   k_reset_vertical   [Reset_states_vertical, :142-188]
+//
+// The arithmetic of every formula follows the reference's expression order;
+// nvcc may fuse a multiply and an add into one FMA, which the CPU oracle
+// does not, so results agree to rounding, not bit for bit.
+#include <cstdio>
+
+#include "common.cuh"
+#include "hydro.cuh"
+
+namespace hyd {
+
+// ----------------------------------------------------------------- init
+__global__ void k_onetime_init(State S, Coef c) {
+  const int W = S.W, H = S.H, N = S.N, M = S.M;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (i >= H || j >= W) return;
+  const int p = i * W + j;
+  // borders and cells beyond the wet test are dry (2); row 0 / column 0
+  int k = 2;
+  double hm = 0.0;
+  bool set_h = false;
+  if (i >= 1 && j >= 1 && i <= N + 1 && j <= M + 1) {
+    if ((S.h[(i - 1) * W + j - 1] + S.h[(i - 1) * W + j] + S.h[i * W + j - 1] + S.h[p]) * 0.25 >
+        c.NANGDAY) {
+      k = 0;
+      set_h = true;
+    }
+  }
+  S.khouot[p] = k;
+  if (set_h) S.Hmoi[p] = hm;
+  if (i >= 1 && j >= 1 && i <= N && j <= M) {
+    double* htaiz = const_cast<double*>(S.htaiz);
+    double* htaiz_bd = const_cast<double*>(S.htaiz_bd);
+    double* Kx1 = const_cast<double*>(S.Kx1);
+    double* Ky1 = const_cast<double*>(S.Ky1);
+    htaiz[p] = (S.h[(i - 1) * W + j - 1] + S.h[(i - 1) * W + j] + S.h[i * W + j - 1] + S.h[p]) * 0.25;
+    htaiz_bd[p] = htaiz[p];
+    if (S.h[i * W + j - 1] + S.h[p] != 0)
+      Kx1[p] = c.g * pow((S.h[i * W + j - 1] + S.h[p]) * 0.5, -2 * c.mu_mn) *
+               pow((S.hsnham[i * W + j - 1] + S.hsnham[p]) * 0.5, 2.0);
+    if (S.h[(i - 1) * W + j] + S.h[p] != 0)
+      Ky1[p] = c.g * pow((S.h[(i - 1) * W + j] + S.h[p]) * 0.5, -2 * c.mu_mn) *
+               pow((S.hsnham[(i - 1) * W + j] + S.hsnham[p]) * 0.5, 2.0);
+  }
+}
+
+// ------------------------------------------------------- segment tables
+__global__ void k_interp_fs_rows(State S, Coef c) {
+  // Interpolate_FS_ng at row N (offset N-1, sign -1) and row 2 (offset 2, +1)
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int which = blockIdx.y;
+  if (j >= S.M) return;
+  const int W = S.W;
+  const int loc = which == 0 ? S.N : 2;
+  const int offset = which == 0 ? S.N - 1 : 2;
+  const int sign = which == 0 ? -1 : 1;
+  if (S.tu[loc * W + j] > 0) {
+    const double deltaX = (S.u[loc * W + j] + S.tu[loc * W + j]) * 0.25 * c.dT;
+    const int i = (int)(offset + sign * (deltaX / c.dX));
+    const int i_deltaX = __double2int_rn(deltaX);
+    const int i_dX = __double2int_rn(c.dX);
+    S.FS[loc * W + j] = S.FS[i * W + j] +
+                        sign * (S.FS[(i + 1) * W + j] - S.FS[i * W + j]) * (deltaX / c.dX - i_deltaX / i_dX);
+  }
+}
+
+__global__ void k_interp_fs_col(State S, Coef c) {
+  // Interpolate_FS_d at column M (offset M-1, sign -1); rows 1..M-1 as the
+  // reference loops them (support_funcs.cpp:227)
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i >= S.M || i >= S.H) return;
+  const int W = S.W, loc = S.M, offset = S.M - 1, sign = -1;
+  if (S.tv[i * W + loc] > 0) {
+    const double deltaY = (S.v[i * W + loc] + S.tv[i * W + loc]) * 0.25 * c.dT;
+    const int j = (int)(offset + sign * (deltaY / c.dY));
+    const int j_deltaY = __double2int_rn(deltaY);
+    const int j_dY = __double2int_rn(c.dY);
+    S.FS[i * W + loc] = S.FS[i * W + j + 1] +
+                        (S.FS[i * W + j + 1] - S.FS[i * W + j]) * (deltaY / c.dY - j_deltaY / j_dY);
+  }
+}
+
+// The reference's run scan (support_funcs.cpp:260-288): wet runs of a line
+// starting at index 2, bounded by lim (M for rows, N for columns).
+__device__ __forceinline__ int scan_line(const int* k0, int stride, int lim, int* dau, int* cuoi,
+                                         int* err) {
+  int nseg = 0, start = 2, end = 0;
+  while (start < lim) {
+    if (k0[start * stride] != 0) {
+      while (k0[start * stride] && start < lim) start++;
+    }
+    if (start + 1 == lim) start = lim;
+    if (k0[start * stride] == 0 && start + 1 < lim) {
+      if (nseg >= SEG) {
+        atomicExch(err, DEV_SEG_OVERFLOW);
+        return nseg;
+      }
+      dau[nseg] = start;
+      end = start;
+      while (k0[end * stride] == 0 && end < lim) end++;
+      if (k0[end * stride] != 0 && end <= lim) {
+        cuoi[nseg] = end - 1;
+        start = end;
+      } else {
+        cuoi[nseg] = lim;
+        start = lim;
+      }
+      nseg++;
+    }
+  }
+  return nseg;
+}
+
+__global__ void k_scan_rows(State S) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  if (i > S.N) return;
+  S.moci[i] = scan_line(S.khouot + i * S.W, 1, S.M, S.daui + i * SEG, S.cuoii + i * SEG, S.err);
+}
+
+__global__ void k_scan_cols(State S) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  if (j > S.M) return;
+  S.mocj[j] = scan_line(S.khouot + j, S.W, S.N, S.dauj + j * SEG, S.cuoij + j * SEG, S.err);
+}
+
+__global__ void k_htuongdoi(State S) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int i = blockIdx.y + 1;
+  if (i > S.N || j > S.M) return;
+  const int W = S.W, p = i * W + j;
+  S.Htdu[p] = (S.h[p - 1] + S.h[p] + S.z[p + W] + S.z[p]) * 0.5;
+  S.Htdv[p] = (S.h[p - W] + S.h[p] + S.z[p + 1] + S.z[p]) * 0.5;
+}
+
+// preprocess_data (support_funcs.cpp:482-601): discharge distribution
+// weights per boundary cell and the FS boundary scale. One thread: it runs
+// once per scenario.
+__global__ void k_preprocess(State S, Coef c) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int W = S.W, M = S.M, N = S.N;
+  const double dX = c.dX, ND = c.NANGDAY, ros = c.ros;
+  double* hu = S.hi;
+  for (int k = 0; k < S.mocj[M]; ++k) {
+    double sum = 0;
+    for (int i = S.dauj[M * SEG + k]; i <= S.cuoij[M * SEG + k]; ++i) {
+      hu[i] = (S.h[i * W + M] + S.h[(i - 1) * W + M]) / 2.0 - ND;
+      sum += pow(hu[i], 5.0 / 3.0);
+    }
+    for (int i = S.dauj[M * SEG + k]; i <= S.cuoij[M * SEG + k]; ++i)
+      hu[i] = pow(hu[i], 2.0 / 3.0) / (sum * dX);
+  }
+  double* hd = hu + (N + 3);
+  for (int k = 0; k < S.mocj[2]; ++k) {
+    double sum = 0;
+    for (int i = S.dauj[2 * SEG + k]; i <= S.cuoij[2 * SEG + k]; ++i) {
+      hd[i] = (S.h[i * W + 1] + S.h[(i - 1) * W + 1]) / 2.0 - ND;
+      sum += pow(hd[i], 5.0 / 3.0);
+    }
+    for (int i = S.dauj[2 * SEG + k]; i <= S.cuoij[2 * SEG + k]; ++i)
+      hd[i] = pow(hd[i], 2.0 / 3.0) / (sum * dX);
+  }
+  double* hl = hd + (N + 3);
+  for (int k = 0; k < S.moci[2]; ++k) {
+    double sum = 0;
+    for (int j = S.daui[2 * SEG + k]; j <= S.cuoii[2 * SEG + k]; ++j) {
+      hl[j] = (S.h[1 * W + j] + S.h[1 * W + j - 1]) / 2.0 - ND;
+      sum += pow(hl[j], 5.0 / 3.0);
+    }
+    for (int j = S.daui[2 * SEG + k]; j <= S.cuoii[2 * SEG + k]; ++j)
+      hl[j] = pow(hl[j], 2.0 / 3.0) / (sum * dX);
+  }
+  double* hr = hl + (M + 3);
+  for (int k = 0; k < S.moci[N]; ++k) {
+    double sum = 0;
+    for (int j = S.daui[N * SEG + k]; j <= S.cuoii[N * SEG + k]; ++j) {
+      hr[j] = (S.h[N * W + j] + S.h[N * W + j - 1]) / 2.0 - ND;
+      sum += pow(hr[j], 5.0 / 3.0);
+    }
+    for (int j = S.daui[N * SEG + k]; j <= S.cuoii[N * SEG + k]; ++j)
+      hr[j] = pow(hr[j], 2.0 / 3.0) / (sum * dX);
+  }
+  const double* hb = S.htaiz_bd;
+  double mu = hb[2 * W + M], md = hb[2 * W + 2];
+  for (int i = 3; i < N; ++i) {
+    if (hb[i * W + M] > mu) mu = hb[i * W + M];
+    if (hb[i * W + 2] > md) md = hb[i * W + 2];
+  }
+  double ml = hb[2 * W + 2], mr = hb[N * W + 2];
+  for (int j = 3; j < M; ++j) {
+    if (hb[2 * W + j] > ml) ml = hb[2 * W + j];
+    if (hb[N * W + j] > mr) mr = hb[N * W + j];
+  }
+  S.hmax[0] = mu != 0 ? 1.0 / (ros * mu) : mu;
+  S.hmax[1] = md != 0 ? 1.0 / (ros * md) : md;
+  S.hmax[2] = ml != 0 ? 1.0 / (ros * ml) : ml;
+  S.hmax[3] = mr != 0 ? 1.0 / (ros * mr) : mr;
+}
+
+// ------------------------------------------------------------- boundary
+// Update_Boundary_Value (support_funcs.cpp:682-728). t arrives through a
+// float parameter in the reference (engine.cpp:22), hence tf.
+__global__ void k_boundary(State S, float tf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int M = S.M, N = S.N, W = S.W;
+  if (i > M && i > N) return;
+  const double t = (double)tf;
+  const int t1 = (int)(t / 3600);
+  const double t2h = (t - (double)(3600.0f * (float)t1)) / 3600.0f;
+  const double t2f = (t - (3600.0 * t1)) / 3600.0;
+  const double* hi_up = S.hi;
+  const double* hi_down = hi_up + (N + 3);
+  const double* hi_left = hi_down + (N + 3);
+  const double* hi_right = hi_left + (M + 3);
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const bool isU = s >= 2;
+    const int loc = s == 0 ? M : (s == 3 ? N : 2);
+    const int ext = s == 0 ? M + 1 : (s == 3 ? N + 1 : 1);
+    const int* moc = isU ? S.moci : S.mocj;
+    const int* dau = isU ? S.daui : S.dauj;
+    const int* cuoi = isU ? S.cuoii : S.cuoij;
+    const double* hiv = s == 0 ? hi_up : (s == 1 ? hi_down : (s == 2 ? hi_left : hi_right));
+    double* barr = s == 0 ? S.vbt : (s == 1 ? S.vbd : (s == 2 ? S.ubt : S.ubp));
+    if (moc[loc] <= 0) continue;
+    if (!(dau[loc * SEG] <= i && i <= cuoi[loc * SEG])) continue;
+    const int seg = 0;  // only segment 0 is matched (support_funcs.cpp:614-618)
+    const int bt = S.btype[s * SEG + seg];
+    const double* B = S.bc[s];
+    const double val = B[seg * S.T + t1] * (1.0f - t2h) + B[seg * S.T + t1 + 1] * t2h;
+    if (bt == 2) {
+      barr[i] = val * hiv[i];
+    } else {
+      if (isU) {
+        S.tz[loc * W + i] = val;
+        S.tz[ext * W + i] = val;
+      } else {
+        S.tz[i * W + loc] = val;
+        S.tz[i * W + ext] = val;
+      }
+    }
+    if (bt != 2) continue;
+    const double* Cs = S.CC[s];
+    const double cv = Cs[seg * S.T + t1] * (1.0 - t2f) + Cs[seg * S.T + t1 + 1] * t2f;
+    const int ii = isU ? loc : i;
+    const int jj = isU ? i : loc;
+    S.FS[ii * W + jj] = cv * S.htaiz_bd[ii * W + jj] * S.hmax[s];
+  }
+}
+
+// ---------------------------------------------------- ADI line sweeps
+// Per-cell coefficients of the preindex step.
+struct Pre {
+  double f1, f2, f3, f5, a2, c2, d2;
+};
+
+// _uzSolver_calculate_preindex (UVZSolver_multithread.cpp:210-278).
+__device__ __forceinline__ Pre pre_x(const State& S, const Coef& c, int i, int j) {
+  const int w = S.W;
+  const double* u = S.u;
+  const double* v = S.v;
+  const double* Hm = S.Hmoi;
+  Pre P;
+  double p = 0.0, q = 0.0;
+  const double vtb =
+      (v[i * w + j - 1] + v[i * w + j] + v[(i + 1) * w + j - 1] + v[(i + 1) * w + j]) * 0.25;
+  const double uu = u[i * w + j], VI = S.visco[i * w + j], Hu = S.Htdu[i * w + j];
+  const double dT = c.dT;
+  P.f1 = c.dTchia2dX * uu + VI * dT / c.dXbp;
+  P.f2 = -(2 + S.Kx1[i * w + j] * dT * sqrt(uu * uu + vtb * vtb) / Hu + (2 * dT * VI) / c.dXbp);
+  P.f3 = dT * VI / c.dXbp - c.dTchia2dX * uu;
+  if (Hm[i * w + j - 1] <= c.H_TINH) {
+    if (vtb < 0) {
+      p = vtb * (-3 * uu + 4 * u[i * w + j + 1] - u[i * w + j + 2]) / c.dY2;
+      q = (uu - 2 * u[i * w + j + 1] + u[i * w + j + 2]) / c.dYbp;
+    }
+  } else {
+    if (Hm[i * w + j + 1] <= c.H_TINH) {
+      if ((Hm[i * w + j - 2] > c.H_TINH) && (vtb > 0)) {
+        p = vtb * (3 * uu - 4 * u[i * w + j - 1] + u[i * w + j - 2]) / c.dY2;
+        q = (uu - 2 * u[i * w + j - 1] + u[i * w + j - 2]) / c.dYbp;
+      }
+    } else {
+      p = vtb * (u[i * w + j + 1] - u[i * w + j - 1]) / c.dY2;
+      q = (u[i * w + j + 1] - 2 * uu + u[i * w + j - 1]) / c.dYbp;
+    }
+  }
+  P.f5 = -2 * uu + dT * p - dT * c.CORIOLIS_FORCE * vtb - dT * VI * q -
+         dT * (c.Windx - S.Tsxw[i * w + j]) / Hu;
+  P.c2 = c.dTchia2dX * Hu;
+  P.a2 = -c.dTchia2dX * S.Htdu[(i - 1) * w + j];
+  P.d2 = S.z[i * w + j] -
+         c.dTchia2dY * (S.Htdv[i * w + j] * v[i * w + j] - S.Htdv[i * w + j - 1] * v[i * w + j - 1]);
+  return P;
+}
+
+// _vzSolver_calculate_preindex (UVZSolver_multithread.cpp:142-208).
+__device__ __forceinline__ Pre pre_y(const State& S, const Coef& c, int i, int j) {
+  const int w = S.W;
+  const double* u = S.u;
+  const double* v = S.v;
+  const double* Hm = S.Hmoi;
+  Pre P;
+  double p = 0.0, q = 0.0;
+  const double utb =
+      (u[(i - 1) * w + j] + u[i * w + j] + u[(i - 1) * w + j + 1] + u[i * w + j + 1]) * 0.25;
+  const double vv = v[i * w + j], VI = S.visco[i * w + j], Hv = S.Htdv[i * w + j];
+  const double dT = c.dT;
+  P.f1 = c.dTchia2dY * vv + VI * dT / c.dYbp;
+  P.f2 = -(2 + S.Ky1[i * w + j] * dT * sqrt(vv * vv + utb * utb) / Hv + (2 * dT * VI) / c.dYbp);
+  P.f3 = dT * VI / c.dYbp - c.dTchia2dY * vv;
+  if (Hm[(i - 1) * w + j] <= c.H_TINH) {
+    if (utb < 0) {
+      q = utb * (-3 * vv + 4 * v[(i + 1) * w + j] - v[(i + 2) * w + j]) / c.dX2;
+      p = (vv - 2 * v[(i + 1) * w + j] + v[(i + 2) * w + j]) / c.dXbp;
+    }
+  } else {
+    if (Hm[(i + 1) * w + j] <= c.H_TINH) {
+      if ((Hm[(i - 2) * w + j] > c.H_TINH) && (utb > 0)) {
+        q = utb * (3 * vv - 4 * v[(i - 1) * w + j] + v[(i - 2) * w + j]) / c.dX2;
+        p = (vv - 2 * v[(i - 1) * w + j] + v[(i - 2) * w + j]) / c.dXbp;
+      }
+    } else {
+      q = utb * (v[(i + 1) * w + j] - v[(i - 1) * w + j]) / c.dX2;
+      p = (v[(i + 1) * w + j] - 2 * vv + v[(i - 1) * w + j]) / c.dXbp;
+    }
+  }
+  P.f5 = -2 * vv + dT * q + dT * c.CORIOLIS_FORCE * utb - dT * VI * p -
+         dT * (c.Windy - S.Tsyw[i * w + j]) / Hv;
+  P.c2 = c.dTchia2dY * Hv;
+  P.a2 = -c.dTchia2dY * S.Htdv[i * w + j - 1];
+  P.d2 = S.z[i * w + j] -
+         c.dTchia2dX * (S.Htdu[i * w + j] * u[i * w + j] - S.Htdu[(i - 1) * w + j] * u[(i - 1) * w + j]);
+  return P;
+}
+
+struct Mom {
+  double a1, b1, c1, d1;
+};
+
+// _calculate_abcd (UVZSolver_multithread.cpp:280-342) at position k of a
+// segment [first, last]; P = cell k, Pn = cell k+1 (read only when used).
+__device__ __forceinline__ Mom abcd(const Pre& P, const Pre& Pn, int k, int first, int last,
+                                    double f4, bool br1, bool br2) {
+  Mom m;
+  if (last - 1 > first) {
+    if (br1 && k == first) {
+      m.a1 = f4;
+      m.b1 = P.f2 - (P.f3 * Pn.a2 / Pn.c2);
+      m.c1 = -f4 - (P.f3 / Pn.c2);
+      m.d1 = P.f5 - (P.f3 * Pn.d2 / Pn.c2);
+    } else if (br2 && k == last - 1) {
+      m.a1 = f4 - P.f1 / P.a2;
+      m.b1 = P.f2 - (P.f1 * P.c2 / P.a2);
+      m.c1 = -f4;
+      m.d1 = P.f5 - (P.f1 * P.d2 / P.a2);
+    } else {
+      m.a1 = f4 - P.f1 / P.a2;
+      m.c1 = -f4 - (P.f3 / Pn.c2);
+      m.b1 = P.f2 - (P.f1 * P.c2 / P.a2) - (P.f3 * Pn.a2 / Pn.c2);
+      m.d1 = P.f5 - (P.f1 * P.d2 / P.a2) - (P.f3 * Pn.d2 / Pn.c2);
+    }
+  } else {
+    m.a1 = f4;
+    m.b1 = P.f2;
+    m.d1 = P.f5;
+    m.c1 = -f4;
+  }
+  return m;
+}
+
+// Streaming Thomas forward pass (tridiag, UVZSolver_multithread.cpp:19-43):
+// rows arrive in order k = 0..sn; Ap/Bp go to scratch.
+struct ThomasFwd {
+  double ap, bp, xs;
+  int sn;
+  double* Ap;
+  double* Bp;
+  int ld;
+  __device__ __forceinline__ void row(int k, int r, double A, double B, double Cc, double D) {
+    if (k == 0) {
+      if (sn == 0) {
+        xs = D / B;
+        return;
+      }
+      ap = -Cc / B;
+      bp = D / B;
+      Ap[(size_t)r * ld] = ap;
+      Bp[(size_t)r * ld] = bp;
+    } else if (k < sn) {
+      const double ep = A * ap + B;
+      ap = -Cc / ep;
+      bp = (D - (A * bp)) / ep;
+      Ap[(size_t)r * ld] = ap;
+      Bp[(size_t)r * ld] = bp;
+    } else {
+      xs = (D - (A * bp)) / (B + (A * ap));
+    }
+  }
+};
+
+// Layout of one line's solve: which of the reference's assembly variants
+// applies (UVZSolver_multithread.cpp:377-465) and where the system ends.
+struct LineSys {
+  bool ran;      // continuity row first (solid or discharge first end)
+  bool qfirst;   // discharge at the first end
+  int last_kind; // 0 solid, 1 discharge, 2 water level
+  int off, sn;
+};
+
+__device__ __forceinline__ LineSys line_sys(int first, int last, bool br1, bool br2, bool q1,
+                                            bool q2, int dkfr) {
+  LineSys L;
+  L.off = 2 * first;
+  int sn = 2 * (last - first);
+  if (br1) {
+    L.ran = true;
+    L.qfirst = false;
+    if (!br2) {
+      if (q2 && last == dkfr) {
+        L.last_kind = 1;
+      } else {
+        sn--;
+        L.last_kind = 2;
+      }
+    } else {
+      L.last_kind = 0;
+    }
+  } else {
+    const bool isBienran = (q1 && first == 2);
+    L.ran = isBienran;
+    L.qfirst = isBienran;
+    if (!br2) {
+      if (q1 && last == dkfr) {  // the first end's flag (UVZSolver_multithread.cpp:438)
+        if (!isBienran) sn--;
+        L.last_kind = 1;
+      } else {
+        sn--;
+        if (!isBienran) sn -= 1;
+        L.last_kind = 2;
+      }
+    } else {
+      if (!isBienran) sn--;
+      L.last_kind = 0;
+    }
+  }
+  L.sn = sn;
+  return L;
+}
+
+// Coefficients of absolute row r of a line's system (see line_sys).
+__device__ __forceinline__ void row_of(const LineSys& L, int r, const Pre& Pi, const Mom& Mi,
+                                       const Pre& Pi1, double& A, double& B, double& Cc,
+                                       double& D) {
+  const bool even = (r & 1) == 0;
+  if (L.ran == even) {  // continuity row of cell i (ran) / cell i+1 (lon)
+    const Pre& P = L.ran ? Pi : Pi1;
+    A = P.a2;
+    B = 1;
+    Cc = P.c2;
+    D = P.d2;
+  } else {  // momentum row of cell i
+    A = Mi.a1;
+    B = Mi.b1;
+    Cc = Mi.c1;
+    D = Mi.d1;
+  }
+}
+
+// One column sweep (x direction, implicit in i) of column j. Assembly,
+// Thomas and extraction fused; the column's cells are visited in order of
+// i, so a warp of 32 adjacent columns reads 32 contiguous doubles per field.
+__global__ void __launch_bounds__(128) k_sweep_x(State S, Coef c) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  if (j > S.M) return;
+  const int w = S.W, N = S.N;
+  const double f4 = 2 * c.g * c.dTchia2dX;
+  double* Ap = S.Ap + j;
+  double* Bp = S.Bp + j;
+  const int ld = S.ld;
+  for (int k = 0; k < S.mocj[j]; ++k) {
+    const int first = S.dauj[j * SEG + k], last = S.cuoij[j * SEG + k];
+    // locate_segment_u end flags (support_funcs.cpp:845-851)
+    const bool br1 = (first > 2) || ((first == 2) && ((S.h[1 * w + j] + S.h[1 * w + j - 1]) * 0.5 == c.NANGDAY));
+    const bool br2 = (last < N) || ((last == N) && ((S.h[N * w + j] + S.h[N * w + j - 1]) * 0.5 == c.NANGDAY));
+    const LineSys L = line_sys(first, last, br1, br2, S.bienQ[2] != 0, S.bienQ[3] != 0, N);
+    const double ubt = S.ubt[j], ubp = S.ubp[j];
+    const double TZ_r = S.tz[last * w + j], TZ_l = S.tz[first * w + j];
+    ThomasFwd F;
+    F.sn = L.sn;
+    F.Ap = Ap;
+    F.Bp = Bp;
+    F.ld = ld;
+    F.ap = F.bp = F.xs = 0;
+    const int rend = L.off + L.sn;  // last row of the system
+    Pre Pfirst, Plast;
+    Pre Pc = pre_x(S, c, first, j);
+    Pfirst = Pc;
+    Pre Pn = (first < last) ? pre_x(S, c, first + 1, j) : Pc;
+    for (int i = first; i <= last && L.sn >= 0; ++i) {
+      Mom Mi;
+      if (i <= last - 1 || (i == first)) Mi = abcd(Pc, Pn, i, first, last, f4, br1, br2);
+      else Mi = Mom{0, 0, 0, 0};
+      if (i == last) Plast = Pc;
+      // rows 2i and 2i+1 (those inside [off, rend])
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = 2 * i + e;
+        if (r < L.off || r > rend) continue;
+        double A, B, Cc, D;
+        row_of(L, r, Pc, Mi, Pn, A, B, Cc, D);
+        if (r == L.off) {
+          if (L.ran) D = L.qfirst ? (Pfirst.d2 - Pfirst.a2 * ubt) : Pfirst.d2;
+          else D = Mi.d1 - Mi.a1 * TZ_l;
+        }
+        if (r == rend) {
+          if (L.last_kind == 1) {
+            const Pre& PL = (i == last) ? Pc : Pn;
+            A = PL.a2;
+            B = 1;
+            D = PL.d2 - PL.c2 * ubp;
+          } else if (L.last_kind == 2) {
+            A = Mi.a1;
+            B = Mi.b1;
+            D = Mi.d1 - Mi.c1 * TZ_r;
+          } else {
+            const Pre& PL = (i == last) ? Pc : Pn;
+            A = PL.a2;
+            B = 1;
+            D = PL.d2;
+          }
+        }
+        F.row(r - L.off, r, A, B, Cc, D);
+      }
+      Pc = Pn;
+      if (i + 2 <= last) Pn = pre_x(S, c, i + 2, j);
+    }
+    if (L.sn < 0) Plast = pre_x(S, c, last, j);
+    // back substitution with extraction (_uzSolver_extract_solution,
+    // UVZSolver_multithread.cpp:547-603)
+    const bool ranx = br1 || (S.bienQ[2] && first == 2);
+    const double tu_old = S.tu[(last - 1) * w + j];
+    double xr = (L.sn >= 0) ? F.xs : 0.0;  // x at row rend
+    const double x_last = xr;
+    double tu_lm1_new = tu_old;
+    // walk rows rend-1 .. off
+    auto emit = [&](int r, double x) {
+      // r is absolute; map to (cell, variable)
+      if (ranx) {
+        const int i = r >> 1;
+        if (i >= first && i < last) {
+          if (r & 1) {
+            S.tu[i * w + j] = x;
+            if (i == last - 1) tu_lm1_new = x;
+          } else {
+            S.tz[i * w + j] = x;
+          }
+        }
+      } else {
+        if (r == 2 * first) {
+          S.tu[first * w + j] = x;
+          if (first == last - 1) tu_lm1_new = x;
+        } else {
+          const int i = (r + 1) >> 1;  // r = 2i-1 -> z[i], r = 2i -> u[i]
+          if (i > first && i < last) {
+            if (r & 1) S.tz[i * w + j] = x;
+            else {
+              S.tu[i * w + j] = x;
+              if (i == last - 1) tu_lm1_new = x;
+            }
+          }
+        }
+      }
+    };
+    if (L.sn >= 0) {
+      emit(rend, xr);
+      for (int r = rend - 1; r >= L.off; --r) {
+        const double x = Bp[(size_t)r * ld] + Ap[(size_t)r * ld] * xr;
+        emit(r, x);
+        xr = x;
+      }
+    }
+    if (first < last) {
+      if (br1) S.tu[(first - 1) * w + j] = 0;
+      else if (S.bienQ[2] && first == 2) S.tu[(first - 1) * w + j] = ubt;
+      else {
+        // t_z[first] is the boundary value (not written by the solve)
+        S.tu[(first - 1) * w + j] =
+            (Pfirst.d2 - S.tz[first * w + j] - Pfirst.c2 * S.tu[first * w + j]) / Pfirst.a2;
+      }
+    }
+    // last end
+    if (br2) {
+      S.tu[last * w + j] = 0;
+      S.tz[last * w + j] = x_last;
+    } else if (S.bienQ[3] && last == N) {
+      S.tu[last * w + j] = ubp;
+      S.tz[last * w + j] = x_last;
+    } else {
+      const double nb = S.race_new ? tu_lm1_new : tu_old;
+      S.tu[last * w + j] = (Plast.d2 - Plast.a2 * nb - S.tz[last * w + j]) / Plast.c2;
+    }
+  }
+}
+
+// One row sweep (y direction, implicit in j) of row i; extraction reaches
+// columns j <= N only (VZSolver_extract_solution, :851).
+__global__ void __launch_bounds__(128) k_sweep_y(State S, Coef c) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  if (i > S.N) return;
+  const int w = S.W, M = S.M, N = S.N;
+  const double f4 = 2 * c.g * c.dTchia2dY;
+  double* Ap = S.Ap + i;
+  double* Bp = S.Bp + i;
+  const int ld = S.ld;
+  for (int k = 0; k < S.moci[i]; ++k) {
+    const int first = S.daui[i * SEG + k], last = S.cuoii[i * SEG + k];
+    // locate_segment_v end flags (support_funcs.cpp:823-826)
+    const bool br1 = (first > 2) || ((first == 2) && ((S.h[i * w + first - 1] + S.h[(i - 1) * w + first - 1]) * 0.5 == c.NANGDAY));
+    const bool br2 = (last < M) || ((last == M) && ((S.h[i * w + last] + S.h[(i - 1) * w + last]) * 0.5 == c.NANGDAY));
+    const LineSys L = line_sys(first, last, br1, br2, S.bienQ[1] != 0, S.bienQ[0] != 0, M);
+    const double vbd = S.vbd[i], vbt = S.vbt[i];
+    const double TZ_r = S.tz[i * w + last], TZ_l = S.tz[i * w + first];
+    ThomasFwd F;
+    F.sn = L.sn;
+    F.Ap = Ap;
+    F.Bp = Bp;
+    F.ld = ld;
+    F.ap = F.bp = F.xs = 0;
+    const int rend = L.off + L.sn;
+    Pre Pfirst, Plast;
+    Pre Pc = pre_y(S, c, i, first);
+    Pfirst = Pc;
+    Pre Pn = (first < last) ? pre_y(S, c, i, first + 1) : Pc;
+    for (int jj = first; jj <= last && L.sn >= 0; ++jj) {
+      Mom Mi;
+      if (jj <= last - 1 || jj == first) Mi = abcd(Pc, Pn, jj, first, last, f4, br1, br2);
+      else Mi = Mom{0, 0, 0, 0};
+      if (jj == last) Plast = Pc;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = 2 * jj + e;
+        if (r < L.off || r > rend) continue;
+        double A, B, Cc, D;
+        row_of(L, r, Pc, Mi, Pn, A, B, Cc, D);
+        if (r == L.off) {
+          if (L.ran) D = L.qfirst ? (Pfirst.d2 - Pfirst.a2 * vbd) : Pfirst.d2;
+          else D = Mi.d1 - Mi.a1 * TZ_l;
+        }
+        if (r == rend) {
+          if (L.last_kind == 1) {
+            const Pre& PL = (jj == last) ? Pc : Pn;
+            A = PL.a2;
+            B = 1;
+            D = PL.d2 - PL.c2 * vbt;
+          } else if (L.last_kind == 2) {
+            A = Mi.a1;
+            B = Mi.b1;
+            D = Mi.d1 - Mi.c1 * TZ_r;
+          } else {
+            const Pre& PL = (jj == last) ? Pc : Pn;
+            A = PL.a2;
+            B = 1;
+            D = PL.d2;
+          }
+        }
+        F.row(r - L.off, r, A, B, Cc, D);
+      }
+      Pc = Pn;
+      if (jj + 2 <= last) Pn = pre_y(S, c, i, jj + 2);
+    }
+    if (L.sn < 0) Plast = pre_y(S, c, i, last);
+    const bool ranx = br1 || (S.bienQ[1] && first == 2);
+    const double tv_old = S.tv[i * w + last - 1];
+    double xr = (L.sn >= 0) ? F.xs : 0.0;
+    const double x_last = xr;
+    double tv_lm1_new = tv_old;
+    auto emit = [&](int r, double x) {
+      if (ranx) {
+        const int jj = r >> 1;
+        if (jj >= first && jj < last && jj <= N) {
+          if (r & 1) {
+            S.tv[i * w + jj] = x;
+            if (jj == last - 1) tv_lm1_new = x;
+          } else {
+            S.tz[i * w + jj] = x;
+          }
+        }
+      } else {
+        if (r == 2 * first) {
+          if (first <= N) S.tv[i * w + first] = x;
+          if (first == last - 1) tv_lm1_new = x;
+        } else {
+          const int jj = (r + 1) >> 1;
+          if (jj > first && jj < last && jj <= N) {
+            if (r & 1) S.tz[i * w + jj] = x;
+            else {
+              S.tv[i * w + jj] = x;
+              if (jj == last - 1) tv_lm1_new = x;
+            }
+          }
+        }
+      }
+    };
+    if (L.sn >= 0) {
+      emit(rend, xr);
+      for (int r = rend - 1; r >= L.off; --r) {
+        const double x = Bp[(size_t)r * ld] + Ap[(size_t)r * ld] * xr;
+        emit(r, x);
+        xr = x;
+      }
+    }
+    if (first < last && first <= N) {
+      if (br1) S.tv[i * w + first - 1] = 0;
+      else if (S.bienQ[1] && first == 2) S.tv[i * w + first - 1] = vbd;
+      else
+        S.tv[i * w + first - 1] =
+            (Pfirst.d2 - S.tz[i * w + first] - Pfirst.c2 * S.tv[i * w + first]) / Pfirst.a2;
+    }
+    if (last <= N) {
+      if (br2) {
+        S.tv[i * w + last] = 0;
+        S.tz[i * w + last] = x_last;
+      } else if (S.bienQ[0] && last == M) {
+        S.tv[i * w + last] = vbt;
+        S.tz[i * w + last] = x_last;
+      } else {
+        const double nb = S.race_new ? tv_lm1_new : tv_old;
+        S.tv[i * w + last] = (Plast.d2 - Plast.a2 * nb - S.tz[i * w + last]) / Plast.c2;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ smoothing
+// _normalize (support_funcs.cpp:761-782): tmp <- smoothed value, interior.
+__global__ void k_smooth(State S, Coef c, int isU) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int i = blockIdx.y + 2;
+  if (i > S.N || j > S.M) return;
+  const int W = S.W, g = i * W + j;
+  const double* val = isU ? S.tu : S.tv;
+  const int close = isU ? W : 1, far = isU ? 1 : W;
+  const double vg = val[g];
+  double out = vg;
+  if (vg != 0) {
+    int count = 2;
+    double nb = val[g - close] + val[g + close];
+    if (S.khouot[g - far] == 0) {
+      nb += val[g - far];
+      count++;
+    }
+    if (S.khouot[g + far] == 0) {
+      nb += val[g + far];
+      count++;
+    }
+    out = out * c.heso + (1 - c.heso) * nb / count;
+  }
+  S.tmp[g] = out;
+}
+
+// update_buffer (support_funcs.cpp:784-800).
+__global__ void k_smooth_commit(State S, int isU) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int i = blockIdx.y + 2;
+  if (i > S.N || j > S.M) return;
+  const int g = i * S.W + j;
+  (isU ? S.tu : S.tv)[g] = S.tmp[g];
+}
+
+// ---------------------------------------------------- explicit updates
+__device__ __forceinline__ bool find_seg(const int* dau, const int* cuoi, int n, int pos, int& first,
+                                         int& last) {
+  for (int k = 0; k < n; ++k) {
+    if (dau[k] <= pos && pos <= cuoi[k]) {
+      first = dau[k];
+      last = cuoi[k];
+      return true;
+    }
+  }
+  return false;
+}
+
+// vSolver driven by solveV (UVZSolver_multithread.cpp:607-663, 961-978).
+__global__ void k_solve_v(State S, Coef c) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int row = blockIdx.y + 2;
+  if (row > S.N || col > S.M) return;
+  int first, last;
+  if (!find_seg(S.daui + row * SEG, S.cuoii + row * SEG, S.moci[row], col, first, last)) return;
+  if (first >= last || col >= last || col < first) return;
+  const int off = S.W;
+  const double* u = S.u;
+  const double* v = S.v;
+  const double* tu = S.tu;
+  const double* Hm = S.Hmoi;
+  double p, q = 0, tmp = 0;
+  const double utb = (u[(row - 1) * off + col] + u[row * off + col] + u[(row - 1) * off + col + 1] +
+                      u[row * off + col + 1]) *
+                     0.25;
+  const double t_utb = (tu[(row - 1) * off + col] + tu[row * off + col] +
+                        tu[(row - 1) * off + col + 1] + tu[row * off + col + 1]) *
+                       0.25;
+  const double vv = v[row * off + col];
+  p = (v[row * off + col + 1] - v[row * off + col - 1]) / c.dY2;
+  p = c.HaiChiadT + p + S.Ky1[row * off + col] * sqrt(utb * utb + vv * vv) / S.Htdv[row * off + col];
+  if (Hm[(row - 1) * off + col] <= c.H_TINH) {
+    if (utb < 0) {
+      q = t_utb * (-3 * vv + 4 * v[(row + 1) * off + col] - v[(row + 2) * off + col]) / c.dX2;
+      tmp = (vv - 2 * v[(row + 1) * off + col] + v[(row + 2) * off + col]) / c.dXbp;
+    }
+  } else {
+    if (Hm[(row + 1) * off + col] <= c.H_TINH) {
+      if ((Hm[(row - 2) * off + col] > c.H_TINH) && (utb > 0)) {
+        q = t_utb * (3 * vv - 4 * v[(row - 1) * off + col] + v[(row - 2) * off + col]) / c.dX2;
+        tmp = (vv - 2 * v[(row - 1) * off + col] + v[(row - 2) * off + col]) / c.dXbp;
+      }
+    } else {
+      q = t_utb * (v[(row + 1) * off + col] - v[(row - 1) * off + col]) / c.dX2;
+      tmp = (v[(row + 1) * off + col] - 2 * vv + v[(row - 1) * off + col]) / c.dXbp;
+    }
+  }
+  q = c.HaiChiadT * vv - q - c.CORIOLIS_FORCE * t_utb;
+  q = (q - c.g * (S.z[row * off + col + 1] - S.z[row * off + col]) / c.dY +
+       S.visco[row * off + col] * (tmp + (v[row * off + col + 1] - 2 * vv + v[row * off + col - 1]) / c.dYbp)) +
+      (c.Windy - S.Tsyw[row * off + col]) / S.Htdv[row * off + col];
+  S.tv[row * off + col] = q / p;
+}
+
+// uSolver driven by solveU (UVZSolver_multithread.cpp:724-795, 938-959);
+// dX and Windx are read from dY and Windy as the reference does (:731,734).
+__global__ void k_solve_u(State S, Coef c) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int row = blockIdx.y + 1;
+  if (row > S.N || col > S.M) return;
+  int first, last;
+  if (!find_seg(S.dauj + col * SEG, S.cuoij + col * SEG, S.mocj[col], row, first, last)) return;
+  if (first > last || row < first - 1 || row >= last) return;
+  const int off = S.W;
+  const double dX = c.dY, dY = c.dY, Windx = c.Windy;
+  const double* u = S.u;
+  const double* v = S.v;
+  const double* tv = S.tv;
+  const double* Hm = S.Hmoi;
+  double p, q = 0, tmp = 0;
+  const int ij = row * off + col, i1j = ij + off;
+  const double vtb = (v[ij - 1] + v[ij] + v[i1j - 1] + v[i1j]) * 0.25;
+  const double t_vtb = (tv[ij - 1] + tv[ij] + tv[i1j - 1] + tv[i1j]) * 0.25;
+  p = (u[i1j] - u[(row - 1) * off + col]) / (dX * 2);
+  p = (c.HaiChiadT + p + S.Kx1[ij] * sqrt(vtb * vtb + u[ij] * u[ij]) / S.Htdu[ij]);
+  if (Hm[ij - 1] <= c.H_TINH) {
+    if (vtb < 0) {
+      q = t_vtb * (-3 * u[ij] + 4 * u[ij + 1] - u[ij + 2]) / (dY * 2);
+      tmp = (u[ij] - 2 * u[ij + 1] + u[ij + 2]) / (dY * dY);
+    }
+  } else {
+    if (Hm[ij + 1] <= c.H_TINH) {
+      if ((Hm[ij - 2] > c.H_TINH) && (vtb > 0)) {
+        q = t_vtb * (3 * u[ij] - 4 * u[ij - 1] + u[ij - 2]) / (dY * 2);
+        tmp = (u[ij] - 2 * u[ij - 1] + u[ij - 2]) / (dY * dY);
+      }
+    } else {
+      q = t_vtb * (u[ij + 1] - u[ij - 1]) / (dY * 2);
+      tmp = (u[ij + 1] - 2 * u[ij] + u[ij - 1]) / (dY * dY);
+    }
+  }
+  q = c.HaiChiadT * u[ij] - q + c.CORIOLIS_FORCE * t_vtb;
+  q = (q - c.g * (S.z[i1j] - S.z[ij]) / dX +
+       S.visco[ij] * (tmp + (u[i1j] - 2 * u[ij] + u[(row - 1) * off + col]) / (dX * dX))) +
+      (Windx - S.Tsxw[ij]) / S.Htdu[ij];
+  S.tu[ij] = q / p;
+}
+
+// update_margin_elem_V (UVZSolver_multithread.cpp:1018-1060).
+__global__ void k_margin_v(State S, Coef c) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  if (i > S.N) return;
+  const int w = S.W, M = S.M;
+  double* tv = S.tv;
+  for (int k = 0; k < S.moci[i]; ++k) {
+    const int first = S.daui[i * SEG + k], last = S.cuoii[i * SEG + k];
+    const bool br1 = (first > 2) || ((first == 2) && (fabs((S.h[i * w + first - 1] + S.h[(i - 1) * w + first - 1]) * 0.5 - c.NANGDAY) < 1e-16));
+    const bool br2 = (last < M) || ((last == M) && (fabs((S.h[i * w + last] + S.h[(i - 1) * w + last]) * 0.5 - c.NANGDAY) < 1e-16));
+    if (br1) tv[i * w + first - 1] = 0;
+    else tv[i * w + first - 1] = 2 * tv[i * w + first] - tv[i * w + first + 1];
+    if (br2) tv[i * w + last] = 0;
+    else tv[i * w + last] = 2 * tv[i * w + last - 1] - tv[i * w + last - 2];
+  }
+}
+
+// update_margin_elem_U (UVZSolver_multithread.cpp:980-1016).
+__global__ void k_margin_u(State S, Coef c) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  if (j > S.M) return;
+  const int w = S.W, N = S.N;
+  double* tu = S.tu;
+  for (int k = 0; k < S.mocj[j]; ++k) {
+    const int first = S.dauj[j * SEG + k], last = S.cuoij[j * SEG + k];
+    const bool br1 = (first > 2) || ((first == 2) && (fabs((S.h[1 * w + j] + S.h[1 * w + j - 1]) * 0.5 - c.NANGDAY) < 1e-16));
+    const bool br2 = (last < N) || ((last == N) && (fabs((S.h[N * w + j] + S.h[N * w + j - 1]) * 0.5 - c.NANGDAY) < 1e-16));
+    if (br1) tu[(first - 1) * w + j] = 0;
+    else tu[(first - 1) * w + j] = 2 * tu[first * w + j] - tu[(first + 1) * w + j];
+    if (br2) tu[last * w + j] = 0;
+    else tu[last * w + j] = 2 * tu[(last - 1) * w + j] - tu[(last - 2) * w + j];
+  }
+}
+
+// update_h_moi (support_funcs.cpp:71-86) over [1,N]x[1,M].
+__global__ void k_update_h_moi(State S) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int i = blockIdx.y + 1;
+  if (i > S.N || j > S.M) return;
+  const int g = i * S.W + j;
+  if (S.khouot[g] == 0) S.Hmoi[g] = S.htaiz[g] + S.tz[g];
+}
+
+// update_uvz (support_funcs.cpp:732-759) over [0,N]x[0,M].
+__global__ void k_update_uvz(State S, Coef c) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (i > S.N || j > S.M) return;
+  const int g = i * S.W + j;
+  S.z[g] = S.tz[g];
+  S.u[g] = S.tu[g] * (1 - c.kenhhepd);
+  S.v[g] = S.tv[g] * (1 - c.kenhhepng);
+}
+
+// Reset_states_vertical (support_funcs.cpp:142-188): one thread per column.
+__global__ void k_reset_vertical(State S, Coef c) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (j > S.M) return;
+  const int off = S.W, N = S.N;
+  double* tz = S.tz;
+  double* Hm = S.Hmoi;
+  int* kh = S.khouot;
+  for (int i = 2; i <= N; ++i) {
+    if (tz[i * off + j] > S.z[i * off + j]) {
+      if (kh[(i - 1) * off + j] == 1) {
+        tz[(i - 1) * off + j] = tz[i * off + j];
+        Hm[(i - 1) * off + j] = S.htaiz[(i - 1) * off + j] + tz[i * off + j];
+        kh[(i - 1) * off + j] = 0;
+        S.FS[(i - 1) * off + j] = S.FS[i * off + j];
+      }
+      if (kh[(i + 1) * off + j] == 1) {
+        tz[(i + 1) * off + j] = tz[i * off + j];
+        Hm[(i + 1) * off + j] = S.htaiz[(i + 1) * off + j] + tz[i * off + j];
+        kh[(i + 1) * off + j] = 0;
+        S.FS[(i + 1) * off + j] = S.FS[i * off + j];
+      }
+    }
+  }
+  for (int i = 2; i <= N; ++i) {
+    if ((kh[i * off + j] == 0) && (Hm[i * off + j] <= c.H_TINH)) {
+      S.tu[(i - 1) * off + j] = 0;
+      S.tu[i * off + j] = 0;
+      S.tv[i * off + j - 1] = 0;
+      S.tv[i * off + j] = 0;
+      kh[i * off + j] = 1;
+      S.FS[i * off + j] = 0;
+    }
+  }
+}
+
+// ------------------------------------------------------------- launchers
+static inline dim3 grid2(int nx, int ny, int bx) { return dim3(cdiv(nx, bx), ny); }
+
+void launch_init(const State& S, const Coef& c, cudaStream_t st) {
+  k_onetime_init<<<dim3(cdiv(S.W, 128), S.H), 128, 0, st>>>(S, c);
+  launch_find_limits(S, c, st);
+  k_htuongdoi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
+  k_preprocess<<<1, 32, 0, st>>>(S, c);
+}
+
+void launch_scan_segments(const State& S, cudaStream_t st) {
+  k_scan_rows<<<cdiv(S.N, 128), 128, 0, st>>>(S);
+  k_scan_cols<<<cdiv(S.M, 128), 128, 0, st>>>(S);
+}
+
+void launch_find_limits(const State& S, const Coef& c, cudaStream_t st) {
+  k_interp_fs_rows<<<dim3(cdiv(S.M, 128), 2), 128, 0, st>>>(S, c);
+  k_scan_rows<<<cdiv(S.N, 128), 128, 0, st>>>(S);
+  k_interp_fs_col<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
+  k_scan_cols<<<cdiv(S.M, 128), 128, 0, st>>>(S);
+}
+
+void launch_half_x(const State& S, const Coef& c, double t, cudaStream_t st) {
+  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, (float)t);
+  k_sweep_x<<<cdiv(S.M - 1, 128), 128, 0, st>>>(S, c);
+  k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 1);
+  k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 1);
+  k_solve_v<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c);
+  k_margin_v<<<cdiv(S.N - 1, 128), 128, 0, st>>>(S, c);
+  k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 0);
+  k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 0);
+  k_update_h_moi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
+  k_update_uvz<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c);
+  launch_find_limits(S, c, st);
+  k_htuongdoi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
+}
+
+void launch_half_y(const State& S, const Coef& c, double t, cudaStream_t st) {
+  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, (float)t);
+  k_sweep_y<<<cdiv(S.N - 1, 128), 128, 0, st>>>(S, c);
+  k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 0);
+  k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 0);
+  k_solve_u<<<grid2(S.M - 1, S.N, 128), 128, 0, st>>>(S, c);
+  k_margin_u<<<cdiv(S.M - 1, 128), 128, 0, st>>>(S, c);
+  k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 1);
+  k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 1);
+  k_update_h_moi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
+  k_reset_vertical<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
+  k_update_uvz<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c);
+  launch_find_limits(S, c, st);
+  k_htuongdoi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
+}
+
+}  // namespace hyd

@@ -1,0 +1,207 @@
+/*
+ * hydist_capi.h -- C ABI of the B200 (sm_100a) implementation of the Hydist_C
+ * ADI time step (2D shallow-water hydraulics + suspended-sediment transport)
+ * and of its batched tridiagonal solver.
+ *
+ * Plain C: pointers, sizes and status codes only. Every function returns an
+ * int status (HYDIST_OK = 0, negative on error; hydist_last_error() gives the
+ * message of the calling thread's last failure). No exception crosses this
+ * boundary.
+ *
+ * Data conventions are the reference's (engine.h:16-89, loader.cpp:224-375):
+ *   - mesh fields are FP64, row-major (N+3) x (M+3), idx = i*(M+3) + j;
+ *     i in [2,N] is the x / u / dX direction ("rows"), j in [2,M] is the
+ *     y / v / dY direction ("columns", contiguous in memory);
+ *   - the wet/dry mask (khouot) is int32 of the same shape: 0 wet, 1 dried
+ *     during the run, 2 dry at initialisation;
+ *   - boundary series are flat [segment * total_time + hour];
+ *   - sides are indexed up (j = M), down (j = 2), left (i = 2), right (i = N).
+ *
+ * Which reference interface each entry point replaces is cited beside it as
+ * reference-file:line (paths relative to the Hydist_C source tree).
+ */
+#ifndef HYDIST_CAPI_H
+#define HYDIST_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HYDIST_SEGMENT_LIMIT 20 /* wet segments per line, engine.h:12 */
+
+/* ---- status codes ---------------------------------------------------- */
+enum HydistStatus {
+  HYDIST_OK = 0,
+  HYDIST_ERR_ARG = -1,        /* bad argument (null pointer, size, enum)   */
+  HYDIST_ERR_CUDA = -2,       /* a CUDA runtime call failed                */
+  HYDIST_ERR_OOM = -3,        /* device allocation failed                  */
+  HYDIST_ERR_SEGMENTS = -4,   /* a line has more than 20 wet segments      */
+  HYDIST_ERR_STATE = -5,      /* call not valid in the handle's state      */
+  HYDIST_ERR_BUDGET = -6,     /* serving: request exceeds the HBM budget   */
+  HYDIST_ERR_TIMEOUT = -7,    /* a bounded device wait gave up             */
+  HYDIST_ERR_NONFINITE = -8,  /* NaN/Inf detected in the state             */
+  HYDIST_ERR_NODEVICE = -9    /* no CUDA device visible                    */
+};
+
+/* ---- fields exchangeable with the host ------------------------------- */
+enum HydistField {
+  HYDIST_FIELD_U = 0,      /* u  (Argument_Pointers::u)                    */
+  HYDIST_FIELD_V = 1,      /* v                                            */
+  HYDIST_FIELD_Z = 2,      /* z  water level                               */
+  HYDIST_FIELD_FS = 3,     /* suspended concentration (volumetric)         */
+  HYDIST_FIELD_TFS = 4,    /* concentration sweep buffer (tFS)             */
+  HYDIST_FIELD_H_MOI = 5,  /* total depth at z points                      */
+  HYDIST_FIELD_KHOUOT = 6, /* int32 wet/dry mask                           */
+  HYDIST_FIELD_DH = 7,     /* accumulated bed change                       */
+  HYDIST_FIELD_HTDU = 8,   /* total depth at u points                      */
+  HYDIST_FIELD_HTDV = 9,   /* total depth at v points                      */
+  HYDIST_FIELD_TU = 10,    /* t_u (provisional u)                          */
+  HYDIST_FIELD_TV = 11,    /* t_v                                          */
+  HYDIST_FIELD_TZ = 12,    /* t_z                                          */
+  HYDIST_FIELD_KX1 = 13,   /* friction coefficient at u points             */
+  HYDIST_FIELD_KY1 = 14,   /* friction coefficient at v points             */
+  HYDIST_FIELD_VTH = 15,   /* speed at cell centre                         */
+  HYDIST_FIELD_KX = 16,    /* sediment diffusivity, x                      */
+  HYDIST_FIELD_KY = 17,    /* sediment diffusivity, y                      */
+  HYDIST_FIELD_H = 18,     /* bed depth at nodes (bandodosau)              */
+  HYDIST_FIELD_HTAIZ = 19, /* bed depth at z points                        */
+  HYDIST_FIELD_QBX = 20,   /* bed-load flux, x                             */
+  HYDIST_FIELD_QBY = 21,   /* bed-load flux, y                             */
+  HYDIST_FIELD_COUNT = 22
+};
+
+/* Precision of the time step. */
+enum HydistPrecision {
+  HYDIST_FP64 = 0,       /* plain FP64 form: reproduces the reference       */
+  HYDIST_FP32_REFINE = 1 /* FP32 bulk, FP64 z/bed state + FP64 refinement   */
+};
+
+/* Physical and numerical constants: the inputs of Load_coeffs
+ * (loader.cpp:4-87, struct Constant_Coeffs engine.h:39-52). The derived
+ * constants (dXbp, dTchia2dX, Ufr, Dxr, ...) are computed from these exactly
+ * as Load_coeffs does. hydist_params_default() fills the reference values. */
+typedef struct HydistParams {
+  double dX, dY, dT;
+  double NANGDAY;   /* bed-raise offset                      loader.cpp:22 */
+  double H_TINH;    /* dry threshold (m)                     loader.cpp:23 */
+  double heso;      /* smoothing weight                      loader.cpp:33 */
+  double mu_mn;     /* Manning exponent parameter            loader.cpp:34 */
+  double NDnen;     /* background concentration              loader.cpp:36 */
+  double Tod, Toe, hstoe, ghtoe, Mbochat; /*                 loader.cpp:46-50 */
+  double ro, ros;                         /*                 loader.cpp:53-54 */
+  double dm, d90, muy, Dorong, Sx;        /*                 loader.cpp:57-66 */
+  double CORIOLIS_FORCE, g;               /*                 loader.cpp:75-76 */
+  double Wind, huonggio;                  /*                 loader.cpp:26-27 */
+  double wss; /* settling velocity; < 0 derives it as loader.cpp:86      */
+  double Ks;  /* roughness height; < 0 derives 2.5*dm as loader.cpp:79    */
+} HydistParams;
+
+/* Run options: the fields of struct Options (engine.h:16-37) that the time
+ * step reads. */
+typedef struct HydistOptions {
+  double t_start;          /* simulated start time (s)         main.cpp:100 */
+  double sediment_start;   /* -b: sediment sweeps from this t  main.cpp:82  */
+  double bed_change_start; /* -B: erosion source and bed change from this t */
+  int32_t ketdinh;         /* cohesive sediment (main.cpp:53 sets 1)        */
+  int32_t bed_change;      /* 1: apply the bed-change update each step      */
+  int32_t precision;       /* enum HydistPrecision                          */
+  int32_t reserved;
+} HydistOptions;
+
+/* One scenario's inputs, host pointers, in the reference's text-input
+ * meaning (loader.cpp:120-168). Series hold at least total_time entries for
+ * segment 0 (the only segment the reference's boundary update reads,
+ * support_funcs.cpp:614-618). All pointers are read during the call only. */
+typedef struct HydistScenario {
+  int32_t M, N;               /* interior extents; arrays are (N+3)x(M+3)     */
+  int32_t total_time;         /* rows of the hourly series (loader.cpp:165)   */
+  int32_t n_boundary_type;    /* entries in boundary_type (80 = 4 sides x 20) */
+  const double* h;            /* bandodosau: bed depth at nodes               */
+  const double* hsnham;       /* Manning roughness                            */
+  const double* visco;        /* hsnhotroiA: eddy viscosity (VISCOIDX)        */
+  const double* Fw;           /* Fw_map                                       */
+  const double* bc_up;        /* hourly Z or Q series per side                */
+  const double* bc_down;
+  const double* bc_left;
+  const double* bc_right;
+  const double* CC_up;        /* hourly FS boundary series per side           */
+  const double* CC_down;
+  const double* CC_left;
+  const double* CC_right;
+  const int32_t* boundary_type; /* side-major, 20 per side; 2 = discharge     */
+  int32_t bienQ[4];           /* discharge flag per side (up,down,left,right)
+                                 as loader.cpp:157-164 derives it            */
+  const double* FS0;          /* optional initial concentration, or NULL      */
+} HydistScenario;
+
+typedef struct HydistHandle HydistHandle;
+
+/* Reference constants of Load_coeffs (loader.cpp:4-87). */
+void hydist_params_default(HydistParams* p);
+/* Options as main.cpp:49-53 defaults them (t_start 0, ketdinh 1, FP64). */
+void hydist_options_default(HydistOptions* o);
+/* bienQ[k] = (boundary_type[k] == 2) for k < 4, as loader.cpp:157-164. */
+void hydist_bienq_from_boundary_type(const int32_t* boundary_type, int32_t n,
+                                     int32_t bienQ[4]);
+
+const char* hydist_last_error(void);
+const char* hydist_version(void);
+
+/* ---- one scenario on the device --------------------------------------
+ * hydist_create replaces the set-up sequence of main.cpp:138-304
+ * (attribute_arrays_memory_alloc loader.cpp:224-330, supporting_arrays_alloc
+ * loader.cpp:333-375, Load_coeffs, Onetime_init support_funcs.cpp:21-69,
+ * Find_Calculation_limits_* :238-343, Htuongdoi :346-362, preprocess_data
+ * :482-601). All device state is allocated here and freed by hydist_destroy.
+ * device < 0 uses the current device. */
+int hydist_create(const HydistScenario* sc, const HydistParams* p,
+                  const HydistOptions* o, int device, HydistHandle** out);
+int hydist_destroy(HydistHandle* h);
+
+/* Advance nsteps full ADI steps (two half-steps each): the body of the time
+ * loop of Hydraulic_Calculation (engine.cpp:65-295). Stream-ordered on the
+ * handle's stream; returns once the work is enqueued. */
+int hydist_step(HydistHandle* h, int32_t nsteps);
+/* Block until the handle's stream is idle (synch_and_check, engine.cpp:13). */
+int hydist_sync(HydistHandle* h);
+/* Simulated time of the state (seconds); set_time supports resuming a
+ * checkpoint (the reference's -T start time, main.cpp:100-102). */
+int hydist_get_time(HydistHandle* h, double* t);
+int hydist_set_time(HydistHandle* h, double t);
+/* Copy one field (HydistField) to/from host memory of (N+3)*(M+3) elements
+ * (int32 for KHOUOT, double otherwise). Synchronous. Uploading KHOUOT
+ * recomputes the wet-segment tables from it. */
+int hydist_download(HydistHandle* h, int32_t field, void* host);
+int hydist_upload(HydistHandle* h, int32_t field, const void* host);
+/* Water volume sum over wet cells of (htaiz + z) * dX * dY, accumulated in
+ * FP64 on the device (mass-conservation check). */
+int hydist_mass(HydistHandle* h, double* volume);
+/* Run nsteps with each step captured once into a CUDA graph and replayed.
+ * Same results as hydist_step. */
+int hydist_step_graph(HydistHandle* h, int32_t nsteps);
+/* The CUDA stream the handle enqueues on (a cudaStream_t). */
+void* hydist_stream(HydistHandle* h);
+
+/* ---- batched tridiagonal solver --------------------------------------
+ * Replaces tridiag() + tridiagSolver (UVZSolver_multithread.cpp:19-43,
+ * 78-109) and gtsv_spike_partial_diag_pivot_v1 (gtsv.cpp:88-193) with one
+ * batched, host-callable entry point. System s occupies rows
+ * [offsets[s], offsets[s] + lengths[s]) of the packed arrays; dl[first row]
+ * and du[last row] of each system are ignored. Arrays are device pointers.
+ * dtype: 0 = FP64, 1 = FP32. algo: 0 = autotuned choice per length band,
+ * 1 = Thomas (thread per system), 2 = partitioned Thomas / SPIKE with
+ * diagonal pivoting, 3 = warp PCR-Thomas. stream is a cudaStream_t (NULL =
+ * default stream). Scratch is allocated by the library on first use. */
+int hydist_gtsv_batched(const void* dl, const void* d, const void* du,
+                        const void* b, void* x, const int32_t* offsets,
+                        const int32_t* lengths, int32_t nsys, int32_t dtype,
+                        int32_t algo, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HYDIST_CAPI_H */

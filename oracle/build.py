@@ -1,0 +1,95 @@
+"""TEST INFRASTRUCTURE: builds the CPU oracle and, where the reference source
+tree is present, the reference driver.
+
+* ``build_oracle()`` compiles hydist_oracle.cpp into
+  ``oracle/_build/libhydist_oracle.so`` (g++, FP64, no fused multiply-add).
+* ``build_reference(src)`` compiles the reference's own CUDA sources where
+  they lie (``src``; nothing is copied) with nvcc for sm_100a, links them
+  with ``ref_driver.cu`` (our driver, which calls the reference's set-up
+  functions and Hydraulic_Calculation and dumps the state in binary) and
+  writes ``oracle/_ref/hydist_ref_driver``. It also builds
+  ``oracle/_ref/hydist_ref_tridiag``, which runs the reference's device
+  tridiag() on batched systems. Outputs go to oracle/_ref/ only.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+BUILD = HERE / "_build"
+REF_OUT = HERE / "_ref"
+ORACLE_SO = BUILD / "libhydist_oracle.so"
+REF_DRIVER = REF_OUT / "hydist_ref_driver"
+REF_TRIDIAG = REF_OUT / "hydist_ref_tridiag"
+REF_SOURCES = ["engine.cpp", "support_funcs.cpp", "UVZSolver_multithread.cpp", "loader.cpp",
+               "sediment_transport.cpp", "gtsv.cpp"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _run(cmd, cwd=None):
+    r = subprocess.run(cmd, cwd=cwd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("command failed: " + " ".join(map(str, cmd)) + "\n" + r.stdout + r.stderr)
+    return r
+
+
+def _stale(out: Path, deps) -> bool:
+    if not out.exists():
+        return True
+    t = out.stat().st_mtime
+    return any(Path(d).stat().st_mtime > t for d in deps)
+
+
+def build_oracle(force=False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    src = HERE / "hydist_oracle.cpp"
+    deps = [src, HERE / "hydist_oracle.h", HERE.parent / "include" / "hydist_capi.h"]
+    if force or _stale(ORACLE_SO, deps):
+        tmp = ORACLE_SO.with_suffix(".so.tmp")
+        _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fopenmp",
+              "-fPIC", "-shared", "-o", str(tmp), str(src)])
+        os.replace(tmp, ORACLE_SO)
+    return ORACLE_SO
+
+
+def build_reference(src="/root/reference", force=False):
+    """Compile the reference CUDA sources from ``src`` into oracle/_ref."""
+    src = Path(src)
+    if not (src / "engine.cpp").exists():
+        return None
+    if shutil.which("nvcc") is None:
+        return None
+    REF_OUT.mkdir(exist_ok=True)
+    objdir = REF_OUT / "obj"
+    objdir.mkdir(exist_ok=True)
+    drv = HERE / "ref_driver.cu"
+    tri = HERE / "ref_tridiag.cu"
+    deps = [drv, tri] + [src / s for s in REF_SOURCES]
+    if not force and not _stale(REF_DRIVER, deps) and not _stale(REF_TRIDIAG, deps):
+        return REF_DRIVER
+    objs = []
+    for s in REF_SOURCES:
+        o = objdir / (Path(s).stem + ".o")
+        _run(["nvcc", "-std=c++11", f"-I{src}", "-x", "cu", *ARCH, "-O3", "-w", "-dc",
+              str(src / s), "-o", str(o)])
+        objs.append(str(o))
+    d_o = objdir / "ref_driver.o"
+    _run(["nvcc", "-std=c++14", f"-I{src}", "-x", "cu", *ARCH, "-O3", "-w", "-dc", str(drv),
+          "-o", str(d_o)])
+    _run(["nvcc", *ARCH, *objs, str(d_o), "-o", str(REF_DRIVER)])
+    t_o = objdir / "ref_tridiag.o"
+    _run(["nvcc", "-std=c++14", f"-I{src}", "-x", "cu", *ARCH, "-O3", "-w", "-dc", str(tri),
+          "-o", str(t_o)])
+    _run(["nvcc", *ARCH, str(objdir / "UVZSolver_multithread.o"), str(objdir / "support_funcs.o"),
+          str(objdir / "gtsv.o"), str(t_o), "-o", str(REF_TRIDIAG)])
+    return REF_DRIVER
+
+
+if __name__ == "__main__":
+    print(build_oracle(force="--force" in sys.argv))
+    if "--ref" in sys.argv:
+        print(build_reference(force="--force" in sys.argv))

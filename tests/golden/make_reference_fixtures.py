@@ -1,0 +1,188 @@
+"""Generates the golden fixtures that pin the CPU oracle to the reference.
+
+Three steps, run where each can run:
+
+1. ``inputs <dir>`` (here, where the reference source tree is): writes the
+   reference-format input directories of the pinned cases under <dir>:
+     - ``channel``   : the 256x128 channel case (dx=dy=10 m, dt=2 s);
+     - ``luy``       : the reference's own river mesh (Inputs/, 464x324) with
+                       its boundary types spread to the 80-entry side-major
+                       layout the kernels index (support_funcs.cpp:705-721);
+     - ``sediment``  : a 128x64 channel with the sediment sweeps and the
+                       erosion source on from t=0 (dx=dy=5 m).
+2. ``run <dir> <out>`` (on the GPU box): runs oracle/_ref/hydist_ref_driver,
+   the reference's own time step built from its sources, on each case and
+   writes full-precision state files under <out>/<case>/.
+3. ``collect <out>`` (here): turns the state files into compact fixtures
+   tests/golden/ref_<case>.npz: a strided subsample of u, v, z (and FS for the
+   sediment case) at each saved step, plus the full wet/dry mask.
+
+``kat`` (here) writes tests/golden/khouot_kat.npz: the reference's shipped
+Inputs/bandodosau.txt and the wet/dry mask its Onetime_init produced from it
+(Outputs/khouot.txt, written by main.cpp:268-280).
+"""
+from __future__ import annotations
+
+import json
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from hydist_c_b200 import scenario as S  # noqa: E402
+
+REF_INPUTS = Path("/root/reference/Inputs")
+CASES = {
+    "channel": dict(steps=[1, 2, 10, 100, 1800], stride=3, fields=["u", "v", "z"],
+                    args=[]),
+    "luy": dict(steps=[1, 10, 100, 600], stride=5, fields=["u", "v", "z"], args=[]),
+    "sediment": dict(steps=[1, 2, 10, 100, 300], stride=3, fields=["u", "v", "z", "FS"],
+                     args=["sediment_start=0", "bed_change_start=0", "dX=5", "Toe=0.2",
+                           "Tod=0.1", "Mbochat=0.0001", "wss=0.0005", "fs0=fs0.bin"]),
+}
+
+
+def sediment_bundle():
+    b = S.make_channel(N=128, M=64, seed=20265000, dx=5.0, dt=2.0, hours=1.0, sediment=True,
+                       sediment_start=0.0)
+    b["options"]["bed_change_start"] = 0.0
+    return b
+
+
+def luy_bundle():
+    """The reference's river inputs as a scenario dict."""
+    h = np.loadtxt(REF_INPUTS / "bandodosau.txt")
+    n = h.size
+    hs = np.loadtxt(REF_INPUTS / "hsnham.txt").ravel()[:n].reshape(h.shape)
+    vi = np.loadtxt(REF_INPUTS / "hsnhotroiA.txt").ravel()[:n].reshape(h.shape)
+    fw = np.loadtxt(REF_INPUTS / "Fw_map.txt").ravel()[:n].reshape(h.shape)
+    rd = lambda f: np.loadtxt(REF_INPUTS / f).ravel()
+    bt4 = np.loadtxt(REF_INPUTS / "boundary_type.txt").astype(np.int32).ravel()
+    bt = np.zeros(80, np.int32)
+    bt[:4] = bt4
+    for s in range(4):
+        bt[s * 20] = bt4[s]
+    T = rd("bienduoi.txt").size
+    sc = dict(M=h.shape[1] - 3, N=h.shape[0] - 3, total_time=T, h=h, hsnham=hs, visco=vi, Fw=fw,
+              bc_up=rd("bientren.txt")[:T], bc_down=rd("bienphai.txt")[:T],
+              bc_left=rd("bientrai.txt")[:T], bc_right=rd("bienduoi.txt")[:T],
+              CC_up=rd("FS_bientren.txt")[:T], CC_down=rd("FS_bienduoi.txt")[:T],
+              CC_left=rd("FS_bientrai.txt")[:T], CC_right=rd("FS_bienphai.txt")[:T],
+              boundary_type=bt, bienQ=[int(bt[k] == 2) for k in range(4)], FS0=None)
+    return dict(scenario=sc, params={}, options=dict(sediment_start=1e12, bed_change_start=1e12),
+                meta=dict(name="luy"))
+
+
+def bundle(case):
+    if case == "channel":
+        return S.config0()
+    if case == "sediment":
+        return sediment_bundle()
+    if case == "luy":
+        return luy_bundle()
+    raise KeyError(case)
+
+
+def write_luy_inputs(d: Path):
+    """Copy the reference's river inputs with an 80-entry boundary_type."""
+    d.mkdir(parents=True, exist_ok=True)
+    for f in REF_INPUTS.glob("*.txt"):
+        if f.name == "boundary_type.txt":
+            continue
+        (d / f.name).write_bytes(f.read_bytes())
+    bt = luy_bundle()["scenario"]["boundary_type"]
+    (d / "boundary_type.txt").write_text("".join(f"{int(v)}\n" for v in bt))
+
+
+def cmd_inputs(root):
+    root = Path(root)
+    for case in CASES:
+        d = root / case
+        if case == "luy":
+            write_luy_inputs(d)
+        else:
+            b = bundle(case)
+            S.write_reference_inputs(b["scenario"], d)
+            if b["scenario"].get("FS0") is not None:
+                np.ascontiguousarray(b["scenario"]["FS0"], dtype="<f8").tofile(d / "fs0.bin")
+    print("inputs written under", root)
+
+
+def cmd_run(root, out):
+    root, out = Path(root), Path(out)
+    drv = ROOT / "oracle" / "_ref" / "hydist_ref_driver"
+    for case, spec in CASES.items():
+        o = out / case
+        o.mkdir(parents=True, exist_ok=True)
+        args = [a.replace("fs0=fs0.bin", f"fs0={root / case / 'fs0.bin'}") for a in spec["args"]]
+        cmd = [str(drv), str(root / case) + "/", str(o), ",".join(map(str, spec["steps"]))] + args
+        with open(o / "stdout.txt", "w") as f:
+            r = subprocess.run(cmd, stdout=f, stderr=subprocess.PIPE, text=True)
+        print(case, r.returncode, r.stderr[-2000:])
+        if r.returncode != 0:
+            raise SystemExit(r.returncode)
+
+
+PACK_FIELDS = {"channel": ["u", "v", "z", "FS", "H_moi", "t_u", "t_v", "t_z", "khouot"],
+               "luy": ["u", "v", "z", "khouot"],
+               "sediment": ["u", "v", "z", "FS", "tFS", "H_moi", "VTH", "Kx", "Ky", "khouot"]}
+
+
+def cmd_pack(out):
+    """On the GPU box: full-precision state files -> one npz per case (the
+    raw files are removed so that the results fit the return channel)."""
+    from oracle.oracle import read_ref_state
+    out = Path(out)
+    for case, spec in CASES.items():
+        arrs = {}
+        for st in spec["steps"]:
+            p = out / case / f"state_{st}.bin"
+            r = read_ref_state(p)
+            for f in PACK_FIELDS[case]:
+                a = r["fields"][f]
+                arrs[f"{f}_{st}"] = a.astype(np.int8) if f == "khouot" else a
+            arrs[f"t_{st}"] = np.float64(r["t"])
+            p.unlink()
+        np.savez_compressed(out / f"full_{case}.npz", **arrs)
+        print("packed", case)
+
+
+def cmd_collect(out):
+    out = Path(out)
+    for case, spec in CASES.items():
+        arrs = {}
+        meta = dict(case=case, steps=spec["steps"], stride=spec["stride"], fields=spec["fields"])
+        s = spec["stride"]
+        full = np.load(out / f"full_{case}.npz")
+        for st in spec["steps"]:
+            for f in spec["fields"]:
+                arrs[f"{f}_{st}"] = full[f"{f}_{st}"][::s, ::s].copy()
+            arrs[f"khouot_{st}"] = full[f"khouot_{st}"].astype(np.int8)
+            arrs[f"t_{st}"] = full[f"t_{st}"]
+        np.savez_compressed(ROOT / "tests" / "golden" / f"ref_{case}.npz", meta=json.dumps(meta),
+                            **arrs)
+        print("wrote", case)
+
+
+def cmd_kat():
+    h = np.loadtxt(REF_INPUTS / "bandodosau.txt")
+    k = np.loadtxt(REF_INPUTS.parent / "Outputs" / "khouot.txt").astype(np.int8)
+    np.savez_compressed(ROOT / "tests" / "golden" / "khouot_kat.npz", h=h, khouot=k)
+
+
+if __name__ == "__main__":
+    cmd = sys.argv[1]
+    if cmd == "kat":
+        cmd_kat()
+    elif cmd == "inputs":
+        cmd_inputs(sys.argv[2])
+    elif cmd == "run":
+        cmd_run(sys.argv[2], sys.argv[3])
+    elif cmd == "pack":
+        cmd_pack(sys.argv[2])
+    elif cmd == "collect":
+        cmd_collect(sys.argv[2])

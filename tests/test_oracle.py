@@ -1,0 +1,153 @@
+"""CPU tests of the oracle: known-answer test from the reference's own output,
+reference-run fixtures, the Thomas solver, and scenario generation."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from hydist_c_b200 import scenario as S
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def _kat_bundle():
+    z = np.load(GOLDEN / "khouot_kat.npz")
+    h = z["h"]
+    b = S.make_channel(N=h.shape[0] - 3, M=h.shape[1] - 3)
+    sc = b["scenario"]
+    sc["h"] = h
+    sc["hsnham"] = np.full_like(h, 0.03)
+    sc["visco"] = np.ones_like(h)
+    sc["Fw"] = np.zeros_like(h)
+    return b, z["khouot"].astype(np.int32)
+
+
+def test_khouot_kat(oracle_mod):
+    """Onetime_init on the reference's river depth map reproduces the wet/dry
+    mask the reference wrote (Outputs/khouot.txt, main.cpp:268-280)."""
+    b, ref = _kat_bundle()
+    o = oracle_mod.OracleSim(b)
+    k = o.get("khouot")
+    assert k.shape == ref.shape
+    assert int((k != ref).sum()) == 0
+    # the river mesh has at most 2 wet runs per row and 3 per column
+    assert o.segments(0)[2].max() == 2
+    assert o.segments(1)[2].max() == 3
+
+
+def _ref_fixture(case):
+    p = GOLDEN / f"ref_{case}.npz"
+    if not p.exists():
+        pytest.skip(f"{p.name} not generated")
+    z = np.load(p)
+    return z, json.loads(str(z["meta"]))
+
+
+def _fixture_bundle(case):
+    import sys
+    sys.path.insert(0, str(GOLDEN))
+    import make_reference_fixtures as F
+    if case == "luy":
+        if not F.REF_INPUTS.exists():
+            pytest.skip("reference inputs not present")
+    return F.bundle(case)
+
+
+@pytest.mark.parametrize("case", ["channel", "sediment", "luy"])
+def test_oracle_matches_reference_run(oracle_mod, case):
+    """The oracle against the reference's own time step, run on a B200 from
+    its sources (tests/golden/make_reference_fixtures.py): u, v, z (FS) on a
+    strided subsample at every saved step, and the full wet/dry mask."""
+    z, meta = _ref_fixture(case)
+    b = _fixture_bundle(case)
+    o = oracle_mod.OracleSim(b, nthreads=4)
+    done = 0
+    s = meta["stride"]
+    for st in meta["steps"]:
+        if st > 300 and case != "channel":
+            break
+        o.step(st - done)
+        done = st
+        assert o.t == pytest.approx(float(z[f"t_{st}"]))
+        assert np.array_equal(o.get("khouot").astype(np.int8), z[f"khouot_{st}"])
+        for f in meta["fields"]:
+            a = o.get(f)[::s, ::s]
+            r = z[f"{f}_{st}"]
+            scale = max(np.abs(r).max(), 1e-300)
+            # FMA contraction on the GPU vs none in the oracle: rounding-level
+            # differences that grow slowly with the step count
+            tol = (1e-10 if st <= 100 else 1e-7) * scale
+            assert np.abs(a - r).max() <= tol, (case, st, f, np.abs(a - r).max(), scale)
+
+
+def test_thomas_vs_dense(oracle_mod):
+    rng = np.random.default_rng(5)
+    for n in (1, 2, 3, 17, 200):
+        a = rng.uniform(-1, 1, n)
+        c = rng.uniform(-1, 1, n)
+        d = np.abs(a) + np.abs(c) + rng.uniform(0.1, 1.0, n)
+        b = rng.standard_normal(n)
+        x = oracle_mod.thomas(a, d, c, b)
+        A = np.diag(d) + np.diag(a[1:], -1) + np.diag(c[:-1], 1)
+        assert np.allclose(A @ x, b, atol=1e-12)
+
+
+def test_thomas_batched(oracle_mod):
+    rng = np.random.default_rng(6)
+    lens = rng.integers(1, 50, 30)
+    off = np.concatenate([[0], np.cumsum(lens)[:-1]])
+    tot = int(lens.sum())
+    a, c = rng.uniform(-1, 1, tot), rng.uniform(-1, 1, tot)
+    d = np.abs(a) + np.abs(c) + 0.5
+    b = rng.standard_normal(tot)
+    x = oracle_mod.thomas_batched(a, d, c, b, off, lens, nthreads=2)
+    for o_, n in zip(off, lens):
+        xs = oracle_mod.thomas(a[o_:o_ + n], d[o_:o_ + n], c[o_:o_ + n], b[o_:o_ + n])
+        assert np.array_equal(xs, x[o_:o_ + n])
+
+
+def test_channel_geometry():
+    b = S.config0()
+    sc = b["scenario"]
+    N, M = sc["N"], sc["M"]
+    assert sc["h"].shape == (N + 3, M + 3)
+    # dry banks: node columns 0..2 and M-1..M+2 at NANGDAY = 0
+    assert np.all(sc["h"][:, :3] == 0) and np.all(sc["h"][:, M - 1:] == 0)
+    assert np.all(sc["h"][:, 3:M - 1] >= 0.1)
+    assert sc["bienQ"] == [0, 0, 1, 0]
+    assert b["meta"]["steps"] == 1800
+
+
+def test_channel_runs_and_conserves_shape(oracle_mod):
+    b = S.make_channel(N=64, M=32, seed=3)
+    o = oracle_mod.OracleSim(b)
+    o.step(20)
+    for f in ("u", "v", "z"):
+        assert np.isfinite(o.get(f)).all()
+    d, c, m = o.segments(0)
+    assert (m[2:65] == 1).all()
+    assert (d[2:65, 0] == 3).all() and (c[2:65, 0] == 31).all()
+
+
+def test_determinism_across_threads(oracle_mod):
+    b = S.make_channel(N=48, M=24, seed=11)
+    o1 = oracle_mod.OracleSim(b, nthreads=1)
+    o4 = oracle_mod.OracleSim(b, nthreads=4)
+    o1.step(15)
+    o4.step(15)
+    for f in ("u", "v", "z"):
+        assert np.array_equal(o1.get(f), o4.get(f))
+
+
+def test_reference_format_roundtrip(tmp_path):
+    b = S.make_channel(N=16, M=12, seed=1)
+    sc = b["scenario"]
+    S.write_reference_inputs(sc, tmp_path)
+    h = np.loadtxt(tmp_path / "bandodosau.txt")
+    assert np.array_equal(h, sc["h"])
+    # the reference's down side reads bienphai.txt, its right side bienduoi.txt
+    assert np.allclose(np.loadtxt(tmp_path / "bienduoi.txt"), sc["bc_right"])
+    assert np.allclose(np.loadtxt(tmp_path / "bienphai.txt"), sc["bc_down"])
+    bt = np.loadtxt(tmp_path / "boundary_type.txt").astype(int)
+    assert bt.size == 80 and bt[40] == 2 and bt[60] == 1
