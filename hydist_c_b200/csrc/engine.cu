@@ -128,6 +128,15 @@ int check_device_err(HydistHandle* h) {
   return HYDIST_OK;
 }
 
+// The boundary update interpolates hour floor(t/3600) and the next one
+// (support_funcs.cpp:624); refuse steps whose time runs past the series.
+int check_horizon(HydistHandle* h, int nsteps) {
+  const double t_end = h->t + nsteps * h->c.dT;
+  if ((int)((double)(float)t_end / 3600) + 1 > h->S.T - 1)
+    return fail(HYDIST_ERR_ARG, "boundary series too short for the requested steps");
+  return HYDIST_OK;
+}
+
 // one full step (engine.cpp:65-295)
 void enqueue_step(HydistHandle* h, double t0, bool sed_x, bool sed_y) {
   const double t1 = t0 + 0.5 * h->c.dT;
@@ -384,6 +393,7 @@ int hydist_step(HydistHandle* h, int32_t nsteps) {
   if (!h) return fail(HYDIST_ERR_ARG, "null handle");
   if (nsteps < 0) return fail(HYDIST_ERR_ARG, "negative step count");
   CK(cudaSetDevice(h->device));
+  TRY(check_horizon(h, nsteps));
   for (int k = 0; k < nsteps; ++k) {
     const double t1 = h->t + 0.5 * h->c.dT;
     const double t2 = t1 + h->c.dT * 0.5;
@@ -399,7 +409,9 @@ int hydist_step_graph(HydistHandle* h, int32_t nsteps) {
   // re-captured when its arguments change; replay is used for the launch
   // overhead of the many small kernels of one step.
   if (!h) return fail(HYDIST_ERR_ARG, "null handle");
+  if (nsteps < 0) return fail(HYDIST_ERR_ARG, "negative step count");
   CK(cudaSetDevice(h->device));
+  TRY(check_horizon(h, nsteps));
   for (int k = 0; k < nsteps; ++k) {
     const double t1 = h->t + 0.5 * h->c.dT;
     const double t2 = t1 + h->c.dT * 0.5;

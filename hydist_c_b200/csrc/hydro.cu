@@ -78,7 +78,11 @@ __global__ void k_interp_fs_rows(State S, Coef c) {
   const int sign = which == 0 ? -1 : 1;
   if (S.tu[loc * W + j] > 0) {
     const double deltaX = (S.u[loc * W + j] + S.tu[loc * W + j]) * 0.25 * c.dT;
-    const int i = (int)(offset + sign * (deltaX / c.dX));
+    const double fi = offset + sign * (deltaX / c.dX);
+    // a source row outside the mesh (reachable only once the state is no
+    // longer finite) is skipped, never read
+    if (!(fi > -1.0 && fi < (double)(S.H - 1))) return;
+    const int i = (int)fi;
     const int i_deltaX = __double2int_rn(deltaX);
     const int i_dX = __double2int_rn(c.dX);
     S.FS[loc * W + j] = S.FS[i * W + j] +
@@ -94,7 +98,9 @@ __global__ void k_interp_fs_col(State S, Coef c) {
   const int W = S.W, loc = S.M, offset = S.M - 1, sign = -1;
   if (S.tv[i * W + loc] > 0) {
     const double deltaY = (S.v[i * W + loc] + S.tv[i * W + loc]) * 0.25 * c.dT;
-    const int j = (int)(offset + sign * (deltaY / c.dY));
+    const double fj = offset + sign * (deltaY / c.dY);
+    if (!(fj > -1.0 && fj < (double)(W - 1))) return;
+    const int j = (int)fj;
     const int j_deltaY = __double2int_rn(deltaY);
     const int j_dY = __double2int_rn(c.dY);
     S.FS[i * W + loc] = S.FS[i * W + j + 1] +
@@ -226,7 +232,8 @@ __global__ void k_boundary(State S, float tf) {
   const int M = S.M, N = S.N, W = S.W;
   if (i > M && i > N) return;
   const double t = (double)tf;
-  const int t1 = (int)(t / 3600);
+  // the host refuses steps past the series; the clamp keeps reads in bounds
+  const int t1 = min(max((int)(t / 3600), 0), S.T - 2);
   const double t2h = (t - (double)(3600.0f * (float)t1)) / 3600.0f;
   const double t2f = (t - (3600.0 * t1)) / 3600.0;
   const double* hi_up = S.hi;

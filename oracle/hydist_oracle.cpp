@@ -252,7 +252,11 @@ struct Sim {
     for (int j = 1; j < M; ++j) {
       if (tu[id(loc, j)] > 0) {
         const double deltaX = (u[id(loc, j)] + tu[id(loc, j)]) * 0.25 * dT;
-        const int i = (int)(offset + sign * (deltaX / dX));
+        const double fi = offset + sign * (deltaX / dX);
+        // a source row outside the mesh (only reachable once the state is
+        // no longer finite) is skipped instead of read out of bounds
+        if (!(fi > -1.0 && fi < (double)(H - 1))) continue;
+        const int i = (int)fi;
         const int i_deltaX = (int)std::nearbyint(deltaX);
         const int i_dX = (int)std::nearbyint(dX);
         FS[id(loc, j)] = FS[id(i, j)] + sign * (FS[id(i + 1, j)] - FS[id(i, j)]) *
@@ -263,10 +267,12 @@ struct Sim {
   // Interpolate_FS_d, support_funcs.cpp:215-237 (loops rows to M, :227).
   void interpolate_fs_d(int loc, int offset, int sign) {
     const double dT = c.dT, dY = c.dY;
-    for (int i = 1; i < M; ++i) {
+    for (int i = 1; i < M && i < H; ++i) {
       if (tv[id(i, loc)] > 0) {
         const double deltaY = (v[id(i, loc)] + tv[id(i, loc)]) * 0.25 * dT;
-        const int j = (int)(offset + sign * (deltaY / dY));
+        const double fj = offset + sign * (deltaY / dY);
+        if (!(fj > -1.0 && fj < (double)(W - 1))) continue;
+        const int j = (int)fj;
         const int j_deltaY = (int)std::nearbyint(deltaY);
         const int j_dY = (int)std::nearbyint(dY);
         FS[id(i, loc)] = FS[id(i, j + 1)] +

@@ -65,8 +65,8 @@ def test_oracle_matches_reference_run(oracle_mod, case):
     done = 0
     s = meta["stride"]
     for st in meta["steps"]:
-        if st > 300 and case != "channel":
-            break
+        if st > 300 and case == "luy":
+            break  # the 600-step river check is in the slow test below
         o.step(st - done)
         done = st
         assert o.t == pytest.approx(float(z[f"t_{st}"]))
@@ -75,9 +75,9 @@ def test_oracle_matches_reference_run(oracle_mod, case):
             a = o.get(f)[::s, ::s]
             r = z[f"{f}_{st}"]
             scale = max(np.abs(r).max(), 1e-300)
-            # FMA contraction on the GPU vs none in the oracle: rounding-level
-            # differences that grow slowly with the step count
-            tol = (1e-10 if st <= 100 else 1e-7) * scale
+            # the reference's GPU build fuses multiply-adds, the oracle does
+            # not: rounding-level differences (measured <= 1e-12 relative)
+            tol = 1e-11 * scale
             assert np.abs(a - r).max() <= tol, (case, st, f, np.abs(a - r).max(), scale)
 
 
