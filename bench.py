@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark of the Hydist ADI time step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64|fp32] [--workload sediment-2048x1024|channel-256x128]
+
+A step is one full ADI step (two half-steps, with the concentration sweeps)
+of the 2048x1024 sediment workload: dx=dy=5 m, dt=2 s, seeded synthetic
+bathymetry, sediment from t=600 s. The state is spun up to t=600 s before
+timing so that every timed step runs the sediment sweeps. value is
+cell-steps/s (N*M interior cells x steps / device seconds), whole job.
+
+Multi-GPU: scenarios are independent, so N GPUs run N replicas with no
+data-path collective (weak scaling); the time is the max over ranks.
+
+--impl reference times the reference's CPU path: the reference has none
+(every computation is a CUDA kernel), so the FP64 CPU restatement of its
+time step runs with all host threads, on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BYTES_PER_CELL_STEP = {  # algorithmic bytes per interior cell and full step
+    ("fp64", False): 168, ("fp64", True): 232, ("fp32", False): 112, ("fp32", True): 152}
+# algorithmic bytes per interior cell of one x-sweep launch (FP64): reads
+# u, v, z, h, Kx1, visco (6 x 8 B) and the wet/dry mask (4 B), writes the
+# provisional u and z (2 x 8 B)
+SWEEP_BYTES_PER_CELL = {"fp64": 68, "fp32": 40}
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(name: str):
+    from hydist_c_b200 import scenario as S
+    if name == "sediment-2048x1024":
+        return S.config1(), 300  # spin-up steps to t = 600 s (sediment on)
+    if name == "channel-256x128":
+        return S.config0(), 0
+    raise SystemExit(f"unknown workload {name}")
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        rank = int(os.environ["RANK"])
+        local = int(os.environ.get("LOCAL_RANK", rank))
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        return rank, local, ws
+    return 0, 0, 1
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(bundle, steps: int, threads: int):
+    """The FP64 CPU oracle on the host cores, on the same workload with the
+    sediment sweeps on from t = 0 (so each step does the timed work)."""
+    from oracle import oracle as O
+    b = dict(bundle)
+    b["options"] = dict(bundle["options"], sediment_start=0.0, bed_change_start=0.0)
+    o = O.OracleSim(b, nthreads=threads)
+    o.step(1)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    cells = bundle["meta"]["cells"]
+    return cells * steps / dt, dt
+
+
+def run_reference(args):
+    rank, local, ws = dist_init()
+    if rank != 0:
+        return
+    bundle, _ = workload(args.workload)
+    threads = os.cpu_count() or 1
+    cells = bundle["meta"]["cells"]
+    from oracle import oracle as O
+    b = dict(bundle)
+    b["options"] = dict(bundle["options"], sediment_start=0.0, bed_change_start=0.0)
+    o = O.OracleSim(b, nthreads=threads)
+    o.step(max(args.warmup, 1))
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        o.step(1)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    v = cells * args.steps / total
+    line = {
+        "metric": "ADI cell-steps/s", "value": v, "unit": "cell-steps/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "cells": cells},
+        "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full steps of the {args.workload} workload, "
+                                   "sediment sweeps on, FP64 CPU restatement of the reference "
+                                   "time step (the reference has no CPU path), OpenMP over lines"},
+        "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import hydist_c_b200 as H
+    rank, local, ws = dist_init()
+    dev = local
+    torch.cuda.set_device(dev)
+    prec = H.FP64 if args.precision == "fp64" else H.FP32_REFINE
+    bundle, spin = workload(args.workload)
+    cells = bundle["meta"]["cells"]
+    sim = H.Simulation(bundle, device=dev, precision=prec)
+    sed = bundle["options"]["sediment_start"] < 1e11
+    # spin-up to the sediment phase (untimed), then warm-up steps
+    if spin:
+        sim.step(spin)
+    sim.step(max(args.warmup, 3) if args.warmup >= 0 else 3)
+    sim.sync()
+    # per-phase device times of one step (tracing), for the roofline
+    phases = sim.step_traced()
+    l0 = sim.kernel_launches
+    stream = torch.cuda.ExternalStream(sim.stream, device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    step_ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    clocks = ClockSampler(torch.cuda.current_device() if ws == 1 else local)
+    barrier(ws)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    e0.record(stream)
+    step_ev[0].record(stream)
+    for k in range(args.steps):
+        if args.graph:
+            sim.step_graph(1)
+        else:
+            sim.step(1)
+        step_ev[k + 1].record(stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    clk = clocks.stop()
+    sim.sync()
+    ms = e0.elapsed_time(e1)
+    launches = sim.kernel_launches - l0
+    per_step = [step_ev[k].elapsed_time(step_ev[k + 1]) for k in range(args.steps)]
+    ms_max = max_over_ranks(ms, ws)
+    value = ws * cells * args.steps / (ms_max * 1e-3)
+    # dominant kernel: the longest phase of the traced step
+    hbm, peak_kind = _peaks()
+    dom = max(phases, key=phases.get)
+    if dom.startswith("sweep"):
+        alg_bytes = SWEEP_BYTES_PER_CELL[args.precision] * cells
+    else:
+        alg_bytes = None
+    step_bytes = BYTES_PER_CELL_STEP[(args.precision, sed)] * cells
+    step_ms = ms / args.steps
+    roof = {"bound": "hbm", "kernel": dom, "phase_ms": round(phases[dom], 4),
+            "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None, "traffic": None,
+            "peak_source": peak_kind,
+            "step_achieved": step_bytes / (step_ms * 1e-3) / 1e9,
+            "step_frac": step_bytes / (step_ms * 1e-3) / 1e9 / hbm}
+    if alg_bytes is not None:
+        ach = alg_bytes / (phases[dom] * 1e-3) / 1e9
+        roof.update(achieved=ach, frac=ach / hbm)
+    traffic_file = ROOT / "profiles" / "traffic.json"
+    if traffic_file.exists():
+        try:
+            tj = json.loads(traffic_file.read_text())
+            roof["traffic"] = tj.get(args.workload, {}).get(dom)
+        except Exception:
+            pass
+    e2e = measure_e2e(H, bundle, dev, prec, args) if rank == 0 and not args.no_e2e else None
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        csteps = args.cpu_steps
+        v_cpu, t_cpu = cpu_baseline(bundle, csteps, threads)
+        cpu = {"value": v_cpu, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+               "sample": f"{csteps} full steps of the {args.workload} workload with the "
+                         f"sediment sweeps on ({t_cpu:.1f} s), FP64 CPU restatement, OpenMP "
+                         "over lines"}
+    if rank == 0:
+        line = {
+            "metric": "ADI cell-steps/s", "value": value, "unit": "cell-steps/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64-refine",
+            "data": "synthetic (seeded bathymetry, Manning, boundaries)",
+            "config": {"workload": args.workload, "N": bundle["meta"]["N"],
+                       "M": bundle["meta"]["M"], "cells": cells, "dx": 5.0, "dt": 2.0,
+                       "sediment": sed, "precision": args.precision,
+                       "cuda_graph": bool(args.graph),
+                       "l2": "inputs larger than L2 (state of ~30 fields of 16.9 MB)",
+                       "parallelism": f"replicas x{ws}"},
+            "p50_step_ms": float(np.percentile(per_step, 50)),
+            "p99_step_ms": float(np.percentile(per_step, 99)),
+            "phases_ms": {k: round(v, 4) for k, v in phases.items()},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def measure_e2e(H, bundle, dev, prec, args):
+    """The same metric through the public API from host buffers: create the
+    scenario from pinned host arrays (H2D of every input), run the timed
+    steps with the sediment sweeps on from the first step (the same work per
+    step as the device-timed region) and a device->host read of the water
+    volume (mass) after each, then download u, v, z, FS."""
+    import torch
+    sc = bundle["scenario"]
+    pinned = {}
+    for k, v in sc.items():
+        if isinstance(v, np.ndarray) and v.dtype == np.float64:
+            t = torch.from_numpy(np.ascontiguousarray(v)).pin_memory()
+            pinned[k] = t.numpy()
+    b = dict(bundle)
+    b["scenario"] = dict(sc, **pinned)
+    sed = bundle["options"]["sediment_start"] < 1e11
+    if sed:
+        b["options"] = dict(bundle["options"], sediment_start=0.0, bed_change_start=0.0)
+    h2d = sum(a.nbytes for a in pinned.values())
+    n = (sc["N"] + 3) * (sc["M"] + 3)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    sim = H.Simulation(b, device=dev, precision=prec)
+    for _ in range(args.steps):
+        sim.step(1)
+        sim.mass()
+    outs = [sim.download(f) for f in ("u", "v", "z", "FS")]
+    dt = time.perf_counter() - t0
+    sim.close()
+    steps = args.steps
+    cells = bundle["meta"]["cells"]
+    return {"value": cells * steps / dt, "unit": "cell-steps/s",
+            "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": (8 * args.steps + 4 * 8 * n) / steps,
+            "wall_s": dt, "steps": steps}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--workload", default="sediment-2048x1024")
+    ap.add_argument("--graph", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=4)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -96,6 +96,19 @@ class Simulation:
     def sync(self):
         capi.check(self._lib, self._lib.hydist_sync(self._h), "hydist_sync")
 
+    def step_traced(self) -> dict:
+        """One full step with per-phase device times (ms)."""
+        ms = (C.c_float * len(capi.PHASES))()
+        capi.check(self._lib, self._lib.hydist_step_traced(self._h, ms), "hydist_step_traced")
+        return dict(zip(capi.PHASES, [float(x) for x in ms]))
+
+    @property
+    def kernel_launches(self) -> int:
+        v = C.c_int64()
+        capi.check(self._lib, self._lib.hydist_kernel_launches(self._h, C.byref(v)),
+                   "hydist_kernel_launches")
+        return int(v.value)
+
     @property
     def t(self) -> float:
         v = C.c_double()

@@ -177,6 +177,8 @@ def _declare(lib):
     lib.hydist_mass.argtypes = [vp, _dp]
     lib.hydist_stream.argtypes = [vp]
     lib.hydist_stream.restype = vp
+    lib.hydist_step_traced.argtypes = [vp, C.POINTER(C.c_float)]
+    lib.hydist_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
     lib.hydist_gtsv_batched.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32,
                                         C.c_int32, vp]
 
@@ -196,5 +198,9 @@ EXPORTED_SYMBOLS = [
     "hydist_params_default", "hydist_options_default", "hydist_bienq_from_boundary_type",
     "hydist_last_error", "hydist_version", "hydist_create", "hydist_destroy", "hydist_step",
     "hydist_sync", "hydist_get_time", "hydist_set_time", "hydist_download", "hydist_upload", "hydist_mass",
-    "hydist_step_graph", "hydist_stream", "hydist_gtsv_batched",
+    "hydist_step_graph", "hydist_stream", "hydist_gtsv_batched", "hydist_step_traced",
+    "hydist_kernel_launches",
 ]
+
+PHASES = ["boundary_x", "sweep_x", "explicit_v", "commit_x", "sediment_x",
+          "boundary_y", "sweep_y", "explicit_u", "commit_y", "sediment_y"]

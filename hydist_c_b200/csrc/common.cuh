@@ -58,4 +58,30 @@ struct State {
 
 __host__ __device__ inline int cdiv(int a, int b) { return (a + b - 1) / b; }
 
+// Phases of one full step, in launch order (engine.cpp:65-295).
+enum Phase {
+  PH_BOUNDARY_X = 0,  // Update_Boundary_Value, first half
+  PH_SWEEP_X,         // x sweep: assembly + tridiagonal solve + extraction
+  PH_EXPLICIT_V,      // smoothing of u, explicit v, margins, smoothing of v
+  PH_COMMIT_X,        // H_moi, commit, segment tables, total depths
+  PH_SEDIMENT_X,      // speed, diffusivity, concentration i-sweep, commit
+  PH_BOUNDARY_Y,
+  PH_SWEEP_Y,
+  PH_EXPLICIT_U,
+  PH_COMMIT_Y,        // + wetting/drying
+  PH_SEDIMENT_Y,
+  PH_COUNT
+};
+
+// Launch bookkeeping: counts kernels and, when events are given, records
+// an event at the end of each phase (the tracing of hydist_step_traced).
+struct Trace {
+  cudaEvent_t* ev = nullptr;  // PH_COUNT + 1 events; ev[0] = step start
+  long long launches = 0;
+  void mark(cudaStream_t st, int phase, int nkernels) {
+    launches += nkernels;
+    if (ev) cudaEventRecord(ev[phase + 1], st);
+  }
+};
+
 }  // namespace hyd

@@ -99,7 +99,8 @@ struct HydistHandle {
   double* mass_part = nullptr;  // per-block partial sums
   int mass_blocks = 0;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [0] hydraulics only, [1] with sediment
-  bool graph_sed_x[2] = {false, false};
+  Trace trace;                                    // kernel launch counter
+  cudaEvent_t ev[PH_COUNT + 1] = {};
 };
 
 namespace {
@@ -138,13 +139,15 @@ int check_horizon(HydistHandle* h, int nsteps) {
 }
 
 // one full step (engine.cpp:65-295)
-void enqueue_step(HydistHandle* h, double t0, bool sed_x, bool sed_y) {
+void enqueue_step(HydistHandle* h, double t0, bool sed_x, bool sed_y, Trace* tr) {
   const double t1 = t0 + 0.5 * h->c.dT;
-  launch_half_x(h->S, h->c, t1, h->stream);
-  if (sed_x) launch_sediment(h->S, h->c, t1, h->o.bed_change_start, true, h->stream);
+  launch_half_x(h->S, h->c, t1, h->stream, tr);
+  if (sed_x) launch_sediment(h->S, h->c, t1, h->o.bed_change_start, true, h->stream, tr);
+  else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_X + 1], h->stream);
   const double t2 = t1 + h->c.dT * 0.5;
-  launch_half_y(h->S, h->c, t2, h->stream);
-  if (sed_y) launch_sediment(h->S, h->c, t2, h->o.bed_change_start, false, h->stream);
+  launch_half_y(h->S, h->c, t2, h->stream, tr);
+  if (sed_y) launch_sediment(h->S, h->c, t2, h->o.bed_change_start, false, h->stream, tr);
+  else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_Y + 1], h->stream);
 }
 
 __global__ void k_mass_partial(State S, double* part) {
@@ -383,6 +386,8 @@ int hydist_destroy(HydistHandle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (auto& g : h->graph)
     if (g) cudaGraphExecDestroy(g);
+  for (auto& e : h->ev)
+    if (e) cudaEventDestroy(e);
   for (void* p : h->allocs) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -397,10 +402,40 @@ int hydist_step(HydistHandle* h, int32_t nsteps) {
   for (int k = 0; k < nsteps; ++k) {
     const double t1 = h->t + 0.5 * h->c.dT;
     const double t2 = t1 + h->c.dT * 0.5;
-    enqueue_step(h, h->t, t1 >= h->o.sediment_start, t2 >= h->o.sediment_start);
+    enqueue_step(h, h->t, t1 >= h->o.sediment_start, t2 >= h->o.sediment_start, &h->trace);
     h->t = t2;
   }
   CK(cudaGetLastError());
+  return HYDIST_OK;
+}
+
+int hydist_step_traced(HydistHandle* h, float* phase_ms) {
+  if (!h || !phase_ms) return fail(HYDIST_ERR_ARG, "null argument");
+  CK(cudaSetDevice(h->device));
+  TRY(check_horizon(h, 1));
+  if (!h->ev[0])
+    for (auto& e : h->ev) CK(cudaEventCreate(&e));
+  Trace tr;
+  tr.ev = h->ev;
+  const double t1 = h->t + 0.5 * h->c.dT;
+  const double t2 = t1 + h->c.dT * 0.5;
+  CK(cudaEventRecord(h->ev[0], h->stream));
+  enqueue_step(h, h->t, t1 >= h->o.sediment_start, t2 >= h->o.sediment_start, &tr);
+  h->trace.launches += tr.launches;
+  h->t = t2;
+  CK(cudaGetLastError());
+  CK(cudaEventSynchronize(h->ev[PH_COUNT]));
+  for (int p = 0; p < PH_COUNT; ++p) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h->ev[p], h->ev[p + 1]));
+    phase_ms[p] = ms;
+  }
+  return HYDIST_OK;
+}
+
+int hydist_kernel_launches(HydistHandle* h, int64_t* count) {
+  if (!h || !count) return fail(HYDIST_ERR_ARG, "null argument");
+  *count = h->trace.launches;
   return HYDIST_OK;
 }
 
@@ -417,9 +452,11 @@ int hydist_step_graph(HydistHandle* h, int32_t nsteps) {
     const double t2 = t1 + h->c.dT * 0.5;
     const bool sx = t1 >= h->o.sediment_start, sy = t2 >= h->o.sediment_start;
     cudaGraph_t g = nullptr;
+    Trace tr;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(h, h->t, sx, sy);
+    enqueue_step(h, h->t, sx, sy, &tr);
     CK(cudaStreamEndCapture(h->stream, &g));
+    h->trace.launches += tr.launches;
     cudaGraphExec_t& ex = h->graph[sx || sy ? 1 : 0];
     if (ex) {
       cudaGraphExecUpdateResultInfo info;

@@ -994,7 +994,7 @@ static inline dim3 grid2(int nx, int ny, int bx) { return dim3(cdiv(nx, bx), ny)
 
 void launch_init(const State& S, const Coef& c, cudaStream_t st) {
   k_onetime_init<<<dim3(cdiv(S.W, 128), S.H), 128, 0, st>>>(S, c);
-  launch_find_limits(S, c, st);
+  launch_find_limits(S, c, st, nullptr);
   k_htuongdoi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
   k_preprocess<<<1, 32, 0, st>>>(S, c);
 }
@@ -1004,42 +1004,51 @@ void launch_scan_segments(const State& S, cudaStream_t st) {
   k_scan_cols<<<cdiv(S.M, 128), 128, 0, st>>>(S);
 }
 
-void launch_find_limits(const State& S, const Coef& c, cudaStream_t st) {
+void launch_find_limits(const State& S, const Coef& c, cudaStream_t st, Trace* tr) {
   k_interp_fs_rows<<<dim3(cdiv(S.M, 128), 2), 128, 0, st>>>(S, c);
   k_scan_rows<<<cdiv(S.N, 128), 128, 0, st>>>(S);
   k_interp_fs_col<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
   k_scan_cols<<<cdiv(S.M, 128), 128, 0, st>>>(S);
+  if (tr) tr->launches += 4;
 }
 
-void launch_half_x(const State& S, const Coef& c, double t, cudaStream_t st) {
+void launch_half_x(const State& S, const Coef& c, double t, cudaStream_t st, Trace* tr) {
   k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, (float)t);
+  if (tr) tr->mark(st, PH_BOUNDARY_X, 1);
   k_sweep_x<<<cdiv(S.M - 1, 128), 128, 0, st>>>(S, c);
+  if (tr) tr->mark(st, PH_SWEEP_X, 1);
   k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 1);
   k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 1);
   k_solve_v<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c);
   k_margin_v<<<cdiv(S.N - 1, 128), 128, 0, st>>>(S, c);
   k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 0);
   k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 0);
+  if (tr) tr->mark(st, PH_EXPLICIT_V, 6);
   k_update_h_moi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
   k_update_uvz<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c);
-  launch_find_limits(S, c, st);
+  launch_find_limits(S, c, st, tr);
   k_htuongdoi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
+  if (tr) tr->mark(st, PH_COMMIT_X, 3);
 }
 
-void launch_half_y(const State& S, const Coef& c, double t, cudaStream_t st) {
+void launch_half_y(const State& S, const Coef& c, double t, cudaStream_t st, Trace* tr) {
   k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, (float)t);
+  if (tr) tr->mark(st, PH_BOUNDARY_Y, 1);
   k_sweep_y<<<cdiv(S.N - 1, 128), 128, 0, st>>>(S, c);
+  if (tr) tr->mark(st, PH_SWEEP_Y, 1);
   k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 0);
   k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 0);
   k_solve_u<<<grid2(S.M - 1, S.N, 128), 128, 0, st>>>(S, c);
   k_margin_u<<<cdiv(S.M - 1, 128), 128, 0, st>>>(S, c);
   k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 1);
   k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 1);
+  if (tr) tr->mark(st, PH_EXPLICIT_U, 6);
   k_update_h_moi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
   k_reset_vertical<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
   k_update_uvz<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c);
-  launch_find_limits(S, c, st);
+  launch_find_limits(S, c, st, tr);
   k_htuongdoi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
+  if (tr) tr->mark(st, PH_COMMIT_Y, 4);
 }
 
 }  // namespace hyd

@@ -261,7 +261,7 @@ __global__ void k_update_fs(State S) {
 }
 
 void launch_sediment(const State& S, const Coef& c, double t, double s_start, bool xdir,
-                     cudaStream_t st) {
+                     cudaStream_t st, Trace* tr) {
   // first half: Find_VTH/hesoK over rows to N; second half: to N-1
   // (launch shape of engine.cpp:259-260 never reaches row N)
   const int i_hi = xdir ? S.N : S.N - 1;
@@ -272,6 +272,7 @@ void launch_sediment(const State& S, const Coef& c, double t, double s_start, bo
   else
     k_fs_sweep_y<<<cdiv(S.N - 3, 128), 128, 0, st>>>(S, c, t, s_start);
   k_update_fs<<<dim3(cdiv(S.M, 128), S.N), 128, 0, st>>>(S);
+  if (tr) tr->mark(st, xdir ? PH_SEDIMENT_X : PH_SEDIMENT_Y, 4);
 }
 
 }  // namespace hyd

@@ -185,6 +185,17 @@ int hydist_step_graph(HydistHandle* h, int32_t nsteps);
 /* The CUDA stream the handle enqueues on (a cudaStream_t). */
 void* hydist_stream(HydistHandle* h);
 
+/* Tracing (the reference has none): run one full step with a CUDA event at
+ * the end of each phase and return the device time of each phase in ms, in
+ * the order boundary-x, sweep-x, explicit-v, commit-x, sediment-x,
+ * boundary-y, sweep-y, explicit-u, commit-y, sediment-y (HYDIST_PHASES
+ * entries). Synchronous. */
+#define HYDIST_PHASES 10
+int hydist_step_traced(HydistHandle* h, float* phase_ms);
+/* Number of kernels the handle has enqueued since creation (set-up
+ * excluded). */
+int hydist_kernel_launches(HydistHandle* h, int64_t* count);
+
 /* ---- batched tridiagonal solver --------------------------------------
  * Replaces tridiag() + tridiagSolver (UVZSolver_multithread.cpp:19-43,
  * 78-109) and gtsv_spike_partial_diag_pivot_v1 (gtsv.cpp:88-193) with one
