@@ -54,6 +54,10 @@ struct State {
   double* Bp;
   int ld;        // line stride of Ap/Bp (max(M,N)+3)
   int* err;      // [0]: DevErr
+  double* lscratch;  // partitioned line solver: one slot per resident CTA
+  int lslots;        // number of slots (CTAs of the persistent sweep grid)
+  int* colflag;      // per column: holds a cell dried during the run
+  double* clock;     // [0]: simulated time, advanced on the device by k_tick
 };
 
 __host__ __device__ inline int cdiv(int a, int b) { return (a + b - 1) / b; }

@@ -98,7 +98,9 @@ struct HydistHandle {
   std::vector<void*> allocs;
   double* mass_part = nullptr;  // per-block partial sums
   int mass_blocks = 0;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [0] hydraulics only, [1] with sediment
+  // one captured step per sediment phase: [sed_x*2 + sed_y]
+  cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+  long long graph_launches[4] = {0, 0, 0, 0};
   Trace trace;                                    // kernel launch counter
   cudaEvent_t ev[PH_COUNT + 1] = {};
 };
@@ -138,16 +140,21 @@ int check_horizon(HydistHandle* h, int nsteps) {
   return HYDIST_OK;
 }
 
-// one full step (engine.cpp:65-295)
-void enqueue_step(HydistHandle* h, double t0, bool sed_x, bool sed_y, Trace* tr) {
-  const double t1 = t0 + 0.5 * h->c.dT;
-  launch_half_x(h->S, h->c, t1, h->stream, tr);
-  if (sed_x) launch_sediment(h->S, h->c, t1, h->o.bed_change_start, true, h->stream, tr);
+// one full step (engine.cpp:65-295); the sediment gates (engine.cpp:149,
+// 258) are decided on the host, the time itself advances on the device
+void enqueue_step(HydistHandle* h, bool sed_x, bool sed_y, Trace* tr) {
+  launch_half_x(h->S, h->c, h->stream, tr);
+  if (sed_x) launch_sediment(h->S, h->c, h->o.bed_change_start, true, h->stream, tr);
   else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_X + 1], h->stream);
-  const double t2 = t1 + h->c.dT * 0.5;
-  launch_half_y(h->S, h->c, t2, h->stream, tr);
-  if (sed_y) launch_sediment(h->S, h->c, t2, h->o.bed_change_start, false, h->stream, tr);
+  launch_half_y(h->S, h->c, h->stream, tr);
+  if (sed_y) launch_sediment(h->S, h->c, h->o.bed_change_start, false, h->stream, tr);
   else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_Y + 1], h->stream);
+}
+
+int set_device_clock(HydistHandle* h) {
+  CK(cudaMemcpyAsync(h->S.clock, &h->t, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return HYDIST_OK;
 }
 
 __global__ void k_mass_partial(State S, double* part) {
@@ -365,6 +372,18 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistO
     TRY(dalloc(h, &S.Ap, nunk * S.ld));
     TRY(dalloc(h, &S.Bp, nunk * S.ld));
     TRY(dalloc(h, &S.err, 4));
+    TRY(dalloc(h, &S.colflag, S.W));
+    TRY(dalloc(h, &S.clock, 4));
+    TRY(set_device_clock(h));
+    // partitioned line solver scratch: 3 doubles per unknown, 4 lines per
+    // slot, one slot per CTA of the persistent sweep grid
+    {
+      int nsm = 0;
+      CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+      S.lslots = 2 * nsm;
+      const size_t U = (size_t)2 * std::max(S.M, S.N);
+      TRY(dalloc(h, &S.lscratch, (size_t)S.lslots * 3 * U * 4));
+    }
     h->mass_blocks = 296;
     TRY(dalloc(h, &h->mass_part, h->mass_blocks + 1));
     launch_init(S, h->c, h->stream);
@@ -402,7 +421,7 @@ int hydist_step(HydistHandle* h, int32_t nsteps) {
   for (int k = 0; k < nsteps; ++k) {
     const double t1 = h->t + 0.5 * h->c.dT;
     const double t2 = t1 + h->c.dT * 0.5;
-    enqueue_step(h, h->t, t1 >= h->o.sediment_start, t2 >= h->o.sediment_start, &h->trace);
+    enqueue_step(h, t1 >= h->o.sediment_start, t2 >= h->o.sediment_start, &h->trace);
     h->t = t2;
   }
   CK(cudaGetLastError());
@@ -420,7 +439,7 @@ int hydist_step_traced(HydistHandle* h, float* phase_ms) {
   const double t1 = h->t + 0.5 * h->c.dT;
   const double t2 = t1 + h->c.dT * 0.5;
   CK(cudaEventRecord(h->ev[0], h->stream));
-  enqueue_step(h, h->t, t1 >= h->o.sediment_start, t2 >= h->o.sediment_start, &tr);
+  enqueue_step(h, t1 >= h->o.sediment_start, t2 >= h->o.sediment_start, &tr);
   h->trace.launches += tr.launches;
   h->t = t2;
   CK(cudaGetLastError());
@@ -440,9 +459,8 @@ int hydist_kernel_launches(HydistHandle* h, int64_t* count) {
 }
 
 int hydist_step_graph(HydistHandle* h, int32_t nsteps) {
-  // The time of each half-step is a kernel argument, so a captured step is
-  // re-captured when its arguments change; replay is used for the launch
-  // overhead of the many small kernels of one step.
+  // The time advances on the device, so the launches of a step are the same
+  // every step: one graph per sediment phase, captured on first use.
   if (!h) return fail(HYDIST_ERR_ARG, "null handle");
   if (nsteps < 0) return fail(HYDIST_ERR_ARG, "negative step count");
   CK(cudaSetDevice(h->device));
@@ -451,24 +469,21 @@ int hydist_step_graph(HydistHandle* h, int32_t nsteps) {
     const double t1 = h->t + 0.5 * h->c.dT;
     const double t2 = t1 + h->c.dT * 0.5;
     const bool sx = t1 >= h->o.sediment_start, sy = t2 >= h->o.sediment_start;
-    cudaGraph_t g = nullptr;
-    Trace tr;
-    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(h, h->t, sx, sy, &tr);
-    CK(cudaStreamEndCapture(h->stream, &g));
-    h->trace.launches += tr.launches;
-    cudaGraphExec_t& ex = h->graph[sx || sy ? 1 : 0];
-    if (ex) {
-      cudaGraphExecUpdateResultInfo info;
-      if (cudaGraphExecUpdate(ex, g, &info) != cudaSuccess) {
-        cudaGetLastError();
-        cudaGraphExecDestroy(ex);
-        ex = nullptr;
-      }
+    const int gi = (sx ? 2 : 0) + (sy ? 1 : 0);
+    cudaGraphExec_t& ex = h->graph[gi];
+    if (!ex) {
+      cudaGraph_t g = nullptr;
+      Trace tr;
+      CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      enqueue_step(h, sx, sy, &tr);
+      CK(cudaStreamEndCapture(h->stream, &g));
+      h->graph_launches[gi] = tr.launches;
+      const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      CK(e);
     }
-    if (!ex) CK(cudaGraphInstantiate(&ex, g, 0));
-    cudaGraphDestroy(g);
     CK(cudaGraphLaunch(ex, h->stream));
+    h->trace.launches += h->graph_launches[gi];
     h->t = t2;
   }
   return HYDIST_OK;
@@ -489,8 +504,9 @@ int hydist_get_time(HydistHandle* h, double* t) {
 
 int hydist_set_time(HydistHandle* h, double t) {
   if (!h) return fail(HYDIST_ERR_ARG, "null handle");
+  CK(cudaSetDevice(h->device));
   h->t = t;
-  return HYDIST_OK;
+  return set_device_clock(h);
 }
 
 int hydist_download(HydistHandle* h, int32_t field, void* host) {

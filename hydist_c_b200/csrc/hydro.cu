@@ -25,6 +25,7 @@
 // does not, so results agree to rounding, not bit for bit.
 #include <cstdio>
 
+#include "assembly.cuh"
 #include "common.cuh"
 #include "hydro.cuh"
 
@@ -225,13 +226,17 @@ __global__ void k_preprocess(State S, Coef c) {
 }
 
 // ------------------------------------------------------------- boundary
+// The simulated time lives on the device so that a captured step replays
+// unchanged: advanced by t += dT/2 per half-step (engine.cpp:66, 176).
+__global__ void k_tick(State S, double half) { S.clock[0] += half; }
+
 // Update_Boundary_Value (support_funcs.cpp:682-728). t arrives through a
-// float parameter in the reference (engine.cpp:22), hence tf.
-__global__ void k_boundary(State S, float tf) {
+// float parameter in the reference (engine.cpp:22), hence the rounding.
+__global__ void k_boundary(State S) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int M = S.M, N = S.N, W = S.W;
   if (i > M && i > N) return;
-  const double t = (double)tf;
+  const double t = (double)(float)S.clock[0];
   // the host refuses steps past the series; the clamp keeps reads in bounds
   const int t1 = min(max((int)(t / 3600), 0), S.T - 2);
   const double t2h = (t - (double)(3600.0f * (float)t1)) / 3600.0f;
@@ -277,224 +282,7 @@ __global__ void k_boundary(State S, float tf) {
 }
 
 // ---------------------------------------------------- ADI line sweeps
-// Per-cell coefficients of the preindex step.
-struct Pre {
-  double f1, f2, f3, f5, a2, c2, d2;
-};
-
-// _uzSolver_calculate_preindex (UVZSolver_multithread.cpp:210-278).
-__device__ __forceinline__ Pre pre_x(const State& S, const Coef& c, int i, int j) {
-  const int w = S.W;
-  const double* u = S.u;
-  const double* v = S.v;
-  const double* Hm = S.Hmoi;
-  Pre P;
-  double p = 0.0, q = 0.0;
-  const double vtb =
-      (v[i * w + j - 1] + v[i * w + j] + v[(i + 1) * w + j - 1] + v[(i + 1) * w + j]) * 0.25;
-  const double uu = u[i * w + j], VI = S.visco[i * w + j], Hu = S.Htdu[i * w + j];
-  const double dT = c.dT;
-  P.f1 = c.dTchia2dX * uu + VI * dT / c.dXbp;
-  P.f2 = -(2 + S.Kx1[i * w + j] * dT * sqrt(uu * uu + vtb * vtb) / Hu + (2 * dT * VI) / c.dXbp);
-  P.f3 = dT * VI / c.dXbp - c.dTchia2dX * uu;
-  if (Hm[i * w + j - 1] <= c.H_TINH) {
-    if (vtb < 0) {
-      p = vtb * (-3 * uu + 4 * u[i * w + j + 1] - u[i * w + j + 2]) / c.dY2;
-      q = (uu - 2 * u[i * w + j + 1] + u[i * w + j + 2]) / c.dYbp;
-    }
-  } else {
-    if (Hm[i * w + j + 1] <= c.H_TINH) {
-      if ((Hm[i * w + j - 2] > c.H_TINH) && (vtb > 0)) {
-        p = vtb * (3 * uu - 4 * u[i * w + j - 1] + u[i * w + j - 2]) / c.dY2;
-        q = (uu - 2 * u[i * w + j - 1] + u[i * w + j - 2]) / c.dYbp;
-      }
-    } else {
-      p = vtb * (u[i * w + j + 1] - u[i * w + j - 1]) / c.dY2;
-      q = (u[i * w + j + 1] - 2 * uu + u[i * w + j - 1]) / c.dYbp;
-    }
-  }
-  P.f5 = -2 * uu + dT * p - dT * c.CORIOLIS_FORCE * vtb - dT * VI * q -
-         dT * (c.Windx - S.Tsxw[i * w + j]) / Hu;
-  P.c2 = c.dTchia2dX * Hu;
-  P.a2 = -c.dTchia2dX * S.Htdu[(i - 1) * w + j];
-  P.d2 = S.z[i * w + j] -
-         c.dTchia2dY * (S.Htdv[i * w + j] * v[i * w + j] - S.Htdv[i * w + j - 1] * v[i * w + j - 1]);
-  return P;
-}
-
-// _vzSolver_calculate_preindex (UVZSolver_multithread.cpp:142-208).
-__device__ __forceinline__ Pre pre_y(const State& S, const Coef& c, int i, int j) {
-  const int w = S.W;
-  const double* u = S.u;
-  const double* v = S.v;
-  const double* Hm = S.Hmoi;
-  Pre P;
-  double p = 0.0, q = 0.0;
-  const double utb =
-      (u[(i - 1) * w + j] + u[i * w + j] + u[(i - 1) * w + j + 1] + u[i * w + j + 1]) * 0.25;
-  const double vv = v[i * w + j], VI = S.visco[i * w + j], Hv = S.Htdv[i * w + j];
-  const double dT = c.dT;
-  P.f1 = c.dTchia2dY * vv + VI * dT / c.dYbp;
-  P.f2 = -(2 + S.Ky1[i * w + j] * dT * sqrt(vv * vv + utb * utb) / Hv + (2 * dT * VI) / c.dYbp);
-  P.f3 = dT * VI / c.dYbp - c.dTchia2dY * vv;
-  if (Hm[(i - 1) * w + j] <= c.H_TINH) {
-    if (utb < 0) {
-      q = utb * (-3 * vv + 4 * v[(i + 1) * w + j] - v[(i + 2) * w + j]) / c.dX2;
-      p = (vv - 2 * v[(i + 1) * w + j] + v[(i + 2) * w + j]) / c.dXbp;
-    }
-  } else {
-    if (Hm[(i + 1) * w + j] <= c.H_TINH) {
-      if ((Hm[(i - 2) * w + j] > c.H_TINH) && (utb > 0)) {
-        q = utb * (3 * vv - 4 * v[(i - 1) * w + j] + v[(i - 2) * w + j]) / c.dX2;
-        p = (vv - 2 * v[(i - 1) * w + j] + v[(i - 2) * w + j]) / c.dXbp;
-      }
-    } else {
-      q = utb * (v[(i + 1) * w + j] - v[(i - 1) * w + j]) / c.dX2;
-      p = (v[(i + 1) * w + j] - 2 * vv + v[(i - 1) * w + j]) / c.dXbp;
-    }
-  }
-  P.f5 = -2 * vv + dT * q + dT * c.CORIOLIS_FORCE * utb - dT * VI * p -
-         dT * (c.Windy - S.Tsyw[i * w + j]) / Hv;
-  P.c2 = c.dTchia2dY * Hv;
-  P.a2 = -c.dTchia2dY * S.Htdv[i * w + j - 1];
-  P.d2 = S.z[i * w + j] -
-         c.dTchia2dX * (S.Htdu[i * w + j] * u[i * w + j] - S.Htdu[(i - 1) * w + j] * u[(i - 1) * w + j]);
-  return P;
-}
-
-struct Mom {
-  double a1, b1, c1, d1;
-};
-
-// _calculate_abcd (UVZSolver_multithread.cpp:280-342) at position k of a
-// segment [first, last]; P = cell k, Pn = cell k+1 (read only when used).
-__device__ __forceinline__ Mom abcd(const Pre& P, const Pre& Pn, int k, int first, int last,
-                                    double f4, bool br1, bool br2) {
-  Mom m;
-  if (last - 1 > first) {
-    if (br1 && k == first) {
-      m.a1 = f4;
-      m.b1 = P.f2 - (P.f3 * Pn.a2 / Pn.c2);
-      m.c1 = -f4 - (P.f3 / Pn.c2);
-      m.d1 = P.f5 - (P.f3 * Pn.d2 / Pn.c2);
-    } else if (br2 && k == last - 1) {
-      m.a1 = f4 - P.f1 / P.a2;
-      m.b1 = P.f2 - (P.f1 * P.c2 / P.a2);
-      m.c1 = -f4;
-      m.d1 = P.f5 - (P.f1 * P.d2 / P.a2);
-    } else {
-      m.a1 = f4 - P.f1 / P.a2;
-      m.c1 = -f4 - (P.f3 / Pn.c2);
-      m.b1 = P.f2 - (P.f1 * P.c2 / P.a2) - (P.f3 * Pn.a2 / Pn.c2);
-      m.d1 = P.f5 - (P.f1 * P.d2 / P.a2) - (P.f3 * Pn.d2 / Pn.c2);
-    }
-  } else {
-    m.a1 = f4;
-    m.b1 = P.f2;
-    m.d1 = P.f5;
-    m.c1 = -f4;
-  }
-  return m;
-}
-
-// Streaming Thomas forward pass (tridiag, UVZSolver_multithread.cpp:19-43):
-// rows arrive in order k = 0..sn; Ap/Bp go to scratch.
-struct ThomasFwd {
-  double ap, bp, xs;
-  int sn;
-  double* Ap;
-  double* Bp;
-  int ld;
-  __device__ __forceinline__ void row(int k, int r, double A, double B, double Cc, double D) {
-    if (k == 0) {
-      if (sn == 0) {
-        xs = D / B;
-        return;
-      }
-      ap = -Cc / B;
-      bp = D / B;
-      Ap[(size_t)r * ld] = ap;
-      Bp[(size_t)r * ld] = bp;
-    } else if (k < sn) {
-      const double ep = A * ap + B;
-      ap = -Cc / ep;
-      bp = (D - (A * bp)) / ep;
-      Ap[(size_t)r * ld] = ap;
-      Bp[(size_t)r * ld] = bp;
-    } else {
-      xs = (D - (A * bp)) / (B + (A * ap));
-    }
-  }
-};
-
-// Layout of one line's solve: which of the reference's assembly variants
-// applies (UVZSolver_multithread.cpp:377-465) and where the system ends.
-struct LineSys {
-  bool ran;      // continuity row first (solid or discharge first end)
-  bool qfirst;   // discharge at the first end
-  int last_kind; // 0 solid, 1 discharge, 2 water level
-  int off, sn;
-};
-
-__device__ __forceinline__ LineSys line_sys(int first, int last, bool br1, bool br2, bool q1,
-                                            bool q2, int dkfr) {
-  LineSys L;
-  L.off = 2 * first;
-  int sn = 2 * (last - first);
-  if (br1) {
-    L.ran = true;
-    L.qfirst = false;
-    if (!br2) {
-      if (q2 && last == dkfr) {
-        L.last_kind = 1;
-      } else {
-        sn--;
-        L.last_kind = 2;
-      }
-    } else {
-      L.last_kind = 0;
-    }
-  } else {
-    const bool isBienran = (q1 && first == 2);
-    L.ran = isBienran;
-    L.qfirst = isBienran;
-    if (!br2) {
-      if (q1 && last == dkfr) {  // the first end's flag (UVZSolver_multithread.cpp:438)
-        if (!isBienran) sn--;
-        L.last_kind = 1;
-      } else {
-        sn--;
-        if (!isBienran) sn -= 1;
-        L.last_kind = 2;
-      }
-    } else {
-      if (!isBienran) sn--;
-      L.last_kind = 0;
-    }
-  }
-  L.sn = sn;
-  return L;
-}
-
-// Coefficients of absolute row r of a line's system (see line_sys).
-__device__ __forceinline__ void row_of(const LineSys& L, int r, const Pre& Pi, const Mom& Mi,
-                                       const Pre& Pi1, double& A, double& B, double& Cc,
-                                       double& D) {
-  const bool even = (r & 1) == 0;
-  if (L.ran == even) {  // continuity row of cell i (ran) / cell i+1 (lon)
-    const Pre& P = L.ran ? Pi : Pi1;
-    A = P.a2;
-    B = 1;
-    Cc = P.c2;
-    D = P.d2;
-  } else {  // momentum row of cell i
-    A = Mi.a1;
-    B = Mi.b1;
-    Cc = Mi.c1;
-    D = Mi.d1;
-  }
-}
-
+// (per-cell assembly: assembly.cuh)
 // One column sweep (x direction, implicit in i) of column j. Assembly,
 // Thomas and extraction fused; the column's cells are visited in order of
 // i, so a warp of 32 adjacent columns reads 32 contiguous doubles per field.
@@ -989,6 +777,121 @@ __global__ void k_reset_vertical(State S, Coef c) {
   }
 }
 
+// ------------------------------------------------------ fused commits
+// Half-step A commit: update_h_moi (support_funcs.cpp:71-86) on [1,N]x[1,M],
+// update_uvz (:732-759) on [0,N]x[0,M] and Htuongdoi (:346-362) on
+// [1,N]x[1,M] in one pass. Htuongdoi reads the committed z of the
+// neighbour: t_z where it was committed, z where it never is (row N+1,
+// column M+1).
+__global__ void k_commit_a(State S, Coef c) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (i > S.N || j > S.M) return;
+  const int W = S.W, g = i * W + j;
+  const double tz = S.tz[g];
+  if (i >= 1 && j >= 1 && S.khouot[g] == 0) S.Hmoi[g] = S.htaiz[g] + tz;
+  S.z[g] = tz;
+  S.u[g] = S.tu[g] * (1 - c.kenhhepd);
+  S.v[g] = S.tv[g] * (1 - c.kenhhepng);
+  if (i >= 1 && j >= 1) {
+    const double zd = (i + 1 <= S.N) ? S.tz[g + W] : S.z[g + W];
+    const double zr = (j + 1 <= S.M) ? S.tz[g + 1] : S.z[g + 1];
+    S.Htdu[g] = (S.h[g - 1] + S.h[g] + zd + tz) * 0.5;
+    S.Htdv[g] = (S.h[g - W] + S.h[g] + zr + tz) * 0.5;
+  }
+}
+
+// Half-step B, before the wetting pass: update_h_moi, and a per-column flag
+// telling whether the column holds a cell dried during the run (khouot 1),
+// the only cells the wetting loop of Reset_states_vertical can change.
+__global__ void k_hmoi_flags(State S, int* colflag) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int i = blockIdx.y + 1;
+  if (i > S.N + 1 || j > S.M) return;
+  const int g = i * S.W + j;
+  const int kh = S.khouot[g];
+  if (i <= S.N && kh == 0) S.Hmoi[g] = S.htaiz[g] + S.tz[g];
+  if (kh == 1) colflag[j] = 1;
+}
+
+// The wetting loop of Reset_states_vertical (support_funcs.cpp:160-175),
+// sequential along i, on flagged columns only.
+__global__ void k_wetting(State S, Coef c, int* colflag) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (j > S.M) return;
+  if (!colflag[j]) return;
+  colflag[j] = 0;
+  const int off = S.W, N = S.N;
+  double* tz = S.tz;
+  double* Hm = S.Hmoi;
+  int* kh = S.khouot;
+  for (int i = 2; i <= N; ++i) {
+    if (tz[i * off + j] > S.z[i * off + j]) {
+      if (kh[(i - 1) * off + j] == 1) {
+        tz[(i - 1) * off + j] = tz[i * off + j];
+        Hm[(i - 1) * off + j] = S.htaiz[(i - 1) * off + j] + tz[i * off + j];
+        kh[(i - 1) * off + j] = 0;
+        S.FS[(i - 1) * off + j] = S.FS[i * off + j];
+      }
+      if (kh[(i + 1) * off + j] == 1) {
+        tz[(i + 1) * off + j] = tz[i * off + j];
+        Hm[(i + 1) * off + j] = S.htaiz[(i + 1) * off + j] + tz[i * off + j];
+        kh[(i + 1) * off + j] = 0;
+        S.FS[(i + 1) * off + j] = S.FS[i * off + j];
+      }
+    }
+  }
+}
+
+// Half-step B commit: the drying loop of Reset_states_vertical (:177-187,
+// independent per cell), update_uvz and Htuongdoi. A drying cell (i,j)
+// zeroes t_u at (i-1,j),(i,j) and t_v at (i,j-1),(i,j); each cell here reads
+// its own test and those of (i+1,j) and (i,j+1).
+__global__ void k_commit_b(State S, Coef c) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (i > S.N || j > S.M) return;
+  const int W = S.W, g = i * W + j;
+  auto dries = [&](int ii, int jj) -> bool {
+    if (ii < 2 || ii > S.N || jj < 1 || jj > S.M) return false;
+    const int q = ii * W + jj;
+    return S.khouot[q] == 0 && S.Hmoi[q] <= c.H_TINH;
+  };
+  const bool d0 = dries(i, j);
+  const bool ddown = dries(i + 1, j);
+  const bool dright = dries(i, j + 1);
+  double tu = S.tu[g], tv = S.tv[g];
+  if (d0 || ddown) {
+    tu = 0;
+    S.tu[g] = 0;
+  }
+  if (d0 || dright) {
+    tv = 0;
+    S.tv[g] = 0;
+  }
+  if (d0) S.FS[g] = 0;  // khouot is set by k_dry_mask after this pass
+  const double tz = S.tz[g];
+  S.z[g] = tz;
+  S.u[g] = tu * (1 - c.kenhhepd);
+  S.v[g] = tv * (1 - c.kenhhepng);
+  if (i >= 1 && j >= 1) {
+    const double zd = (i + 1 <= S.N) ? S.tz[g + W] : S.z[g + W];
+    const double zr = (j + 1 <= S.M) ? S.tz[g + 1] : S.z[g + 1];
+    S.Htdu[g] = (S.h[g - 1] + S.h[g] + zd + tz) * 0.5;
+    S.Htdv[g] = (S.h[g - W] + S.h[g] + zr + tz) * 0.5;
+  }
+}
+
+// The drying cells' mask (khouot = 1), written after k_commit_b has read
+// every neighbour's test.
+__global__ void k_dry_mask(State S, Coef c) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int i = blockIdx.y + 2;
+  if (i > S.N || j > S.M) return;
+  const int g = i * S.W + j;
+  if (S.khouot[g] == 0 && S.Hmoi[g] <= c.H_TINH) S.khouot[g] = 1;
+}
+
 // ------------------------------------------------------------- launchers
 static inline dim3 grid2(int nx, int ny, int bx) { return dim3(cdiv(nx, bx), ny); }
 
@@ -1012,10 +915,11 @@ void launch_find_limits(const State& S, const Coef& c, cudaStream_t st, Trace* t
   if (tr) tr->launches += 4;
 }
 
-void launch_half_x(const State& S, const Coef& c, double t, cudaStream_t st, Trace* tr) {
-  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, (float)t);
-  if (tr) tr->mark(st, PH_BOUNDARY_X, 1);
-  k_sweep_x<<<cdiv(S.M - 1, 128), 128, 0, st>>>(S, c);
+void launch_half_x(const State& S, const Coef& c, cudaStream_t st, Trace* tr) {
+  k_tick<<<1, 1, 0, st>>>(S, 0.5 * c.dT);
+  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
+  if (tr) tr->mark(st, PH_BOUNDARY_X, 2);
+  launch_sweep(S, c, 0, st);
   if (tr) tr->mark(st, PH_SWEEP_X, 1);
   k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 1);
   k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 1);
@@ -1024,17 +928,20 @@ void launch_half_x(const State& S, const Coef& c, double t, cudaStream_t st, Tra
   k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 0);
   k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 0);
   if (tr) tr->mark(st, PH_EXPLICIT_V, 6);
-  k_update_h_moi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
-  k_update_uvz<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c);
-  launch_find_limits(S, c, st, tr);
-  k_htuongdoi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
+  // update_h_moi + update_uvz + Htuongdoi; the wet/dry mask does not change
+  // in this half-step, so the segment tables are not rescanned, only the
+  // boundary concentration is interpolated (support_funcs.cpp:255-258, 311)
+  k_commit_a<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c);
+  k_interp_fs_rows<<<dim3(cdiv(S.M, 128), 2), 128, 0, st>>>(S, c);
+  k_interp_fs_col<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
   if (tr) tr->mark(st, PH_COMMIT_X, 3);
 }
 
-void launch_half_y(const State& S, const Coef& c, double t, cudaStream_t st, Trace* tr) {
-  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, (float)t);
-  if (tr) tr->mark(st, PH_BOUNDARY_Y, 1);
-  k_sweep_y<<<cdiv(S.N - 1, 128), 128, 0, st>>>(S, c);
+void launch_half_y(const State& S, const Coef& c, cudaStream_t st, Trace* tr) {
+  k_tick<<<1, 1, 0, st>>>(S, c.dT * 0.5);
+  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
+  if (tr) tr->mark(st, PH_BOUNDARY_Y, 2);
+  launch_sweep(S, c, 1, st);
   if (tr) tr->mark(st, PH_SWEEP_Y, 1);
   k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 0);
   k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 0);
@@ -1043,11 +950,13 @@ void launch_half_y(const State& S, const Coef& c, double t, cudaStream_t st, Tra
   k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 1);
   k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 1);
   if (tr) tr->mark(st, PH_EXPLICIT_U, 6);
-  k_update_h_moi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
-  k_reset_vertical<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
-  k_update_uvz<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c);
+  // update_h_moi, Reset_states_vertical (wetting on flagged columns, drying
+  // per cell), update_uvz, Htuongdoi, then the segment tables
+  k_hmoi_flags<<<grid2(S.M, S.N + 1, 128), 128, 0, st>>>(S, S.colflag);
+  k_wetting<<<cdiv(S.M, 128), 128, 0, st>>>(S, c, S.colflag);
+  k_commit_b<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c);
+  k_dry_mask<<<grid2(S.M, S.N - 1, 128), 128, 0, st>>>(S, c);
   launch_find_limits(S, c, st, tr);
-  k_htuongdoi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
   if (tr) tr->mark(st, PH_COMMIT_Y, 4);
 }
 

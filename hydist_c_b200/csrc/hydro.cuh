@@ -1,4 +1,8 @@
 // hydro.cuh -- launchers of the hydraulic and sediment kernels.
+//
+// The simulated time is read by the kernels from State::clock (advanced on
+// the device at the start of each half-step), so one step's launches are
+// the same every step and can be captured once into a CUDA graph.
 #pragma once
 #include "common.cuh"
 
@@ -10,12 +14,18 @@ void launch_init(const State& S, const Coef& c, cudaStream_t st);
 void launch_scan_segments(const State& S, cudaStream_t st);
 // segment tables + boundary concentration interpolation
 void launch_find_limits(const State& S, const Coef& c, cudaStream_t st, Trace* tr);
-// hydraulic half-step A: boundary at t, x sweep, explicit v, commit
-void launch_half_x(const State& S, const Coef& c, double t, cudaStream_t st, Trace* tr);
-// hydraulic half-step B: boundary at t, y sweep, explicit u, wet/dry, commit
-void launch_half_y(const State& S, const Coef& c, double t, cudaStream_t st, Trace* tr);
-// concentration sweeps: xdir = the i-sweep after half-step A
-void launch_sediment(const State& S, const Coef& c, double t, double s_start, bool xdir,
-                     cudaStream_t st, Trace* tr);
+// hydraulic half-step A: t += dT/2, boundary, x sweep, explicit v, commit
+void launch_half_x(const State& S, const Coef& c, cudaStream_t st, Trace* tr);
+// hydraulic half-step B: t += dT/2, boundary, y sweep, explicit u, wet/dry,
+// commit
+void launch_half_y(const State& S, const Coef& c, cudaStream_t st, Trace* tr);
+// partitioned hydraulic line sweep: dir 0 = x (columns), 1 = y (rows)
+void launch_sweep(const State& S, const Coef& c, int dir, cudaStream_t st);
+// partitioned concentration line sweep: dir 0 = i-sweep (columns), 1 = rows;
+// the erosion source is on from s_start
+void launch_fs_sweep(const State& S, const Coef& c, int dir, double s_start, cudaStream_t st);
+// concentration step: xdir = the i-sweep after half-step A
+void launch_sediment(const State& S, const Coef& c, double s_start, bool xdir, cudaStream_t st,
+                     Trace* tr);
 
 }  // namespace hyd

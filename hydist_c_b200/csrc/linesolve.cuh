@@ -1,0 +1,223 @@
+// linesolve.cuh -- partitioned tridiagonal line solver for the ADI sweeps.
+//
+// One CTA solves LPB = 4 adjacent lines at a time (a persistent loop walks
+// the line groups). Each line is split into P chunks of consecutive cells;
+// thread (chunk k, line l) = threadIdx.x = k*LPB + l, so a warp covers 8
+// chunks x 4 adjacent lines and every global access of the x sweep reads
+// 4 adjacent columns (one 32-byte sector).
+//
+// The line's tridiagonal system (all wet segments of the line, identity rows
+// between them) is solved by the partition method:
+//   pass A  each chunk eliminates its interior rows forward, keeping the
+//           spike of the unknown left of the chunk: x_r = y'_r + v'_r x_L
+//           - c'_r x_{r+1}; (c', y', v') go to an L2-resident scratch slot;
+//           the chunk's last unknown is a separator;
+//   pass B  backward over the interior gives the first and last interior
+//           rows in terms of the two neighbouring separators;
+//   reduce  the separators form a tridiagonal Schur-complement system of P
+//           unknowns per line, solved by parallel cyclic reduction in
+//           shared memory;
+//   pass C  backward substitution of every interior unknown, emitted to
+//           the mesh fields as it is produced; then the per-segment end
+//           fix-ups run.
+// The row coefficients are generated on the fly by a generator class (the
+// reference builds them in global arrays a1..d2, AA..DD first,
+// UVZSolver_multithread.cpp:210-470, and solves each segment serially with
+// tridiag(), :19-43).
+#pragma once
+
+#include "common.cuh"
+
+namespace hyd {
+
+constexpr int LPB = 4;  // lines per CTA
+
+// One wet segment of a line, with its system layout.
+struct SegD {
+  int first, last;
+  int off, rend;  // absolute rows [off, rend] of the segment's system
+  unsigned char br1, br2, ran, qfirst, last_kind, xq_first, xq_last, pad;
+};
+
+struct LineSeg {
+  int nseg;
+  SegD s[SEG];
+};
+
+// Shared-memory layout of one CTA.
+template <int P>
+struct LSShared {
+  LineSeg seg[LPB];
+  double sep[4][P * LPB];   // separator rows a, b, c, d
+  double tri[6][P * LPB];   // yF vF wF yL vL wL per chunk
+  double red[4][P * LPB];   // reduced system during PCR
+  double xsep[P * LPB];     // separator solutions
+  double xlast[LPB][SEG];   // solution at each segment's last row
+};
+
+// Reciprocal with one Newton correction of the hardware estimate is not
+// used: a plain FP64 division keeps the rounding of the reference's
+// formulas within one ulp.
+__device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+
+template <class Gen, int P>
+__global__ void __launch_bounds__(LPB * P, 1) k_line_solve(Gen G) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  LSShared<P>& sh = *reinterpret_cast<LSShared<P>*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int l = tid % LPB, k = tid / LPB;
+  const int cidx = k * LPB + l;
+  const int U = G.unknowns_per_line();
+  double* scr = G.scratch + (size_t)blockIdx.x * 3 * (size_t)U * LPB;
+  double* sc_c = scr;
+  double* sc_y = scr + (size_t)U * LPB;
+  double* sc_v = scr + 2 * (size_t)U * LPB;
+  const int ncells = G.cells_per_line();
+  const int upc = Gen::UPC;
+  const int ngroups = cdiv(G.lines(), LPB);
+
+  for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    const int line = grp * LPB + l;
+    // ---- segment descriptors of the group's lines
+    for (int e = tid; e < LPB * (SEG + 1); e += blockDim.x) {
+      const int ll = e / (SEG + 1), s = e % (SEG + 1);
+      G.load_segment(sh.seg[ll], grp * LPB + ll, s);
+    }
+    __syncthreads();
+    const LineSeg& LS = sh.seg[l];
+    // ---- chunk bounds (balanced split of the line's cells)
+    const int c0 = (int)(((long long)k * ncells) / P);
+    const int c1 = (int)(((long long)(k + 1) * ncells) / P);
+    const int q0 = c0 * upc, nu = (c1 - c0) * upc;  // chunk unknowns [q0, q0+nu)
+
+    // ---- pass A: forward elimination of the interior, separator row
+    {
+      typename Gen::Walker W;
+      W.init(G, LS, line, c0);
+      double cp = 0, yp = 0, vp = 0;
+      int s = 0;
+      for (int c = c0; c < c1; ++c) {
+        W.cell(G, LS, c);
+#pragma unroll
+        for (int e = 0; e < Gen::UPC; ++e, ++s) {
+          double A, B, C, D;
+          W.row(G, LS, e, A, B, C, D);
+          if (s == nu - 1) {
+            sh.sep[0][cidx] = A;
+            sh.sep[1][cidx] = B;
+            sh.sep[2][cidx] = C;
+            sh.sep[3][cidx] = D;
+          } else {
+            if (s == 0) {
+              const double m = rcp(B);
+              cp = C * m;
+              yp = D * m;
+              vp = -A * m;
+            } else {
+              const double m = rcp(B - A * cp);
+              yp = (D - A * yp) * m;
+              vp = -A * vp * m;
+              cp = C * m;
+            }
+            const size_t o = (size_t)(q0 + s) * LPB + l;
+            sc_c[o] = cp;
+            sc_y[o] = yp;
+            sc_v[o] = vp;
+          }
+        }
+      }
+      // ---- pass B: interior rows in terms of the neighbouring separators
+      double y = yp, v = vp, w = -cp;
+      sh.tri[3][cidx] = y;
+      sh.tri[4][cidx] = v;
+      sh.tri[5][cidx] = w;
+      for (int t = nu - 3; t >= 0; --t) {
+        const size_t o = (size_t)(q0 + t) * LPB + l;
+        const double cc = sc_c[o];
+        y = sc_y[o] - cc * y;
+        v = sc_v[o] - cc * v;
+        w = -cc * w;
+      }
+      sh.tri[0][cidx] = y;
+      sh.tri[1][cidx] = v;
+      sh.tri[2][cidx] = w;
+    }
+    __syncthreads();
+    // ---- reduced (Schur complement) system of the separators
+    double ra, rb, rc, rd;
+    {
+      const double as = sh.sep[0][cidx], bs = sh.sep[1][cidx], cs = sh.sep[2][cidx],
+                   ds = sh.sep[3][cidx];
+      const double yL = sh.tri[3][cidx], vL = sh.tri[4][cidx], wL = sh.tri[5][cidx];
+      double yF = 0, vF = 0, wF = 0;
+      if (k + 1 < P) {
+        const int n1 = cidx + LPB;
+        yF = sh.tri[0][n1];
+        vF = sh.tri[1][n1];
+        wF = sh.tri[2][n1];
+      }
+      ra = as * vL;
+      rb = bs + as * wL + cs * vF;
+      rc = cs * wF;
+      rd = ds - as * yL - cs * yF;
+    }
+    // parallel cyclic reduction
+    for (int st = 1; st < P; st <<= 1) {
+      sh.red[0][cidx] = ra;
+      sh.red[1][cidx] = rb;
+      sh.red[2][cidx] = rc;
+      sh.red[3][cidx] = rd;
+      __syncthreads();
+      double am = 0, bm = 1, cm = 0, dm = 0, an = 0, bn = 1, cn = 0, dn = 0;
+      if (k - st >= 0) {
+        const int o = cidx - st * LPB;
+        am = sh.red[0][o];
+        bm = sh.red[1][o];
+        cm = sh.red[2][o];
+        dm = sh.red[3][o];
+      }
+      if (k + st < P) {
+        const int o = cidx + st * LPB;
+        an = sh.red[0][o];
+        bn = sh.red[1][o];
+        cn = sh.red[2][o];
+        dn = sh.red[3][o];
+      }
+      __syncthreads();
+      const double k1 = ra / bm, k2 = rc / bn;
+      const double na = -am * k1, nc = -cn * k2;
+      const double nb = rb - cm * k1 - an * k2;
+      const double nd = rd - dm * k1 - dn * k2;
+      ra = na;
+      rb = nb;
+      rc = nc;
+      rd = nd;
+    }
+    sh.xsep[cidx] = rd / rb;
+    __syncthreads();
+    // ---- pass C: back substitution and emission
+    {
+      const double xr = sh.xsep[cidx];
+      const double xl = (k > 0) ? sh.xsep[cidx - LPB] : 0.0;
+      typename Gen::Emitter E;
+      E.init(G, LS, line);
+      E.emit(G, LS, sh.xlast[l], q0 + nu - 1, xr);
+      double xn = xr;
+      for (int t = nu - 2; t >= 0; --t) {
+        const size_t o = (size_t)(q0 + t) * LPB + l;
+        const double x = sc_y[o] + sc_v[o] * xl - sc_c[o] * xn;
+        E.emit(G, LS, sh.xlast[l], q0 + t, x);
+        xn = x;
+      }
+    }
+    __syncthreads();
+    // ---- per-segment end fix-ups
+    for (int e = tid; e < LPB * SEG; e += blockDim.x) {
+      const int ll = e / SEG, s = e % SEG;
+      if (s < sh.seg[ll].nseg) G.fixup(sh.seg[ll], sh.xlast[ll], grp * LPB + ll, s);
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace hyd

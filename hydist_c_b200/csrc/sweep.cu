@@ -1,0 +1,413 @@
+// sweep.cu -- the hydraulic ADI line sweeps on the partitioned line solver.
+//
+// HydroGen<0> is the x sweep (UZ half-step: lines are columns j, cells run
+// along i, unknowns z_i and u_i interleaved); HydroGen<1> is the y sweep (VZ
+// half-step: lines are rows i, cells along j, unknowns z_j and v_j). Both
+// generate the reference's tridiagonal rows on the fly (assembly.cuh) and
+// write the extraction of UZSolver_extract_solution / VZSolver_extract_
+// solution (UVZSolver_multithread.cpp:472-603) directly from the solution.
+#include "assembly.cuh"
+#include "common.cuh"
+#include "hydro.cuh"
+#include "linesolve.cuh"
+#include "sediment_cell.cuh"
+
+namespace hyd {
+
+// chunks per line: as many as keep at least `min_cells` cells per chunk
+int line_chunks(int ncells, int min_cells) {
+  int P = 128;
+  while (P > 16 && ncells < P * min_cells) P >>= 1;
+  return P;
+}
+
+template <int DIR>
+struct HydroGen {
+  static constexpr int UPC = 2;
+  State S;
+  Coef c;
+  double* scratch;
+  double f4;
+
+  __device__ int lines() const { return DIR == 0 ? S.M - 1 : S.N - 1; }
+  __device__ int cells_per_line() const { return DIR == 0 ? S.N - 1 : S.M - 1; }
+  __device__ int unknowns_per_line() const { return 2 * cells_per_line(); }
+  __device__ int end_pos() const { return DIR == 0 ? S.N : S.M; }
+  // field index of position p on line position lp
+  __device__ int at(int lp, int p) const { return DIR == 0 ? p * S.W + lp : lp * S.W + p; }
+  __device__ Pre pre(int lp, int p) const {
+    return DIR == 0 ? pre_x(S, c, p, lp) : pre_y(S, c, lp, p);
+  }
+  __device__ double* vel() const { return DIR == 0 ? S.tu : S.tv; }
+  // the VZ extraction reaches columns j <= N only (UVZSolver_multithread.cpp:851)
+  __device__ bool extract_ok(int p) const { return DIR == 0 ? true : p <= S.N; }
+
+  __device__ void load_segment(LineSeg& LS, int line, int s) const {
+    const bool ok = line < lines();
+    const int lp = line + 2;
+    if (s == SEG) {
+      LS.nseg = ok ? (DIR == 0 ? S.mocj[lp] : S.moci[lp]) : 0;
+      return;
+    }
+    if (!ok) return;
+    const int n = DIR == 0 ? S.mocj[lp] : S.moci[lp];
+    if (s >= n) return;
+    const int w = S.W;
+    SegD& d = LS.s[s];
+    int first, last;
+    bool br1, br2;
+    bool q1, q2;
+    if (DIR == 0) {
+      first = S.dauj[lp * SEG + s];
+      last = S.cuoij[lp * SEG + s];
+      // locate_segment_u (support_funcs.cpp:845-851)
+      br1 = (first > 2) || ((first == 2) && ((S.h[1 * w + lp] + S.h[1 * w + lp - 1]) * 0.5 == c.NANGDAY));
+      br2 = (last < S.N) || ((last == S.N) && ((S.h[S.N * w + lp] + S.h[S.N * w + lp - 1]) * 0.5 == c.NANGDAY));
+      q1 = S.bienQ[2] != 0;
+      q2 = S.bienQ[3] != 0;
+    } else {
+      first = S.daui[lp * SEG + s];
+      last = S.cuoii[lp * SEG + s];
+      // locate_segment_v (support_funcs.cpp:823-826)
+      br1 = (first > 2) || ((first == 2) && ((S.h[lp * w + first - 1] + S.h[(lp - 1) * w + first - 1]) * 0.5 == c.NANGDAY));
+      br2 = (last < S.M) || ((last == S.M) && ((S.h[lp * w + last] + S.h[(lp - 1) * w + last]) * 0.5 == c.NANGDAY));
+      q1 = S.bienQ[1] != 0;
+      q2 = S.bienQ[0] != 0;
+    }
+    const LineSys L = line_sys(first, last, br1, br2, q1, q2, end_pos());
+    d.first = first;
+    d.last = last;
+    d.off = L.off;
+    d.rend = L.off + L.sn;
+    d.br1 = br1;
+    d.br2 = br2;
+    d.ran = L.ran;
+    d.qfirst = L.qfirst;
+    d.last_kind = (unsigned char)L.last_kind;
+    d.xq_first = q1;
+    d.xq_last = q2;
+  }
+
+  // Generates the rows of the line system cell by cell (two unknowns per cell).
+  struct Walker {
+    int lp, si, pos, prev;
+    bool in;
+    Pre Pc, Pn;
+    Mom Mi;
+    __device__ void init(const HydroGen& G, const LineSeg& LS, int line, int c0) {
+      lp = line + 2;
+      si = 0;
+      prev = -10;
+      in = false;
+    }
+    __device__ void cell(const HydroGen& G, const LineSeg& LS, int c) {
+      pos = c + 2;
+      while (si < LS.nseg && LS.s[si].last < pos) ++si;
+      in = si < LS.nseg && LS.s[si].first <= pos;
+      if (!in) {
+        prev = -10;
+        return;
+      }
+      const SegD& d = LS.s[si];
+      if (prev == pos - 1 && pos > d.first) Pc = Pn;
+      else Pc = G.pre(lp, pos);
+      if (pos + 1 <= d.last) Pn = G.pre(lp, pos + 1);
+      else Pn = Pc;
+      if (pos <= d.last - 1 || pos == d.first) Mi = abcd(Pc, Pn, pos, d.first, d.last, G.f4, d.br1, d.br2);
+      else Mi = Mom{0, 0, 0, 0};
+      prev = pos;
+    }
+    __device__ void row(const HydroGen& G, const LineSeg& LS, int e, double& A, double& B,
+                        double& C, double& D) const {
+      const int r = 2 * pos + e;
+      if (!in) {
+        A = 0; B = 1; C = 0; D = 0;
+        return;
+      }
+      const SegD& d = LS.s[si];
+      if (r < d.off || r > d.rend) {
+        A = 0; B = 1; C = 0; D = 0;
+        return;
+      }
+      const bool even = (r & 1) == 0;
+      if ((bool)d.ran == even) {
+        const Pre& P = d.ran ? Pc : Pn;
+        A = P.a2; B = 1; C = P.c2; D = P.d2;
+      } else {
+        A = Mi.a1; B = Mi.b1; C = Mi.c1; D = Mi.d1;
+      }
+      if (r == d.off) {
+        if (d.ran) {
+          if (d.qfirst) {
+            const double ub = DIR == 0 ? G.S.ubt[lp] : G.S.vbd[lp];
+            D = Pc.d2 - Pc.a2 * ub;
+          } else {
+            D = Pc.d2;
+          }
+        } else {
+          const double TZ_l = G.S.tz[G.at(lp, d.first)];
+          D = Mi.d1 - Mi.a1 * TZ_l;
+        }
+        A = 0;  // the system starts here
+      }
+      if (r == d.rend) {
+        const Pre& PL = (pos == d.last) ? Pc : Pn;
+        if (d.last_kind == 1) {
+          const double ub = DIR == 0 ? G.S.ubp[lp] : G.S.vbt[lp];
+          A = PL.a2; B = 1; D = PL.d2 - PL.c2 * ub;
+        } else if (d.last_kind == 2) {
+          const double TZ_r = G.S.tz[G.at(lp, d.last)];
+          A = Mi.a1; B = Mi.b1; D = Mi.d1 - Mi.c1 * TZ_r;
+        } else {
+          A = PL.a2; B = 1; D = PL.d2;
+        }
+        C = 0;  // and ends here
+      }
+    }
+  };
+
+  // Writes each solved unknown to t_z / t_u (t_v) as the extraction does.
+  struct Emitter {
+    int lp, si;
+    __device__ void init(const HydroGen& G, const LineSeg& LS, int line) {
+      lp = line + 2;
+      si = LS.nseg - 1;
+    }
+    __device__ void emit(const HydroGen& G, const LineSeg& LS, double* xlast, int q,
+                         double x) {
+      const int r = q + 4, pos = r >> 1;
+      while (si >= 0 && LS.s[si].first > pos) --si;
+      if (si < 0) return;
+      const SegD& d = LS.s[si];
+      if (pos > d.last || r < d.off || r > d.rend) return;
+      if (r == d.rend) xlast[si] = x;
+      double* vel = G.vel();
+      if (d.ran) {
+        const int i = r >> 1;
+        if (i < d.last && G.extract_ok(i)) {
+          if (r & 1) vel[G.at(lp, i)] = x;
+          else G.S.tz[G.at(lp, i)] = x;
+        }
+      } else {
+        if (r == 2 * d.first) {
+          if (G.extract_ok(d.first)) vel[G.at(lp, d.first)] = x;
+        } else {
+          const int i = (r + 1) >> 1;
+          if (i > d.first && i < d.last && G.extract_ok(i)) {
+            if (r & 1) G.S.tz[G.at(lp, i)] = x;
+            else vel[G.at(lp, i)] = x;
+          }
+        }
+      }
+    }
+  };
+
+  // Segment ends (_uzSolver_extract_solution :558-601 / _vzSolver_ :488-536).
+  __device__ void fixup(const LineSeg& LS, const double* xlast, int line, int s) const {
+    const SegD& d = LS.s[s];
+    const int lp = line + 2, first = d.first, last = d.last;
+    double* vel = vel_ptr();
+    double* tz = S.tz;
+    if (first < last && extract_ok(first)) {
+      if (d.br1) {
+        vel[at(lp, first - 1)] = 0;
+      } else if (d.xq_first && first == 2) {
+        vel[at(lp, first - 1)] = DIR == 0 ? S.ubt[lp] : S.vbd[lp];
+      } else {
+        const Pre Pf = pre(lp, first);
+        vel[at(lp, first - 1)] = (Pf.d2 - tz[at(lp, first)] - Pf.c2 * vel[at(lp, first)]) / Pf.a2;
+      }
+    }
+    if (!extract_ok(last)) return;
+    const double xl = (d.rend >= d.off) ? xlast[s] : 0.0;
+    if (d.br2) {
+      vel[at(lp, last)] = 0;
+      tz[at(lp, last)] = xl;
+    } else if (d.xq_last && last == end_pos()) {
+      vel[at(lp, last)] = DIR == 0 ? S.ubp[lp] : S.vbt[lp];
+      tz[at(lp, last)] = xl;
+    } else {
+      const Pre Pl = pre(lp, last);
+      vel[at(lp, last)] = (Pl.d2 - Pl.a2 * vel[at(lp, last - 1)] - tz[at(lp, last)]) / Pl.c2;
+    }
+  }
+  __device__ double* vel_ptr() const { return DIR == 0 ? S.tu : S.tv; }
+};
+
+template <class Gen, int P>
+static void launch_gen(const Gen& G, cudaStream_t st, int grid) {
+  const size_t smem = sizeof(LSShared<P>);
+  static bool attr[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr[dev]) {
+    cudaFuncSetAttribute(k_line_solve<Gen, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    attr[dev] = true;
+  }
+  k_line_solve<Gen, P><<<grid, LPB * P, smem, st>>>(G);
+}
+
+template <class Gen>
+static void launch_any(const Gen& G, int P, cudaStream_t st, int grid) {
+  if (P == 128) launch_gen<Gen, 128>(G, st, grid);
+  else if (P == 64) launch_gen<Gen, 64>(G, st, grid);
+  else if (P == 32) launch_gen<Gen, 32>(G, st, grid);
+  else launch_gen<Gen, 16>(G, st, grid);
+}
+
+template <int DIR>
+static void launch_dir(const State& S, const Coef& c, cudaStream_t st, int grid, int P) {
+  HydroGen<DIR> G;
+  G.S = S;
+  G.c = c;
+  G.scratch = S.lscratch;
+  G.f4 = DIR == 0 ? 2 * c.g * c.dTchia2dX : 2 * c.g * c.dTchia2dY;
+  launch_any(G, P, st, grid);
+}
+
+// ---------------------------------------------------------------------
+// Concentration sweeps: one unknown per cell, cells first+1..last-1 of each
+// wet segment of at least three cells (Scan_FSj / Scan_FSi,
+// sediment_transport.cpp:51-164, 204-313; extraction :167-201, 316-349).
+// DIR 0: columns j = 3..M-1 along i; DIR 1: rows i = 3..N-1 along j.
+template <int DIR>
+struct FSGen {
+  static constexpr int UPC = 1;
+  State S;
+  Coef c;
+  double* scratch;
+  double s_start;
+
+  __device__ int lines() const { return DIR == 0 ? S.M - 3 : S.N - 3; }
+  __device__ int cells_per_line() const { return DIR == 0 ? S.N - 1 : S.M - 1; }
+  __device__ int unknowns_per_line() const { return cells_per_line(); }
+  __device__ int at(int lp, int p) const { return DIR == 0 ? p * S.W + lp : lp * S.W + p; }
+  __device__ const double* vel() const { return DIR == 0 ? S.tu : S.tv; }
+
+  __device__ void load_segment(LineSeg& LS, int line, int s) const {
+    const bool ok = line < lines();
+    const int lp = line + 3;
+    if (s == SEG) {
+      LS.nseg = ok ? (DIR == 0 ? S.mocj[lp] : S.moci[lp]) : 0;
+      return;
+    }
+    if (!ok) return;
+    const int n = DIR == 0 ? S.mocj[lp] : S.moci[lp];
+    if (s >= n) return;
+    const int w = S.W;
+    SegD& d = LS.s[s];
+    int first, last;
+    bool br1, br2;
+    if (DIR == 0) {
+      first = S.dauj[lp * SEG + s];
+      last = S.cuoij[lp * SEG + s];
+      br1 = (first > 2) || ((first == 2) && ((S.h[1 * w + lp] + S.h[1 * w + lp - 1]) * 0.5 == c.NANGDAY));
+      br2 = (last < S.N) || ((last == S.N) && ((S.h[S.N * w + lp] + S.h[S.N * w + lp - 1]) * 0.5 == c.NANGDAY));
+    } else {
+      first = S.daui[lp * SEG + s];
+      last = S.cuoii[lp * SEG + s];
+      br1 = (first > 2) || ((first == 2) && ((S.h[lp * w + first - 1] + S.h[(lp - 1) * w + first - 1]) * 0.5 == c.NANGDAY));
+      br2 = (last < S.M) || ((last == S.M) && ((S.h[lp * w + last] + S.h[(lp - 1) * w + last]) * 0.5 == c.NANGDAY));
+    }
+    d.first = first;
+    d.last = last;
+    d.off = first + 1;
+    d.rend = last - 1;  // rend < off: no interior row, nothing solved
+    d.br1 = br1;
+    d.br2 = br2;
+    d.ran = d.qfirst = d.last_kind = d.xq_first = d.xq_last = 0;
+  }
+
+  struct Walker {
+    int lp, si, pos;
+    bool in;
+    __device__ void init(const FSGen& G, const LineSeg& LS, int line, int c0) {
+      lp = line + 3;
+      si = 0;
+      in = false;
+    }
+    __device__ void cell(const FSGen& G, const LineSeg& LS, int cc) {
+      pos = cc + 2;
+      while (si < LS.nseg && LS.s[si].last < pos) ++si;
+      in = si < LS.nseg && LS.s[si].off <= pos && pos <= LS.s[si].rend;
+    }
+    __device__ void row(const FSGen& G, const LineSeg& LS, int e, double& A, double& B,
+                        double& C, double& D) const {
+      if (!in) {
+        A = 0; B = 1; C = 0; D = 0;
+        return;
+      }
+      const SegD& d = LS.s[si];
+      const int i = DIR == 0 ? pos : lp, j = DIR == 0 ? lp : pos;
+      fs_cell(G.S, G.c, DIR == 0, i, j, G.S.clock[0], G.s_start, A, B, C, D);
+      const double* vel = G.vel();
+      if (pos == d.first + 1) {
+        if (d.br1 || vel[G.at(lp, d.first)] == 0) B = B + A;
+        else D = D - A * G.S.FS[G.at(lp, d.first)];
+        A = 0;
+      }
+      if (pos == d.last - 1) {
+        // '&&' in the i-sweep (sediment_transport.cpp:304), '||' in the j-sweep (:153)
+        const bool zero = vel[G.at(lp, d.last)] == 0;
+        if (DIR == 0 ? (d.br2 && zero) : (d.br2 || zero)) B = B + C;
+        else D = D - C * G.S.FS[G.at(lp, d.last)];
+        C = 0;
+      }
+    }
+  };
+
+  struct Emitter {
+    int lp, si;
+    __device__ void init(const FSGen& G, const LineSeg& LS, int line) {
+      lp = line + 3;
+      si = LS.nseg - 1;
+    }
+    __device__ void emit(const FSGen& G, const LineSeg& LS, double* xlast, int q, double x) {
+      const int pos = q + 2;
+      while (si >= 0 && LS.s[si].first > pos) --si;
+      if (si < 0) return;
+      const SegD& d = LS.s[si];
+      if (pos < d.off || pos > d.rend) return;
+      G.S.tFS[G.at(lp, pos)] = (x < 0) ? G.c.NDnen : x;
+    }
+  };
+
+  __device__ void fixup(const LineSeg& LS, const double* xlast, int line, int s) const {
+    const SegD& d = LS.s[s];
+    if (d.rend < d.off) return;
+    const int lp = line + 3;
+    const double* v = vel();
+    double* tFS = S.tFS;
+    tFS[at(lp, d.first)] = (d.br1 || v[at(lp, d.first)] == 0) ? tFS[at(lp, d.first + 1)]
+                                                               : S.FS[at(lp, d.first)];
+    tFS[at(lp, d.last)] = (d.br2 || v[at(lp, d.last)] == 0) ? tFS[at(lp, d.last - 1)]
+                                                             : S.FS[at(lp, d.last)];
+  }
+};
+
+void launch_fs_sweep(const State& S, const Coef& c, int dir, double s_start, cudaStream_t st) {
+  const int ncells = dir == 0 ? S.N - 1 : S.M - 1;
+  const int lines = dir == 0 ? S.M - 3 : S.N - 3;
+  if (lines <= 0) return;
+  const int grid = min(cdiv(lines, LPB), S.lslots);
+  const int P = line_chunks(ncells, 4);
+  if (dir == 0) {
+    FSGen<0> G{S, c, S.lscratch, s_start};
+    launch_any(G, P, st, grid);
+  } else {
+    FSGen<1> G{S, c, S.lscratch, s_start};
+    launch_any(G, P, st, grid);
+  }
+}
+
+void launch_sweep(const State& S, const Coef& c, int dir, cudaStream_t st) {
+  const int ncells = dir == 0 ? S.N - 1 : S.M - 1;
+  const int lines = dir == 0 ? S.M - 1 : S.N - 1;
+  const int grid = min(cdiv(lines, LPB), S.lslots);
+  const int P = line_chunks(ncells, 4);
+  if (dir == 0) launch_dir<0>(S, c, st, grid, P);
+  else launch_dir<1>(S, c, st, grid, P);
+}
+
+}  // namespace hyd

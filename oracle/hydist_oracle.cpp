@@ -1235,6 +1235,33 @@ struct Sim {
     for (auto& b : bufs) b.size(nmax + 2, 2 * nmax + 4);
   }
 
+  // The same step split into its operations, for inspecting intermediate
+  // states: runs operations [0, nops) of one step and returns how many exist.
+  int step_ops(int nops) {
+    int k = 0;
+    auto op = [&](auto&& f) {
+      if (k < nops) f();
+      ++k;
+    };
+    op([&] { t += 0.5 * c.dT; boundary(t); });
+    op([&] { for_lines(2, M, [&](LineBuf& L, int j) { uz_column(L, j); }); });
+    op([&] { normalize(true, tmpbuf); });
+    op([&] { solve_v(); });
+    op([&] { margin_v(); });
+    op([&] { normalize(false, tmpbuf); });
+    op([&] { update_h_moi(); update_uvz(); find_limits(); htuongdoi(); });
+    op([&] { t += c.dT * 0.5; boundary(t); });
+    op([&] { for_lines(2, N, [&](LineBuf& L, int i) { vz_row(L, i); }); });
+    op([&] { normalize(false, tmpbuf); });
+    op([&] { solve_u(); });
+    op([&] { margin_u(); });
+    op([&] { normalize(true, tmpbuf); });
+    op([&] { update_h_moi(); });
+    op([&] { reset_states_vertical(); });
+    op([&] { update_uvz(); find_limits(); htuongdoi(); });
+    return k;
+  }
+
   // One full step: the body of the while-loop of Hydraulic_Calculation,
   // engine.cpp:65-295.
   void step() {
@@ -1379,6 +1406,9 @@ int oracle_step(OracleSim* os, int nsteps) {
 }
 
 double oracle_time(OracleSim* os) { return os->s.t; }
+
+// Debug: run the first nops operations of one hydraulic step (no sediment).
+int oracle_step_ops(OracleSim* os, int nops) { return os->s.step_ops(nops); }
 
 int oracle_get(OracleSim* os, int field, void* out) {
   Sim& s = os->s;
