@@ -215,7 +215,8 @@ def run_ours(args):
     # spin-up to the sediment phase (untimed), then warm-up steps
     if spin:
         sim.step(spin)
-    sim.step(max(args.warmup, 3) if args.warmup >= 0 else 3)
+    # warm-up in the timed mode (a graph is captured on its first step)
+    (sim.step_graph if args.graph else sim.step)(max(args.warmup, 3))
     sim.sync()
     # per-phase device times of one step (tracing), for the roofline
     phases = sim.step_traced()

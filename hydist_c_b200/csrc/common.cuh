@@ -50,6 +50,7 @@ struct State {
   int *daui, *cuoii, *moci, *dauj, *cuoij, *mocj;
   // scratch
   double* tmp;   // smoothing buffer, (N+3)*(M+3)
+  double *su, *sv;  // t_u / t_v after the smoothing of the current half-step
   double* Ap;    // Thomas scratch, [unknown][line]
   double* Bp;
   int ld;        // line stride of Ap/Bp (max(M,N)+3)
@@ -57,6 +58,7 @@ struct State {
   double* lscratch;  // partitioned line solver: one slot per resident CTA
   int lslots;        // number of slots (CTAs of the persistent sweep grid)
   int* colflag;      // per column: holds a cell dried during the run
+  int* segcnt;       // run-start / run-end counters of the segment scan
   double* clock;     // [0]: simulated time, advanced on the device by k_tick
 };
 

@@ -347,9 +347,10 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistO
     S.Tsyw = tmp;
     // state
     double** st[] = {&S.u, &S.v, &S.z, &S.tu, &S.tv, &S.tz, &S.Hmoi, &S.Htdu, &S.Htdv, &S.FS,
-                     &S.tFS, &S.VTH, &S.Kx, &S.Ky, &S.dH, &S.Qbx, &S.Qby, &S.tmp};
+                     &S.tFS, &S.VTH, &S.Kx, &S.Ky, &S.dH, &S.Qbx, &S.Qby, &S.tmp, &S.sv};
     for (double** q : st) TRY(dalloc(h, q, n));
     TRY(dalloc(h, &S.khouot, n));
+    S.su = S.tmp;
     if (sc->FS0) {
       CK(cudaMemcpyAsync(S.FS, sc->FS0, n * 8, cudaMemcpyHostToDevice, h->stream));
       CK(cudaMemcpyAsync(S.tFS, sc->FS0, n * 8, cudaMemcpyHostToDevice, h->stream));
@@ -373,6 +374,7 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistO
     TRY(dalloc(h, &S.Bp, nunk * S.ld));
     TRY(dalloc(h, &S.err, 4));
     TRY(dalloc(h, &S.colflag, S.W));
+    TRY(dalloc(h, &S.segcnt, 2 * S.H + 2 * S.W));
     TRY(dalloc(h, &S.clock, 4));
     TRY(set_device_clock(h));
     // partitioned line solver scratch: 3 doubles per unknown, 4 lines per

@@ -140,16 +140,160 @@ __device__ __forceinline__ int scan_line(const int* k0, int stride, int lim, int
   return nseg;
 }
 
+// The same tables as scan_line, in a fixed-trip loop whose loads do not
+// depend on the scan state (so they pipeline). The reference's loop yields
+// the maximal wet runs [s, e] of [2, lim] with s <= lim-2 (a run starting
+// at lim-1 or lim is dropped by its `start + 1 == lim` test); e is capped at
+// lim.
+__device__ __forceinline__ int scan_runs(const int* k0, int stride, int lim, int* dau, int* cuoi,
+                                         int* err) {
+  int nseg = 0, s = 0;
+  bool in = false;
+#pragma unroll 8
+  for (int p = 2; p <= lim; ++p) {
+    const bool wet = k0[p * stride] == 0;
+    if (wet && !in) {
+      in = true;
+      s = p;
+    } else if (!wet && in) {
+      in = false;
+      if (s <= lim - 2) {
+        if (nseg < SEG) {
+          dau[nseg] = s;
+          cuoi[nseg] = p - 1;
+        }
+        ++nseg;
+      }
+    }
+  }
+  if (in && s <= lim - 2) {
+    if (nseg < SEG) {
+      dau[nseg] = s;
+      cuoi[nseg] = lim;
+    }
+    ++nseg;
+  }
+  if (nseg > SEG) {
+    atomicExch(err, DEV_SEG_OVERFLOW);
+    nseg = SEG;
+  }
+  return nseg;
+}
+
+// Parallel form of the same tables. A cell p of a line (positions 2..lim) is
+// the start of a recorded run when it is wet, p == 2 or p-1 is dry, and
+// p <= lim-2; it is the end of a recorded run when it is wet, p == lim or
+// p+1 is dry, and the run it ends starts at or before lim-2 (for p = lim-1
+// that needs lim-2 wet, for p = lim both lim-2 and lim-1 wet). Starts and
+// ends claim slots with atomics; k_runs_sort orders each line's slots.
+// seg_cnt: [0..H) row starts, [H..2H) row ends, [2H..2H+W) column starts,
+// [2H+W..2H+2W) column ends.
+__device__ __forceinline__ void run_flags(bool wm1, bool w, bool wp1, bool wm2_lim, int p,
+                                          int lim, bool& start, bool& end) {
+  start = w && (p == 2 || !wm1) && p <= lim - 2;
+  bool ok = true;
+  if (p == lim - 1) ok = wm1;        // wm1 = wet(lim-2)
+  else if (p == lim) ok = wm1 && wm2_lim;  // wet(lim-1) and wet(lim-2)
+  end = w && (p == lim || !wp1) && ok;
+}
+
+__global__ void k_runs_flags(State S, int* seg_cnt) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int i = blockIdx.y + 2;
+  if (i > S.N || j > S.M) return;
+  const int W = S.W, H = S.H, g = i * W + j;
+  const int* K = S.khouot;
+  const bool w = K[g] == 0;
+  if (!w) return;
+  // row i, position j, lim M
+  {
+    const bool wm1 = K[g - 1] == 0, wp1 = K[g + 1] == 0;
+    const bool wm2 = K[g - 2] == 0;
+    bool st, en;
+    run_flags(wm1, w, wp1, wm2, j, S.M, st, en);
+    if (st) {
+      const int s = atomicAdd(&seg_cnt[i], 1);
+      if (s < SEG) S.daui[i * SEG + s] = j;
+    }
+    if (en) {
+      const int s = atomicAdd(&seg_cnt[H + i], 1);
+      if (s < SEG) S.cuoii[i * SEG + s] = j;
+    }
+  }
+  // column j, position i, lim N
+  {
+    const bool wm1 = K[g - W] == 0, wp1 = K[g + W] == 0;
+    const bool wm2 = K[g - 2 * W] == 0;
+    bool st, en;
+    run_flags(wm1, w, wp1, wm2, i, S.N, st, en);
+    if (st) {
+      const int s = atomicAdd(&seg_cnt[2 * H + j], 1);
+      if (s < SEG) S.dauj[j * SEG + s] = i;
+    }
+    if (en) {
+      const int s = atomicAdd(&seg_cnt[2 * H + W + j], 1);
+      if (s < SEG) S.cuoij[j * SEG + s] = i;
+    }
+  }
+}
+
+__device__ __forceinline__ void sort_small(int* a, int n) {
+  for (int x = 1; x < n; ++x) {
+    const int v = a[x];
+    int y = x - 1;
+    while (y >= 0 && a[y] > v) {
+      a[y + 1] = a[y];
+      --y;
+    }
+    a[y + 1] = v;
+  }
+}
+
+// One thread per line: order the claimed slots, set the counts, clear the
+// counters for the next scan.
+__global__ void k_runs_sort(State S, int* seg_cnt) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int H = S.H, W = S.W;
+  const int nrow = S.N - 1, ncol = S.M - 1;
+  if (t >= nrow + ncol) return;
+  int *dau, *cuoi, *moc, *cs, *ce;
+  if (t < nrow) {
+    const int i = t + 2;
+    dau = S.daui + i * SEG;
+    cuoi = S.cuoii + i * SEG;
+    moc = S.moci + i;
+    cs = seg_cnt + i;
+    ce = seg_cnt + H + i;
+  } else {
+    const int j = t - nrow + 2;
+    dau = S.dauj + j * SEG;
+    cuoi = S.cuoij + j * SEG;
+    moc = S.mocj + j;
+    cs = seg_cnt + 2 * H + j;
+    ce = seg_cnt + 2 * H + W + j;
+  }
+  int n = *cs;
+  if (n > SEG || *ce != n) {
+    atomicExch(S.err, DEV_SEG_OVERFLOW);
+    n = min(n, SEG);
+  }
+  sort_small(dau, n);
+  sort_small(cuoi, n);
+  *moc = n;
+  *cs = 0;
+  *ce = 0;
+}
+
 __global__ void k_scan_rows(State S) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   if (i > S.N) return;
-  S.moci[i] = scan_line(S.khouot + i * S.W, 1, S.M, S.daui + i * SEG, S.cuoii + i * SEG, S.err);
+  S.moci[i] = scan_runs(S.khouot + i * S.W, 1, S.M, S.daui + i * SEG, S.cuoii + i * SEG, S.err);
 }
 
 __global__ void k_scan_cols(State S) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
   if (j > S.M) return;
-  S.mocj[j] = scan_line(S.khouot + j, S.W, S.N, S.dauj + j * SEG, S.cuoij + j * SEG, S.err);
+  S.mocj[j] = scan_runs(S.khouot + j, S.W, S.N, S.dauj + j * SEG, S.cuoij + j * SEG, S.err);
 }
 
 __global__ void k_htuongdoi(State S) {
@@ -550,6 +694,36 @@ __global__ void __launch_bounds__(128) k_sweep_y(State S, Coef c) {
 
 // ------------------------------------------------------------ smoothing
 // _normalize (support_funcs.cpp:761-782): tmp <- smoothed value, interior.
+// The same smoothing into a complete array (su / sv): smoothed on the
+// interior [2,N]x[2,M], the unsmoothed value elsewhere, i.e. t_u / t_v as
+// they stand after update_buffer. Readers of the smoothed velocity use it
+// directly and the half-step commit writes it back to t_u / t_v, u / v.
+__global__ void k_smooth_full(State S, Coef c, int isU) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (i >= S.H || j >= S.W) return;
+  const int W = S.W, g = i * W + j;
+  const double* val = isU ? S.tu : S.tv;
+  double* out_arr = isU ? S.su : S.sv;
+  const double vg = val[g];
+  double out = vg;
+  if (i >= 2 && i <= S.N && j >= 2 && j <= S.M && vg != 0) {
+    const int close = isU ? W : 1, far = isU ? 1 : W;
+    int count = 2;
+    double nb = val[g - close] + val[g + close];
+    if (S.khouot[g - far] == 0) {
+      nb += val[g - far];
+      count++;
+    }
+    if (S.khouot[g + far] == 0) {
+      nb += val[g + far];
+      count++;
+    }
+    out = out * c.heso + (1 - c.heso) * nb / count;
+  }
+  out_arr[g] = out;
+}
+
 __global__ void k_smooth(State S, Coef c, int isU) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int i = blockIdx.y + 2;
@@ -608,7 +782,7 @@ __global__ void k_solve_v(State S, Coef c) {
   const int off = S.W;
   const double* u = S.u;
   const double* v = S.v;
-  const double* tu = S.tu;
+  const double* tu = S.su;  // t_u after its smoothing
   const double* Hm = S.Hmoi;
   double p, q = 0, tmp = 0;
   const double utb = (u[(row - 1) * off + col] + u[row * off + col] + u[(row - 1) * off + col + 1] +
@@ -656,7 +830,7 @@ __global__ void k_solve_u(State S, Coef c) {
   const double dX = c.dY, dY = c.dY, Windx = c.Windy;
   const double* u = S.u;
   const double* v = S.v;
-  const double* tv = S.tv;
+  const double* tv = S.sv;  // t_v after its smoothing
   const double* Hm = S.Hmoi;
   double p, q = 0, tmp = 0;
   const int ij = row * off + col, i1j = ij + off;
@@ -790,9 +964,13 @@ __global__ void k_commit_a(State S, Coef c) {
   const int W = S.W, g = i * W + j;
   const double tz = S.tz[g];
   if (i >= 1 && j >= 1 && S.khouot[g] == 0) S.Hmoi[g] = S.htaiz[g] + tz;
+  // t_u, t_v after their smoothing (update_buffer) and the commit
+  const double tu = S.su[g], tv = S.sv[g];
+  S.tu[g] = tu;
+  S.tv[g] = tv;
   S.z[g] = tz;
-  S.u[g] = S.tu[g] * (1 - c.kenhhepd);
-  S.v[g] = S.tv[g] * (1 - c.kenhhepng);
+  S.u[g] = tu * (1 - c.kenhhepd);
+  S.v[g] = tv * (1 - c.kenhhepng);
   if (i >= 1 && j >= 1) {
     const double zd = (i + 1 <= S.N) ? S.tz[g + W] : S.z[g + W];
     const double zr = (j + 1 <= S.M) ? S.tz[g + 1] : S.z[g + 1];
@@ -860,15 +1038,12 @@ __global__ void k_commit_b(State S, Coef c) {
   const bool d0 = dries(i, j);
   const bool ddown = dries(i + 1, j);
   const bool dright = dries(i, j + 1);
-  double tu = S.tu[g], tv = S.tv[g];
-  if (d0 || ddown) {
-    tu = 0;
-    S.tu[g] = 0;
-  }
-  if (d0 || dright) {
-    tv = 0;
-    S.tv[g] = 0;
-  }
+  // t_u, t_v after their smoothing, zeroed by the drying pass
+  double tu = S.su[g], tv = S.sv[g];
+  if (d0 || ddown) tu = 0;
+  if (d0 || dright) tv = 0;
+  S.tu[g] = tu;
+  S.tv[g] = tv;
   if (d0) S.FS[g] = 0;  // khouot is set by k_dry_mask after this pass
   const double tz = S.tz[g];
   S.z[g] = tz;
@@ -903,15 +1078,14 @@ void launch_init(const State& S, const Coef& c, cudaStream_t st) {
 }
 
 void launch_scan_segments(const State& S, cudaStream_t st) {
-  k_scan_rows<<<cdiv(S.N, 128), 128, 0, st>>>(S);
-  k_scan_cols<<<cdiv(S.M, 128), 128, 0, st>>>(S);
+  k_runs_flags<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, S.segcnt);
+  k_runs_sort<<<cdiv(S.N + S.M - 2, 128), 128, 0, st>>>(S, S.segcnt);
 }
 
 void launch_find_limits(const State& S, const Coef& c, cudaStream_t st, Trace* tr) {
   k_interp_fs_rows<<<dim3(cdiv(S.M, 128), 2), 128, 0, st>>>(S, c);
-  k_scan_rows<<<cdiv(S.N, 128), 128, 0, st>>>(S);
   k_interp_fs_col<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
-  k_scan_cols<<<cdiv(S.M, 128), 128, 0, st>>>(S);
+  launch_scan_segments(S, st);
   if (tr) tr->launches += 4;
 }
 
@@ -921,13 +1095,14 @@ void launch_half_x(const State& S, const Coef& c, cudaStream_t st, Trace* tr) {
   if (tr) tr->mark(st, PH_BOUNDARY_X, 2);
   launch_sweep(S, c, 0, st);
   if (tr) tr->mark(st, PH_SWEEP_X, 1);
-  k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 1);
-  k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 1);
+  // smoothing of t_u into su, explicit v from it, margins, smoothing of t_v
+  // into sv; k_commit_a writes both back (Normalize/update_buffer pairs,
+  // engine.cpp:109-124)
+  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 1);
   k_solve_v<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c);
   k_margin_v<<<cdiv(S.N - 1, 128), 128, 0, st>>>(S, c);
-  k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 0);
-  k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 0);
-  if (tr) tr->mark(st, PH_EXPLICIT_V, 6);
+  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 0);
+  if (tr) tr->mark(st, PH_EXPLICIT_V, 4);
   // update_h_moi + update_uvz + Htuongdoi; the wet/dry mask does not change
   // in this half-step, so the segment tables are not rescanned, only the
   // boundary concentration is interpolated (support_funcs.cpp:255-258, 311)
@@ -943,13 +1118,11 @@ void launch_half_y(const State& S, const Coef& c, cudaStream_t st, Trace* tr) {
   if (tr) tr->mark(st, PH_BOUNDARY_Y, 2);
   launch_sweep(S, c, 1, st);
   if (tr) tr->mark(st, PH_SWEEP_Y, 1);
-  k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 0);
-  k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 0);
+  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 0);
   k_solve_u<<<grid2(S.M - 1, S.N, 128), 128, 0, st>>>(S, c);
   k_margin_u<<<cdiv(S.M - 1, 128), 128, 0, st>>>(S, c);
-  k_smooth<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, 1);
-  k_smooth_commit<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, 1);
-  if (tr) tr->mark(st, PH_EXPLICIT_U, 6);
+  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 1);
+  if (tr) tr->mark(st, PH_EXPLICIT_U, 4);
   // update_h_moi, Reset_states_vertical (wetting on flagged columns, drying
   // per cell), update_uvz, Htuongdoi, then the segment tables
   k_hmoi_flags<<<grid2(S.M, S.N + 1, 128), 128, 0, st>>>(S, S.colflag);

@@ -206,7 +206,9 @@ def test_wetting_and_drying(hyd, oracle_mod):
     skips exact zeros (support_funcs.cpp:770), so such cells differ visibly.
     The reference's own GPU build departs from the oracle this way too
     (tests/golden/make_reference_fixtures.py, case wetdry). Within 3 cells of
-    a dry cell the fields are held to 2e-2 relative."""
+    a dry cell the fields are held to 2e-2 relative; the implicit sweeps
+    carry that local difference along its lines, decayed, so elsewhere the
+    bound is 1e-6 relative in a step where it occurs (1e-10 otherwise)."""
     b = wetdry_bundle()
     orc = oracle_mod.OracleSim(b)
     sim = hyd.Simulation(b)
@@ -230,12 +232,15 @@ def test_wetting_and_drying(hyd, oracle_mod):
             seen_rewet |= bool(((k_before == 1) & (k == 0)).any())
             assert np.array_equal(sim.download("khouot"), k), orc.t
             front = _front_mask(k_before) | _front_mask(k)
+            diffs = {}
             for f in FIELDS_STEP:
                 a, r = sim.download(f), orc.get(f)
                 scale = max(np.abs(r).max(), 1e-300)
-                d = np.abs(a - r) / scale
-                assert d[~front].max() <= 1e-10, (orc.t, f, d[~front].max())
+                diffs[f] = np.abs(a - r) / scale
+            front_hit = any(d[front].max() > 1e-10 for d in diffs.values())
+            for f, d in diffs.items():
                 assert d.max() <= 2e-2, (orc.t, f, d.max())
+                assert d[~front].max() <= (1e-6 if front_hit else 1e-10), (orc.t, f, d[~front].max())
             for f in STATE:
                 sim.upload(f, orc.get(f))
             sim.upload("khouot", k)
