@@ -2,9 +2,14 @@
 //
 // pre_x / pre_y restate _uzSolver_calculate_preindex / _vzSolver_calculate_
 // preindex (UVZSolver_multithread.cpp:210-278, 142-208), abcd restates
-// _calculate_abcd (:280-342), line_sys and row_of the row layout of
+// _calculate_abcd (:280-342), line_sys the row layout of
 // _calculate_matrix_coeff with bienrandau / bienlongdau (:110-139, 345-470).
-// Expression order follows the reference.
+//
+// The formulas keep the reference's structure; divisions by constants are
+// multiplications by precomputed reciprocals (Coef::r_*), and each cell
+// takes one reciprocal of Htdu (or Htdv), of a2 and of the next cell's c2
+// instead of the reference's repeated divisions. This changes results by a
+// rounding at most per operation, and keeps exact zeros exact.
 #pragma once
 
 #include "common.cuh"
@@ -19,80 +24,82 @@ struct Pre {
 // _uzSolver_calculate_preindex (UVZSolver_multithread.cpp:210-278).
 __device__ __forceinline__ Pre pre_x(const State& S, const Coef& c, int i, int j) {
   const int w = S.W;
+  const int g = i * w + j;
   const double* u = S.u;
   const double* v = S.v;
   const double* Hm = S.Hmoi;
   Pre P;
   double p = 0.0, q = 0.0;
-  const double vtb =
-      (v[i * w + j - 1] + v[i * w + j] + v[(i + 1) * w + j - 1] + v[(i + 1) * w + j]) * 0.25;
-  const double uu = u[i * w + j], VI = S.visco[i * w + j], Hu = S.Htdu[i * w + j];
+  const double vtb = (v[g - 1] + v[g] + v[g + w - 1] + v[g + w]) * 0.25;
+  const double uu = u[g], VI = S.visco[g], Hu = S.Htdu[g];
   const double dT = c.dT;
-  P.f1 = c.dTchia2dX * uu + VI * dT / c.dXbp;
-  P.f2 = -(2 + S.Kx1[i * w + j] * dT * sqrt(uu * uu + vtb * vtb) / Hu + (2 * dT * VI) / c.dXbp);
-  P.f3 = dT * VI / c.dXbp - c.dTchia2dX * uu;
-  if (Hm[i * w + j - 1] <= c.H_TINH) {
+  const double rH = 1.0 / Hu;
+  const double visc = VI * c.dT_dXbp;
+  P.f1 = c.dTchia2dX * uu + visc;
+  P.f2 = -(2 + S.Kx1[g] * dT * sqrt(uu * uu + vtb * vtb) * rH + 2 * visc);
+  P.f3 = visc - c.dTchia2dX * uu;
+  if (Hm[g - 1] <= c.H_TINH) {
     if (vtb < 0) {
-      p = vtb * (-3 * uu + 4 * u[i * w + j + 1] - u[i * w + j + 2]) / c.dY2;
-      q = (uu - 2 * u[i * w + j + 1] + u[i * w + j + 2]) / c.dYbp;
+      p = vtb * (-3 * uu + 4 * u[g + 1] - u[g + 2]) * c.r_dY2;
+      q = (uu - 2 * u[g + 1] + u[g + 2]) * c.r_dYbp;
     }
   } else {
-    if (Hm[i * w + j + 1] <= c.H_TINH) {
-      if ((Hm[i * w + j - 2] > c.H_TINH) && (vtb > 0)) {
-        p = vtb * (3 * uu - 4 * u[i * w + j - 1] + u[i * w + j - 2]) / c.dY2;
-        q = (uu - 2 * u[i * w + j - 1] + u[i * w + j - 2]) / c.dYbp;
+    if (Hm[g + 1] <= c.H_TINH) {
+      if ((Hm[g - 2] > c.H_TINH) && (vtb > 0)) {
+        p = vtb * (3 * uu - 4 * u[g - 1] + u[g - 2]) * c.r_dY2;
+        q = (uu - 2 * u[g - 1] + u[g - 2]) * c.r_dYbp;
       }
     } else {
-      p = vtb * (u[i * w + j + 1] - u[i * w + j - 1]) / c.dY2;
-      q = (u[i * w + j + 1] - 2 * uu + u[i * w + j - 1]) / c.dYbp;
+      p = vtb * (u[g + 1] - u[g - 1]) * c.r_dY2;
+      q = (u[g + 1] - 2 * uu + u[g - 1]) * c.r_dYbp;
     }
   }
   P.f5 = -2 * uu + dT * p - dT * c.CORIOLIS_FORCE * vtb - dT * VI * q -
-         dT * (c.Windx - S.Tsxw[i * w + j]) / Hu;
+         dT * (c.Windx - S.Tsxw[g]) * rH;
   P.c2 = c.dTchia2dX * Hu;
-  P.a2 = -c.dTchia2dX * S.Htdu[(i - 1) * w + j];
-  P.d2 = S.z[i * w + j] -
-         c.dTchia2dY * (S.Htdv[i * w + j] * v[i * w + j] - S.Htdv[i * w + j - 1] * v[i * w + j - 1]);
+  P.a2 = -c.dTchia2dX * S.Htdu[g - w];
+  P.d2 = S.z[g] - c.dTchia2dY * (S.Htdv[g] * v[g] - S.Htdv[g - 1] * v[g - 1]);
   return P;
 }
 
 // _vzSolver_calculate_preindex (UVZSolver_multithread.cpp:142-208).
 __device__ __forceinline__ Pre pre_y(const State& S, const Coef& c, int i, int j) {
   const int w = S.W;
+  const int g = i * w + j;
   const double* u = S.u;
   const double* v = S.v;
   const double* Hm = S.Hmoi;
   Pre P;
   double p = 0.0, q = 0.0;
-  const double utb =
-      (u[(i - 1) * w + j] + u[i * w + j] + u[(i - 1) * w + j + 1] + u[i * w + j + 1]) * 0.25;
-  const double vv = v[i * w + j], VI = S.visco[i * w + j], Hv = S.Htdv[i * w + j];
+  const double utb = (u[g - w] + u[g] + u[g - w + 1] + u[g + 1]) * 0.25;
+  const double vv = v[g], VI = S.visco[g], Hv = S.Htdv[g];
   const double dT = c.dT;
-  P.f1 = c.dTchia2dY * vv + VI * dT / c.dYbp;
-  P.f2 = -(2 + S.Ky1[i * w + j] * dT * sqrt(vv * vv + utb * utb) / Hv + (2 * dT * VI) / c.dYbp);
-  P.f3 = dT * VI / c.dYbp - c.dTchia2dY * vv;
-  if (Hm[(i - 1) * w + j] <= c.H_TINH) {
+  const double rH = 1.0 / Hv;
+  const double visc = VI * c.dT_dYbp;
+  P.f1 = c.dTchia2dY * vv + visc;
+  P.f2 = -(2 + S.Ky1[g] * dT * sqrt(vv * vv + utb * utb) * rH + 2 * visc);
+  P.f3 = visc - c.dTchia2dY * vv;
+  if (Hm[g - w] <= c.H_TINH) {
     if (utb < 0) {
-      q = utb * (-3 * vv + 4 * v[(i + 1) * w + j] - v[(i + 2) * w + j]) / c.dX2;
-      p = (vv - 2 * v[(i + 1) * w + j] + v[(i + 2) * w + j]) / c.dXbp;
+      q = utb * (-3 * vv + 4 * v[g + w] - v[g + 2 * w]) * c.r_dX2;
+      p = (vv - 2 * v[g + w] + v[g + 2 * w]) * c.r_dXbp;
     }
   } else {
-    if (Hm[(i + 1) * w + j] <= c.H_TINH) {
-      if ((Hm[(i - 2) * w + j] > c.H_TINH) && (utb > 0)) {
-        q = utb * (3 * vv - 4 * v[(i - 1) * w + j] + v[(i - 2) * w + j]) / c.dX2;
-        p = (vv - 2 * v[(i - 1) * w + j] + v[(i - 2) * w + j]) / c.dXbp;
+    if (Hm[g + w] <= c.H_TINH) {
+      if ((Hm[g - 2 * w] > c.H_TINH) && (utb > 0)) {
+        q = utb * (3 * vv - 4 * v[g - w] + v[g - 2 * w]) * c.r_dX2;
+        p = (vv - 2 * v[g - w] + v[g - 2 * w]) * c.r_dXbp;
       }
     } else {
-      q = utb * (v[(i + 1) * w + j] - v[(i - 1) * w + j]) / c.dX2;
-      p = (v[(i + 1) * w + j] - 2 * vv + v[(i - 1) * w + j]) / c.dXbp;
+      q = utb * (v[g + w] - v[g - w]) * c.r_dX2;
+      p = (v[g + w] - 2 * vv + v[g - w]) * c.r_dXbp;
     }
   }
   P.f5 = -2 * vv + dT * q + dT * c.CORIOLIS_FORCE * utb - dT * VI * p -
-         dT * (c.Windy - S.Tsyw[i * w + j]) / Hv;
+         dT * (c.Windy - S.Tsyw[g]) * rH;
   P.c2 = c.dTchia2dY * Hv;
-  P.a2 = -c.dTchia2dY * S.Htdv[i * w + j - 1];
-  P.d2 = S.z[i * w + j] -
-         c.dTchia2dX * (S.Htdu[i * w + j] * u[i * w + j] - S.Htdu[(i - 1) * w + j] * u[(i - 1) * w + j]);
+  P.a2 = -c.dTchia2dY * S.Htdv[g - 1];
+  P.d2 = S.z[g] - c.dTchia2dX * (S.Htdu[g] * u[g] - S.Htdu[g - w] * u[g - w]);
   return P;
 }
 
@@ -107,20 +114,23 @@ __device__ __forceinline__ Mom abcd(const Pre& P, const Pre& Pn, int k, int firs
   Mom m;
   if (last - 1 > first) {
     if (br1 && k == first) {
+      const double rc = P.f3 / Pn.c2;
       m.a1 = f4;
-      m.b1 = P.f2 - (P.f3 * Pn.a2 / Pn.c2);
-      m.c1 = -f4 - (P.f3 / Pn.c2);
-      m.d1 = P.f5 - (P.f3 * Pn.d2 / Pn.c2);
+      m.b1 = P.f2 - rc * Pn.a2;
+      m.c1 = -f4 - rc;
+      m.d1 = P.f5 - rc * Pn.d2;
     } else if (br2 && k == last - 1) {
-      m.a1 = f4 - P.f1 / P.a2;
-      m.b1 = P.f2 - (P.f1 * P.c2 / P.a2);
+      const double ra = P.f1 / P.a2;
+      m.a1 = f4 - ra;
+      m.b1 = P.f2 - ra * P.c2;
       m.c1 = -f4;
-      m.d1 = P.f5 - (P.f1 * P.d2 / P.a2);
+      m.d1 = P.f5 - ra * P.d2;
     } else {
-      m.a1 = f4 - P.f1 / P.a2;
-      m.c1 = -f4 - (P.f3 / Pn.c2);
-      m.b1 = P.f2 - (P.f1 * P.c2 / P.a2) - (P.f3 * Pn.a2 / Pn.c2);
-      m.d1 = P.f5 - (P.f1 * P.d2 / P.a2) - (P.f3 * Pn.d2 / Pn.c2);
+      const double ra = P.f1 / P.a2, rc = P.f3 / Pn.c2;
+      m.a1 = f4 - ra;
+      m.c1 = -f4 - rc;
+      m.b1 = P.f2 - ra * P.c2 - rc * Pn.a2;
+      m.d1 = P.f5 - ra * P.d2 - rc * Pn.d2;
     }
   } else {
     m.a1 = f4;
@@ -130,36 +140,6 @@ __device__ __forceinline__ Mom abcd(const Pre& P, const Pre& Pn, int k, int firs
   }
   return m;
 }
-
-// Streaming Thomas forward pass (tridiag, UVZSolver_multithread.cpp:19-43):
-// rows arrive in order k = 0..sn; Ap/Bp go to scratch.
-struct ThomasFwd {
-  double ap, bp, xs;
-  int sn;
-  double* Ap;
-  double* Bp;
-  int ld;
-  __device__ __forceinline__ void row(int k, int r, double A, double B, double Cc, double D) {
-    if (k == 0) {
-      if (sn == 0) {
-        xs = D / B;
-        return;
-      }
-      ap = -Cc / B;
-      bp = D / B;
-      Ap[(size_t)r * ld] = ap;
-      Bp[(size_t)r * ld] = bp;
-    } else if (k < sn) {
-      const double ep = A * ap + B;
-      ap = -Cc / ep;
-      bp = (D - (A * bp)) / ep;
-      Ap[(size_t)r * ld] = ap;
-      Bp[(size_t)r * ld] = bp;
-    } else {
-      xs = (D - (A * bp)) / (B + (A * ap));
-    }
-  }
-};
 
 // Layout of one line's solve: which of the reference's assembly variants
 // applies (UVZSolver_multithread.cpp:377-465) and where the system ends.
@@ -208,25 +188,6 @@ __device__ __forceinline__ LineSys line_sys(int first, int last, bool br1, bool 
   }
   L.sn = sn;
   return L;
-}
-
-// Coefficients of absolute row r of a line's system (see line_sys).
-__device__ __forceinline__ void row_of(const LineSys& L, int r, const Pre& Pi, const Mom& Mi,
-                                       const Pre& Pi1, double& A, double& B, double& Cc,
-                                       double& D) {
-  const bool even = (r & 1) == 0;
-  if (L.ran == even) {  // continuity row of cell i (ran) / cell i+1 (lon)
-    const Pre& P = L.ran ? Pi : Pi1;
-    A = P.a2;
-    B = 1;
-    Cc = P.c2;
-    D = P.d2;
-  } else {  // momentum row of cell i
-    A = Mi.a1;
-    B = Mi.b1;
-    Cc = Mi.c1;
-    D = Mi.d1;
-  }
 }
 
 }  // namespace hyd

@@ -24,6 +24,9 @@ struct Coef {
   double NDnen, Tod, Toe, hstoe, ghtoe, Mbochat;
   double ro, ros, dm, muy, d90, Dorong, Sx;
   double CORIOLIS_FORCE, g, Ks, Windx, Windy, Ufr, Dxr, wss;
+  // reciprocals and products of constants, so that the kernels multiply
+  // where the reference divides by a constant (one rounding of difference)
+  double r_dX2, r_dY2, r_dXbp, r_dYbp, dT_dXbp, dT_dYbp, sqrt_g;
 };
 
 // Device error codes recorded in State::err[0].

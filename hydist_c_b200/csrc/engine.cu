@@ -84,6 +84,13 @@ void derive(const HydistParams& p, Coef& c) {
                            (std::sqrt(1 + 0.01 * (c.Sx - 1) * 9.81 * std::pow(c.dm, 3) /
                                               std::pow(c.muy, 2)) -
                             1);
+  c.r_dX2 = 1.0 / c.dX2;
+  c.r_dY2 = 1.0 / c.dY2;
+  c.r_dXbp = 1.0 / c.dXbp;
+  c.r_dYbp = 1.0 / c.dYbp;
+  c.dT_dXbp = c.dT / c.dXbp;
+  c.dT_dYbp = c.dT / c.dYbp;
+  c.sqrt_g = std::sqrt(c.g);
 }
 
 }  // namespace

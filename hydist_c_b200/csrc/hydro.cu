@@ -1,28 +1,27 @@
 // hydro.cu -- hydraulic ADI half-steps and the wet/dry bookkeeping on the GPU.
 //
 // Kernels (reference kernel each one replaces in brackets):
-//   k_onetime_init     [Onetime_init, support_funcs.cpp:21-69]
-//   k_interp_fs_rows   [Interpolate_FS_ng, support_funcs.cpp:191-213]
-//   k_interp_fs_col    [Interpolate_FS_d, support_funcs.cpp:215-237]
-//   k_scan_rows/cols   [Find_Calculation_limits_Horizontal/Vertical, :238-343]
-//   k_htuongdoi        [Htuongdoi, :346-362]
-//   k_preprocess       [preprocess_data, :482-601]
-//   k_boundary         [Update_Boundary_Value/Boundary_value/FS_boundary, :603-728]
-//   k_sweep_x          [UZSolver_calculate_preindex/abcd/matrix_coeff +
-//                       tridiagSolver + UZSolver_extract_solution,
-//                       UVZSolver_multithread.cpp:19-43, 78-139, 210-470,
-//                       547-603, 861-933]: one thread per column, the whole
-//                       half-step solve of that column fused.
-//   k_sweep_y          [the VZSolver_* kernels, :142-208, 472-544, 798-859]
-//   k_smooth / k_smooth_commit [Normalize/_normalize/update_buffer, :761-808]
-//   k_solve_v / k_solve_u      [solveV/vSolver, solveU/uSolver, :607-795, 938-978]
-//   k_margin_v / k_margin_u    [update_margin_elem_V/U, :980-1060]
-//   k_commit           [update_h_moi + update_uvz, support_funcs.cpp:71-86, 732-759]
-//   k_reset_vertical   [Reset_states_vertical, :142-188]
+//   k_onetime_init      [Onetime_init, support_funcs.cpp:21-69]
+//   k_interp_fs_rows    [Interpolate_FS_ng, support_funcs.cpp:191-213]
+//   k_interp_fs_col     [Interpolate_FS_d, support_funcs.cpp:215-237]
+//   k_runs_flags/sort   [Find_Calculation_limits_Horizontal/Vertical, :238-343]
+//   k_htuongdoi         [Htuongdoi, :346-362] (set-up; per step in the commits)
+//   k_preprocess_sides  [preprocess_data, :482-601]
+//   k_tick, k_boundary  [Update_Boundary_Value/Boundary_value/FS_boundary, :603-728]
+//   the line sweeps     [UZSolver_*/VZSolver_* + tridiagSolver,
+//                        UVZSolver_multithread.cpp:19-139, 142-603, 798-933]:
+//                        sweep.cu on the partitioned solver of linesolve.cuh
+//   k_smooth_full       [Normalize/_normalize/update_buffer, :761-808]
+//   k_solve_v/k_solve_u [solveV/vSolver, solveU/uSolver, :607-795, 938-978]
+//   k_margin_v/k_margin_u [update_margin_elem_V/U, :980-1060]
+//   k_commit_a          [update_h_moi + update_uvz + Htuongdoi, :71-86, 732-759, 346-362]
+//   k_hmoi_flags, k_wetting, k_commit_b, k_dry_mask
+//                       [update_h_moi + Reset_states_vertical + update_uvz +
+//                        Htuongdoi, support_funcs.cpp:71-86, 142-188, 732-759]
 //
-// The arithmetic of every formula follows the reference's expression order;
-// nvcc may fuse a multiply and an add into one FMA, which the CPU oracle
-// does not, so results agree to rounding, not bit for bit.
+// Formulas keep the reference's structure; nvcc may fuse a multiply and an
+// add into one FMA, which the CPU oracle does not, so results agree to
+// rounding, not bit for bit.
 #include <cstdio>
 
 #include "assembly.cuh"
@@ -369,6 +368,67 @@ __global__ void k_preprocess(State S, Coef c) {
   S.hmax[3] = mr != 0 ? 1.0 / (ros * mr) : mr;
 }
 
+// preprocess_data with one CTA per side: the per-cell powers in parallel,
+// each segment's sum in the reference's order by one thread (so the sums
+// round as the reference's), the boundary-depth maximum by one thread.
+// side: 0 up (column M), 1 down (column 2, node column 1), 2 left (row 2,
+// node row 1), 3 right (row N).
+__global__ void k_preprocess_sides(State S, Coef c, double* p53) {
+  const int side = blockIdx.x;
+  const int W = S.W, M = S.M, N = S.N;
+  const double dX = c.dX, ND = c.NANGDAY, ros = c.ros;
+  const bool col = side < 2;
+  const int loc = side == 0 ? M : (side == 3 ? N : 2);
+  const int* moc = col ? S.mocj : S.moci;
+  const int* dau = col ? S.dauj : S.daui;
+  const int* cuoi = col ? S.cuoij : S.cuoii;
+  double* hi = S.hi + (side == 0 ? 0 : side == 1 ? (N + 3) : side == 2 ? 2 * (N + 3) : 2 * (N + 3) + (M + 3));
+  double* pw = p53 + side * (max(M, N) + 3);
+  __shared__ double sums[SEG];
+  const int nseg = moc[loc];
+  for (int k = 0; k < nseg; ++k) {
+    const int a = dau[loc * SEG + k], b = cuoi[loc * SEG + k];
+    for (int p = a + threadIdx.x; p <= b; p += blockDim.x) {
+      double v;
+      if (side == 0) v = (S.h[p * W + M] + S.h[(p - 1) * W + M]) / 2.0 - ND;
+      else if (side == 1) v = (S.h[p * W + 1] + S.h[(p - 1) * W + 1]) / 2.0 - ND;
+      else if (side == 2) v = (S.h[1 * W + p] + S.h[1 * W + p - 1]) / 2.0 - ND;
+      else v = (S.h[N * W + p] + S.h[N * W + p - 1]) / 2.0 - ND;
+      hi[p] = v;
+      pw[p] = pow(v, 5.0 / 3.0);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < nseg) {
+    const int k = threadIdx.x;
+    double sum = 0;
+    for (int p = dau[loc * SEG + k]; p <= cuoi[loc * SEG + k]; ++p) sum += pw[p];
+    sums[k] = sum;
+  }
+  __syncthreads();
+  for (int k = 0; k < nseg; ++k) {
+    const int a = dau[loc * SEG + k], b = cuoi[loc * SEG + k];
+    for (int p = a + threadIdx.x; p <= b; p += blockDim.x)
+      hi[p] = pow(hi[p], 2.0 / 3.0) / (sums[k] * dX);
+  }
+  if (threadIdx.x == 0) {
+    const double* hb = S.htaiz_bd;
+    double mx;
+    if (side == 0 || side == 1) {
+      const int jj = side == 0 ? M : 2;
+      mx = hb[2 * W + jj];
+      for (int i = 3; i < N; ++i)
+        if (hb[i * W + jj] > mx) mx = hb[i * W + jj];
+    } else {
+      const int ii = side == 2 ? 2 : N;
+      mx = hb[ii * W + 2];
+      for (int j = 3; j < M; ++j)
+        if (hb[ii * W + j] > mx) mx = hb[ii * W + j];
+    }
+    S.hmax[side] = mx != 0 ? 1.0 / (ros * mx) : mx;
+  }
+}
+
 // ------------------------------------------------------------- boundary
 // The simulated time lives on the device so that a captured step replays
 // unchanged: advanced by t += dT/2 per half-step (engine.cpp:66, 176).
@@ -427,271 +487,6 @@ __global__ void k_boundary(State S) {
 
 // ---------------------------------------------------- ADI line sweeps
 // (per-cell assembly: assembly.cuh)
-// One column sweep (x direction, implicit in i) of column j. Assembly,
-// Thomas and extraction fused; the column's cells are visited in order of
-// i, so a warp of 32 adjacent columns reads 32 contiguous doubles per field.
-__global__ void __launch_bounds__(128) k_sweep_x(State S, Coef c) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
-  if (j > S.M) return;
-  const int w = S.W, N = S.N;
-  const double f4 = 2 * c.g * c.dTchia2dX;
-  double* Ap = S.Ap + j;
-  double* Bp = S.Bp + j;
-  const int ld = S.ld;
-  for (int k = 0; k < S.mocj[j]; ++k) {
-    const int first = S.dauj[j * SEG + k], last = S.cuoij[j * SEG + k];
-    // locate_segment_u end flags (support_funcs.cpp:845-851)
-    const bool br1 = (first > 2) || ((first == 2) && ((S.h[1 * w + j] + S.h[1 * w + j - 1]) * 0.5 == c.NANGDAY));
-    const bool br2 = (last < N) || ((last == N) && ((S.h[N * w + j] + S.h[N * w + j - 1]) * 0.5 == c.NANGDAY));
-    const LineSys L = line_sys(first, last, br1, br2, S.bienQ[2] != 0, S.bienQ[3] != 0, N);
-    const double ubt = S.ubt[j], ubp = S.ubp[j];
-    const double TZ_r = S.tz[last * w + j], TZ_l = S.tz[first * w + j];
-    ThomasFwd F;
-    F.sn = L.sn;
-    F.Ap = Ap;
-    F.Bp = Bp;
-    F.ld = ld;
-    F.ap = F.bp = F.xs = 0;
-    const int rend = L.off + L.sn;  // last row of the system
-    Pre Pfirst, Plast;
-    Pre Pc = pre_x(S, c, first, j);
-    Pfirst = Pc;
-    Pre Pn = (first < last) ? pre_x(S, c, first + 1, j) : Pc;
-    for (int i = first; i <= last && L.sn >= 0; ++i) {
-      Mom Mi;
-      if (i <= last - 1 || (i == first)) Mi = abcd(Pc, Pn, i, first, last, f4, br1, br2);
-      else Mi = Mom{0, 0, 0, 0};
-      if (i == last) Plast = Pc;
-      // rows 2i and 2i+1 (those inside [off, rend])
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int r = 2 * i + e;
-        if (r < L.off || r > rend) continue;
-        double A, B, Cc, D;
-        row_of(L, r, Pc, Mi, Pn, A, B, Cc, D);
-        if (r == L.off) {
-          if (L.ran) D = L.qfirst ? (Pfirst.d2 - Pfirst.a2 * ubt) : Pfirst.d2;
-          else D = Mi.d1 - Mi.a1 * TZ_l;
-        }
-        if (r == rend) {
-          if (L.last_kind == 1) {
-            const Pre& PL = (i == last) ? Pc : Pn;
-            A = PL.a2;
-            B = 1;
-            D = PL.d2 - PL.c2 * ubp;
-          } else if (L.last_kind == 2) {
-            A = Mi.a1;
-            B = Mi.b1;
-            D = Mi.d1 - Mi.c1 * TZ_r;
-          } else {
-            const Pre& PL = (i == last) ? Pc : Pn;
-            A = PL.a2;
-            B = 1;
-            D = PL.d2;
-          }
-        }
-        F.row(r - L.off, r, A, B, Cc, D);
-      }
-      Pc = Pn;
-      if (i + 2 <= last) Pn = pre_x(S, c, i + 2, j);
-    }
-    if (L.sn < 0) Plast = pre_x(S, c, last, j);
-    // back substitution with extraction (_uzSolver_extract_solution,
-    // UVZSolver_multithread.cpp:547-603)
-    const bool ranx = br1 || (S.bienQ[2] && first == 2);
-    const double tu_old = S.tu[(last - 1) * w + j];
-    double xr = (L.sn >= 0) ? F.xs : 0.0;  // x at row rend
-    const double x_last = xr;
-    double tu_lm1_new = tu_old;
-    // walk rows rend-1 .. off
-    auto emit = [&](int r, double x) {
-      // r is absolute; map to (cell, variable)
-      if (ranx) {
-        const int i = r >> 1;
-        if (i >= first && i < last) {
-          if (r & 1) {
-            S.tu[i * w + j] = x;
-            if (i == last - 1) tu_lm1_new = x;
-          } else {
-            S.tz[i * w + j] = x;
-          }
-        }
-      } else {
-        if (r == 2 * first) {
-          S.tu[first * w + j] = x;
-          if (first == last - 1) tu_lm1_new = x;
-        } else {
-          const int i = (r + 1) >> 1;  // r = 2i-1 -> z[i], r = 2i -> u[i]
-          if (i > first && i < last) {
-            if (r & 1) S.tz[i * w + j] = x;
-            else {
-              S.tu[i * w + j] = x;
-              if (i == last - 1) tu_lm1_new = x;
-            }
-          }
-        }
-      }
-    };
-    if (L.sn >= 0) {
-      emit(rend, xr);
-      for (int r = rend - 1; r >= L.off; --r) {
-        const double x = Bp[(size_t)r * ld] + Ap[(size_t)r * ld] * xr;
-        emit(r, x);
-        xr = x;
-      }
-    }
-    if (first < last) {
-      if (br1) S.tu[(first - 1) * w + j] = 0;
-      else if (S.bienQ[2] && first == 2) S.tu[(first - 1) * w + j] = ubt;
-      else {
-        // t_z[first] is the boundary value (not written by the solve)
-        S.tu[(first - 1) * w + j] =
-            (Pfirst.d2 - S.tz[first * w + j] - Pfirst.c2 * S.tu[first * w + j]) / Pfirst.a2;
-      }
-    }
-    // last end
-    if (br2) {
-      S.tu[last * w + j] = 0;
-      S.tz[last * w + j] = x_last;
-    } else if (S.bienQ[3] && last == N) {
-      S.tu[last * w + j] = ubp;
-      S.tz[last * w + j] = x_last;
-    } else {
-      const double nb = S.race_new ? tu_lm1_new : tu_old;
-      S.tu[last * w + j] = (Plast.d2 - Plast.a2 * nb - S.tz[last * w + j]) / Plast.c2;
-    }
-  }
-}
-
-// One row sweep (y direction, implicit in j) of row i; extraction reaches
-// columns j <= N only (VZSolver_extract_solution, :851).
-__global__ void __launch_bounds__(128) k_sweep_y(State S, Coef c) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
-  if (i > S.N) return;
-  const int w = S.W, M = S.M, N = S.N;
-  const double f4 = 2 * c.g * c.dTchia2dY;
-  double* Ap = S.Ap + i;
-  double* Bp = S.Bp + i;
-  const int ld = S.ld;
-  for (int k = 0; k < S.moci[i]; ++k) {
-    const int first = S.daui[i * SEG + k], last = S.cuoii[i * SEG + k];
-    // locate_segment_v end flags (support_funcs.cpp:823-826)
-    const bool br1 = (first > 2) || ((first == 2) && ((S.h[i * w + first - 1] + S.h[(i - 1) * w + first - 1]) * 0.5 == c.NANGDAY));
-    const bool br2 = (last < M) || ((last == M) && ((S.h[i * w + last] + S.h[(i - 1) * w + last]) * 0.5 == c.NANGDAY));
-    const LineSys L = line_sys(first, last, br1, br2, S.bienQ[1] != 0, S.bienQ[0] != 0, M);
-    const double vbd = S.vbd[i], vbt = S.vbt[i];
-    const double TZ_r = S.tz[i * w + last], TZ_l = S.tz[i * w + first];
-    ThomasFwd F;
-    F.sn = L.sn;
-    F.Ap = Ap;
-    F.Bp = Bp;
-    F.ld = ld;
-    F.ap = F.bp = F.xs = 0;
-    const int rend = L.off + L.sn;
-    Pre Pfirst, Plast;
-    Pre Pc = pre_y(S, c, i, first);
-    Pfirst = Pc;
-    Pre Pn = (first < last) ? pre_y(S, c, i, first + 1) : Pc;
-    for (int jj = first; jj <= last && L.sn >= 0; ++jj) {
-      Mom Mi;
-      if (jj <= last - 1 || jj == first) Mi = abcd(Pc, Pn, jj, first, last, f4, br1, br2);
-      else Mi = Mom{0, 0, 0, 0};
-      if (jj == last) Plast = Pc;
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int r = 2 * jj + e;
-        if (r < L.off || r > rend) continue;
-        double A, B, Cc, D;
-        row_of(L, r, Pc, Mi, Pn, A, B, Cc, D);
-        if (r == L.off) {
-          if (L.ran) D = L.qfirst ? (Pfirst.d2 - Pfirst.a2 * vbd) : Pfirst.d2;
-          else D = Mi.d1 - Mi.a1 * TZ_l;
-        }
-        if (r == rend) {
-          if (L.last_kind == 1) {
-            const Pre& PL = (jj == last) ? Pc : Pn;
-            A = PL.a2;
-            B = 1;
-            D = PL.d2 - PL.c2 * vbt;
-          } else if (L.last_kind == 2) {
-            A = Mi.a1;
-            B = Mi.b1;
-            D = Mi.d1 - Mi.c1 * TZ_r;
-          } else {
-            const Pre& PL = (jj == last) ? Pc : Pn;
-            A = PL.a2;
-            B = 1;
-            D = PL.d2;
-          }
-        }
-        F.row(r - L.off, r, A, B, Cc, D);
-      }
-      Pc = Pn;
-      if (jj + 2 <= last) Pn = pre_y(S, c, i, jj + 2);
-    }
-    if (L.sn < 0) Plast = pre_y(S, c, i, last);
-    const bool ranx = br1 || (S.bienQ[1] && first == 2);
-    const double tv_old = S.tv[i * w + last - 1];
-    double xr = (L.sn >= 0) ? F.xs : 0.0;
-    const double x_last = xr;
-    double tv_lm1_new = tv_old;
-    auto emit = [&](int r, double x) {
-      if (ranx) {
-        const int jj = r >> 1;
-        if (jj >= first && jj < last && jj <= N) {
-          if (r & 1) {
-            S.tv[i * w + jj] = x;
-            if (jj == last - 1) tv_lm1_new = x;
-          } else {
-            S.tz[i * w + jj] = x;
-          }
-        }
-      } else {
-        if (r == 2 * first) {
-          if (first <= N) S.tv[i * w + first] = x;
-          if (first == last - 1) tv_lm1_new = x;
-        } else {
-          const int jj = (r + 1) >> 1;
-          if (jj > first && jj < last && jj <= N) {
-            if (r & 1) S.tz[i * w + jj] = x;
-            else {
-              S.tv[i * w + jj] = x;
-              if (jj == last - 1) tv_lm1_new = x;
-            }
-          }
-        }
-      }
-    };
-    if (L.sn >= 0) {
-      emit(rend, xr);
-      for (int r = rend - 1; r >= L.off; --r) {
-        const double x = Bp[(size_t)r * ld] + Ap[(size_t)r * ld] * xr;
-        emit(r, x);
-        xr = x;
-      }
-    }
-    if (first < last && first <= N) {
-      if (br1) S.tv[i * w + first - 1] = 0;
-      else if (S.bienQ[1] && first == 2) S.tv[i * w + first - 1] = vbd;
-      else
-        S.tv[i * w + first - 1] =
-            (Pfirst.d2 - S.tz[i * w + first] - Pfirst.c2 * S.tv[i * w + first]) / Pfirst.a2;
-    }
-    if (last <= N) {
-      if (br2) {
-        S.tv[i * w + last] = 0;
-        S.tz[i * w + last] = x_last;
-      } else if (S.bienQ[0] && last == M) {
-        S.tv[i * w + last] = vbt;
-        S.tz[i * w + last] = x_last;
-      } else {
-        const double nb = S.race_new ? tv_lm1_new : tv_old;
-        S.tv[i * w + last] = (Plast.d2 - Plast.a2 * nb - S.tz[i * w + last]) / Plast.c2;
-      }
-    }
-  }
-}
-
 // ------------------------------------------------------------ smoothing
 // _normalize (support_funcs.cpp:761-782): tmp <- smoothed value, interior.
 // The same smoothing into a complete array (su / sv): smoothed on the
@@ -1074,7 +869,8 @@ void launch_init(const State& S, const Coef& c, cudaStream_t st) {
   k_onetime_init<<<dim3(cdiv(S.W, 128), S.H), 128, 0, st>>>(S, c);
   launch_find_limits(S, c, st, nullptr);
   k_htuongdoi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
-  k_preprocess<<<1, 32, 0, st>>>(S, c);
+  // the per-side scratch of the powers: the line-solver scratch is free here
+  k_preprocess_sides<<<4, 256, 0, st>>>(S, c, S.lscratch);
 }
 
 void launch_scan_segments(const State& S, cudaStream_t st) {

@@ -11,9 +11,10 @@
 //   pass A  each chunk eliminates its interior rows forward, keeping the
 //           spike of the unknown left of the chunk: x_r = y'_r + v'_r x_L
 //           - c'_r x_{r+1}; (c', y', v') go to an L2-resident scratch slot;
-//           the chunk's last unknown is a separator;
-//   pass B  backward over the interior gives the first and last interior
-//           rows in terms of the two neighbouring separators;
+//           the chunk's last unknown is a separator. The first interior
+//           row in terms of both neighbouring separators is accumulated on
+//           the way (x_0 = sum_k P_k (y'_k + v'_k x_L) + P_L x_R with
+//           P_{k+1} = -c'_k P_k), the last one is the final state;
 //   reduce  the separators form a tridiagonal Schur-complement system of P
 //           unknowns per line, solved by parallel cyclic reduction in
 //           shared memory;
@@ -95,6 +96,9 @@ __global__ void __launch_bounds__(LPB * P, 1) k_line_solve(Gen G) {
       typename Gen::Walker W;
       W.init(G, LS, line, c0);
       double cp = 0, yp = 0, vp = 0;
+      // first interior row in terms of both separators, accumulated forward:
+      // x_0 = sum_k P_k (y'_k + v'_k x_L) + P_L x_R, P_0 = 1, P_{k+1} = -c'_k P_k
+      double Pk = 1, fy = 0, fv = 0;
       int s = 0;
       for (int c = c0; c < c1; ++c) {
         W.cell(G, LS, c);
@@ -123,24 +127,19 @@ __global__ void __launch_bounds__(LPB * P, 1) k_line_solve(Gen G) {
             sc_c[o] = cp;
             sc_y[o] = yp;
             sc_v[o] = vp;
+            fy += Pk * yp;
+            fv += Pk * vp;
+            Pk *= -cp;
           }
         }
       }
-      // ---- pass B: interior rows in terms of the neighbouring separators
-      double y = yp, v = vp, w = -cp;
-      sh.tri[3][cidx] = y;
-      sh.tri[4][cidx] = v;
-      sh.tri[5][cidx] = w;
-      for (int t = nu - 3; t >= 0; --t) {
-        const size_t o = (size_t)(q0 + t) * LPB + l;
-        const double cc = sc_c[o];
-        y = sc_y[o] - cc * y;
-        v = sc_v[o] - cc * v;
-        w = -cc * w;
-      }
-      sh.tri[0][cidx] = y;
-      sh.tri[1][cidx] = v;
-      sh.tri[2][cidx] = w;
+      // first and last interior rows in terms of the neighbouring separators
+      sh.tri[0][cidx] = fy;
+      sh.tri[1][cidx] = fv;
+      sh.tri[2][cidx] = Pk;
+      sh.tri[3][cidx] = yp;
+      sh.tri[4][cidx] = vp;
+      sh.tri[5][cidx] = -cp;
     }
     __syncthreads();
     // ---- reduced (Schur complement) system of the separators
@@ -203,6 +202,7 @@ __global__ void __launch_bounds__(LPB * P, 1) k_line_solve(Gen G) {
       E.init(G, LS, line);
       E.emit(G, LS, sh.xlast[l], q0 + nu - 1, xr);
       double xn = xr;
+#pragma unroll 4
       for (int t = nu - 2; t >= 0; --t) {
         const size_t o = (size_t)(q0 + t) * LPB + l;
         const double x = sc_y[o] + sc_v[o] * xl - sc_c[o] * xn;
