@@ -181,6 +181,8 @@ def _declare(lib):
     lib.hydist_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
     lib.hydist_gtsv_batched.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32,
                                         C.c_int32, vp]
+    lib.hydist_gtsv_batched_noalloc.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int32,
+                                                C.c_int32, C.c_int32, vp]
 
 
 class HydistError(RuntimeError):
@@ -199,7 +201,7 @@ EXPORTED_SYMBOLS = [
     "hydist_last_error", "hydist_version", "hydist_create", "hydist_destroy", "hydist_step",
     "hydist_sync", "hydist_get_time", "hydist_set_time", "hydist_download", "hydist_upload", "hydist_mass",
     "hydist_step_graph", "hydist_stream", "hydist_gtsv_batched", "hydist_step_traced",
-    "hydist_kernel_launches",
+    "hydist_kernel_launches", "hydist_gtsv_batched_noalloc",
 ]
 
 PHASES = ["boundary_x", "sweep_x", "explicit_v", "commit_x", "sediment_x",

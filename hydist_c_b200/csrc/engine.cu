@@ -225,6 +225,12 @@ double* field_ptr(HydistHandle* h, int f) {
 
 }  // namespace
 
+namespace hyd {
+// Lets the other translation units of the library set the message that
+// hydist_last_error() returns.
+void set_last_error(const char* m) { g_err = m; }
+}  // namespace hyd
+
 extern "C" {
 
 const char* hydist_last_error(void) { return g_err.c_str(); }

@@ -211,6 +211,27 @@ int hydist_gtsv_batched(const void* dl, const void* d, const void* du,
                         const int32_t* lengths, int32_t nsys, int32_t dtype,
                         int32_t algo, void* stream);
 
+/* Allocation-free batched Thomas solve (no counterpart in the reference,
+ * whose gtsv allocates per call). Same arrays and results as
+ * hydist_gtsv_batched with algo = 1, for callers that must not allocate
+ * device memory while they run. The forward-sweep scratch is a fixed array
+ * of HYDIST_GTSV_NOALLOC_MAX_ROWS rows inside the library (8 MiB per device,
+ * reserved when the library is loaded on the device); nothing is allocated
+ * by any call.
+ *   rows   packed rows of the arrays: every system must lie in [0, rows);
+ *          a system outside is left unsolved. rows above the limit return
+ *          HYDIST_ERR_BUDGET without launching anything.
+ * The first call on each device (with that device current) looks up the
+ * scratch address; make that call before capturing a stream. Nothing needs
+ * zeroing beforehand. The scratch is shared by all calls on a device, so
+ * calls that overlap in time on one device (two streams or host threads)
+ * race and must be serialised by the caller. */
+#define HYDIST_GTSV_NOALLOC_MAX_ROWS (1 << 20)
+int hydist_gtsv_batched_noalloc(const void* dl, const void* d, const void* du,
+                                const void* b, void* x, const int32_t* offsets,
+                                const int32_t* lengths, int32_t nsys,
+                                int32_t rows, int32_t dtype, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
