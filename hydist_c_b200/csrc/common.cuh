@@ -27,6 +27,7 @@ struct Coef {
   // reciprocals and products of constants, so that the kernels multiply
   // where the reference divides by a constant (one rounding of difference)
   double r_dX2, r_dY2, r_dXbp, r_dYbp, dT_dXbp, dT_dYbp, sqrt_g;
+  double Mb_ros, r_Tod, r_Ufr2, Dxr_m03;  // Mbochat/ros, 1/Tod, 1/Ufr^2, Dxr^-0.3
 };
 
 // Device error codes recorded in State::err[0].

@@ -91,6 +91,10 @@ void derive(const HydistParams& p, Coef& c) {
   c.dT_dXbp = c.dT / c.dXbp;
   c.dT_dYbp = c.dT / c.dYbp;
   c.sqrt_g = std::sqrt(c.g);
+  c.Mb_ros = c.Mbochat / c.ros;
+  c.r_Tod = 1.0 / c.Tod;
+  c.r_Ufr2 = 1.0 / (c.Ufr * c.Ufr);
+  c.Dxr_m03 = std::pow(c.Dxr, -0.3);
 }
 
 }  // namespace

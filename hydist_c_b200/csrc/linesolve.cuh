@@ -61,8 +61,10 @@ struct LSShared {
 // formulas within one ulp.
 __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
 
+// Gen::MIN_BLOCKS: resident CTAs per SM the P = 128 solver is compiled for
+// (2 caps registers at 64 per thread).
 template <class Gen, int P>
-__global__ void __launch_bounds__(LPB * P, 1) k_line_solve(Gen G) {
+__global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_line_solve(Gen G) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   LSShared<P>& sh = *reinterpret_cast<LSShared<P>*>(smem_raw);
   const int tid = threadIdx.x;

@@ -1,4 +1,10 @@
 // sediment_cell.cuh -- per-cell coefficients of the concentration sweeps.
+//
+// The formulas keep the structure of the reference's (sources below); the
+// powers with constant exponents are products and square roots
+// ((1-FS)^4, Pd^2.5, Tx^1.5), pow(Dxr, -0.3) is a constant of Coef, and the
+// divisions by constants and by H_moi are multiplications by reciprocals.
+// Each changes a result by a few roundings at most.
 #pragma once
 
 #include "common.cuh"
@@ -9,15 +15,14 @@ namespace hyd {
 __device__ __forceinline__ double source_chs(const Coef& c, double wsm, double Zf, double fs,
                                              double fw, double vth, double h_moi) {
   double toee = c.Toe;
-  const double todd = c.Tod;
   double S = 0;
   const double tob = c.ro * fw * (vth * vth);
   if (h_moi > c.ghtoe) toee = toee * (1 + c.hstoe * ((h_moi - c.ghtoe)));
   if (tob > toee) {
-    S = c.Mbochat / c.ros * (tob - toee) / toee;
-  } else if (tob < todd) {
-    const double Pd = 1 - (tob / todd);
-    const double beta = 1 + (Zf / (1.25 + 4.75 * pow(Pd, 2.5)));
+    S = c.Mb_ros * (tob - toee) / toee;
+  } else if (tob < c.Tod) {
+    const double Pd = 1 - tob * c.r_Tod;
+    const double beta = 1 + (Zf / (1.25 + 4.75 * (Pd * Pd * sqrt(Pd))));
     const double Cb = beta * fs;
     S = -wsm * Cb * Pd;
   }
@@ -26,67 +31,67 @@ __device__ __forceinline__ double source_chs(const Coef& c, double wsm, double Z
 
 // source_nchs (sediment_transport.cpp:41-49)
 __device__ __forceinline__ double source_nchs(const Coef& c, double wsm, double Zf, double Uf,
-                                              double h_moi, double fs) {
+                                              double r_hmoi, double fs) {
   const double gamac = 0.434 + 5.975 * Zf + 2.888 * Zf * Zf;
-  const double Tx = fmax(0.0, (Uf * Uf - c.Ufr * c.Ufr) / (c.Ufr * c.Ufr));
-  const double Cac = 0.015 * c.dm * pow(Tx, 1.5) * pow(c.Dxr, (-0.3)) / (0.05 * h_moi);
+  const double Tx = fmax(0.0, (Uf * Uf - c.Ufr * c.Ufr) * c.r_Ufr2);
+  const double Cac = 0.015 * c.dm * (Tx * sqrt(Tx)) * c.Dxr_m03 * (20.0 * r_hmoi);
   return wsm * (Cac - gamac * fs);
 }
 
 // One cell's row of a concentration sweep: xdir = _FSj (:204-313), else
-// _FSi (:51-164).
+// _FSi (:51-164). The along-line values are passed in by the caller, which
+// carries them from cell to cell: vel_c / hk_c are the sweep-direction
+// velocity and Htd*K product of this cell (x: tu, Htdu*Kx at pos; y: tv,
+// Htdv*Ky at pos), vel_p / hk_p those of the cell before it (pos-W in x,
+// pos-1 in y).
 __device__ __forceinline__ void fs_cell(const State& S, const Coef& c, bool xdir, int i, int j,
+                                        double vel_c, double hk_c, double vel_p, double hk_p,
                                         double tt, double s_start, double& A, double& B,
                                         double& Cc, double& D) {
   const int w = S.W, pos = i * w + j;
   const double* Hm = S.Hmoi;
   const double* FS = S.FS;
-  const double dX = c.dX, dY = c.dY, dT = c.dT, H_TINH = c.H_TINH;
-  const double cc = 18 * log(12 * Hm[pos] / c.Ks);
-  const double Uf = sqrt(c.g) * fabs(S.VTH[pos]) / cc;
-  const double wsm = c.wss * pow((1 - FS[pos]), 4.0);
+  const double H_TINH = c.H_TINH;
+  const double Hc = Hm[pos], fs = FS[pos], vth = S.VTH[pos];
+  const double rH = 1.0 / Hc;
+  const double cc = 18 * log(12 * Hc / c.Ks);
+  const double Uf = c.sqrt_g * fabs(vth) / cc;
+  const double om = 1 - fs, om2 = om * om;
+  const double wsm = c.wss * (om2 * om2);
   double Zf = 0, Sx;
-  double gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;
-  if (FS[pos] > 0.00001) Zf = wsm / (0.4 * (Uf + 2 * wsm));
+  if (fs > 0.00001) Zf = wsm / (0.4 * (Uf + 2 * wsm));
+  // the i-sweep evaluates gamav before Zf (:247), the j-sweep after it (:109)
+  const double gamav = xdir ? 0.98 : 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;
   if (S.ketdinh)
-    Sx = source_chs(c, wsm, Zf, FS[pos], S.Fw[pos], S.VTH[pos], Hm[pos]);
+    Sx = source_chs(c, wsm, Zf, fs, S.Fw[pos], vth, Hc);
   else
-    Sx = source_nchs(c, wsm, Zf, Uf, Hm[pos], FS[pos]);
+    Sx = source_nchs(c, wsm, Zf, Uf, rH, fs);
   if (tt < s_start) Sx = 0;
+  // along-line terms
+  const double r_d2 = xdir ? c.r_dX2 : c.r_dY2;      // 1 / (2 d)
+  const double r_dd = (xdir ? c.r_dXbp : c.r_dYbp) * rH;  // 1 / (H_moi d^2)
+  const double adv = gamav * 0.5 * (vel_c + vel_p) * r_d2;
+  A = -adv - hk_p * r_dd;
+  Cc = adv - hk_c * r_dd;
+  B = c.HaiChiadT + (hk_c + hk_p) * r_dd;
+  // cross-line terms
+  const int s = xdir ? 1 : w;  // stride across the sweep
+  const double* vx = xdir ? S.tv : S.tu;
+  const double* hx = xdir ? S.Htdv : S.Htdu;
+  const double* kx = xdir ? S.Ky : S.Kx;
+  const double hm1 = Hm[pos - s], hp1 = Hm[pos + s], hm2 = Hm[pos - 2 * s], hp2 = Hm[pos + 2 * s];
+  const double fm = FS[pos - s], fp = FS[pos + s];
   double p = 0, q = 0;
-  if (xdir) {
-    A = -gamav * 0.5 * (S.tu[pos] + S.tu[pos - w]) / (dX * 2) -
-        S.Htdu[pos - w] * S.Kx[pos - w] / (Hm[pos] * (dX * dX));
-    Cc = gamav * 0.5 * (S.tu[pos] + S.tu[pos - w]) / (dX * 2) -
-         S.Htdu[pos] * S.Kx[pos] / (Hm[pos] * (dX * dX));
-    B = 2.0 / dT + (S.Htdu[pos] * S.Kx[pos] + S.Htdu[pos - w] * S.Kx[pos - w]) / (Hm[pos] * (dX * dX));
-    if ((Hm[pos - 1] > H_TINH) && (Hm[pos + 2] > H_TINH)) p = (FS[pos + 1] - FS[pos]);
-    if ((Hm[pos - 2] > H_TINH) && (Hm[pos + 1] > H_TINH)) q = (FS[pos] - FS[pos - 1]);
-    p = (1 / (Hm[pos] * (dY * dY))) * (S.Htdv[pos] * S.Ky[pos] * p - S.Htdv[pos - 1] * S.Ky[pos - 1] * q);
-    if ((Hm[pos - 2] > H_TINH) && (Hm[pos + 2] > H_TINH)) {
-      q = (FS[pos + 1] - FS[pos - 1]) / (dY * 2);
-      q = (S.tv[pos] + S.tv[pos - 1]) * 0.5 * q * gamav;
-    } else {
-      q = 0;
-    }
+  if ((hm1 > H_TINH) && (hp2 > H_TINH)) p = (fp - fs);
+  if ((hm2 > H_TINH) && (hp1 > H_TINH)) q = (fs - fm);
+  p = (rH * (xdir ? c.r_dYbp : c.r_dXbp)) * (hx[pos] * kx[pos] * p - hx[pos - s] * kx[pos - s] * q);
+  if ((hm2 > H_TINH) && (hp2 > H_TINH)) {
+    q = (fp - fm) * (xdir ? c.r_dY2 : c.r_dX2);
+    q = (vx[pos] + vx[pos - s]) * 0.5 * q * gamav;
   } else {
-    gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;
-    A = -gamav * 0.5 * (S.tv[pos - 1] + S.tv[pos]) / (dY * 2) -
-        S.Htdv[pos - 1] * S.Ky[pos - 1] / (Hm[pos] * (dY * dY));
-    Cc = gamav * 0.5 * (S.tv[pos - 1] + S.tv[pos]) / (dY * 2) -
-         S.Htdv[pos] * S.Ky[pos] / (Hm[pos] * (dY * dY));
-    B = 2.0 / dT + (S.Htdv[pos] * S.Ky[pos] + S.Htdv[pos - 1] * S.Ky[pos - 1]) / (Hm[pos] * (dY * dY));
-    if ((Hm[pos + 2 * w] > H_TINH) && (Hm[pos - w] > H_TINH)) p = (FS[pos + w] - FS[pos]);
-    if (Hm[pos - 2 * w] > H_TINH && Hm[pos + w] > H_TINH) q = (FS[pos] - FS[pos - w]);
-    p = (1 / (Hm[pos] * (dX * dX))) * (S.Htdu[pos] * S.Kx[pos] * p - S.Htdu[pos - w] * S.Kx[pos - w] * q);
-    if (Hm[pos + 2 * w] > H_TINH && Hm[pos - 2 * w] > H_TINH) {
-      q = (FS[pos + w] - FS[pos - w]) / (dX * 2);
-      q = (S.tu[pos] + S.tu[pos - w]) * 0.5 * q * gamav;
-    } else {
-      q = 0;
-    }
+    q = 0;
   }
-  D = FS[pos] / (dT * 0.5) - q + p + (Sx / Hm[pos]);
+  D = fs * c.HaiChiadT - q + p + Sx * rH;
 }
 
 }  // namespace hyd

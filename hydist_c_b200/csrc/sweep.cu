@@ -24,6 +24,9 @@ int line_chunks(int ncells, int min_cells) {
 template <int DIR>
 struct HydroGen {
   static constexpr int UPC = 2;
+  // x sweeps (columns, 4 adjacent per warp) run faster with two CTAs per SM
+  // despite the register cap; y sweeps (rows) slower
+  static constexpr int MIN_BLOCKS = DIR == 0 ? 2 : 1;
   State S;
   Coef c;
   double* scratch;
@@ -274,6 +277,7 @@ static void launch_dir(const State& S, const Coef& c, cudaStream_t st, int grid,
 template <int DIR>
 struct FSGen {
   static constexpr int UPC = 1;
+  static constexpr int MIN_BLOCKS = DIR == 0 ? 2 : 1;
   State S;
   Coef c;
   double* scratch;
@@ -319,18 +323,37 @@ struct FSGen {
     d.ran = d.qfirst = d.last_kind = d.xq_first = d.xq_last = 0;
   }
 
+  // sweep-direction diffusivity product Htd*K of cell g
+  __device__ double hk(int g) const {
+    return DIR == 0 ? S.Htdu[g] * S.Kx[g] : S.Htdv[g] * S.Ky[g];
+  }
+
+  // Walks a chunk cell by cell, carrying the previous cell's velocity and
+  // Htd*K product so that each is loaded once.
   struct Walker {
     int lp, si, pos;
     bool in;
+    double tt;             // simulated time of the sweep
+    double vel_c, hk_c;    // this cell
+    double vel_p, hk_p;    // the cell before it along the line
     __device__ void init(const FSGen& G, const LineSeg& LS, int line, int c0) {
       lp = line + 3;
       si = 0;
       in = false;
+      tt = G.S.clock[0];
+      const int g = G.at(lp, c0 + 1);  // the cell before the chunk's first
+      vel_c = G.vel()[g];
+      hk_c = G.hk(g);
     }
     __device__ void cell(const FSGen& G, const LineSeg& LS, int cc) {
       pos = cc + 2;
       while (si < LS.nseg && LS.s[si].last < pos) ++si;
       in = si < LS.nseg && LS.s[si].off <= pos && pos <= LS.s[si].rend;
+      const int g = G.at(lp, pos);
+      vel_p = vel_c;
+      hk_p = hk_c;
+      vel_c = G.vel()[g];
+      hk_c = G.hk(g);
     }
     __device__ void row(const FSGen& G, const LineSeg& LS, int e, double& A, double& B,
                         double& C, double& D) const {
@@ -340,10 +363,11 @@ struct FSGen {
       }
       const SegD& d = LS.s[si];
       const int i = DIR == 0 ? pos : lp, j = DIR == 0 ? lp : pos;
-      fs_cell(G.S, G.c, DIR == 0, i, j, G.S.clock[0], G.s_start, A, B, C, D);
+      fs_cell(G.S, G.c, DIR == 0, i, j, vel_c, hk_c, vel_p, hk_p, tt, G.s_start, A, B, C, D);
       const double* vel = G.vel();
       if (pos == d.first + 1) {
-        if (d.br1 || vel[G.at(lp, d.first)] == 0) B = B + A;
+        // the velocity at the segment's first cell is the previous cell's
+        if (d.br1 || vel_p == 0) B = B + A;
         else D = D - A * G.S.FS[G.at(lp, d.first)];
         A = 0;
       }
