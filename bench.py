@@ -2,7 +2,7 @@
 """Benchmark of the Hydist ADI time step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64|fp32] [--workload sediment-2048x1024|channel-256x128]
+                    [--precision fp64] [--workload sediment-2048x1024|channel-256x128]
 
 A step is one full ADI step (two half-steps, with the concentration sweeps)
 of the 2048x1024 sediment workload: dx=dy=5 m, dt=2 s, seeded synthetic
@@ -36,11 +36,22 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 BYTES_PER_CELL_STEP = {  # algorithmic bytes per interior cell and full step
-    ("fp64", False): 168, ("fp64", True): 232, ("fp32", False): 112, ("fp32", True): 152}
-# algorithmic bytes per interior cell of one x-sweep launch (FP64): reads
-# u, v, z, h, Kx1, visco (6 x 8 B) and the wet/dry mask (4 B), writes the
-# provisional u and z (2 x 8 B)
-SWEEP_BYTES_PER_CELL = {"fp64": 68, "fp32": 40}
+    ("fp64", False): 168, ("fp64", True): 232}
+# Algorithmic bytes per cell of one line-solver launch (FP64), each field the
+# kernel's formulas read counted once and each field it writes once:
+#   hydraulic sweeps: read u, v, z, H_moi, Htdu, Htdv, visco, Kx1 (Ky1),
+#     Tsxw (Tsyw) = 9 x 8 B; write t_z and t_u (t_v) = 2 x 8 B  -> 88 B
+#   concentration sweeps: read FS, H_moi, VTH, Fw, t_u, t_v, Htdu, Htdv, Kx,
+#     Ky = 10 x 8 B; write tFS = 8 B                             -> 88 B
+# The line-solver scratch (3 doubles per unknown, L2-resident) is not counted.
+SWEEP_BYTES_PER_CELL = {"line_solve_hydro_x": 88, "line_solve_hydro_y": 88,
+                        "line_solve_conc_x": 88, "line_solve_conc_y": 88}
+
+
+def sweep_cells(name, N, M):
+    """Cells one launch of a line solver processes (lines x cells per line)."""
+    return {"line_solve_hydro_x": (M - 1) * (N - 1), "line_solve_hydro_y": (N - 1) * (M - 1),
+            "line_solve_conc_x": (M - 3) * (N - 1), "line_solve_conc_y": (N - 3) * (M - 1)}[name]
 
 
 def _peaks():
@@ -210,6 +221,7 @@ def run_ours(args):
         bundle["options"] = dict(bundle["options"], sediment_start=0.0, bed_change_start=0.0)
         spin = 0
     cells = bundle["meta"]["cells"]
+    N, M = bundle["meta"]["N"], bundle["meta"]["M"]
     sim = H.Simulation(bundle, device=dev, precision=prec)
     sed = bundle["options"]["sediment_start"] < 1e11
     # spin-up to the sediment phase (untimed), then warm-up steps
@@ -218,8 +230,6 @@ def run_ours(args):
     # warm-up in the timed mode (a graph is captured on its first step)
     (sim.step_graph if args.graph else sim.step)(max(args.warmup, 3))
     sim.sync()
-    # per-phase device times of one step (tracing), for the roofline
-    phases = sim.step_traced()
     l0 = sim.kernel_launches
     stream = torch.cuda.ExternalStream(sim.stream, device=dev)
     e0 = torch.cuda.Event(enable_timing=True)
@@ -247,23 +257,34 @@ def run_ours(args):
     per_step = [step_ev[k].elapsed_time(step_ev[k + 1]) for k in range(args.steps)]
     ms_max = max_over_ranks(ms, ws)
     value = ws * cells * args.steps / (ms_max * 1e-3)
-    # dominant kernel: the longest phase of the traced step
+    # per-kernel times: the same K steps again, each traced (an event at the
+    # end of every phase and around every line-solver launch)
+    ph_sum, sw_sum, sw_n = {}, {}, {}
+    for _ in range(args.steps):
+        ph, sw = sim.step_traced_sweeps()
+        for k, v in ph.items():
+            ph_sum[k] = ph_sum.get(k, 0.0) + v
+        for k, v in sw.items():
+            if v > 0:
+                sw_sum[k] = sw_sum.get(k, 0.0) + v
+                sw_n[k] = sw_n.get(k, 0) + 1
+    phases = {k: v / args.steps for k, v in ph_sum.items()}
+    sweeps = {k: sw_sum[k] / sw_n[k] for k in sw_sum}
     hbm, peak_kind = _peaks()
-    dom = max(phases, key=phases.get)
-    if dom.startswith("sweep"):
-        alg_bytes = SWEEP_BYTES_PER_CELL[args.precision] * cells
-    else:
-        alg_bytes = None
+    # dominant kernel: the longest line-solver launch (the launch list shows
+    # the four line solvers as the top kernels)
+    dom = max(sweeps, key=sweeps.get)
+    dom_cells = sweep_cells(dom, N, M)
+    alg_bytes = SWEEP_BYTES_PER_CELL[dom] * dom_cells
+    ach = alg_bytes / (sweeps[dom] * 1e-3) / 1e9
     step_bytes = BYTES_PER_CELL_STEP[(args.precision, sed)] * cells
     step_ms = ms / args.steps
-    roof = {"bound": "hbm", "kernel": dom, "phase_ms": round(phases[dom], 4),
-            "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None, "traffic": None,
-            "peak_source": peak_kind,
+    roof = {"bound": "hbm", "kernel": dom, "kernel_ms": round(sweeps[dom], 4),
+            "bytes_per_launch": alg_bytes, "achieved": ach, "peak": hbm, "unit": "GB/s",
+            "frac": ach / hbm, "traffic": None, "peak_source": peak_kind,
+            "sweeps_ms": {k: round(v, 4) for k, v in sweeps.items()},
             "step_achieved": step_bytes / (step_ms * 1e-3) / 1e9,
             "step_frac": step_bytes / (step_ms * 1e-3) / 1e9 / hbm}
-    if alg_bytes is not None:
-        ach = alg_bytes / (phases[dom] * 1e-3) / 1e9
-        roof.update(achieved=ach, frac=ach / hbm)
     traffic_file = ROOT / "profiles" / "traffic.json"
     if traffic_file.exists():
         try:
@@ -353,7 +374,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64"])
     ap.add_argument("--workload", default="sediment-2048x1024")
     ap.add_argument("--graph", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

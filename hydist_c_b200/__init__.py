@@ -102,6 +102,16 @@ class Simulation:
         capi.check(self._lib, self._lib.hydist_step_traced(self._h, ms), "hydist_step_traced")
         return dict(zip(capi.PHASES, [float(x) for x in ms]))
 
+    def step_traced_sweeps(self):
+        """One full step with per-phase device times and the device time of
+        each line-solver launch (ms): (phases, sweeps)."""
+        ms = (C.c_float * len(capi.PHASES))()
+        sw = (C.c_float * len(capi.SWEEPS))()
+        capi.check(self._lib, self._lib.hydist_step_traced_sweeps(self._h, ms, sw),
+                   "hydist_step_traced_sweeps")
+        return (dict(zip(capi.PHASES, [float(x) for x in ms])),
+                dict(zip(capi.SWEEPS, [float(x) for x in sw])))
+
     @property
     def kernel_launches(self) -> int:
         v = C.c_int64()

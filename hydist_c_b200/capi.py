@@ -178,6 +178,7 @@ def _declare(lib):
     lib.hydist_stream.argtypes = [vp]
     lib.hydist_stream.restype = vp
     lib.hydist_step_traced.argtypes = [vp, C.POINTER(C.c_float)]
+    lib.hydist_step_traced_sweeps.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
     lib.hydist_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
     lib.hydist_gtsv_batched.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32,
                                         C.c_int32, vp]
@@ -201,8 +202,10 @@ EXPORTED_SYMBOLS = [
     "hydist_last_error", "hydist_version", "hydist_create", "hydist_destroy", "hydist_step",
     "hydist_sync", "hydist_get_time", "hydist_set_time", "hydist_download", "hydist_upload", "hydist_mass",
     "hydist_step_graph", "hydist_stream", "hydist_gtsv_batched", "hydist_step_traced",
-    "hydist_kernel_launches", "hydist_gtsv_batched_noalloc",
+    "hydist_kernel_launches", "hydist_gtsv_batched_noalloc", "hydist_step_traced_sweeps",
 ]
 
 PHASES = ["boundary_x", "sweep_x", "explicit_v", "commit_x", "sediment_x",
           "boundary_y", "sweep_y", "explicit_u", "commit_y", "sediment_y"]
+# the line-solver launches hydist_step_traced_sweeps times one by one
+SWEEPS = ["line_solve_hydro_x", "line_solve_hydro_y", "line_solve_conc_x", "line_solve_conc_y"]

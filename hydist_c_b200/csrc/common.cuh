@@ -83,14 +83,35 @@ enum Phase {
   PH_COUNT
 };
 
+// The line-solver launches of one step, timed one by one when traced.
+enum SweepKernel {
+  KS_SWEEP_X = 0,  // hydraulic x sweep
+  KS_SWEEP_Y,      // hydraulic y sweep
+  KS_FS_X,         // concentration x sweep
+  KS_FS_Y,         // concentration y sweep
+  KS_COUNT
+};
+
 // Launch bookkeeping: counts kernels and, when events are given, records
-// an event at the end of each phase (the tracing of hydist_step_traced).
+// an event at the end of each phase and around each line-solver launch (the
+// tracing of hydist_step_traced / hydist_step_traced_sweeps).
 struct Trace {
-  cudaEvent_t* ev = nullptr;  // PH_COUNT + 1 events; ev[0] = step start
+  cudaEvent_t* ev = nullptr;   // PH_COUNT + 1 events; ev[0] = step start
+  cudaEvent_t* kev = nullptr;  // 2 * KS_COUNT events: begin, end of each sweep
+  bool krec[KS_COUNT] = {};
   long long launches = 0;
   void mark(cudaStream_t st, int phase, int nkernels) {
     launches += nkernels;
     if (ev) cudaEventRecord(ev[phase + 1], st);
+  }
+  void kbegin(cudaStream_t st, int k) {
+    if (kev) cudaEventRecord(kev[2 * k], st);
+  }
+  void kend(cudaStream_t st, int k) {
+    if (kev) {
+      cudaEventRecord(kev[2 * k + 1], st);
+      krec[k] = true;
+    }
   }
 };
 

@@ -114,6 +114,7 @@ struct HydistHandle {
   long long graph_launches[4] = {0, 0, 0, 0};
   Trace trace;                                    // kernel launch counter
   cudaEvent_t ev[PH_COUNT + 1] = {};
+  cudaEvent_t kev[2 * KS_COUNT] = {};
 };
 
 namespace {
@@ -299,6 +300,10 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistO
   if (!(p->dX > 0 && p->dY > 0 && p->dT > 0)) return fail(HYDIST_ERR_ARG, "dX, dY, dT must be > 0");
   if (o->precision != HYDIST_FP64 && o->precision != HYDIST_FP32_REFINE)
     return fail(HYDIST_ERR_ARG, "unknown precision");
+  if (o->precision == HYDIST_FP32_REFINE)
+    return fail(HYDIST_ERR_ARG, "precision HYDIST_FP32_REFINE is not implemented yet");
+  if (o->bed_change != 0)
+    return fail(HYDIST_ERR_ARG, "the bed-change update is not implemented yet");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(HYDIST_ERR_NODEVICE, "no CUDA device");
@@ -447,14 +452,17 @@ int hydist_step(HydistHandle* h, int32_t nsteps) {
   return HYDIST_OK;
 }
 
-int hydist_step_traced(HydistHandle* h, float* phase_ms) {
+int hydist_step_traced_sweeps(HydistHandle* h, float* phase_ms, float* sweep_ms) {
   if (!h || !phase_ms) return fail(HYDIST_ERR_ARG, "null argument");
   CK(cudaSetDevice(h->device));
   TRY(check_horizon(h, 1));
   if (!h->ev[0])
     for (auto& e : h->ev) CK(cudaEventCreate(&e));
+  if (sweep_ms && !h->kev[0])
+    for (auto& e : h->kev) CK(cudaEventCreate(&e));
   Trace tr;
   tr.ev = h->ev;
+  if (sweep_ms) tr.kev = h->kev;
   const double t1 = h->t + 0.5 * h->c.dT;
   const double t2 = t1 + h->c.dT * 0.5;
   CK(cudaEventRecord(h->ev[0], h->stream));
@@ -468,7 +476,18 @@ int hydist_step_traced(HydistHandle* h, float* phase_ms) {
     CK(cudaEventElapsedTime(&ms, h->ev[p], h->ev[p + 1]));
     phase_ms[p] = ms;
   }
+  if (sweep_ms) {
+    for (int k = 0; k < KS_COUNT; ++k) {
+      float ms = 0;
+      if (tr.krec[k]) CK(cudaEventElapsedTime(&ms, h->kev[2 * k], h->kev[2 * k + 1]));
+      sweep_ms[k] = ms;
+    }
+  }
   return HYDIST_OK;
+}
+
+int hydist_step_traced(HydistHandle* h, float* phase_ms) {
+  return hydist_step_traced_sweeps(h, phase_ms, nullptr);
 }
 
 int hydist_kernel_launches(HydistHandle* h, int64_t* count) {

@@ -889,7 +889,9 @@ void launch_half_x(const State& S, const Coef& c, cudaStream_t st, Trace* tr) {
   k_tick<<<1, 1, 0, st>>>(S, 0.5 * c.dT);
   k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
   if (tr) tr->mark(st, PH_BOUNDARY_X, 2);
+  if (tr) tr->kbegin(st, KS_SWEEP_X);
   launch_sweep(S, c, 0, st);
+  if (tr) tr->kend(st, KS_SWEEP_X);
   if (tr) tr->mark(st, PH_SWEEP_X, 1);
   // smoothing of t_u into su, explicit v from it, margins, smoothing of t_v
   // into sv; k_commit_a writes both back (Normalize/update_buffer pairs,
@@ -912,7 +914,9 @@ void launch_half_y(const State& S, const Coef& c, cudaStream_t st, Trace* tr) {
   k_tick<<<1, 1, 0, st>>>(S, c.dT * 0.5);
   k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
   if (tr) tr->mark(st, PH_BOUNDARY_Y, 2);
+  if (tr) tr->kbegin(st, KS_SWEEP_Y);
   launch_sweep(S, c, 1, st);
+  if (tr) tr->kend(st, KS_SWEEP_Y);
   if (tr) tr->mark(st, PH_SWEEP_Y, 1);
   k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 0);
   k_solve_u<<<grid2(S.M - 1, S.N, 128), 128, 0, st>>>(S, c);

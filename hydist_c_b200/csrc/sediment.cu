@@ -57,7 +57,9 @@ void launch_sediment(const State& S, const Coef& c, double s_start, bool xdir, c
   // (launch shape of engine.cpp:259-260 never reaches row N)
   const int i_hi = xdir ? S.N : S.N - 1;
   k_vth_heso<<<dim3(cdiv(S.M, 128), i_hi), 128, 0, st>>>(S, c, i_hi);
+  if (tr) tr->kbegin(st, xdir ? KS_FS_X : KS_FS_Y);
   launch_fs_sweep(S, c, xdir ? 0 : 1, s_start, st);
+  if (tr) tr->kend(st, xdir ? KS_FS_X : KS_FS_Y);
   k_update_fs<<<dim3(cdiv(S.M, 128), S.N), 128, 0, st>>>(S);
   if (tr) tr->mark(st, xdir ? PH_SEDIMENT_X : PH_SEDIMENT_Y, 3);
 }

@@ -57,8 +57,11 @@ __global__ void k_thomas_batched(const T* __restrict__ dl, const T* __restrict__
 
 }  // namespace hyd
 
+namespace hyd {
+void set_last_error(const char* m);
+}
+
 namespace {
-thread_local std::string g_terr;
 struct Scratch {
   void* p = nullptr;
   size_t bytes = 0;
@@ -73,6 +76,10 @@ extern "C" int hydist_gtsv_batched(const void* dl, const void* d, const void* du
   if (!dl || !d || !du || !b || !x || !offsets || !lengths || nsys < 0) return HYDIST_ERR_ARG;
   if (dtype != 0 && dtype != 1) return HYDIST_ERR_ARG;
   if (algo < 0 || algo > 3) return HYDIST_ERR_ARG;
+  if (algo >= 2) {
+    hyd::set_last_error("hydist_gtsv_batched: algo 2 and 3 are not implemented yet");
+    return HYDIST_ERR_ARG;
+  }
   if (nsys == 0) return HYDIST_OK;
   cudaStream_t st = (cudaStream_t)stream;
   // total rows = max(off+len): read the last system's extent from device

@@ -76,7 +76,8 @@ enum HydistField {
 /* Precision of the time step. */
 enum HydistPrecision {
   HYDIST_FP64 = 0,       /* plain FP64 form: reproduces the reference       */
-  HYDIST_FP32_REFINE = 1 /* FP32 bulk, FP64 z/bed state + FP64 refinement   */
+  HYDIST_FP32_REFINE = 1 /* FP32 bulk, FP64 z/bed state + FP64 refinement
+                            (not implemented yet: hydist_create refuses it) */
 };
 
 /* Physical and numerical constants: the inputs of Load_coeffs
@@ -106,7 +107,8 @@ typedef struct HydistOptions {
   double sediment_start;   /* -b: sediment sweeps from this t  main.cpp:82  */
   double bed_change_start; /* -B: erosion source and bed change from this t */
   int32_t ketdinh;         /* cohesive sediment (main.cpp:53 sets 1)        */
-  int32_t bed_change;      /* 1: apply the bed-change update each step      */
+  int32_t bed_change;      /* 1: apply the bed-change update each step (not
+                              implemented yet: hydist_create refuses 1)     */
   int32_t precision;       /* enum HydistPrecision                          */
   int32_t reserved;
 } HydistOptions;
@@ -192,6 +194,12 @@ void* hydist_stream(HydistHandle* h);
  * entries). Synchronous. */
 #define HYDIST_PHASES 10
 int hydist_step_traced(HydistHandle* h, float* phase_ms);
+/* The same, also timing each line-solver launch of the step on its own:
+ * sweep_ms[HYDIST_SWEEPS] = hydraulic x sweep, hydraulic y sweep,
+ * concentration x sweep, concentration y sweep (0 for a sweep the step did
+ * not run). */
+#define HYDIST_SWEEPS 4
+int hydist_step_traced_sweeps(HydistHandle* h, float* phase_ms, float* sweep_ms);
 /* Number of kernels the handle has enqueued since creation (set-up
  * excluded). */
 int hydist_kernel_launches(HydistHandle* h, int64_t* count);
@@ -202,10 +210,12 @@ int hydist_kernel_launches(HydistHandle* h, int64_t* count);
  * batched, host-callable entry point. System s occupies rows
  * [offsets[s], offsets[s] + lengths[s]) of the packed arrays; dl[first row]
  * and du[last row] of each system are ignored. Arrays are device pointers.
- * dtype: 0 = FP64, 1 = FP32. algo: 0 = autotuned choice per length band,
- * 1 = Thomas (thread per system), 2 = partitioned Thomas / SPIKE with
- * diagonal pivoting, 3 = warp PCR-Thomas. stream is a cudaStream_t (NULL =
- * default stream). Scratch is allocated by the library on first use. */
+ * dtype: 0 = FP64, 1 = FP32. algo: 0 = the library's choice (Thomas for
+ * now), 1 = Thomas (thread per system); 2 (partitioned Thomas / SPIKE) and
+ * 3 (PCR-Thomas) are reserved and refused with HYDIST_ERR_ARG until they
+ * exist. stream is a cudaStream_t (NULL = default stream). Scratch is
+ * allocated by the library on first use; the call synchronises the stream
+ * once to read the packed row count. */
 int hydist_gtsv_batched(const void* dl, const void* d, const void* du,
                         const void* b, void* x, const int32_t* offsets,
                         const int32_t* lengths, int32_t nsys, int32_t dtype,
