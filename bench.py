@@ -354,9 +354,12 @@ def measure_e2e(H, bundle, dev, prec, args):
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     sim = H.Simulation(b, device=dev, precision=prec)
+    sim.sync()
+    t1 = time.perf_counter()
     for _ in range(args.steps):
         sim.step(1)
         sim.mass()
+    t2 = time.perf_counter()
     outs = [sim.download(f) for f in ("u", "v", "z", "FS")]
     dt = time.perf_counter() - t0
     sim.close()
@@ -365,7 +368,8 @@ def measure_e2e(H, bundle, dev, prec, args):
     return {"value": cells * steps / dt, "unit": "cell-steps/s",
             "h2d_bytes_per_step": h2d / steps,
             "d2h_bytes_per_step": (8 * args.steps + 4 * 8 * n) / steps,
-            "wall_s": dt, "steps": steps}
+            "wall_s": dt, "create_s": t1 - t0, "steps_s": t2 - t1,
+            "download_s": dt - (t2 - t0), "steps": steps}
 
 
 def main():

@@ -26,7 +26,7 @@ struct Coef {
   double CORIOLIS_FORCE, g, Ks, Windx, Windy, Ufr, Dxr, wss;
   // reciprocals and products of constants, so that the kernels multiply
   // where the reference divides by a constant (one rounding of difference)
-  double r_dX2, r_dY2, r_dXbp, r_dYbp, dT_dXbp, dT_dYbp, sqrt_g;
+  double r_dX, r_dY, r_dX2, r_dY2, r_dXbp, r_dYbp, dT_dXbp, dT_dYbp, sqrt_g;
   double Mb_ros, r_Tod, r_Ufr2, Dxr_m03;  // Mbochat/ros, 1/Tod, 1/Ufr^2, Dxr^-0.3
 };
 
@@ -55,9 +55,6 @@ struct State {
   // scratch
   double* tmp;   // smoothing buffer, (N+3)*(M+3)
   double *su, *sv;  // t_u / t_v after the smoothing of the current half-step
-  double* Ap;    // Thomas scratch, [unknown][line]
-  double* Bp;
-  int ld;        // line stride of Ap/Bp (max(M,N)+3)
   int* err;      // [0]: DevErr
   double* lscratch;  // partitioned line solver: one slot per resident CTA
   int lslots;        // number of slots (CTAs of the persistent sweep grid)

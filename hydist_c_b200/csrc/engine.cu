@@ -84,6 +84,8 @@ void derive(const HydistParams& p, Coef& c) {
                            (std::sqrt(1 + 0.01 * (c.Sx - 1) * 9.81 * std::pow(c.dm, 3) /
                                               std::pow(c.muy, 2)) -
                             1);
+  c.r_dX = 1.0 / c.dX;
+  c.r_dY = 1.0 / c.dY;
   c.r_dX2 = 1.0 / c.dX2;
   c.r_dY2 = 1.0 / c.dY2;
   c.r_dXbp = 1.0 / c.dXbp;
@@ -389,11 +391,6 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistO
     TRY(dalloc(h, &S.dauj, S.W * SEG));
     TRY(dalloc(h, &S.cuoij, S.W * SEG));
     TRY(dalloc(h, &S.mocj, S.W));
-    // Thomas scratch [unknown][line]
-    S.ld = std::max(S.W, S.H);
-    const size_t nunk = (size_t)2 * std::max(S.M, S.N) + 4;
-    TRY(dalloc(h, &S.Ap, nunk * S.ld));
-    TRY(dalloc(h, &S.Bp, nunk * S.ld));
     TRY(dalloc(h, &S.err, 4));
     TRY(dalloc(h, &S.colflag, S.W));
     TRY(dalloc(h, &S.segcnt, 2 * S.H + 2 * S.W));

@@ -502,19 +502,24 @@ __global__ void k_smooth_full(State S, Coef c, int isU) {
   double* out_arr = isU ? S.su : S.sv;
   const double vg = val[g];
   double out = vg;
-  if (i >= 2 && i <= S.N && j >= 2 && j <= S.M && vg != 0) {
+  if (i >= 2 && i <= S.N && j >= 2 && j <= S.M) {
+    // every operand is loaded up front, one round of memory latency
     const int close = isU ? W : 1, far = isU ? 1 : W;
-    int count = 2;
-    double nb = val[g - close] + val[g + close];
-    if (S.khouot[g - far] == 0) {
-      nb += val[g - far];
-      count++;
+    const double a = val[g - close], b = val[g + close], l = val[g - far], r = val[g + far];
+    const int kl = S.khouot[g - far], kr = S.khouot[g + far];
+    if (vg != 0) {
+      int count = 2;
+      double nb = a + b;
+      if (kl == 0) {
+        nb += l;
+        count++;
+      }
+      if (kr == 0) {
+        nb += r;
+        count++;
+      }
+      out = out * c.heso + (1 - c.heso) * nb / count;
     }
-    if (S.khouot[g + far] == 0) {
-      nb += val[g + far];
-      count++;
-    }
-    out = out * c.heso + (1 - c.heso) * nb / count;
   }
   out_arr[g] = out;
 }
@@ -568,48 +573,60 @@ __device__ __forceinline__ bool find_seg(const int* dau, const int* cuoi, int n,
 
 // vSolver driven by solveV (UVZSolver_multithread.cpp:607-663, 961-978).
 __global__ void k_solve_v(State S, Coef c) {
+  // the block's cells share one row: its segment table goes to shared memory
+  __shared__ int s_first[SEG], s_last[SEG];
+  __shared__ int s_n;
   const int col = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int row = blockIdx.y + 2;
+  if (threadIdx.x < SEG) {
+    s_first[threadIdx.x] = S.daui[row * SEG + threadIdx.x];
+    s_last[threadIdx.x] = S.cuoii[row * SEG + threadIdx.x];
+  }
+  if (threadIdx.x == 0) s_n = S.moci[row];
+  __syncthreads();
   if (row > S.N || col > S.M) return;
   int first, last;
-  if (!find_seg(S.daui + row * SEG, S.cuoii + row * SEG, S.moci[row], col, first, last)) return;
+  if (!find_seg(s_first, s_last, s_n, col, first, last)) return;
   if (first >= last || col >= last || col < first) return;
-  const int off = S.W;
+  const int off = S.W, g = row * off + col;
   const double* u = S.u;
   const double* v = S.v;
   const double* tu = S.su;  // t_u after its smoothing
   const double* Hm = S.Hmoi;
+  // every operand up front: one round of memory latency
+  const double u00 = u[g - off], u01 = u[g], u10 = u[g - off + 1], u11 = u[g + 1];
+  const double t00 = tu[g - off], t01 = tu[g], t10 = tu[g - off + 1], t11 = tu[g + 1];
+  const double vv = v[g], vl = v[g - 1], vr = v[g + 1];
+  const double vm1 = v[g - off], vm2 = v[g - 2 * off], vp1 = v[g + off], vp2 = v[g + 2 * off];
+  const double hm1 = Hm[g - off], hm2 = Hm[g - 2 * off], hp1 = Hm[g + off];
+  const double Hv = S.Htdv[g], Ky1 = S.Ky1[g], zc = S.z[g], zr = S.z[g + 1], vis = S.visco[g],
+               tsy = S.Tsyw[g];
   double p, q = 0, tmp = 0;
-  const double utb = (u[(row - 1) * off + col] + u[row * off + col] + u[(row - 1) * off + col + 1] +
-                      u[row * off + col + 1]) *
-                     0.25;
-  const double t_utb = (tu[(row - 1) * off + col] + tu[row * off + col] +
-                        tu[(row - 1) * off + col + 1] + tu[row * off + col + 1]) *
-                       0.25;
-  const double vv = v[row * off + col];
-  p = (v[row * off + col + 1] - v[row * off + col - 1]) / c.dY2;
-  p = c.HaiChiadT + p + S.Ky1[row * off + col] * sqrt(utb * utb + vv * vv) / S.Htdv[row * off + col];
-  if (Hm[(row - 1) * off + col] <= c.H_TINH) {
+  const double utb = (u00 + u01 + u10 + u11) * 0.25;
+  const double t_utb = (t00 + t01 + t10 + t11) * 0.25;
+  const double rHv = 1.0 / Hv;
+  p = (vr - vl) * c.r_dY2;
+  p = c.HaiChiadT + p + Ky1 * sqrt(utb * utb + vv * vv) * rHv;
+  if (hm1 <= c.H_TINH) {
     if (utb < 0) {
-      q = t_utb * (-3 * vv + 4 * v[(row + 1) * off + col] - v[(row + 2) * off + col]) / c.dX2;
-      tmp = (vv - 2 * v[(row + 1) * off + col] + v[(row + 2) * off + col]) / c.dXbp;
+      q = t_utb * (-3 * vv + 4 * vp1 - vp2) * c.r_dX2;
+      tmp = (vv - 2 * vp1 + vp2) * c.r_dXbp;
     }
   } else {
-    if (Hm[(row + 1) * off + col] <= c.H_TINH) {
-      if ((Hm[(row - 2) * off + col] > c.H_TINH) && (utb > 0)) {
-        q = t_utb * (3 * vv - 4 * v[(row - 1) * off + col] + v[(row - 2) * off + col]) / c.dX2;
-        tmp = (vv - 2 * v[(row - 1) * off + col] + v[(row - 2) * off + col]) / c.dXbp;
+    if (hp1 <= c.H_TINH) {
+      if ((hm2 > c.H_TINH) && (utb > 0)) {
+        q = t_utb * (3 * vv - 4 * vm1 + vm2) * c.r_dX2;
+        tmp = (vv - 2 * vm1 + vm2) * c.r_dXbp;
       }
     } else {
-      q = t_utb * (v[(row + 1) * off + col] - v[(row - 1) * off + col]) / c.dX2;
-      tmp = (v[(row + 1) * off + col] - 2 * vv + v[(row - 1) * off + col]) / c.dXbp;
+      q = t_utb * (vp1 - vm1) * c.r_dX2;
+      tmp = (vp1 - 2 * vv + vm1) * c.r_dXbp;
     }
   }
   q = c.HaiChiadT * vv - q - c.CORIOLIS_FORCE * t_utb;
-  q = (q - c.g * (S.z[row * off + col + 1] - S.z[row * off + col]) / c.dY +
-       S.visco[row * off + col] * (tmp + (v[row * off + col + 1] - 2 * vv + v[row * off + col - 1]) / c.dYbp)) +
-      (c.Windy - S.Tsyw[row * off + col]) / S.Htdv[row * off + col];
-  S.tv[row * off + col] = q / p;
+  q = (q - c.g * (zr - zc) * c.r_dY + vis * (tmp + (vr - 2 * vv + vl) * c.r_dYbp)) +
+      (c.Windy - tsy) * rHv;
+  S.tv[g] = q / p;
 }
 
 // uSolver driven by solveU (UVZSolver_multithread.cpp:724-795, 938-959);
@@ -618,41 +635,51 @@ __global__ void k_solve_u(State S, Coef c) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int row = blockIdx.y + 1;
   if (row > S.N || col > S.M) return;
-  int first, last;
-  if (!find_seg(S.dauj + col * SEG, S.cuoij + col * SEG, S.mocj[col], row, first, last)) return;
-  if (first > last || row < first - 1 || row >= last) return;
   const int off = S.W;
-  const double dX = c.dY, dY = c.dY, Windx = c.Windy;
+  const int ij = row * off + col, i1j = ij + off;
   const double* u = S.u;
   const double* v = S.v;
   const double* tv = S.sv;  // t_v after its smoothing
   const double* Hm = S.Hmoi;
+  // every operand is loaded before the segment lookup (all in bounds for
+  // rows 1..N, columns 2..M), so both take one round of memory latency
+  const double v00 = v[ij - 1], v01 = v[ij], v10 = v[i1j - 1], v11 = v[i1j];
+  const double t00 = tv[ij - 1], t01 = tv[ij], t10 = tv[i1j - 1], t11 = tv[i1j];
+  const double uu = u[ij], ud = u[i1j], uup = u[ij - off];
+  const double ul1 = u[ij - 1], ul2 = u[ij - 2], ur1 = u[ij + 1], ur2 = u[ij + 2];
+  const double hl1 = Hm[ij - 1], hl2 = Hm[ij - 2], hr1 = Hm[ij + 1];
+  const double Hu = S.Htdu[ij], Kx1 = S.Kx1[ij], zc = S.z[ij], zd = S.z[i1j], vis = S.visco[ij],
+               tsx = S.Tsxw[ij];
+  int first, last;
+  if (!find_seg(S.dauj + col * SEG, S.cuoij + col * SEG, S.mocj[col], row, first, last)) return;
+  if (first > last || row < first - 1 || row >= last) return;
+  const double Windx = c.Windy;
+  // dX is read from dY: 1/(2dX) = r_dY2, 1/dX^2 = r_dYbp, 1/dX = r_dY
   double p, q = 0, tmp = 0;
-  const int ij = row * off + col, i1j = ij + off;
-  const double vtb = (v[ij - 1] + v[ij] + v[i1j - 1] + v[i1j]) * 0.25;
-  const double t_vtb = (tv[ij - 1] + tv[ij] + tv[i1j - 1] + tv[i1j]) * 0.25;
-  p = (u[i1j] - u[(row - 1) * off + col]) / (dX * 2);
-  p = (c.HaiChiadT + p + S.Kx1[ij] * sqrt(vtb * vtb + u[ij] * u[ij]) / S.Htdu[ij]);
-  if (Hm[ij - 1] <= c.H_TINH) {
+  const double vtb = (v00 + v01 + v10 + v11) * 0.25;
+  const double t_vtb = (t00 + t01 + t10 + t11) * 0.25;
+  const double rHu = 1.0 / Hu;
+  p = (ud - uup) * c.r_dY2;
+  p = (c.HaiChiadT + p + Kx1 * sqrt(vtb * vtb + uu * uu) * rHu);
+  if (hl1 <= c.H_TINH) {
     if (vtb < 0) {
-      q = t_vtb * (-3 * u[ij] + 4 * u[ij + 1] - u[ij + 2]) / (dY * 2);
-      tmp = (u[ij] - 2 * u[ij + 1] + u[ij + 2]) / (dY * dY);
+      q = t_vtb * (-3 * uu + 4 * ur1 - ur2) * c.r_dY2;
+      tmp = (uu - 2 * ur1 + ur2) * c.r_dYbp;
     }
   } else {
-    if (Hm[ij + 1] <= c.H_TINH) {
-      if ((Hm[ij - 2] > c.H_TINH) && (vtb > 0)) {
-        q = t_vtb * (3 * u[ij] - 4 * u[ij - 1] + u[ij - 2]) / (dY * 2);
-        tmp = (u[ij] - 2 * u[ij - 1] + u[ij - 2]) / (dY * dY);
+    if (hr1 <= c.H_TINH) {
+      if ((hl2 > c.H_TINH) && (vtb > 0)) {
+        q = t_vtb * (3 * uu - 4 * ul1 + ul2) * c.r_dY2;
+        tmp = (uu - 2 * ul1 + ul2) * c.r_dYbp;
       }
     } else {
-      q = t_vtb * (u[ij + 1] - u[ij - 1]) / (dY * 2);
-      tmp = (u[ij + 1] - 2 * u[ij] + u[ij - 1]) / (dY * dY);
+      q = t_vtb * (ur1 - ul1) * c.r_dY2;
+      tmp = (ur1 - 2 * uu + ul1) * c.r_dYbp;
     }
   }
-  q = c.HaiChiadT * u[ij] - q + c.CORIOLIS_FORCE * t_vtb;
-  q = (q - c.g * (S.z[i1j] - S.z[ij]) / dX +
-       S.visco[ij] * (tmp + (u[i1j] - 2 * u[ij] + u[(row - 1) * off + col]) / (dX * dX))) +
-      (Windx - S.Tsxw[ij]) / S.Htdu[ij];
+  q = c.HaiChiadT * uu - q + c.CORIOLIS_FORCE * t_vtb;
+  q = (q - c.g * (zd - zc) * c.r_dY + vis * (tmp + (ud - 2 * uu + uup) * c.r_dYbp)) +
+      (Windx - tsx) * rHu;
   S.tu[ij] = q / p;
 }
 
