@@ -35,6 +35,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+from hydist_c_b200 import replicas as R  # noqa: E402
+
 BYTES_PER_CELL_STEP = {  # algorithmic bytes per interior cell and full step
     ("fp64", False): 168, ("fp64", True): 232}
 # Algorithmic bytes per cell of one line-solver launch (FP64), each field the
@@ -117,44 +119,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def workload(name: str):
+def workload(name: str, rank: int = 0):
+    """The scenario of one replica (rank r solves its own seeded scenario)
+    and the untimed spin-up steps."""
     from hydist_c_b200 import scenario as S
+    from hydist_c_b200.replicas import replica_seed
     if name == "sediment-2048x1024":
-        return S.config1(), 300  # spin-up steps to t = 600 s (sediment on)
+        # spin-up to t = 600 s, where the sediment sweeps start
+        return S.config1(seed=replica_seed(20260001, rank)), 300
     if name == "channel-256x128":
-        return S.config0(), 0
+        return S.config0(seed=replica_seed(20260000, rank)), 0
     raise SystemExit(f"unknown workload {name}")
-
-
-def dist_init():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    if ws > 1:
-        import torch
-        import torch.distributed as dist
-        rank = int(os.environ["RANK"])
-        local = int(os.environ.get("LOCAL_RANK", rank))
-        torch.cuda.set_device(local)
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-        return rank, local, ws
-    return 0, 0, 1
-
-
-def max_over_ranks(x: float, ws: int) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
 
 
 def cpu_baseline(bundle, steps: int, threads: int):
@@ -173,7 +148,8 @@ def cpu_baseline(bundle, steps: int, threads: int):
 
 
 def run_reference(args):
-    rank, local, ws = dist_init()
+    # rank 0 alone times the CPU implementation; no process group is needed
+    rank, local, ws = R.env_ranks()
     if rank != 0:
         return
     bundle, _ = workload(args.workload)
@@ -210,11 +186,11 @@ def run_reference(args):
 def run_ours(args):
     import torch
     import hydist_c_b200 as H
-    rank, local, ws = dist_init()
+    rank, local, ws = R.init("nccl")
     dev = local
     torch.cuda.set_device(dev)
     prec = H.FP64 if args.precision == "fp64" else H.FP32_REFINE
-    bundle, spin = workload(args.workload)
+    bundle, spin = workload(args.workload, rank)
     if args.sed0 and bundle["options"]["sediment_start"] < 1e11:
         # sediment sweeps from the first step: the same per-step work without
         # the spin-up (used for short profiling runs)
@@ -236,7 +212,7 @@ def run_ours(args):
     e1 = torch.cuda.Event(enable_timing=True)
     step_ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     clocks = ClockSampler(torch.cuda.current_device() if ws == 1 else local)
-    barrier(ws)
+    R.barrier(ws)
     torch.cuda.synchronize(dev)
     clocks.start()
     e0.record(stream)
@@ -249,13 +225,13 @@ def run_ours(args):
         step_ev[k + 1].record(stream)
     e1.record(stream)
     torch.cuda.synchronize(dev)
-    barrier(ws)
+    R.barrier(ws)
     clk = clocks.stop()
     sim.sync()
     ms = e0.elapsed_time(e1)
     launches = sim.kernel_launches - l0
     per_step = [step_ev[k].elapsed_time(step_ev[k + 1]) for k in range(args.steps)]
-    ms_max = max_over_ranks(ms, ws)
+    ms_max = R.max_over_ranks(ms, ws)
     value = ws * cells * args.steps / (ms_max * 1e-3)
     # per-kernel times: the same K steps again, each traced (an event at the
     # end of every phase and around every line-solver launch)
@@ -326,9 +302,7 @@ def run_ours(args):
         }
         print(json.dumps(line), flush=True)
     sim.close()
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    R.finish(ws)
 
 
 def measure_e2e(H, bundle, dev, prec, args):
