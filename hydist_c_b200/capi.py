@@ -184,6 +184,8 @@ def _declare(lib):
                                         C.c_int32, vp]
     lib.hydist_gtsv_batched_noalloc.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int32,
                                                 C.c_int32, C.c_int32, vp]
+    lib.hydist_gtsv_autotune.argtypes = [C.c_int32, vp, _ip]
+    lib.hydist_gtsv_band_bounds.argtypes = [_ip]
 
 
 class HydistError(RuntimeError):
@@ -203,7 +205,10 @@ EXPORTED_SYMBOLS = [
     "hydist_sync", "hydist_get_time", "hydist_set_time", "hydist_download", "hydist_upload", "hydist_mass",
     "hydist_step_graph", "hydist_stream", "hydist_gtsv_batched", "hydist_step_traced",
     "hydist_kernel_launches", "hydist_gtsv_batched_noalloc", "hydist_step_traced_sweeps",
+    "hydist_gtsv_autotune", "hydist_gtsv_band_bounds",
 ]
+GTSV_AUTO, GTSV_THOMAS, GTSV_PARTITION, GTSV_WARP, GTSV_PARTITION_512 = 0, 1, 2, 3, 4
+GTSV_BANDS = 7
 
 PHASES = ["boundary_x", "sweep_x", "explicit_v", "commit_x", "sediment_x",
           "boundary_y", "sweep_y", "explicit_u", "commit_y", "sediment_y"]

@@ -5,33 +5,61 @@
 // threads per line) and the SPIKE solver gtsv_spike_partial_diag_pivot_v1
 // (gtsv.cpp:88-193, called per line with device-side allocation).
 //
-// Packed batch: system s occupies rows [off[s], off[s]+len[s]).
+// Packed batch: system s occupies rows [off[s], off[s]+len[s]); dl of its
+// first row and du of its last row are ignored.
+//
+// Three solvers, chosen per length band:
+//   Thomas      one thread per system, in place in global memory (any length);
+//   warp        one warp per system staged in shared memory, partition
+//               method with a shuffle PCR of the 32 chunk separators
+//               (systems up to GT_WARP_MAX rows);
+//   CTA         one 256-thread CTA per system staged in shared memory,
+//               partition method with a shared-memory PCR (systems up to the
+//               shared memory of one CTA, about 6000 FP64 / 12000 FP32 rows).
+// A classification kernel files each system under its length band on the
+// device; the bands' solvers then run over their lists. The autotuner times
+// the feasible solvers per band on synthetic diagonally dominant batches and
+// keeps the fastest (per device and dtype).
+#include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 
+#include <climits>
+#include <cmath>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
+#include "partsolve.cuh"
 
 namespace hyd {
 
-// Plain Thomas, one thread per system (the reference's algorithm; scratch
-// for the forward sweep is the output array x and a second array w).
+void set_last_error(const char* m);
+
+constexpr int GT_NB = HYDIST_GTSV_BANDS;
+constexpr int GT_WARPS = 4;      // warps per CTA of the warp solver
+constexpr int GT_WARP_MAX = 512;  // longest system of the warp solver
+
+// upper length bound of each band (the last is open)
+__host__ __device__ inline int gt_band_hi(int b) {
+  switch (b) {
+    case 0: return 32;
+    case 1: return 128;
+    case 2: return 512;
+    case 3: return 2048;
+    case 4: return 4096;
+    case 5: return 6144;
+    default: return INT_MAX;
+  }
+}
+
+// ---------------------------------------------------------------- Thomas
+// The reference's algorithm (no pivoting): forward sweep with the modified
+// super-diagonal in W and the modified right-hand side in X, then back
+// substitution in X.
 template <class T>
-__global__ void k_thomas_batched(const T* __restrict__ dl, const T* __restrict__ d,
-                                 const T* __restrict__ du, const T* __restrict__ b, T* __restrict__ x,
-                                 T* __restrict__ w, const int* __restrict__ off,
-                                 const int* __restrict__ len, int nsys) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nsys) return;
-  const int o = off[s], n = len[s];
-  if (n <= 0) return;
-  const T* A = dl + o;
-  const T* B = d + o;
-  const T* C = du + o;
-  const T* D = b + o;
-  T* X = x + o;
-  T* Wp = w + o;
+__device__ __forceinline__ void thomas_system(const T* A, const T* B, const T* C, const T* D, T* X,
+                                              T* Wp, int n) {
   if (n == 1) {
     X[0] = D[0] / B[0];
     return;
@@ -55,65 +83,483 @@ __global__ void k_thomas_batched(const T* __restrict__ dl, const T* __restrict__
   }
 }
 
-}  // namespace hyd
-
-namespace hyd {
-void set_last_error(const char* m);
+// the systems of one band's list, one thread each
+template <class T>
+__global__ void k_thomas_list(const T* __restrict__ dl, const T* __restrict__ d,
+                              const T* __restrict__ du, const T* __restrict__ b, T* __restrict__ x,
+                              T* __restrict__ w, const int* __restrict__ off,
+                              const int* __restrict__ len, const int* __restrict__ list,
+                              const int* __restrict__ count) {
+  const int cnt = *count;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    const int s = list[i];
+    const int o = off[s];
+    thomas_system(dl + o, d + o, du + o, b + o, x + o, w + o, len[s]);
+  }
 }
 
+// ------------------------------------------------- staged partition solvers
+// Stages a system's rows into shared memory with asynchronous copies
+// (cp.async): every thread's copies are in flight at once instead of one
+// load latency per row. The caller synchronises the threads afterwards.
+template <class T>
+__device__ __forceinline__ void gt_load(const T* dl, const T* d, const T* du, const T* b, int o,
+                                        int n, int S, T* rA, T* rB, T* rC, T* rD, int t0, int dt) {
+  for (PartStrideIdx it(t0, dt, S); it.q < n; it.next(dt)) {
+    const int i = it.q, q = it.idx();
+    if (i > 0) __pipeline_memcpy_async(&rA[q], &dl[o + i], sizeof(T));
+    else rA[q] = T(0);
+    __pipeline_memcpy_async(&rB[q], &d[o + i], sizeof(T));
+    if (i < n - 1) __pipeline_memcpy_async(&rC[q], &du[o + i], sizeof(T));
+    else rC[q] = T(0);
+    __pipeline_memcpy_async(&rD[q], &b[o + i], sizeof(T));
+  }
+  __pipeline_commit();
+  __pipeline_wait_prior(0);
+}
+
+// one system per CTA of NT threads (the tile size of the partition)
+template <class T, int NT>
+__global__ void __launch_bounds__(NT) k_gtsv_cta(const T* __restrict__ dl, const T* __restrict__ d,
+                                                 const T* __restrict__ du, const T* __restrict__ b,
+                                                 T* __restrict__ x, const int* __restrict__ off,
+                                                 const int* __restrict__ len,
+                                                 const int* __restrict__ list,
+                                                 const int* __restrict__ count) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto& sh = *reinterpret_cast<PartCtaShared<T, NT>*>(smem_raw);
+  T* rows = reinterpret_cast<T*>(smem_raw + sizeof(PartCtaShared<T, NT>));
+  const int cnt = *count;
+  for (int i = blockIdx.x; i < cnt; i += gridDim.x) {
+    const int s = list[i];
+    const int o = off[s], n = len[s];
+    const PartGeom g = part_geom(n, NT);
+    T* rA = rows;
+    T* rB = rA + g.stride;
+    T* rC = rB + g.stride;
+    T* rD = rC + g.stride;
+    gt_load(dl, d, du, b, o, n, g.S, rA, rB, rC, rD, (int)threadIdx.x, NT);
+    __syncthreads();
+    part_solve_cta<T, NT>(rA, rB, rC, rD, g, sh, n);
+    for (PartStrideIdx it(threadIdx.x, NT, g.S); it.q < n; it.next(NT)) x[o + it.q] = rD[it.idx()];
+    __syncthreads();
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(GT_WARPS * 32) k_gtsv_warp(
+    const T* __restrict__ dl, const T* __restrict__ d, const T* __restrict__ du,
+    const T* __restrict__ b, T* __restrict__ x, const int* __restrict__ off,
+    const int* __restrict__ len, const int* __restrict__ list, const int* __restrict__ count,
+    int slice) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* base = reinterpret_cast<T*>(smem_raw) + (size_t)warp * 4 * slice;
+  const int cnt = *count;
+  for (int i = blockIdx.x * GT_WARPS + warp; i < cnt; i += gridDim.x * GT_WARPS) {
+    const int s = list[i];
+    const int o = off[s], n = len[s];
+    const PartGeom g = part_geom(n, 32);
+    T* rA = base;
+    T* rB = rA + g.stride;
+    T* rC = rB + g.stride;
+    T* rD = rC + g.stride;
+    gt_load(dl, d, du, b, o, n, g.S, rA, rB, rC, rD, lane, 32);
+    __syncwarp();
+    part_solve_warp<T>(rA, rB, rC, rD, g, n, lane);
+    for (PartStrideIdx it(lane, 32, g.S); it.q < n; it.next(32)) x[o + it.q] = rD[it.idx()];
+    __syncwarp();
+  }
+}
+
+// Files system s under its length band (empty systems under none). Also
+// counts[GT_NB] = the packed extent max(off + len), counts[GT_NB + 1] = 1 if
+// a system has a negative offset (the batch is then refused).
+__global__ void k_gt_classify(const int* __restrict__ off, const int* __restrict__ len, int nsys,
+                              int* __restrict__ lists, int* __restrict__ counts) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys) return;
+  const int n = len[s];
+  if (n <= 0) return;
+  const int o = off[s];
+  if (o < 0 || o > INT_MAX - n) {
+    counts[GT_NB + 1] = 1;
+    return;
+  }
+  atomicMax(&counts[GT_NB], o + n);
+  int b = 0;
+  while (b < GT_NB - 1 && n > gt_band_hi(b)) ++b;
+  const int idx = atomicAdd(&counts[b], 1);
+  lists[(size_t)b * nsys + idx] = s;
+}
+
+// diagonally dominant synthetic systems for the autotuner (a counter hash)
+__device__ __forceinline__ double gt_unit(unsigned long long k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ULL;
+  k ^= k >> 33;
+  return (double)(k >> 11) * (1.0 / 9007199254740992.0);
+}
+
+template <class T>
+__global__ void k_gt_synth(T* dl, T* d, T* du, T* b, size_t rows, unsigned seed) {
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < rows;
+       r += (size_t)gridDim.x * blockDim.x) {
+    const unsigned long long k = ((unsigned long long)seed << 40) ^ (r * 4);
+    const double a = 2 * gt_unit(k) - 1, c = 2 * gt_unit(k + 1) - 1;
+    dl[r] = (T)a;
+    du[r] = (T)c;
+    d[r] = (T)(fabs(a) + fabs(c) + 0.1 + 0.9 * gt_unit(k + 2));
+    b[r] = (T)(2 * gt_unit(k + 3) - 1);
+  }
+}
+
+}  // namespace hyd
+
+// ====================================================================== host
 namespace {
-struct Scratch {
-  void* p = nullptr;
-  size_t bytes = 0;
-  int device = -1;
+
+using hyd::GT_NB;
+
+struct DevScratch {
+  void* w = nullptr;  // Thomas forward-sweep scratch (rows x 8 B)
+  size_t w_bytes = 0;
+  int* lists = nullptr;  // GT_NB x nsys
+  size_t lists_cap = 0;  // systems
+  int* counts = nullptr;  // GT_NB
 };
-Scratch g_scratch;  // per process; guarded by the caller's stream order
+
+struct DevInfo {
+  int nsm = 0, optin = 0;
+  bool init = false;
+  int table[2][GT_NB] = {};  // autotuned solver per dtype and band (0: not tuned)
+  DevScratch scr;
+};
+
+std::mutex g_mu;
+DevInfo g_dev[64];
+
+DevInfo* dev_info(int dev) {
+  if (dev < 0 || dev >= 64) return nullptr;
+  DevInfo& D = g_dev[dev];
+  if (!D.init) {
+    cudaDeviceGetAttribute(&D.nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&D.optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    D.init = true;
+  }
+  return &D;
+}
+
+// shared memory for systems of up to nmax rows (monotonic in nmax)
+template <class T, int NT>
+size_t cta_smem(int nmax) {
+  return sizeof(hyd::PartCtaShared<T, NT>) + 4 * sizeof(T) * (size_t)hyd::part_stride_bound(nmax, NT);
+}
+
+template <class T>
+size_t warp_smem(int nmax) {
+  return (size_t)hyd::GT_WARPS * 4 * sizeof(T) * (size_t)hyd::part_stride_bound(nmax, 32);
+}
+
+// longest system the CTA solver with NT threads takes on this device
+template <class T, int NT>
+int cta_max_rows(const DevInfo& D) {
+  int lo = 2, hi = 1 << 16;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (cta_smem<T, NT>(mid) <= (size_t)D.optin) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+struct Caps {
+  int cta256, cta512;  // longest systems of the two CTA tiles
+};
+
+template <class T>
+Caps caps_of(const DevInfo& D) {
+  return Caps{cta_max_rows<T, 256>(D), cta_max_rows<T, 512>(D)};
+}
+
+bool feasible(int algo, int band, const Caps& c) {
+  const int hi = hyd::gt_band_hi(band);
+  if (algo == HYDIST_GTSV_THOMAS) return true;
+  if (algo == HYDIST_GTSV_WARP) return hi <= hyd::GT_WARP_MAX;
+  if (algo == HYDIST_GTSV_PARTITION) return hi <= c.cta256;
+  if (algo == HYDIST_GTSV_PARTITION_512) return hi <= c.cta512;
+  return false;
+}
+
+// solver of a band when nothing was tuned: warp for short systems, the
+// 512-thread tile for long ones that fit, the 256-thread tile beyond,
+// Thomas for what fits no shared memory
+int default_algo(int band, const Caps& c) {
+  if (feasible(HYDIST_GTSV_WARP, band, c)) return HYDIST_GTSV_WARP;
+  if (feasible(HYDIST_GTSV_PARTITION_512, band, c)) return HYDIST_GTSV_PARTITION_512;
+  if (feasible(HYDIST_GTSV_PARTITION, band, c)) return HYDIST_GTSV_PARTITION;
+  return HYDIST_GTSV_THOMAS;
+}
+
+template <class T, int NT>
+int launch_cta(int nmax, const T* dl, const T* d, const T* du, const T* b, T* x, const int* off,
+               const int* len, const int* list, const int* count, int nsys_band, const DevInfo& D,
+               cudaStream_t st) {
+  const size_t smem = cta_smem<T, NT>(nmax);
+  static bool attr[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr[dev]) {
+    cudaFuncSetAttribute(hyd::k_gtsv_cta<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, D.optin);
+    attr[dev] = true;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hyd::k_gtsv_cta<T, NT>, NT, smem);
+  if (per_sm < 1) return HYDIST_ERR_CUDA;
+  const int grid = std::min(nsys_band, per_sm * D.nsm);
+  hyd::k_gtsv_cta<T, NT><<<grid, NT, smem, st>>>(dl, d, du, b, x, off, len, list, count);
+  return HYDIST_OK;
+}
+
+template <class T>
+int launch_band(int algo, int band, const T* dl, const T* d, const T* du, const T* b, T* x, T* w,
+                const int* off, const int* len, const int* list, const int* count, int nsys_band,
+                const DevInfo& D, cudaStream_t st) {
+  if (nsys_band <= 0) return HYDIST_OK;
+  const int hi = hyd::gt_band_hi(band);
+  int rc = HYDIST_OK;
+  if (algo == HYDIST_GTSV_PARTITION) {
+    rc = launch_cta<T, 256>(hi, dl, d, du, b, x, off, len, list, count, nsys_band, D, st);
+  } else if (algo == HYDIST_GTSV_PARTITION_512) {
+    rc = launch_cta<T, 512>(hi, dl, d, du, b, x, off, len, list, count, nsys_band, D, st);
+  } else if (algo == HYDIST_GTSV_WARP) {
+    const int nmax = std::min(hi, hyd::GT_WARP_MAX);
+    const int slice = hyd::part_stride_bound(nmax, 32);
+    const size_t smem = warp_smem<T>(nmax);
+    static bool attr[64][2] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attr[dev][sizeof(T) == 4]) {
+      cudaFuncSetAttribute(hyd::k_gtsv_warp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, D.optin);
+      attr[dev][sizeof(T) == 4] = true;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hyd::k_gtsv_warp<T>, hyd::GT_WARPS * 32,
+                                                  smem);
+    if (per_sm < 1) return HYDIST_ERR_CUDA;
+    const int grid = std::min((nsys_band + hyd::GT_WARPS - 1) / hyd::GT_WARPS, per_sm * D.nsm);
+    hyd::k_gtsv_warp<T><<<grid, hyd::GT_WARPS * 32, smem, st>>>(dl, d, du, b, x, off, len, list,
+                                                                  count, slice);
+  } else {
+    const int bs = 128;
+    const int grid = std::min((nsys_band + bs - 1) / bs, 8 * D.nsm);
+    hyd::k_thomas_list<T><<<grid, bs, 0, st>>>(dl, d, du, b, x, w, off, len, list, count);
+  }
+  if (rc != HYDIST_OK) return rc;
+  return cudaGetLastError() == cudaSuccess ? HYDIST_OK : HYDIST_ERR_CUDA;
+}
+
+int ensure_scratch(DevScratch& s, size_t w_bytes, size_t nsys) {
+  if (w_bytes > 0 && s.w_bytes < w_bytes) {
+    if (s.w) cudaFree(s.w);
+    s.w = nullptr;
+    s.w_bytes = 0;
+    if (cudaMalloc(&s.w, w_bytes + 256) != cudaSuccess) return HYDIST_ERR_OOM;
+    s.w_bytes = w_bytes;
+  }
+  if (s.lists_cap < nsys) {
+    if (s.lists) cudaFree(s.lists);
+    s.lists = nullptr;
+    s.lists_cap = 0;
+    if (cudaMalloc(&s.lists, (size_t)GT_NB * nsys * sizeof(int)) != cudaSuccess) return HYDIST_ERR_OOM;
+    s.lists_cap = nsys;
+  }
+  if (!s.counts && cudaMalloc(&s.counts, (GT_NB + 2) * sizeof(int)) != cudaSuccess)
+    return HYDIST_ERR_OOM;
+  return HYDIST_OK;
+}
+
+// one batched solve with a given solver per band (table[b])
+template <class T>
+int solve_batch(const T* dl, const T* d, const T* du, const T* b, T* x, const int* off,
+                const int* len, int nsys, const int table[GT_NB], DevInfo& D, cudaStream_t st) {
+  int rc = ensure_scratch(D.scr, 0, (size_t)nsys);
+  if (rc != HYDIST_OK) return rc;
+  if (cudaMemsetAsync(D.scr.counts, 0, (GT_NB + 2) * sizeof(int), st) != cudaSuccess)
+    return HYDIST_ERR_CUDA;
+  hyd::k_gt_classify<<<(nsys + 255) / 256, 256, 0, st>>>(off, len, nsys, D.scr.lists, D.scr.counts);
+  // band sizes, packed extent and the offset check in one synchronisation
+  int counts[GT_NB + 2];
+  if (cudaMemcpyAsync(counts, D.scr.counts, sizeof(counts), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return HYDIST_ERR_CUDA;
+  if (counts[GT_NB + 1]) return HYDIST_ERR_ARG;
+  bool thomas = false;
+  for (int bnd = 0; bnd < GT_NB; ++bnd) thomas |= counts[bnd] > 0 && table[bnd] == HYDIST_GTSV_THOMAS;
+  if (thomas) {
+    rc = ensure_scratch(D.scr, (size_t)counts[GT_NB] * sizeof(T), (size_t)nsys);
+    if (rc != HYDIST_OK) return rc;
+  }
+  for (int bnd = 0; bnd < GT_NB; ++bnd) {
+    rc = launch_band<T>(table[bnd], bnd, dl, d, du, b, x, (T*)D.scr.w, off, len,
+                        D.scr.lists + (size_t)bnd * nsys, D.scr.counts + bnd, counts[bnd], D, st);
+    if (rc != HYDIST_OK) return rc;
+  }
+  return HYDIST_OK;
+}
+
+template <class T>
+int autotune(DevInfo& D, int dtype, cudaStream_t st) {
+  const Caps caps = caps_of<T>(D);
+  for (int bnd = 0; bnd < GT_NB; ++bnd) {
+    int cands[4], nc = 0;
+    for (int a : {HYDIST_GTSV_THOMAS, HYDIST_GTSV_PARTITION, HYDIST_GTSV_PARTITION_512,
+                  HYDIST_GTSV_WARP})
+      if (feasible(a, bnd, caps)) cands[nc++] = a;
+    if (nc == 1) {
+      D.table[dtype][bnd] = cands[0];
+      continue;
+    }
+    // synthetic batch: lengths log-uniform within the band, about 4M rows
+    const int lo = bnd == 0 ? 1 : hyd::gt_band_hi(bnd - 1) + 1;
+    const int hi = std::min(hyd::gt_band_hi(bnd), 1 << 16);
+    std::vector<int> off, len;
+    size_t rows = 0;
+    unsigned long long r = 0x9e3779b97f4a7c15ULL * (bnd + 1);
+    while (rows < (4u << 20) && (int)len.size() < 16384) {
+      r = r * 6364136223846793005ULL + 1442695040888963407ULL;
+      const double u = (double)(r >> 11) * (1.0 / 9007199254740992.0);
+      const int n = std::max(lo, std::min(hi, (int)std::exp(std::log((double)lo) +
+                                                            u * (std::log((double)hi) - std::log((double)lo)))));
+      off.push_back((int)rows);
+      len.push_back(n);
+      rows += n;
+    }
+    const int ns = (int)len.size();
+    T *dl = nullptr, *dd = nullptr, *du = nullptr, *bb = nullptr, *xx = nullptr;
+    int *doff = nullptr, *dlen = nullptr;
+    bool ok = cudaMalloc(&dl, rows * sizeof(T)) == cudaSuccess &&
+              cudaMalloc(&dd, rows * sizeof(T)) == cudaSuccess &&
+              cudaMalloc(&du, rows * sizeof(T)) == cudaSuccess &&
+              cudaMalloc(&bb, rows * sizeof(T)) == cudaSuccess &&
+              cudaMalloc(&xx, rows * sizeof(T)) == cudaSuccess &&
+              cudaMalloc(&doff, ns * sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&dlen, ns * sizeof(int)) == cudaSuccess;
+    int rc = ok ? HYDIST_OK : HYDIST_ERR_OOM;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ok) {
+      cudaMemcpyAsync(doff, off.data(), ns * sizeof(int), cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(dlen, len.data(), ns * sizeof(int), cudaMemcpyHostToDevice, st);
+      hyd::k_gt_synth<T><<<4 * D.nsm, 256, 0, st>>>(dl, dd, du, bb, rows, 77u + bnd);
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      float best = 1e30f;
+      int best_a = cands[0];
+      for (int c = 0; c < nc && rc == HYDIST_OK; ++c) {
+        int table[GT_NB];
+        for (int k = 0; k < GT_NB; ++k) table[k] = cands[c];
+        float tmin = 1e30f;
+        for (int rep = 0; rep < 4 && rc == HYDIST_OK; ++rep) {
+          cudaEventRecord(e0, st);
+          rc = solve_batch<T>(dl, dd, du, bb, xx, doff, dlen, ns, table, D, st);
+          cudaEventRecord(e1, st);
+          cudaEventSynchronize(e1);
+          float ms = 0;
+          cudaEventElapsedTime(&ms, e0, e1);
+          if (rep > 0) tmin = std::min(tmin, ms);  // the first run warms up
+        }
+        if (tmin < best) {
+          best = tmin;
+          best_a = cands[c];
+        }
+      }
+      D.table[dtype][bnd] = best_a;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    for (void* p : {(void*)dl, (void*)dd, (void*)du, (void*)bb, (void*)xx, (void*)doff, (void*)dlen})
+      if (p) cudaFree(p);
+    if (rc != HYDIST_OK) return rc;
+  }
+  return cudaGetLastError() == cudaSuccess ? HYDIST_OK : HYDIST_ERR_CUDA;
+}
+
 }  // namespace
+
+extern "C" int hydist_gtsv_autotune(int32_t dtype, void* stream, int32_t* algo_per_band) {
+  if (dtype != 0 && dtype != 1) {
+    hyd::set_last_error("hydist_gtsv_autotune: dtype must be 0 (FP64) or 1 (FP32)");
+    return HYDIST_ERR_ARG;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return HYDIST_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(g_mu);
+  DevInfo* D = dev_info(dev);
+  if (!D) return HYDIST_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int rc = dtype == 0 ? autotune<double>(*D, 0, st) : autotune<float>(*D, 1, st);
+  if (rc != HYDIST_OK) {
+    hyd::set_last_error("hydist_gtsv_autotune: a CUDA call failed");
+    return rc;
+  }
+  if (algo_per_band)
+    for (int b = 0; b < GT_NB; ++b) algo_per_band[b] = D->table[dtype][b];
+  return HYDIST_OK;
+}
+
+extern "C" int hydist_gtsv_band_bounds(int32_t* hi) {
+  if (!hi) return HYDIST_ERR_ARG;
+  for (int b = 0; b < GT_NB; ++b) hi[b] = hyd::gt_band_hi(b);
+  return HYDIST_OK;
+}
 
 extern "C" int hydist_gtsv_batched(const void* dl, const void* d, const void* du, const void* b,
                                    void* x, const int32_t* offsets, const int32_t* lengths,
                                    int32_t nsys, int32_t dtype, int32_t algo, void* stream) {
-  if (!dl || !d || !du || !b || !x || !offsets || !lengths || nsys < 0) return HYDIST_ERR_ARG;
-  if (dtype != 0 && dtype != 1) return HYDIST_ERR_ARG;
-  if (algo < 0 || algo > 3) return HYDIST_ERR_ARG;
-  if (algo >= 2) {
-    hyd::set_last_error("hydist_gtsv_batched: algo 2 and 3 are not implemented yet");
+  if (!dl || !d || !du || !b || !x || !offsets || !lengths || nsys < 0) {
+    hyd::set_last_error("hydist_gtsv_batched: null pointer or negative count");
+    return HYDIST_ERR_ARG;
+  }
+  if (dtype != 0 && dtype != 1) {
+    hyd::set_last_error("hydist_gtsv_batched: dtype must be 0 (FP64) or 1 (FP32)");
+    return HYDIST_ERR_ARG;
+  }
+  if (algo < HYDIST_GTSV_AUTO || algo > HYDIST_GTSV_PARTITION_512) {
+    hyd::set_last_error("hydist_gtsv_batched: unknown algo");
     return HYDIST_ERR_ARG;
   }
   if (nsys == 0) return HYDIST_OK;
   cudaStream_t st = (cudaStream_t)stream;
-  // total rows = max(off+len): read the last system's extent from device
-  // memory is avoided; the caller's x buffer bounds the rows, so scratch is
-  // sized from the packed layout through a small reduction on the host side
-  // of the caller. Here: scratch sized lazily to the x span.
-  int last_off = 0, last_len = 0;
-  if (cudaMemcpyAsync(&last_off, offsets + (nsys - 1), 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaMemcpyAsync(&last_len, lengths + (nsys - 1), 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess)
-    return HYDIST_ERR_CUDA;
-  const size_t rows = (size_t)last_off + (size_t)last_len;
-  const size_t esz = dtype == 0 ? 8 : 4;
   int dev = 0;
-  cudaGetDevice(&dev);
-  if (g_scratch.bytes < rows * esz || g_scratch.device != dev) {
-    if (g_scratch.p) cudaFree(g_scratch.p);
-    g_scratch.p = nullptr;
-    g_scratch.bytes = 0;
-    if (cudaMalloc(&g_scratch.p, rows * esz + 256) != cudaSuccess) return HYDIST_ERR_OOM;
-    g_scratch.bytes = rows * esz;
-    g_scratch.device = dev;
+  if (cudaGetDevice(&dev) != cudaSuccess) return HYDIST_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(g_mu);
+  DevInfo* D = dev_info(dev);
+  if (!D) return HYDIST_ERR_ARG;
+  const Caps caps = dtype == 0 ? caps_of<double>(*D) : caps_of<float>(*D);
+  int table[GT_NB];
+  for (int bnd = 0; bnd < GT_NB; ++bnd) {
+    int a = algo;
+    if (a == HYDIST_GTSV_AUTO) a = D->table[dtype][bnd] ? D->table[dtype][bnd] : default_algo(bnd, caps);
+    // a solver that cannot take the band's lengths hands it to the next
+    // more general one: warp -> 512-thread tile -> 256-thread tile -> Thomas
+    if (a == HYDIST_GTSV_WARP && !feasible(a, bnd, caps)) a = HYDIST_GTSV_PARTITION_512;
+    if (a == HYDIST_GTSV_PARTITION_512 && !feasible(a, bnd, caps)) a = HYDIST_GTSV_PARTITION;
+    if (a == HYDIST_GTSV_PARTITION && !feasible(a, bnd, caps)) a = HYDIST_GTSV_THOMAS;
+    table[bnd] = a;
   }
-  const int bs = 128, gs = (nsys + bs - 1) / bs;
-  if (dtype == 0)
-    hyd::k_thomas_batched<double><<<gs, bs, 0, st>>>(
-        (const double*)dl, (const double*)d, (const double*)du, (const double*)b, (double*)x,
-        (double*)g_scratch.p, offsets, lengths, nsys);
-  else
-    hyd::k_thomas_batched<float><<<gs, bs, 0, st>>>((const float*)dl, (const float*)d,
-                                                    (const float*)du, (const float*)b, (float*)x,
-                                                    (float*)g_scratch.p, offsets, lengths, nsys);
-  if (cudaGetLastError() != cudaSuccess) return HYDIST_ERR_CUDA;
-  return HYDIST_OK;
+  int rc;
+  if (dtype == 0) {
+    rc = solve_batch<double>((const double*)dl, (const double*)d, (const double*)du,
+                             (const double*)b, (double*)x, offsets, lengths, nsys, table, *D, st);
+  } else {
+    rc = solve_batch<float>((const float*)dl, (const float*)d, (const float*)du, (const float*)b,
+                            (float*)x, offsets, lengths, nsys, table, *D, st);
+  }
+  if (rc == HYDIST_ERR_ARG) hyd::set_last_error("hydist_gtsv_batched: a system has a negative offset");
+  else if (rc != HYDIST_OK) hyd::set_last_error("hydist_gtsv_batched: a CUDA call failed");
+  return rc;
 }
 
 // ---- allocation-free variant --------------------------------------------
@@ -131,8 +577,6 @@ extern "C" int hydist_gtsv_batched(const void* dl, const void* d, const void* du
 // (different streams or host threads) race on it.
 namespace hyd {
 
-void set_last_error(const char* m);
-
 __device__ __align__(256) double g_noalloc_w[HYDIST_GTSV_NOALLOC_MAX_ROWS];
 
 // Thomas for systems that lie inside the packed rows [0, rows); a system
@@ -147,33 +591,7 @@ __global__ void k_thomas_noalloc(const T* __restrict__ dl, const T* __restrict__
   if (s >= nsys) return;
   const int o = off[s], n = len[s];
   if (n <= 0 || o < 0 || o > rows - n) return;
-  const T* A = dl + o;
-  const T* B = d + o;
-  const T* C = du + o;
-  const T* D = b + o;
-  T* X = x + o;
-  T* Wp = w + o;
-  if (n == 1) {
-    X[0] = D[0] / B[0];
-    return;
-  }
-  T ap = -C[0] / B[0];
-  T bp = D[0] / B[0];
-  Wp[0] = ap;
-  X[0] = bp;
-  for (int i = 1; i < n - 1; ++i) {
-    const T ep = A[i] * ap + B[i];
-    ap = -C[i] / ep;
-    bp = (D[i] - A[i] * bp) / ep;
-    Wp[i] = ap;
-    X[i] = bp;
-  }
-  T xr = (D[n - 1] - A[n - 1] * bp) / (B[n - 1] + A[n - 1] * ap);
-  X[n - 1] = xr;
-  for (int i = n - 2; i >= 0; --i) {
-    xr = X[i] + Wp[i] * xr;
-    X[i] = xr;
-  }
+  thomas_system(dl + o, d + o, du + o, b + o, x + o, w + o, n);
 }
 
 }  // namespace hyd

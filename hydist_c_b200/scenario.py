@@ -123,6 +123,25 @@ def config3_member(k, seed=20263000):
 SERVING_MESHES = ((256, 128), (512, 256), (1024, 512), (2048, 1024))
 
 
+def tridiag_batch(nsys=16384, seed=20262000, lo=16, hi=4096, lengths=None):
+    """The batched tridiagonal microbenchmark: nsys diagonally dominant
+    systems with lengths log-uniform in [lo, hi] (uneven wet segments), packed
+    one after another. a, c ~ U(-1, 1); b = |a| + |c| + U(0.1, 1.0); rhs
+    ~ N(0, 1). Returns dl, d, du, rhs (FP64), offsets, lengths (int32)."""
+    rng = np.random.default_rng(seed)
+    if lengths is None:
+        lengths = np.exp(rng.uniform(np.log(lo), np.log(hi), nsys)).astype(np.int32)
+    lengths = np.asarray(lengths, dtype=np.int32)
+    offsets = np.zeros(len(lengths), np.int32)
+    offsets[1:] = np.cumsum(lengths[:-1])
+    rows = int(lengths.sum())
+    a = rng.uniform(-1, 1, rows)
+    c = rng.uniform(-1, 1, rows)
+    d = np.abs(a) + np.abs(c) + rng.uniform(0.1, 1.0, rows)
+    b = rng.standard_normal(rows)
+    return a, d, c, b, offsets, lengths
+
+
 def serving_requests(n, rate=20.0, seed=20264000):
     """Poisson request stream: arrival times, mesh drawn uniformly from
     SERVING_MESHES, horizon U(10,60) simulated minutes."""

@@ -210,16 +210,52 @@ int hydist_kernel_launches(HydistHandle* h, int64_t* count);
  * batched, host-callable entry point. System s occupies rows
  * [offsets[s], offsets[s] + lengths[s]) of the packed arrays; dl[first row]
  * and du[last row] of each system are ignored. Arrays are device pointers.
- * dtype: 0 = FP64, 1 = FP32. algo: 0 = the library's choice (Thomas for
- * now), 1 = Thomas (thread per system); 2 (partitioned Thomas / SPIKE) and
- * 3 (PCR-Thomas) are reserved and refused with HYDIST_ERR_ARG until they
- * exist. stream is a cudaStream_t (NULL = default stream). Scratch is
- * allocated by the library on first use; the call synchronises the stream
- * once to read the packed row count. */
+ * dtype: 0 = FP64, 1 = FP32. algo (enum HydistGtsvAlgo):
+ *   AUTO       per length band, the solver hydist_gtsv_autotune chose on
+ *              this device (before any tuning: WARP up to 512 rows, then
+ *              PARTITION_512 or PARTITION where the system fits a CTA's
+ *              shared memory, THOMAS beyond);
+ *   THOMAS     one thread per system, in place in global memory;
+ *   PARTITION  one 256-thread CTA per system staged in shared memory:
+ *              chunked Thomas with the chunk separators' reduced system
+ *              solved by parallel cyclic reduction (SPIKE-style partition,
+ *              no pivoting);
+ *   WARP       one warp per system staged in shared memory, partition with
+ *              a shuffle PCR of 32 separators (systems up to 512 rows);
+ *   PARTITION_512  PARTITION with 512-thread tiles (more warps per system,
+ *              less shared memory left for long systems).
+ * A solver that cannot take a band's lengths passes it on (WARP ->
+ * PARTITION_512 -> PARTITION -> THOMAS). Systems of length 0 are skipped.
+ * No pivoting: the systems are expected to be diagonally dominant, as the
+ * ADI sweeps' are.
+ * stream is a cudaStream_t (NULL = default stream). Scratch is allocated by
+ * the library on first use and grown as needed; the call synchronises the
+ * stream once, to read the band sizes and the packed extent. A batch with a
+ * negative offset is refused with HYDIST_ERR_ARG. */
+enum HydistGtsvAlgo {
+  HYDIST_GTSV_AUTO = 0,
+  HYDIST_GTSV_THOMAS = 1,
+  HYDIST_GTSV_PARTITION = 2,
+  HYDIST_GTSV_WARP = 3,
+  HYDIST_GTSV_PARTITION_512 = 4
+};
 int hydist_gtsv_batched(const void* dl, const void* d, const void* du,
                         const void* b, void* x, const int32_t* offsets,
                         const int32_t* lengths, int32_t nsys, int32_t dtype,
                         int32_t algo, void* stream);
+
+/* Length bands of the batched solver: band b holds the systems with
+ * hi[b-1] < length <= hi[b] (hi[-1] = 0), HYDIST_GTSV_BANDS entries. */
+#define HYDIST_GTSV_BANDS 7
+int hydist_gtsv_band_bounds(int32_t* hi);
+
+/* Autotuner (the reference has none): for each length band, times every
+ * solver that can take the band's lengths on a synthetic diagonally
+ * dominant batch of that band (about 4M rows) on this device and keeps the
+ * fastest for algo = AUTO. Allocates temporary device memory and
+ * synchronises the stream. algo_per_band (may be NULL) receives the choice
+ * per band. */
+int hydist_gtsv_autotune(int32_t dtype, void* stream, int32_t* algo_per_band);
 
 /* Allocation-free batched Thomas solve (no counterpart in the reference,
  * whose gtsv allocates per call). Same arrays and results as
