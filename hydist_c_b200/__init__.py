@@ -96,6 +96,11 @@ class Simulation:
     def sync(self):
         capi.check(self._lib, self._lib.hydist_sync(self._h), "hydist_sync")
 
+    def half_step(self, half: int):
+        """One half of a step (0: x sweep half, 1: y sweep half); halves
+        alternate starting with 0."""
+        capi.check(self._lib, self._lib.hydist_half_step(self._h, int(half)), "hydist_half_step")
+
     def step_traced(self) -> dict:
         """One full step with per-phase device times (ms)."""
         ms = (C.c_float * len(capi.PHASES))()

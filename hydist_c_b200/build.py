@@ -18,7 +18,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "libhydist_b200.so"
-SOURCES = ["engine.cu", "hydro.cu", "sweep.cu", "sediment.cu", "tridiag.cu"]
+SOURCES = ["engine.cu", "hydro.cu", "sweep.cu", "sediment.cu", "tridiag.cu", "compat.cu"]
 HEADERS = ["common.cuh", "hydro.cuh", "assembly.cuh", "linesolve.cuh", "partsolve.cuh", "sediment_cell.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -42,7 +42,8 @@ def _stale(out: Path, deps) -> bool:
 def build(force: bool = False, verbose: bool = False) -> Path:
     OBJ.mkdir(exist_ok=True)
     nvcc = _nvcc()
-    hdrs = [CSRC / h for h in HEADERS] + [ROOT / "include" / "hydist_capi.h"]
+    hdrs = [CSRC / h for h in HEADERS] + [ROOT / "include" / "hydist_capi.h",
+                                            ROOT / "include" / "hydist_compat.h"]
     objs = []
     logs = []
     for s in SOURCES:

@@ -58,6 +58,22 @@ class HydistScenario(C.Structure):
                 ("boundary_type", _ip), ("bienQ", C.c_int32 * 4), ("FS0", _dp)]
 
 
+_vp = C.c_void_p
+EXTERNAL_READONLY = ("h", "hsnham", "visco", "Fw", "htaiz", "htaiz_bd", "Kx1", "Ky1", "Tsxw", "Tsyw",
+                     "bc_up", "bc_down", "bc_left", "bc_right", "CC_up", "CC_down", "CC_left",
+                     "CC_right", "boundary_type")
+EXTERNAL_STATE = ("u", "v", "z", "t_u", "t_v", "t_z", "H_moi", "Htdu", "Htdv", "FS", "tFS", "VTH",
+                  "Kx", "Ky", "dH", "Qbx", "Qby", "khouot", "daui", "cuoii", "moci", "dauj",
+                  "cuoij", "mocj", "ubt", "ubp", "vbt", "vbd")
+
+
+class HydistExternal(C.Structure):
+    """Caller-owned device arrays (include/hydist_capi.h); pointers as ints."""
+    _fields_ = ([("M", C.c_int32), ("N", C.c_int32), ("total_time", C.c_int32),
+                 ("bienQ", C.c_int32 * 4)] +
+                [(k, _vp) for k in EXTERNAL_READONLY + EXTERNAL_STATE])
+
+
 def default_params() -> HydistParams:
     """Reference constants of Load_coeffs (loader.cpp:4-87)."""
     p = HydistParams()
@@ -185,6 +201,10 @@ def _declare(lib):
     lib.hydist_gtsv_batched_noalloc.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int32,
                                                 C.c_int32, C.c_int32, vp]
     lib.hydist_gtsv_autotune.argtypes = [C.c_int32, vp, _ip]
+    lib.hydist_create_external.argtypes = [C.POINTER(HydistExternal), C.POINTER(HydistParams),
+                                           C.POINTER(HydistOptions), C.c_int, C.POINTER(vp)]
+    lib.hydist_half_step.argtypes = [vp, C.c_int32]
+    lib.hydist_update_boundary.argtypes = [vp, C.c_double]
     lib.hydist_gtsv_band_bounds.argtypes = [_ip]
 
 
@@ -205,7 +225,8 @@ EXPORTED_SYMBOLS = [
     "hydist_sync", "hydist_get_time", "hydist_set_time", "hydist_download", "hydist_upload", "hydist_mass",
     "hydist_step_graph", "hydist_stream", "hydist_gtsv_batched", "hydist_step_traced",
     "hydist_kernel_launches", "hydist_gtsv_batched_noalloc", "hydist_step_traced_sweeps",
-    "hydist_gtsv_autotune", "hydist_gtsv_band_bounds",
+    "hydist_gtsv_autotune", "hydist_gtsv_band_bounds", "hydist_create_external",
+    "hydist_half_step", "hydist_update_boundary",
 ]
 GTSV_AUTO, GTSV_THOMAS, GTSV_PARTITION, GTSV_WARP, GTSV_PARTITION_512 = 0, 1, 2, 3, 4
 GTSV_BANDS = 7

@@ -117,6 +117,7 @@ struct HydistHandle {
   Trace trace;                                    // kernel launch counter
   cudaEvent_t ev[PH_COUNT + 1] = {};
   cudaEvent_t kev[2 * KS_COUNT] = {};
+  int next_half = 0;  // 1 while the second half of a step is pending
 };
 
 namespace {
@@ -289,16 +290,9 @@ void hydist_bienq_from_boundary_type(const int32_t* bt, int32_t n, int32_t bienQ
   for (int k = 0; k < 4; ++k) bienQ[k] = (bt && k < n && bt[k] == 2) ? 1 : 0;
 }
 
-int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistOptions* o,
-                  int device, HydistHandle** out) {
-  if (!sc || !p || !o || !out) return fail(HYDIST_ERR_ARG, "null argument");
-  *out = nullptr;
-  if (sc->M < 4 || sc->N < 4 || sc->total_time < 2)
-    return fail(HYDIST_ERR_ARG, "mesh must be at least 4x4 and series at least 2 hours long");
-  if (!sc->h || !sc->hsnham || !sc->visco || !sc->Fw || !sc->boundary_type)
-    return fail(HYDIST_ERR_ARG, "missing input array");
-  if (sc->n_boundary_type < 4 * SEG)
-    return fail(HYDIST_ERR_ARG, "boundary_type needs 4 sides x 20 segments");
+namespace {
+
+int check_params(const HydistParams* p, const HydistOptions* o) {
   if (!(p->dX > 0 && p->dY > 0 && p->dT > 0)) return fail(HYDIST_ERR_ARG, "dX, dY, dT must be > 0");
   if (o->precision != HYDIST_FP64 && o->precision != HYDIST_FP32_REFINE)
     return fail(HYDIST_ERR_ARG, "unknown precision");
@@ -309,24 +303,77 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistO
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(HYDIST_ERR_NODEVICE, "no CUDA device");
+  return HYDIST_OK;
+}
+
+// Handle, stream and constants of a new scenario (no arrays yet).
+int new_handle(const HydistParams* p, const HydistOptions* o, int device, int M, int N, int T,
+               const int32_t bienQ[4], HydistHandle** out) {
   auto* h = new HydistHandle();
+  *out = h;
   if (device < 0) cudaGetDevice(&device);
   h->device = device;
-  int rc = [&]() -> int {
-    CK(cudaSetDevice(device));
-    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-    derive(*p, h->c);
-    h->o = *o;
-    h->t = o->t_start;
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  derive(*p, h->c);
+  h->o = *o;
+  h->t = o->t_start;
+  State& S = h->S;
+  S.M = M;
+  S.N = N;
+  S.W = S.M + 3;
+  S.H = S.N + 3;
+  S.T = T;
+  for (int k = 0; k < 4; ++k) S.bienQ[k] = bienQ[k] ? 1 : 0;
+  S.ketdinh = o->ketdinh ? 1 : 0;
+  S.race_new = 1;
+  return HYDIST_OK;
+}
+
+// The arrays only this library uses: smoothing buffers, boundary weights,
+// line-solver scratch, flags, counters, the device clock.
+int private_arrays(HydistHandle* h) {
+  State& S = h->S;
+  const size_t n = (size_t)S.W * S.H;
+  TRY(dalloc(h, &S.tmp, n));
+  TRY(dalloc(h, &S.sv, n));
+  S.su = S.tmp;
+  TRY(dalloc(h, &S.hi, 2 * (S.M + S.N + 6)));
+  TRY(dalloc(h, &S.hmax, 4));
+  TRY(dalloc(h, &S.err, 4));
+  TRY(dalloc(h, &S.colflag, S.W));
+  TRY(dalloc(h, &S.segcnt, 2 * S.H + 2 * S.W));
+  TRY(dalloc(h, &S.clock, 4));
+  TRY(set_device_clock(h));
+  // partitioned line solver scratch: 3 doubles per unknown, 4 lines per
+  // slot, one slot per CTA of the persistent sweep grid
+  int nsm = 0;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+  S.lslots = 2 * nsm;
+  const size_t U = (size_t)2 * std::max(S.M, S.N);
+  TRY(dalloc(h, &S.lscratch, (size_t)S.lslots * 3 * U * 4));
+  h->mass_blocks = 296;
+  TRY(dalloc(h, &h->mass_part, h->mass_blocks + 1));
+  return HYDIST_OK;
+}
+
+}  // namespace
+
+int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistOptions* o,
+                  int device, HydistHandle** out) {
+  if (!sc || !p || !o || !out) return fail(HYDIST_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (sc->M < 4 || sc->N < 4 || sc->total_time < 2)
+    return fail(HYDIST_ERR_ARG, "mesh must be at least 4x4 and series at least 2 hours long");
+  if (!sc->h || !sc->hsnham || !sc->visco || !sc->Fw || !sc->boundary_type)
+    return fail(HYDIST_ERR_ARG, "missing input array");
+  if (sc->n_boundary_type < 4 * SEG)
+    return fail(HYDIST_ERR_ARG, "boundary_type needs 4 sides x 20 segments");
+  TRY(check_params(p, o));
+  HydistHandle* h = nullptr;
+  int rc = new_handle(p, o, device, sc->M, sc->N, sc->total_time, sc->bienQ, &h);
+  if (rc == HYDIST_OK) rc = [&]() -> int {
     State& S = h->S;
-    S.M = sc->M;
-    S.N = sc->N;
-    S.W = S.M + 3;
-    S.H = S.N + 3;
-    S.T = sc->total_time;
-    for (int k = 0; k < 4; ++k) S.bienQ[k] = sc->bienQ[k] ? 1 : 0;
-    S.ketdinh = o->ketdinh ? 1 : 0;
-    S.race_new = 1;
     const size_t n = (size_t)S.W * S.H;
     double* tmp;
     // static inputs
@@ -371,10 +418,9 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistO
     S.Tsyw = tmp;
     // state
     double** st[] = {&S.u, &S.v, &S.z, &S.tu, &S.tv, &S.tz, &S.Hmoi, &S.Htdu, &S.Htdv, &S.FS,
-                     &S.tFS, &S.VTH, &S.Kx, &S.Ky, &S.dH, &S.Qbx, &S.Qby, &S.tmp, &S.sv};
+                     &S.tFS, &S.VTH, &S.Kx, &S.Ky, &S.dH, &S.Qbx, &S.Qby};
     for (double** q : st) TRY(dalloc(h, q, n));
     TRY(dalloc(h, &S.khouot, n));
-    S.su = S.tmp;
     if (sc->FS0) {
       CK(cudaMemcpyAsync(S.FS, sc->FS0, n * 8, cudaMemcpyHostToDevice, h->stream));
       CK(cudaMemcpyAsync(S.tFS, sc->FS0, n * 8, cudaMemcpyHostToDevice, h->stream));
@@ -383,30 +429,13 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistO
     TRY(dalloc(h, &S.ubp, S.W));
     TRY(dalloc(h, &S.vbt, S.H));
     TRY(dalloc(h, &S.vbd, S.H));
-    TRY(dalloc(h, &S.hi, 2 * (S.M + S.N + 6)));
-    TRY(dalloc(h, &S.hmax, 4));
     TRY(dalloc(h, &S.daui, S.H * SEG));
     TRY(dalloc(h, &S.cuoii, S.H * SEG));
     TRY(dalloc(h, &S.moci, S.H));
     TRY(dalloc(h, &S.dauj, S.W * SEG));
     TRY(dalloc(h, &S.cuoij, S.W * SEG));
     TRY(dalloc(h, &S.mocj, S.W));
-    TRY(dalloc(h, &S.err, 4));
-    TRY(dalloc(h, &S.colflag, S.W));
-    TRY(dalloc(h, &S.segcnt, 2 * S.H + 2 * S.W));
-    TRY(dalloc(h, &S.clock, 4));
-    TRY(set_device_clock(h));
-    // partitioned line solver scratch: 3 doubles per unknown, 4 lines per
-    // slot, one slot per CTA of the persistent sweep grid
-    {
-      int nsm = 0;
-      CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-      S.lslots = 2 * nsm;
-      const size_t U = (size_t)2 * std::max(S.M, S.N);
-      TRY(dalloc(h, &S.lscratch, (size_t)S.lslots * 3 * U * 4));
-    }
-    h->mass_blocks = 296;
-    TRY(dalloc(h, &h->mass_part, h->mass_blocks + 1));
+    TRY(private_arrays(h));
     launch_init(S, h->c, h->stream);
     CK(cudaGetLastError());
     TRY(check_device_err(h));
@@ -418,6 +447,129 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistO
   }
   *out = h;
   return HYDIST_OK;
+}
+
+int hydist_create_external(const HydistExternal* e, const HydistParams* p, const HydistOptions* o,
+                           int device, HydistHandle** out) {
+  if (!e || !p || !o || !out) return fail(HYDIST_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (e->M < 4 || e->N < 4 || e->total_time < 2)
+    return fail(HYDIST_ERR_ARG, "mesh must be at least 4x4 and series at least 2 hours long");
+  const void* need[] = {e->h, e->hsnham, e->visco, e->Fw, e->htaiz, e->htaiz_bd, e->Kx1, e->Ky1,
+                        e->Tsxw, e->Tsyw, e->bc_up, e->bc_down, e->bc_left, e->bc_right,
+                        e->CC_up, e->CC_down, e->CC_left, e->CC_right, e->boundary_type,
+                        e->u, e->v, e->z, e->t_u, e->t_v, e->t_z, e->H_moi, e->Htdu, e->Htdv,
+                        e->FS, e->tFS, e->VTH, e->Kx, e->Ky, e->dH, e->Qbx, e->Qby, e->khouot,
+                        e->daui, e->cuoii, e->moci, e->dauj, e->cuoij, e->mocj, e->ubt, e->ubp,
+                        e->vbt, e->vbd};
+  for (const void* q : need)
+    if (!q) return fail(HYDIST_ERR_ARG, "missing device array");
+  TRY(check_params(p, o));
+  HydistHandle* h = nullptr;
+  int rc = new_handle(p, o, device, e->M, e->N, e->total_time, e->bienQ, &h);
+  if (rc == HYDIST_OK) rc = [&]() -> int {
+    State& S = h->S;
+    S.h = e->h;
+    S.hsnham = e->hsnham;
+    S.visco = e->visco;
+    S.Fw = e->Fw;
+    S.htaiz = e->htaiz;
+    S.htaiz_bd = e->htaiz_bd;
+    S.Kx1 = e->Kx1;
+    S.Ky1 = e->Ky1;
+    S.Tsxw = e->Tsxw;
+    S.Tsyw = e->Tsyw;
+    S.bc[0] = e->bc_up;
+    S.bc[1] = e->bc_down;
+    S.bc[2] = e->bc_left;
+    S.bc[3] = e->bc_right;
+    S.CC[0] = e->CC_up;
+    S.CC[1] = e->CC_down;
+    S.CC[2] = e->CC_left;
+    S.CC[3] = e->CC_right;
+    S.btype = e->boundary_type;
+    S.u = e->u;
+    S.v = e->v;
+    S.z = e->z;
+    S.tu = e->t_u;
+    S.tv = e->t_v;
+    S.tz = e->t_z;
+    S.Hmoi = e->H_moi;
+    S.Htdu = e->Htdu;
+    S.Htdv = e->Htdv;
+    S.FS = e->FS;
+    S.tFS = e->tFS;
+    S.VTH = e->VTH;
+    S.Kx = e->Kx;
+    S.Ky = e->Ky;
+    S.dH = e->dH;
+    S.Qbx = e->Qbx;
+    S.Qby = e->Qby;
+    S.khouot = e->khouot;
+    S.daui = e->daui;
+    S.cuoii = e->cuoii;
+    S.moci = e->moci;
+    S.dauj = e->dauj;
+    S.cuoij = e->cuoij;
+    S.mocj = e->mocj;
+    S.ubt = e->ubt;
+    S.ubp = e->ubp;
+    S.vbt = e->vbt;
+    S.vbd = e->vbd;
+    TRY(private_arrays(h));
+    // the boundary discharge weights from the caller's depths; everything
+    // else was set up by the caller (Onetime_init, the segment scans and
+    // Htuongdoi, as the reference's main does before the time loop)
+    launch_preprocess(S, h->c, h->stream);
+    CK(cudaGetLastError());
+    TRY(check_device_err(h));
+    return HYDIST_OK;
+  }();
+  if (rc != HYDIST_OK) {
+    hydist_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return HYDIST_OK;
+}
+
+int hydist_half_step(HydistHandle* h, int32_t half) {
+  if (!h) return fail(HYDIST_ERR_ARG, "null handle");
+  if (half != 0 && half != 1) return fail(HYDIST_ERR_ARG, "half must be 0 or 1");
+  if (half != h->next_half)
+    return fail(HYDIST_ERR_STATE, half == 0 ? "the second half-step is pending"
+                                            : "the first half-step has not run");
+  CK(cudaSetDevice(h->device));
+  if (half == 0) TRY(check_horizon(h, 1));
+  const double t = h->t + 0.5 * h->c.dT;
+  const bool sed = t >= h->o.sediment_start;
+  if (half == 0) {
+    launch_half_x(h->S, h->c, h->stream, &h->trace);
+    if (sed) launch_sediment(h->S, h->c, h->o.bed_change_start, true, h->stream, &h->trace);
+  } else {
+    launch_half_y(h->S, h->c, h->stream, &h->trace);
+    if (sed) launch_sediment(h->S, h->c, h->o.bed_change_start, false, h->stream, &h->trace);
+  }
+  h->t = t;
+  h->next_half = 1 - half;
+  CK(cudaGetLastError());
+  return HYDIST_OK;
+}
+
+int hydist_update_boundary(HydistHandle* h, double t) {
+  if (!h) return fail(HYDIST_ERR_ARG, "null handle");
+  CK(cudaSetDevice(h->device));
+  const double keep = h->t;
+  h->t = t;
+  int rc = set_device_clock(h);
+  if (rc == HYDIST_OK) {
+    launch_boundary(h->S, h->stream);
+    h->trace.launches += 1;
+    rc = cudaGetLastError() == cudaSuccess ? HYDIST_OK : fail(HYDIST_ERR_CUDA, "boundary launch failed");
+  }
+  h->t = keep;
+  const int rc2 = set_device_clock(h);
+  return rc != HYDIST_OK ? rc : rc2;
 }
 
 int hydist_destroy(HydistHandle* h) {
@@ -436,6 +588,7 @@ int hydist_destroy(HydistHandle* h) {
 
 int hydist_step(HydistHandle* h, int32_t nsteps) {
   if (!h) return fail(HYDIST_ERR_ARG, "null handle");
+  if (h->next_half) return fail(HYDIST_ERR_STATE, "the second half-step is pending");
   if (nsteps < 0) return fail(HYDIST_ERR_ARG, "negative step count");
   CK(cudaSetDevice(h->device));
   TRY(check_horizon(h, nsteps));
@@ -451,6 +604,7 @@ int hydist_step(HydistHandle* h, int32_t nsteps) {
 
 int hydist_step_traced_sweeps(HydistHandle* h, float* phase_ms, float* sweep_ms) {
   if (!h || !phase_ms) return fail(HYDIST_ERR_ARG, "null argument");
+  if (h->next_half) return fail(HYDIST_ERR_STATE, "the second half-step is pending");
   CK(cudaSetDevice(h->device));
   TRY(check_horizon(h, 1));
   if (!h->ev[0])
@@ -497,6 +651,7 @@ int hydist_step_graph(HydistHandle* h, int32_t nsteps) {
   // The time advances on the device, so the launches of a step are the same
   // every step: one graph per sediment phase, captured on first use.
   if (!h) return fail(HYDIST_ERR_ARG, "null handle");
+  if (h->next_half) return fail(HYDIST_ERR_STATE, "the second half-step is pending");
   if (nsteps < 0) return fail(HYDIST_ERR_ARG, "negative step count");
   CK(cudaSetDevice(h->device));
   TRY(check_horizon(h, nsteps));

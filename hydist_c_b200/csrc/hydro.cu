@@ -900,6 +900,14 @@ void launch_init(const State& S, const Coef& c, cudaStream_t st) {
   k_preprocess_sides<<<4, 256, 0, st>>>(S, c, S.lscratch);
 }
 
+void launch_preprocess(const State& S, const Coef& c, cudaStream_t st) {
+  k_preprocess_sides<<<4, 256, 0, st>>>(S, c, S.lscratch);
+}
+
+void launch_boundary(const State& S, cudaStream_t st) {
+  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
+}
+
 void launch_scan_segments(const State& S, cudaStream_t st) {
   k_runs_flags<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, S.segcnt);
   k_runs_sort<<<cdiv(S.N + S.M - 2, 128), 128, 0, st>>>(S, S.segcnt);

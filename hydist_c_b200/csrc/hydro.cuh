@@ -10,6 +10,11 @@ namespace hyd {
 
 // set-up sequence (Onetime_init, segment tables, Htuongdoi, preprocess_data)
 void launch_init(const State& S, const Coef& c, cudaStream_t st);
+// preprocess_data alone (support_funcs.cpp:482-601): the boundary discharge
+// weights hi and the FS boundary scale hmax from the depths
+void launch_preprocess(const State& S, const Coef& c, cudaStream_t st);
+// Update_Boundary_Value (support_funcs.cpp:603-728) at the device clock's time
+void launch_boundary(const State& S, cudaStream_t st);
 // segment tables only (from khouot)
 void launch_scan_segments(const State& S, cudaStream_t st);
 // segment tables + boundary concentration interpolation

@@ -163,10 +163,51 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p,
                   const HydistOptions* o, int device, HydistHandle** out);
 int hydist_destroy(HydistHandle* h);
 
+/* Device arrays of one scenario owned by the caller, in the reference's
+ * layout: the arrays of Argument_Pointers (engine.h:56-72) after the
+ * reference's set-up (main.cpp:260-309: Onetime_init, the segment scans,
+ * Htuongdoi). bienQ holds the four discharge flags as values. */
+typedef struct HydistExternal {
+  int32_t M, N, total_time;
+  int32_t bienQ[4];
+  /* read only */
+  const double *h, *hsnham, *visco, *Fw, *htaiz, *htaiz_bd, *Kx1, *Ky1, *Tsxw, *Tsyw;
+  const double *bc_up, *bc_down, *bc_left, *bc_right;
+  const double *CC_up, *CC_down, *CC_left, *CC_right;
+  const int32_t* boundary_type; /* 4 sides x 20 segments */
+  /* state, read and written in place */
+  double *u, *v, *z, *t_u, *t_v, *t_z, *H_moi, *Htdu, *Htdv;
+  double *FS, *tFS, *VTH, *Kx, *Ky, *dH, *Qbx, *Qby;
+  int32_t *khouot, *daui, *cuoii, *moci, *dauj, *cuoij, *mocj;
+  double *ubt, *ubp, *vbt, *vbd;
+} HydistExternal;
+
+/* A handle over caller-owned device state (the reference's ownership:
+ * loader.cpp:224-375 allocates, the time loop works in place). Nothing of
+ * the caller's is copied or freed; the library allocates only its own
+ * scratch (smoothing buffers, line-solver scratch, the boundary discharge
+ * weights of preprocess_data, which it recomputes from h and htaiz_bd).
+ * The arrays must stay valid until hydist_destroy. */
+int hydist_create_external(const HydistExternal* ext, const HydistParams* p,
+                           const HydistOptions* o, int device,
+                           HydistHandle** out);
+
 /* Advance nsteps full ADI steps (two half-steps each): the body of the time
  * loop of Hydraulic_Calculation (engine.cpp:65-295). Stream-ordered on the
  * handle's stream; returns once the work is enqueued. */
 int hydist_step(HydistHandle* h, int32_t nsteps);
+
+/* One half of a step: half 0 = t += dT/2, the x sweep (UZ), explicit v,
+ * commit and the concentration i-sweep (engine.cpp:65-171); half 1 = the y
+ * sweep (VZ), explicit u, wetting/drying, commit and the concentration
+ * j-sweep (:175-288). Halves alternate 0, 1, 0, ...; a full-step call while
+ * half 1 is pending returns HYDIST_ERR_STATE. */
+int hydist_half_step(HydistHandle* h, int32_t half);
+
+/* The boundary update at time t alone: update_boundary_at_t
+ * (engine.cpp:22-36) / Update_Boundary_Value (support_funcs.cpp:603-728).
+ * The handle's time is unchanged. */
+int hydist_update_boundary(HydistHandle* h, double t);
 /* Block until the handle's stream is idle (synch_and_check, engine.cpp:13). */
 int hydist_sync(HydistHandle* h);
 /* Simulated time of the state (seconds); set_time supports resuming a

@@ -25,6 +25,10 @@ REF_OUT = HERE / "_ref"
 ORACLE_SO = BUILD / "libhydist_oracle.so"
 REF_DRIVER = REF_OUT / "hydist_ref_driver"
 REF_TRIDIAG = REF_OUT / "hydist_ref_tridiag"
+# the reference's own main.cpp + loader.cpp + set-up kernels, linked against
+# this repository's library in place of engine.cpp (the drop-in check)
+REF_MAIN_B200 = REF_OUT / "hydist_ref_main_b200"
+PRODUCT_DIR = HERE.parent / "hydist_c_b200"
 REF_SOURCES = ["engine.cpp", "support_funcs.cpp", "UVZSolver_multithread.cpp", "loader.cpp",
                "sediment_transport.cpp", "gtsv.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -86,7 +90,32 @@ def build_reference(src="/root/reference", force=False):
           "-o", str(t_o)])
     _run(["nvcc", *ARCH, str(objdir / "UVZSolver_multithread.o"), str(objdir / "support_funcs.o"),
           str(objdir / "gtsv.o"), str(t_o), "-o", str(REF_TRIDIAG)])
+    build_reference_main_on_library(src)
     return REF_DRIVER
+
+
+def build_reference_main_on_library(src="/root/reference"):
+    """Link the reference's main.cpp, loader.cpp and support_funcs.cpp (its
+    set-up kernels) with libhydist_b200.so instead of engine.cpp: the
+    library's Hydraulic_Calculation / update_boundary_at_t / synch_and_check
+    (include/hydist_compat.h) must satisfy the reference's own main unchanged.
+    The executable finds the library through an rpath relative to itself."""
+    src = Path(src)
+    lib = PRODUCT_DIR / "libhydist_b200.so"
+    if not (src / "main.cpp").exists() or not lib.exists():
+        return None
+    objdir = REF_OUT / "obj"
+    objdir.mkdir(parents=True, exist_ok=True)
+    objs = []
+    for s in ("main.cpp", "loader.cpp", "support_funcs.cpp"):
+        o = objdir / (Path(s).stem + ".o")
+        if _stale(o, [src / s]):
+            _run(["nvcc", "-std=c++11", f"-I{src}", "-x", "cu", *ARCH, "-O3", "-w", "-dc",
+                  str(src / s), "-o", str(o)])
+        objs.append(str(o))
+    _run(["nvcc", *ARCH, *objs, f"-L{PRODUCT_DIR}", "-lhydist_b200",
+          "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/../../hydist_c_b200", "-o", str(REF_MAIN_B200)])
+    return REF_MAIN_B200
 
 
 if __name__ == "__main__":
