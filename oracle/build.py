@@ -9,7 +9,10 @@ tree is present, the reference driver.
   functions and Hydraulic_Calculation and dumps the state in binary) and
   writes ``oracle/_ref/hydist_ref_driver``. It also builds
   ``oracle/_ref/hydist_ref_tridiag``, which runs the reference's device
-  tridiag() on batched systems. Outputs go to oracle/_ref/ only.
+  tridiag() on batched systems, and ``oracle/_ref/hydist_ref_main_b200``:
+  the reference's own main.cpp, loader.cpp and set-up kernels linked against
+  this repository's library in place of the reference's engine.cpp (the
+  drop-in check of tests/test_compat.py). Outputs go to oracle/_ref/ only.
 """
 from __future__ import annotations
 
@@ -74,6 +77,8 @@ def build_reference(src="/root/reference", force=False):
     tri = HERE / "ref_tridiag.cu"
     deps = [drv, tri] + [src / s for s in REF_SOURCES]
     if not force and not _stale(REF_DRIVER, deps) and not _stale(REF_TRIDIAG, deps):
+        if not REF_MAIN_B200.exists():
+            build_reference_main_on_library(src)
         return REF_DRIVER
     objs = []
     for s in REF_SOURCES:
