@@ -160,6 +160,116 @@ def tridiag_workload(rank: int = 0):
     return S.tridiag_batch(16384, seed=replica_seed(20262000, rank))
 
 
+ENSEMBLE = "ensemble-64x1024x512"
+
+
+def run_ensemble(args):
+    """64 scenarios of 1024x512 (config 3: per-member bathymetry, Manning,
+    inflow and tide; sediment from 300 s) stepped as one ensemble: one graph
+    launch per step covering every member. The members are spun up to the
+    sediment start untimed, then K steps are timed on the ensemble's stream."""
+    import torch
+    import hydist_c_b200 as H
+    from hydist_c_b200 import scenario as S
+    from hydist_c_b200.replicas import replica_seed
+    rank, local, ws = R.init("nccl")
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    torch.cuda.set_device(dev)
+    nmem = 64
+    bundles = [S.config3_member(k, seed=replica_seed(20263000, rank)) for k in range(nmem)]
+    cells = sum(b["meta"]["cells"] for b in bundles)
+    sims = [H.Simulation(b, device=dev.index) for b in bundles]
+    ens = H.Ensemble(sims)
+    spin = int(round(300.0 / 2.0))  # to t = 300 s, where the sediment sweeps start
+    ens.step(spin)
+    ens.step(max(args.warmup, 3))
+    ens.sync()
+    stream = torch.cuda.ExternalStream(ens.stream, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    l0 = sims[0].kernel_launches
+    clocks = ClockSampler(torch.cuda.current_device())
+    R.barrier(ws)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    ev[0].record(stream)
+    for k in range(args.steps):
+        ens.step(1)
+        ev[k + 1].record(stream)
+    torch.cuda.synchronize(dev)
+    R.barrier(ws)
+    clk = clocks.stop()
+    per = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    ms = sum(per)
+    ms_max = R.max_over_ranks(ms, ws)
+    launches = sims[0].kernel_launches - l0
+    value = ws * cells * args.steps / (ms_max * 1e-3)
+    hbm, peak_kind = _peaks()
+    step_bytes = BYTES_PER_CELL_STEP[("fp64", True)] * cells
+    ach = step_bytes / (ms / args.steps * 1e-3) / 1e9
+    mass = [m.mass() for m in sims[:4]]
+    ens.close()
+    for m in sims:
+        m.close()
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        v_cpu, t_cpu = cpu_baseline(bundles[0], args.cpu_steps, threads)
+        cpu = {"value": v_cpu, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+               "sample": f"{args.cpu_steps} full steps of one member (1024x512) with the sediment "
+                         f"sweeps on ({t_cpu:.1f} s), FP64 CPU restatement, OpenMP over lines"}
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        # the public API from pinned host buffers: create every member, the
+        # timed steps with a mass read-back per member per step, downloads
+        import time as _t
+        pinned = []
+        for b in bundles:
+            sc = dict(b["scenario"])
+            for k, v in list(sc.items()):
+                if isinstance(v, np.ndarray) and v.dtype == np.float64:
+                    sc[k] = torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
+            pinned.append(dict(b, scenario=sc,
+                               options=dict(b["options"], sediment_start=0.0, bed_change_start=0.0)))
+        torch.cuda.synchronize(dev)
+        t0 = _t.perf_counter()
+        ms2 = [H.Simulation(b, device=dev.index) for b in pinned]
+        en2 = H.Ensemble(ms2)
+        for _ in range(args.steps):
+            en2.step(1)
+            for m in ms2:
+                m.mass()
+        outs = [m.download("z") for m in ms2]
+        wall = _t.perf_counter() - t0
+        en2.close()
+        for m in ms2:
+            m.close()
+        n = (bundles[0]["scenario"]["N"] + 3) * (bundles[0]["scenario"]["M"] + 3)
+        h2d = sum(a.nbytes for b in pinned for a in b["scenario"].values() if isinstance(a, np.ndarray))
+        e2e = {"value": cells * args.steps / wall, "unit": "cell-steps/s",
+               "h2d_bytes_per_step": h2d / args.steps,
+               "d2h_bytes_per_step": (8 * nmem * args.steps + 8 * n * nmem) / args.steps,
+               "wall_s": wall, "steps": args.steps}
+    if rank == 0:
+        line = {
+            "metric": "ADI cell-steps/s", "value": value, "unit": "cell-steps/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded per member)",
+            "config": {"workload": ENSEMBLE, "members": nmem, "N": 1024, "M": 512, "cells": cells,
+                       "sediment": True, "cuda_graph": "one graph launch per step for all members",
+                       "l2": "inputs larger than L2", "parallelism": f"replicas x{ws}"},
+            "p50_step_ms": float(np.percentile(per, 50)), "p99_step_ms": float(np.percentile(per, 99)),
+            "member_mass": mass,
+            "roofline": {"bound": "hbm", "kernel": "ensemble step (all members' kernels)",
+                         "bytes_per_launch": step_bytes, "achieved": ach, "peak": hbm,
+                         "unit": "GB/s", "frac": ach / hbm, "traffic": None,
+                         "peak_source": peak_kind},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    R.finish(ws)
+
+
 def run_tridiag_reference(args):
     """The reference's algorithm for a batch (serial Thomas per system) on the
     host cores: the oracle's batched Thomas with OpenMP over systems."""
@@ -512,7 +622,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64"])
     ap.add_argument("--workload", default="sediment-2048x1024",
-                    help="sediment-2048x1024 | channel-256x128 | " + TRIDIAG)
+                    help="sediment-2048x1024 | channel-256x128 | " + TRIDIAG + " | " + ENSEMBLE)
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"],
                     help="arithmetic of the " + TRIDIAG + " workload")
     ap.add_argument("--graph", action="store_true")
@@ -528,6 +638,8 @@ def main():
         run_reference(args)
     elif args.workload == TRIDIAG:
         run_tridiag(args)
+    elif args.workload == ENSEMBLE:
+        run_ensemble(args)
     else:
         run_ours(args)
 

@@ -25,7 +25,7 @@ import numpy as np
 from . import capi, scenario
 from .capi import FIELDS, FP32_REFINE, FP64, HydistError
 
-__all__ = ["Simulation", "gtsv_batched", "HydistError", "scenario", "FP64", "FP32_REFINE",
+__all__ = ["Simulation", "Ensemble", "gtsv_batched", "HydistError", "scenario", "FP64", "FP32_REFINE",
            "FIELDS", "library"]
 
 
@@ -157,6 +157,42 @@ class Simulation:
         v = C.c_double()
         capi.check(self._lib, self._lib.hydist_mass(self._h, C.byref(v)), "hydist_mass")
         return v.value
+
+
+class Ensemble:
+    """Scenarios stepped together by one graph launch per step
+    (hydist_ensemble_*). The members stay usable as Simulations."""
+
+    def __init__(self, members):
+        self._lib = capi.load_library()
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m._h.value for m in self.members])
+        e = C.c_void_p()
+        capi.check(self._lib, self._lib.hydist_ensemble_create(arr, len(self.members), C.byref(e)),
+                   "hydist_ensemble_create")
+        self._e = e
+
+    def step(self, n: int = 1):
+        capi.check(self._lib, self._lib.hydist_ensemble_step(self._e, int(n)), "hydist_ensemble_step")
+
+    def sync(self):
+        capi.check(self._lib, self._lib.hydist_ensemble_sync(self._e), "hydist_ensemble_sync")
+
+    @property
+    def stream(self) -> int:
+        """The cudaStream_t the ensemble's graphs run on."""
+        return self._lib.hydist_ensemble_stream(self._e)
+
+    def close(self):
+        if getattr(self, "_e", None) is not None and self._e.value:
+            self._lib.hydist_ensemble_destroy(self._e)
+            self._e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def gtsv_batched(dl, d, du, b, offsets, lengths, algo: int = 0, x=None, stream=None):

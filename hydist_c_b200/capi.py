@@ -204,6 +204,12 @@ def _declare(lib):
     lib.hydist_create_external.argtypes = [C.POINTER(HydistExternal), C.POINTER(HydistParams),
                                            C.POINTER(HydistOptions), C.c_int, C.POINTER(vp)]
     lib.hydist_half_step.argtypes = [vp, C.c_int32]
+    lib.hydist_ensemble_create.argtypes = [C.POINTER(vp), C.c_int32, C.POINTER(vp)]
+    lib.hydist_ensemble_step.argtypes = [vp, C.c_int32]
+    lib.hydist_ensemble_sync.argtypes = [vp]
+    lib.hydist_ensemble_destroy.argtypes = [vp]
+    lib.hydist_ensemble_stream.argtypes = [vp]
+    lib.hydist_ensemble_stream.restype = vp
     lib.hydist_update_boundary.argtypes = [vp, C.c_double]
     lib.hydist_gtsv_band_bounds.argtypes = [_ip]
 
@@ -226,7 +232,9 @@ EXPORTED_SYMBOLS = [
     "hydist_step_graph", "hydist_stream", "hydist_gtsv_batched", "hydist_step_traced",
     "hydist_kernel_launches", "hydist_gtsv_batched_noalloc", "hydist_step_traced_sweeps",
     "hydist_gtsv_autotune", "hydist_gtsv_band_bounds", "hydist_create_external",
-    "hydist_half_step", "hydist_update_boundary",
+    "hydist_half_step", "hydist_update_boundary", "hydist_ensemble_create",
+    "hydist_ensemble_step", "hydist_ensemble_sync", "hydist_ensemble_destroy",
+    "hydist_ensemble_stream",
 ]
 GTSV_AUTO, GTSV_THOMAS, GTSV_PARTITION, GTSV_WARP, GTSV_PARTITION_512 = 0, 1, 2, 3, 4
 GTSV_BANDS = 7

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -689,6 +690,134 @@ int hydist_sync(HydistHandle* h) {
 int hydist_get_time(HydistHandle* h, double* t) {
   if (!h || !t) return fail(HYDIST_ERR_ARG, "null argument");
   *t = h->t;
+  return HYDIST_OK;
+}
+
+// ---- ensembles: many scenarios stepped by one graph launch -------------
+struct HydistEnsemble {
+  int device = 0;
+  std::vector<HydistHandle*> m;
+  cudaStream_t origin = nullptr;
+  cudaEvent_t fork = nullptr, done = nullptr;
+  std::vector<cudaEvent_t> join;
+  // one graph per pattern of the members' sediment phases
+  std::map<std::vector<unsigned char>, std::pair<cudaGraphExec_t, long long>> graphs;
+};
+
+int hydist_ensemble_create(HydistHandle* const* members, int32_t n, HydistEnsemble** out) {
+  if (!members || !out || n < 1) return fail(HYDIST_ERR_ARG, "null argument or empty ensemble");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (!members[i]) return fail(HYDIST_ERR_ARG, "null member");
+    if (members[i]->device != members[0]->device)
+      return fail(HYDIST_ERR_ARG, "members must be on one device");
+    if (members[i]->next_half) return fail(HYDIST_ERR_STATE, "a member has a half-step pending");
+    for (int j = 0; j < i; ++j)
+      if (members[j] == members[i]) return fail(HYDIST_ERR_ARG, "a member appears twice");
+  }
+  auto* e = new HydistEnsemble();
+  e->device = members[0]->device;
+  e->m.assign(members, members + n);
+  int rc = [&]() -> int {
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamCreateWithFlags(&e->origin, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming));
+    e->join.resize(n);
+    for (auto& ev : e->join) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    return HYDIST_OK;
+  }();
+  if (rc != HYDIST_OK) {
+    hydist_ensemble_destroy(e);
+    return rc;
+  }
+  *out = e;
+  return HYDIST_OK;
+}
+
+int hydist_ensemble_destroy(HydistEnsemble* e) {
+  if (!e) return HYDIST_OK;
+  cudaSetDevice(e->device);
+  if (e->origin) cudaStreamSynchronize(e->origin);
+  for (auto& kv : e->graphs)
+    if (kv.second.first) cudaGraphExecDestroy(kv.second.first);
+  for (auto& ev : e->join)
+    if (ev) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->done) cudaEventDestroy(e->done);
+  if (e->origin) cudaStreamDestroy(e->origin);
+  delete e;
+  return HYDIST_OK;
+}
+
+int hydist_ensemble_step(HydistEnsemble* e, int32_t nsteps) {
+  if (!e) return fail(HYDIST_ERR_ARG, "null ensemble");
+  if (nsteps < 0) return fail(HYDIST_ERR_ARG, "negative step count");
+  const int n = (int)e->m.size();
+  CK(cudaSetDevice(e->device));
+  for (HydistHandle* h : e->m) {
+    if (h->next_half) return fail(HYDIST_ERR_STATE, "a member has a half-step pending");
+    TRY(check_horizon(h, nsteps));
+  }
+  if (nsteps == 0) return HYDIST_OK;
+  // the graph runs after each member's earlier work ...
+  for (int i = 0; i < n; ++i) {
+    CK(cudaEventRecord(e->join[i], e->m[i]->stream));
+    CK(cudaStreamWaitEvent(e->origin, e->join[i], 0));
+  }
+  std::vector<unsigned char> key(2 * n);
+  for (int k = 0; k < nsteps; ++k) {
+    for (int i = 0; i < n; ++i) {
+      const HydistHandle* h = e->m[i];
+      const double t1 = h->t + 0.5 * h->c.dT, t2 = t1 + h->c.dT * 0.5;
+      key[2 * i] = t1 >= h->o.sediment_start;
+      key[2 * i + 1] = t2 >= h->o.sediment_start;
+    }
+    auto it = e->graphs.find(key);
+    if (it == e->graphs.end()) {
+      // one step of every member: fork from the origin stream onto the
+      // members' streams, join back
+      cudaGraph_t g = nullptr;
+      long long launches = 0;
+      CK(cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal));
+      CK(cudaEventRecord(e->fork, e->origin));
+      for (int i = 0; i < n; ++i) {
+        HydistHandle* h = e->m[i];
+        CK(cudaStreamWaitEvent(h->stream, e->fork, 0));
+        Trace tr;
+        enqueue_step(h, key[2 * i], key[2 * i + 1], &tr);
+        launches += tr.launches;
+        CK(cudaEventRecord(e->join[i], h->stream));
+        CK(cudaStreamWaitEvent(e->origin, e->join[i], 0));
+      }
+      CK(cudaStreamEndCapture(e->origin, &g));
+      cudaGraphExec_t ex = nullptr;
+      const cudaError_t err = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      CK(err);
+      it = e->graphs.emplace(key, std::make_pair(ex, launches)).first;
+    }
+    CK(cudaGraphLaunch(it->second.first, e->origin));
+    for (int i = 0; i < n; ++i) {
+      HydistHandle* h = e->m[i];
+      const double t1 = h->t + 0.5 * h->c.dT;
+      h->t = t1 + h->c.dT * 0.5;
+    }
+    e->m[0]->trace.launches += it->second.second;  // counted once, on the first member
+  }
+  // ... and each member's later work runs after the graph
+  CK(cudaEventRecord(e->done, e->origin));
+  for (HydistHandle* h : e->m) CK(cudaStreamWaitEvent(h->stream, e->done, 0));
+  return HYDIST_OK;
+}
+
+void* hydist_ensemble_stream(HydistEnsemble* e) { return e ? (void*)e->origin : nullptr; }
+
+int hydist_ensemble_sync(HydistEnsemble* e) {
+  if (!e) return fail(HYDIST_ERR_ARG, "null ensemble");
+  CK(cudaSetDevice(e->device));
+  CK(cudaStreamSynchronize(e->origin));
+  for (HydistHandle* h : e->m) TRY(check_device_err(h));
   return HYDIST_OK;
 }
 

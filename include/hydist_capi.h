@@ -228,6 +228,23 @@ int hydist_step_graph(HydistHandle* h, int32_t nsteps);
 /* The CUDA stream the handle enqueues on (a cudaStream_t). */
 void* hydist_stream(HydistHandle* h);
 
+/* ---- ensembles (the reference has none) ---------------------------------
+ * Many scenarios on one device stepped together: one step of every member is
+ * captured into one CUDA graph (forked from the ensemble's stream onto the
+ * members' streams and joined back), replayed once per step, so the members'
+ * kernels overlap on the device. A graph is captured per pattern of the
+ * members' sediment phases. Members keep their own handles (download,
+ * mass, ...); their own stream work before and after an ensemble step is
+ * ordered with it. The ensemble does not own the members. */
+typedef struct HydistEnsemble HydistEnsemble;
+int hydist_ensemble_create(HydistHandle* const* members, int32_t n,
+                           HydistEnsemble** out);
+int hydist_ensemble_step(HydistEnsemble* e, int32_t nsteps);
+int hydist_ensemble_sync(HydistEnsemble* e);
+/* The stream the ensemble's graphs are launched on (a cudaStream_t). */
+void* hydist_ensemble_stream(HydistEnsemble* e);
+int hydist_ensemble_destroy(HydistEnsemble* e);
+
 /* Tracing (the reference has none): run one full step with a CUDA event at
  * the end of each phase and return the device time of each phase in ms, in
  * the order boundary-x, sweep-x, explicit-v, commit-x, sediment-x,
