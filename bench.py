@@ -270,6 +270,80 @@ def run_ensemble(args):
     R.finish(ws)
 
 
+SERVING = "serving-poisson"
+
+
+def run_serving(args):
+    """Config 4: a Poisson stream of scenario solves at 20 requests/s, meshes
+    drawn from {256x128, 512x256, 1024x512, 2048x1024}, horizons U(10, 60)
+    simulated minutes, each request a channel scenario of its own seed.
+    Requests are submitted to the server at their arrival times (wall clock)
+    and admitted against a fixed HBM budget; latency is arrival -> retired.
+    --steps sets the number of requests."""
+    import torch
+    import hydist_c_b200 as H
+    from hydist_c_b200 import scenario as S
+    rank, local, ws = R.init("nccl")
+    dev = torch.device("cuda", local if ws > 1 else 0)
+    torch.cuda.set_device(dev)
+    nreq = max(args.steps, 4)
+    reqs = S.serving_requests(nreq, rate=20.0, seed=20264000 + 7919 * rank)
+    dt = 2.0
+    for r in reqs:  # inputs are built before the clock starts
+        r["bundle"] = S.make_channel(N=r["N"], M=r["M"], seed=r["seed"], dx=10.0, dt=dt,
+                                     hours=r["minutes"] / 60.0)
+        r["nsteps"] = int(round(r["minutes"] * 60.0 / dt))
+    budget = int(args.budget_gb * (1 << 30))
+    srv = H.Server(budget, steps_per_round=args.round_steps, device=dev.index)
+    pending = sorted(reqs, key=lambda r: r["arrival"])
+    by_id, lat, work = {}, [], 0.0
+    max_active = 0
+    R.barrier(ws)
+    t0 = time.perf_counter()
+    while pending or by_id:
+        now = time.perf_counter() - t0
+        while pending and pending[0]["arrival"] <= now:
+            r = pending.pop(0)
+            by_id[srv.submit(r["bundle"], r["nsteps"])] = r
+        q, a, _ = srv.counts()
+        max_active = max(max_active, a)
+        if a == 0 and q == 0:
+            if pending:
+                time.sleep(max(0.0, pending[0]["arrival"] - (time.perf_counter() - t0)))
+            continue
+        for rid in srv.round():
+            r = by_id.pop(rid)
+            done_t = time.perf_counter() - t0
+            lat.append(done_t - r["arrival"])
+            work += r["N"] * r["M"] * r["nsteps"]
+            srv.release(rid)
+    makespan = time.perf_counter() - t0
+    srv.close()
+    R.barrier(ws)
+    span = R.max_over_ranks(makespan, ws)
+    value = R.sum_over_ranks(work, ws) / span
+    if rank == 0:
+        line = {
+            "metric": "ADI cell-steps/s", "value": value, "unit": "cell-steps/s",
+            "n_gpus": ws, "steps": nreq, "warmup": 0, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded per request)",
+            "config": {"workload": SERVING, "requests": nreq, "rate_per_s": 20.0,
+                       "meshes": [list(m) for m in S.SERVING_MESHES], "horizon_min": [10, 60],
+                       "budget_gb": args.budget_gb, "steps_per_round": args.round_steps,
+                       "max_active": max_active, "parallelism": f"replicas x{ws}"},
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "max": float(np.max(lat))},
+            "makespan_s": makespan, "cell_steps": work,
+            "offered_cell_steps_per_s": work / (reqs[-1]["arrival"] + 1e-9),
+            "e2e": {"value": value, "unit": "cell-steps/s",
+                    "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                    "note": "wall clock from the first arrival, host inputs copied at submit"},
+        }
+        print(json.dumps(line), flush=True)
+    R.finish(ws)
+
+
 def run_tridiag_reference(args):
     """The reference's algorithm for a batch (serial Thomas per system) on the
     host cores: the oracle's batched Thomas with OpenMP over systems."""
@@ -622,7 +696,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64"])
     ap.add_argument("--workload", default="sediment-2048x1024",
-                    help="sediment-2048x1024 | channel-256x128 | " + TRIDIAG + " | " + ENSEMBLE)
+                    help="sediment-2048x1024 | channel-256x128 | " + TRIDIAG + " | " + ENSEMBLE +
+                         " | " + SERVING)
+    ap.add_argument("--budget-gb", type=float, default=120.0,
+                    help="HBM budget of the " + SERVING + " workload")
+    ap.add_argument("--round-steps", type=int, default=100,
+                    help="steps per request and scheduling round (" + SERVING + ")")
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"],
                     help="arithmetic of the " + TRIDIAG + " workload")
     ap.add_argument("--graph", action="store_true")
@@ -640,6 +719,8 @@ def main():
         run_tridiag(args)
     elif args.workload == ENSEMBLE:
         run_ensemble(args)
+    elif args.workload == SERVING:
+        run_serving(args)
     else:
         run_ours(args)
 

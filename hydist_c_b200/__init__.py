@@ -25,7 +25,7 @@ import numpy as np
 from . import capi, scenario
 from .capi import FIELDS, FP32_REFINE, FP64, HydistError
 
-__all__ = ["Simulation", "Ensemble", "gtsv_batched", "HydistError", "scenario", "FP64", "FP32_REFINE",
+__all__ = ["Simulation", "Ensemble", "Server", "gtsv_batched", "HydistError", "scenario", "FP64", "FP32_REFINE",
            "FIELDS", "library"]
 
 
@@ -187,6 +187,84 @@ class Ensemble:
         if getattr(self, "_e", None) is not None and self._e.value:
             self._lib.hydist_ensemble_destroy(self._e)
             self._e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous batching of scenario solves on one device
+    (hydist_server_*): submit requests at any time, run rounds, collect
+    finished requests."""
+
+    QUEUED, ACTIVE, DONE = 0, 1, 2
+
+    def __init__(self, budget_bytes: int, steps_per_round: int = 50, device: int = 0):
+        self._lib = capi.load_library()
+        s = C.c_void_p()
+        capi.check(self._lib, self._lib.hydist_server_create(int(device), int(budget_bytes),
+                                                             int(steps_per_round), C.byref(s)),
+                   "hydist_server_create")
+        self._s = s
+        self._shape = {}
+
+    @staticmethod
+    def scenario_bytes(M: int, N: int) -> int:
+        return int(capi.load_library().hydist_scenario_bytes(int(M), int(N)))
+
+    def submit(self, bundle: dict, nsteps: int) -> int:
+        sc = bundle["scenario"]
+        ss = capi.ScenarioStruct(sc)
+        p = capi.params_from_dict(bundle.get("params", {}))
+        o = capi.options_from_dict(bundle.get("options", {}))
+        rid = C.c_int64()
+        capi.check(self._lib, self._lib.hydist_server_submit(self._s, C.byref(ss.struct), C.byref(p),
+                                                             C.byref(o), int(nsteps), C.byref(rid)),
+                   "hydist_server_submit")
+        self._shape[rid.value] = (int(sc["N"]) + 3, int(sc["M"]) + 3)
+        return rid.value
+
+    def round(self) -> list:
+        """One scheduling round; returns the ids finished in it."""
+        cap = 4096
+        done = (C.c_int64 * cap)()
+        nd = C.c_int32()
+        capi.check(self._lib, self._lib.hydist_server_round(self._s, done, cap, C.byref(nd)),
+                   "hydist_server_round")
+        return [done[i] for i in range(min(nd.value, cap))]
+
+    def status(self, rid: int):
+        st, k = C.c_int32(), C.c_int32()
+        capi.check(self._lib, self._lib.hydist_server_status(self._s, int(rid), C.byref(st), C.byref(k)),
+                   "hydist_server_status")
+        return st.value, k.value
+
+    def counts(self):
+        q, a, b = C.c_int32(), C.c_int32(), C.c_uint64()
+        capi.check(self._lib, self._lib.hydist_server_counts(self._s, C.byref(q), C.byref(a), C.byref(b)),
+                   "hydist_server_counts")
+        return q.value, a.value, b.value
+
+    def download(self, rid: int, name: str) -> np.ndarray:
+        h = self._lib.hydist_server_handle(self._s, int(rid))
+        if not h:
+            raise capi.HydistError(f"request {rid} is not finished")
+        out = np.empty(self._shape[rid], dtype=np.int32 if name == "khouot" else np.float64)
+        capi.check(self._lib, self._lib.hydist_download(C.c_void_p(h), FIELDS[name], out.ctypes.data),
+                   "hydist_download")
+        return out
+
+    def release(self, rid: int):
+        capi.check(self._lib, self._lib.hydist_server_release(self._s, int(rid)), "hydist_server_release")
+        self._shape.pop(rid, None)
+
+    def close(self):
+        if getattr(self, "_s", None) is not None and self._s.value:
+            self._lib.hydist_server_destroy(self._s)
+            self._s = None
 
     def __del__(self):
         try:

@@ -18,7 +18,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "libhydist_b200.so"
-SOURCES = ["engine.cu", "hydro.cu", "sweep.cu", "sediment.cu", "tridiag.cu", "compat.cu"]
+SOURCES = ["engine.cu", "hydro.cu", "sweep.cu", "sediment.cu", "tridiag.cu", "compat.cu", "server.cu"]
 HEADERS = ["common.cuh", "hydro.cuh", "assembly.cuh", "linesolve.cuh", "partsolve.cuh", "sediment_cell.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

@@ -210,6 +210,18 @@ def _declare(lib):
     lib.hydist_ensemble_destroy.argtypes = [vp]
     lib.hydist_ensemble_stream.argtypes = [vp]
     lib.hydist_ensemble_stream.restype = vp
+    lib.hydist_scenario_bytes.argtypes = [C.c_int32, C.c_int32]
+    lib.hydist_scenario_bytes.restype = C.c_int64
+    lib.hydist_server_create.argtypes = [C.c_int, C.c_uint64, C.c_int32, C.POINTER(vp)]
+    lib.hydist_server_destroy.argtypes = [vp]
+    lib.hydist_server_submit.argtypes = [vp, C.POINTER(HydistScenario), C.POINTER(HydistParams),
+                                         C.POINTER(HydistOptions), C.c_int32, C.POINTER(C.c_int64)]
+    lib.hydist_server_round.argtypes = [vp, C.POINTER(C.c_int64), C.c_int32, _ip]
+    lib.hydist_server_status.argtypes = [vp, C.c_int64, _ip, _ip]
+    lib.hydist_server_counts.argtypes = [vp, _ip, _ip, C.POINTER(C.c_uint64)]
+    lib.hydist_server_handle.argtypes = [vp, C.c_int64]
+    lib.hydist_server_handle.restype = vp
+    lib.hydist_server_release.argtypes = [vp, C.c_int64]
     lib.hydist_update_boundary.argtypes = [vp, C.c_double]
     lib.hydist_gtsv_band_bounds.argtypes = [_ip]
 
@@ -234,7 +246,10 @@ EXPORTED_SYMBOLS = [
     "hydist_gtsv_autotune", "hydist_gtsv_band_bounds", "hydist_create_external",
     "hydist_half_step", "hydist_update_boundary", "hydist_ensemble_create",
     "hydist_ensemble_step", "hydist_ensemble_sync", "hydist_ensemble_destroy",
-    "hydist_ensemble_stream",
+    "hydist_ensemble_stream", "hydist_scenario_bytes", "hydist_server_create",
+    "hydist_server_destroy", "hydist_server_submit", "hydist_server_round",
+    "hydist_server_status", "hydist_server_counts", "hydist_server_handle",
+    "hydist_server_release",
 ]
 GTSV_AUTO, GTSV_THOMAS, GTSV_PARTITION, GTSV_WARP, GTSV_PARTITION_512 = 0, 1, 2, 3, 4
 GTSV_BANDS = 7

@@ -245,6 +245,35 @@ int hydist_ensemble_sync(HydistEnsemble* e);
 void* hydist_ensemble_stream(HydistEnsemble* e);
 int hydist_ensemble_destroy(HydistEnsemble* e);
 
+/* ---- serving (the reference has none) ------------------------------------
+ * Continuous batching of scenario solves on one device. A request is a
+ * scenario (host inputs copied at submit; the pointers are not kept) and a
+ * horizon in steps. hydist_server_round: admits queued requests in arrival
+ * order while their device footprint fits the budget; advances every active
+ * request by up to steps_per_round steps, each on its own stream (their
+ * kernels overlap on the device); waits; retires those at their horizon and
+ * returns their ids. A retired request keeps its device state (and its share
+ * of the budget) until hydist_server_release; hydist_server_handle gives its
+ * handle for hydist_download / hydist_mass. Each request is computed by its
+ * own handle, so its result is the same alone and in the mix. */
+typedef struct HydistServer HydistServer;
+enum HydistRequestState { HYDIST_RQ_QUEUED = 0, HYDIST_RQ_ACTIVE = 1, HYDIST_RQ_DONE = 2 };
+/* Device bytes hydist_create allocates for an M x N scenario (upper bound). */
+int64_t hydist_scenario_bytes(int32_t M, int32_t N);
+int hydist_server_create(int device, uint64_t budget_bytes, int32_t steps_per_round,
+                         HydistServer** out);
+int hydist_server_destroy(HydistServer* s);
+/* HYDIST_ERR_BUDGET if the scenario alone exceeds the budget. */
+int hydist_server_submit(HydistServer* s, const HydistScenario* sc,
+                         const HydistParams* p, const HydistOptions* o,
+                         int32_t nsteps, int64_t* id);
+int hydist_server_round(HydistServer* s, int64_t* done, int32_t cap, int32_t* ndone);
+int hydist_server_status(HydistServer* s, int64_t id, int32_t* state, int32_t* steps_done);
+int hydist_server_counts(HydistServer* s, int32_t* queued, int32_t* active,
+                         uint64_t* held_bytes);
+HydistHandle* hydist_server_handle(HydistServer* s, int64_t id);
+int hydist_server_release(HydistServer* s, int64_t id);
+
 /* Tracing (the reference has none): run one full step with a CUDA event at
  * the end of each phase and return the device time of each phase in ms, in
  * the order boundary-x, sweep-x, explicit-v, commit-x, sediment-x,
