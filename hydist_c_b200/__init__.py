@@ -153,6 +153,16 @@ class Simulation:
             raise ValueError(f"{name}: expected shape {self.shape}, got {a.shape}")
         capi.check(self._lib, self._lib.hydist_upload(self._h, f, a.ctypes.data), "hydist_upload")
 
+    def save(self, path):
+        """Checkpoint the state and time to a file (hydist_checkpoint_save)."""
+        capi.check(self._lib, self._lib.hydist_checkpoint_save(self._h, str(path).encode()),
+                   "hydist_checkpoint_save")
+
+    def load(self, path):
+        """Restore a checkpoint of this scenario (hydist_checkpoint_load)."""
+        capi.check(self._lib, self._lib.hydist_checkpoint_load(self._h, str(path).encode()),
+                   "hydist_checkpoint_load")
+
     def mass(self) -> float:
         v = C.c_double()
         capi.check(self._lib, self._lib.hydist_mass(self._h, C.byref(v)), "hydist_mass")

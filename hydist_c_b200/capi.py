@@ -210,6 +210,8 @@ def _declare(lib):
     lib.hydist_ensemble_destroy.argtypes = [vp]
     lib.hydist_ensemble_stream.argtypes = [vp]
     lib.hydist_ensemble_stream.restype = vp
+    lib.hydist_checkpoint_save.argtypes = [vp, C.c_char_p]
+    lib.hydist_checkpoint_load.argtypes = [vp, C.c_char_p]
     lib.hydist_scenario_bytes.argtypes = [C.c_int32, C.c_int32]
     lib.hydist_scenario_bytes.restype = C.c_int64
     lib.hydist_server_create.argtypes = [C.c_int, C.c_uint64, C.c_int32, C.POINTER(vp)]
@@ -249,7 +251,7 @@ EXPORTED_SYMBOLS = [
     "hydist_ensemble_stream", "hydist_scenario_bytes", "hydist_server_create",
     "hydist_server_destroy", "hydist_server_submit", "hydist_server_round",
     "hydist_server_status", "hydist_server_counts", "hydist_server_handle",
-    "hydist_server_release",
+    "hydist_server_release", "hydist_checkpoint_save", "hydist_checkpoint_load",
 ]
 GTSV_AUTO, GTSV_THOMAS, GTSV_PARTITION, GTSV_WARP, GTSV_PARTITION_512 = 0, 1, 2, 3, 4
 GTSV_BANDS = 7

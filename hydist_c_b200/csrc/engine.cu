@@ -821,6 +821,98 @@ int hydist_ensemble_sync(HydistEnsemble* e) {
   return HYDIST_OK;
 }
 
+// ---- checkpoint / resume -------------------------------------------------
+// File: a fixed header, then the fields that carry from step to step, each
+// (N+3)*(M+3) FP64 in the HydistField order of kCheckpointFields, then the
+// int32 mask. The segment tables are derived from the mask (rescanned on
+// load), the boundary arrays and smoothing buffers are rewritten every
+// half-step before they are read.
+namespace {
+
+const int kCheckpointFields[] = {
+    HYDIST_FIELD_U,   HYDIST_FIELD_V,  HYDIST_FIELD_Z,    HYDIST_FIELD_TU,  HYDIST_FIELD_TV,
+    HYDIST_FIELD_TZ,  HYDIST_FIELD_H_MOI, HYDIST_FIELD_HTDU, HYDIST_FIELD_HTDV, HYDIST_FIELD_FS,
+    HYDIST_FIELD_TFS, HYDIST_FIELD_VTH, HYDIST_FIELD_KX,  HYDIST_FIELD_KY,  HYDIST_FIELD_DH,
+    HYDIST_FIELD_QBX, HYDIST_FIELD_QBY};
+
+struct CheckpointHeader {
+  char magic[8];  // "HYDISTCK"
+  int32_t version, M, N, nfields;
+  double t;
+  int32_t next_half, reserved;
+};
+
+}  // namespace
+
+int hydist_checkpoint_save(HydistHandle* h, const char* path) {
+  if (!h || !path) return fail(HYDIST_ERR_ARG, "null argument");
+  if (h->next_half) return fail(HYDIST_ERR_STATE, "save between full steps");
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  const size_t n = (size_t)h->S.W * h->S.H;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(HYDIST_ERR_ARG, std::string("cannot open ") + path);
+  CheckpointHeader hd{};
+  std::memcpy(hd.magic, "HYDISTCK", 8);
+  hd.version = 1;
+  hd.M = h->S.M;
+  hd.N = h->S.N;
+  hd.nfields = (int32_t)(sizeof(kCheckpointFields) / sizeof(int));
+  hd.t = h->t;
+  hd.next_half = 0;
+  bool ok = std::fwrite(&hd, sizeof(hd), 1, f) == 1;
+  std::vector<double> buf(n);
+  for (int fid : kCheckpointFields) {
+    if (!ok) break;
+    ok = cudaMemcpy(buf.data(), field_ptr(h, fid), n * 8, cudaMemcpyDeviceToHost) == cudaSuccess &&
+         std::fwrite(buf.data(), 8, n, f) == n;
+  }
+  std::vector<int32_t> mask(n);
+  ok = ok && cudaMemcpy(mask.data(), h->S.khouot, n * 4, cudaMemcpyDeviceToHost) == cudaSuccess &&
+       std::fwrite(mask.data(), 4, n, f) == n;
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) return fail(HYDIST_ERR_CUDA, std::string("writing the checkpoint failed: ") + path);
+  return HYDIST_OK;
+}
+
+int hydist_checkpoint_load(HydistHandle* h, const char* path) {
+  if (!h || !path) return fail(HYDIST_ERR_ARG, "null argument");
+  if (h->next_half) return fail(HYDIST_ERR_STATE, "load between full steps");
+  CK(cudaSetDevice(h->device));
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(HYDIST_ERR_ARG, std::string("cannot open ") + path);
+  CheckpointHeader hd{};
+  const int nf = (int)(sizeof(kCheckpointFields) / sizeof(int));
+  if (std::fread(&hd, sizeof(hd), 1, f) != 1 || std::memcmp(hd.magic, "HYDISTCK", 8) != 0 ||
+      hd.version != 1 || hd.nfields != nf) {
+    std::fclose(f);
+    return fail(HYDIST_ERR_ARG, "not a checkpoint of this format");
+  }
+  if (hd.M != h->S.M || hd.N != h->S.N) {
+    std::fclose(f);
+    return fail(HYDIST_ERR_ARG, "the checkpoint is of another mesh size");
+  }
+  const size_t n = (size_t)h->S.W * h->S.H;
+  std::vector<double> buf(n);
+  std::vector<int32_t> mask(n);
+  bool ok = true;
+  CK(cudaStreamSynchronize(h->stream));
+  for (int fid : kCheckpointFields) {
+    ok = std::fread(buf.data(), 8, n, f) == n &&
+         cudaMemcpy(field_ptr(h, fid), buf.data(), n * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok) break;
+  }
+  ok = ok && std::fread(mask.data(), 4, n, f) == n &&
+       cudaMemcpy(h->S.khouot, mask.data(), n * 4, cudaMemcpyHostToDevice) == cudaSuccess;
+  std::fclose(f);
+  if (!ok) return fail(HYDIST_ERR_ARG, std::string("truncated or unreadable checkpoint: ") + path);
+  launch_scan_segments(h->S, h->stream);
+  CK(cudaGetLastError());
+  h->t = hd.t;
+  TRY(set_device_clock(h));
+  return check_device_err(h);
+}
+
 int hydist_set_time(HydistHandle* h, double t) {
   if (!h) return fail(HYDIST_ERR_ARG, "null handle");
   CK(cudaSetDevice(h->device));

@@ -228,6 +228,16 @@ int hydist_step_graph(HydistHandle* h, int32_t nsteps);
 /* The CUDA stream the handle enqueues on (a cudaStream_t). */
 void* hydist_stream(HydistHandle* h);
 
+/* ---- checkpoint / resume ----------------------------------------------
+ * The reference's resume is a stub (main.cpp:283-284). A checkpoint holds
+ * the time and every field that carries from one step to the next, in a
+ * binary file (header + FP64 fields + the int32 mask). Load restores them
+ * into a handle created for the same scenario (same mesh and inputs) and
+ * rescans the segment tables from the mask; stepping on is bit-identical to
+ * not having stopped. Both are synchronous and allowed between full steps. */
+int hydist_checkpoint_save(HydistHandle* h, const char* path);
+int hydist_checkpoint_load(HydistHandle* h, const char* path);
+
 /* ---- ensembles (the reference has none) ---------------------------------
  * Many scenarios on one device stepped together: one step of every member is
  * captured into one CUDA graph (forked from the ensemble's stream onto the

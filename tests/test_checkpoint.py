@@ -1,0 +1,39 @@
+"""Checkpoint / resume (hydist_checkpoint_*): stop after some steps, save,
+restore into a fresh handle of the same scenario, step on -- bit-identical
+to the uninterrupted run, through the sediment start and wetting/drying. A
+checkpoint of another mesh size or a foreign file is refused."""
+import numpy as np
+import pytest
+
+
+def _bundle(N=64, M=32):
+    from hydist_c_b200 import scenario as S
+    return S.make_channel(N=N, M=M, seed=20268000, dx=10.0, dt=2.0, hours=1.0,
+                          sediment=True, sediment_start=30.0)
+
+
+@pytest.mark.gpu
+def test_resume_is_bit_identical(hyd, tmp_path):
+    ref = hyd.Simulation(_bundle())
+    ref.step(40)
+    want = {f: ref.download(f) for f in ("u", "v", "z", "FS", "khouot", "H_moi")}
+    ref.close()
+    a = hyd.Simulation(_bundle())
+    a.step(17)
+    ck = tmp_path / "state.ck"
+    a.save(ck)
+    a.close()
+    b = hyd.Simulation(_bundle())
+    b.load(ck)
+    assert b.t == pytest.approx(34.0)
+    b.step(23)
+    for f, w in want.items():
+        np.testing.assert_array_equal(b.download(f), w, err_msg=f)
+    with pytest.raises(hyd.HydistError, match="mesh size"):
+        c = hyd.Simulation(_bundle(N=48, M=24))
+        c.load(ck)
+    bad = tmp_path / "bad.ck"
+    bad.write_bytes(b"not a checkpoint" * 8)
+    with pytest.raises(hyd.HydistError, match="format"):
+        b.load(bad)
+    b.close()
