@@ -28,6 +28,7 @@ struct Coef {
   // where the reference divides by a constant (one rounding of difference)
   double r_dX, r_dY, r_dX2, r_dY2, r_dXbp, r_dYbp, dT_dXbp, dT_dYbp, sqrt_g;
   double Mb_ros, r_Tod, r_Ufr2, Dxr_m03;  // Mbochat/ros, 1/Tod, 1/Ufr^2, Dxr^-0.3
+  double qb_k;  // 0.053 sqrt((Sx-1) g) dm^1.5 of the bed-load flux
 };
 
 // Device error codes recorded in State::err[0].

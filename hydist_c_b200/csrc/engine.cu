@@ -98,6 +98,7 @@ void derive(const HydistParams& p, Coef& c) {
   c.r_Tod = 1.0 / c.Tod;
   c.r_Ufr2 = 1.0 / (c.Ufr * c.Ufr);
   c.Dxr_m03 = std::pow(c.Dxr, -0.3);
+  c.qb_k = 0.053 * std::sqrt((c.Sx - 1) * c.g) * std::pow(c.dm, 1.5);
 }
 
 }  // namespace
@@ -112,9 +113,9 @@ struct HydistHandle {
   std::vector<void*> allocs;
   double* mass_part = nullptr;  // per-block partial sums
   int mass_blocks = 0;
-  // one captured step per sediment phase: [sed_x*2 + sed_y]
-  cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
-  long long graph_launches[4] = {0, 0, 0, 0};
+  // one captured step per sediment phase: [bed*4 + sed_x*2 + sed_y]
+  cudaGraphExec_t graph[8] = {};
+  long long graph_launches[8] = {};
   Trace trace;                                    // kernel launch counter
   cudaEvent_t ev[PH_COUNT + 1] = {};
   cudaEvent_t kev[2 * KS_COUNT] = {};
@@ -158,13 +159,19 @@ int check_horizon(HydistHandle* h, int nsteps) {
 
 // one full step (engine.cpp:65-295); the sediment gates (engine.cpp:149,
 // 258) are decided on the host, the time itself advances on the device
-void enqueue_step(HydistHandle* h, bool sed_x, bool sed_y, Trace* tr) {
+void enqueue_step(HydistHandle* h, bool sed_x, bool sed_y, bool bed, Trace* tr) {
   launch_half_x(h->S, h->c, h->stream, tr);
-  if (sed_x) launch_sediment(h->S, h->c, h->o.bed_change_start, true, h->stream, tr);
+  if (sed_x) launch_sediment(h->S, h->c, h->o.bed_change_start, true, false, h->stream, tr);
   else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_X + 1], h->stream);
   launch_half_y(h->S, h->c, h->stream, tr);
-  if (sed_y) launch_sediment(h->S, h->c, h->o.bed_change_start, false, h->stream, tr);
+  if (sed_y) launch_sediment(h->S, h->c, h->o.bed_change_start, false, bed, h->stream, tr);
   else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_Y + 1], h->stream);
+}
+
+// the bed change runs after the j-sweep of a step ending at t2 once both the
+// sweeps and the bed change have started
+bool bed_on(const HydistHandle* h, double t2) {
+  return h->o.bed_change && t2 >= h->o.sediment_start && t2 >= h->o.bed_change_start;
 }
 
 int set_device_clock(HydistHandle* h) {
@@ -299,8 +306,6 @@ int check_params(const HydistParams* p, const HydistOptions* o) {
     return fail(HYDIST_ERR_ARG, "unknown precision");
   if (o->precision == HYDIST_FP32_REFINE)
     return fail(HYDIST_ERR_ARG, "precision HYDIST_FP32_REFINE is not implemented yet");
-  if (o->bed_change != 0)
-    return fail(HYDIST_ERR_ARG, "the bed-change update is not implemented yet");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(HYDIST_ERR_NODEVICE, "no CUDA device");
@@ -546,10 +551,12 @@ int hydist_half_step(HydistHandle* h, int32_t half) {
   const bool sed = t >= h->o.sediment_start;
   if (half == 0) {
     launch_half_x(h->S, h->c, h->stream, &h->trace);
-    if (sed) launch_sediment(h->S, h->c, h->o.bed_change_start, true, h->stream, &h->trace);
+    if (sed) launch_sediment(h->S, h->c, h->o.bed_change_start, true, false, h->stream, &h->trace);
   } else {
     launch_half_y(h->S, h->c, h->stream, &h->trace);
-    if (sed) launch_sediment(h->S, h->c, h->o.bed_change_start, false, h->stream, &h->trace);
+    if (sed)
+      launch_sediment(h->S, h->c, h->o.bed_change_start, false, bed_on(h, t), h->stream,
+                      &h->trace);
   }
   h->t = t;
   h->next_half = 1 - half;
@@ -596,7 +603,8 @@ int hydist_step(HydistHandle* h, int32_t nsteps) {
   for (int k = 0; k < nsteps; ++k) {
     const double t1 = h->t + 0.5 * h->c.dT;
     const double t2 = t1 + h->c.dT * 0.5;
-    enqueue_step(h, t1 >= h->o.sediment_start, t2 >= h->o.sediment_start, &h->trace);
+    enqueue_step(h, t1 >= h->o.sediment_start, t2 >= h->o.sediment_start, bed_on(h, t2),
+                 &h->trace);
     h->t = t2;
   }
   CK(cudaGetLastError());
@@ -618,7 +626,7 @@ int hydist_step_traced_sweeps(HydistHandle* h, float* phase_ms, float* sweep_ms)
   const double t1 = h->t + 0.5 * h->c.dT;
   const double t2 = t1 + h->c.dT * 0.5;
   CK(cudaEventRecord(h->ev[0], h->stream));
-  enqueue_step(h, t1 >= h->o.sediment_start, t2 >= h->o.sediment_start, &tr);
+  enqueue_step(h, t1 >= h->o.sediment_start, t2 >= h->o.sediment_start, bed_on(h, t2), &tr);
   h->trace.launches += tr.launches;
   h->t = t2;
   CK(cudaGetLastError());
@@ -660,13 +668,14 @@ int hydist_step_graph(HydistHandle* h, int32_t nsteps) {
     const double t1 = h->t + 0.5 * h->c.dT;
     const double t2 = t1 + h->c.dT * 0.5;
     const bool sx = t1 >= h->o.sediment_start, sy = t2 >= h->o.sediment_start;
-    const int gi = (sx ? 2 : 0) + (sy ? 1 : 0);
+    const bool bd = bed_on(h, t2);
+    const int gi = (bd ? 4 : 0) + (sx ? 2 : 0) + (sy ? 1 : 0);
     cudaGraphExec_t& ex = h->graph[gi];
     if (!ex) {
       cudaGraph_t g = nullptr;
       Trace tr;
       CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-      enqueue_step(h, sx, sy, &tr);
+      enqueue_step(h, sx, sy, bd, &tr);
       CK(cudaStreamEndCapture(h->stream, &g));
       h->graph_launches[gi] = tr.launches;
       const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
@@ -765,13 +774,14 @@ int hydist_ensemble_step(HydistEnsemble* e, int32_t nsteps) {
     CK(cudaEventRecord(e->join[i], e->m[i]->stream));
     CK(cudaStreamWaitEvent(e->origin, e->join[i], 0));
   }
-  std::vector<unsigned char> key(2 * n);
+  std::vector<unsigned char> key(3 * n);
   for (int k = 0; k < nsteps; ++k) {
     for (int i = 0; i < n; ++i) {
       const HydistHandle* h = e->m[i];
       const double t1 = h->t + 0.5 * h->c.dT, t2 = t1 + h->c.dT * 0.5;
-      key[2 * i] = t1 >= h->o.sediment_start;
-      key[2 * i + 1] = t2 >= h->o.sediment_start;
+      key[3 * i] = t1 >= h->o.sediment_start;
+      key[3 * i + 1] = t2 >= h->o.sediment_start;
+      key[3 * i + 2] = bed_on(h, t2);
     }
     auto it = e->graphs.find(key);
     if (it == e->graphs.end()) {
@@ -785,7 +795,7 @@ int hydist_ensemble_step(HydistEnsemble* e, int32_t nsteps) {
         HydistHandle* h = e->m[i];
         CK(cudaStreamWaitEvent(h->stream, e->fork, 0));
         Trace tr;
-        enqueue_step(h, key[2 * i], key[2 * i + 1], &tr);
+        enqueue_step(h, key[3 * i], key[3 * i + 1], key[3 * i + 2], &tr);
         launches += tr.launches;
         CK(cudaEventRecord(e->join[i], h->stream));
         CK(cudaStreamWaitEvent(e->origin, e->join[i], 0));

@@ -29,8 +29,9 @@ void launch_sweep(const State& S, const Coef& c, int dir, cudaStream_t st);
 // partitioned concentration line sweep: dir 0 = i-sweep (columns), 1 = rows;
 // the erosion source is on from s_start
 void launch_fs_sweep(const State& S, const Coef& c, int dir, double s_start, cudaStream_t st);
-// concentration step: xdir = the i-sweep after half-step A
-void launch_sediment(const State& S, const Coef& c, double s_start, bool xdir, cudaStream_t st,
-                     Trace* tr);
+// concentration step: xdir = the i-sweep after half-step A; bed: the bed
+// change after the j-sweep
+void launch_sediment(const State& S, const Coef& c, double s_start, bool xdir, bool bed,
+                     cudaStream_t st, Trace* tr);
 
 }  // namespace hyd

@@ -6,6 +6,8 @@
 //                   solution, :51-349, 604-651]: the partitioned line solver
 //                   with FSGen (sweep.cu), cell rows in sediment_cell.cuh
 //   k_update_fs    [Update_FS, :654-663]
+//   k_calc_qb      [Calculate_Qb, :352-434]
+//   k_bed_load     [_bed_load / BedLoad, :436-537, :664-673]
 #include "common.cuh"
 #include "hydro.cuh"
 #include "sediment_cell.cuh"
@@ -43,6 +45,138 @@ __global__ void k_vth_heso(State S, Coef c, int i_hi) {
   }
 }
 
+// ---- bed change: Calculate_Qb (sediment_transport.cpp:352-434) and
+// _bed_load / BedLoad (:436-537, :664-673), which the reference never
+// launches (engine.cpp:290-293). Read as intended where the code cannot be
+// meant literally: the flux where the speed is not zero (:385 divides by
+// the VTH it tests to be zero), Toee starting from the coefficient Toe
+// (:359), both components in the corner copies (:410-419), t_u[pos] > 0 in
+// the downwind test (:479).
+__global__ void k_calc_qb(State S, Coef c) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int i = blockIdx.y + 2;
+  if (i > S.N || j > S.M) return;
+  const int w = S.W, pos = i * w + j, N = S.N, M = S.M;
+  double qx = 0, qy = 0;
+  const double vth = S.VTH[pos];
+  if (vth != 0 && S.khouot[pos] == 0) {
+    double Toee = c.Toe, Tx = 0;
+    const double Hm = S.Hmoi[pos];
+    const double Tob = c.ro * S.Fw[pos] * (vth * vth);
+    if (Hm > c.ghtoe) Toee = c.Toe * (1 + c.hstoe * ((Hm - c.ghtoe)));
+    if (Tob > Toee) Tx = Tob / Toee - 1;
+    const double base = c.qb_k * pow(Tx, 2.1) * c.Dxr_m03;
+    qx = base * (S.tu[pos] + S.tu[pos - w]) * 0.5 / vth;
+    qy = base * (S.tv[pos] + S.tv[pos - 1]) * 0.5 / vth;
+  }
+  double* Qbx = S.Qbx;
+  double* Qby = S.Qby;
+  Qbx[pos] = qx;
+  Qby[pos] = qy;
+  // margins and corners copy the nearest interior value (:402-431)
+  if (i == 2) {
+    Qbx[pos - w] = qx;
+    Qby[pos - w] = qy;
+  }
+  if (i == N) {
+    Qbx[pos + w] = qx;
+    Qby[pos + w] = qy;
+  }
+  if (j == 2) {
+    Qbx[pos - 1] = qx;
+    Qby[pos - 1] = qy;
+    if (i == 2) {
+      Qbx[1 * w + 1] = qx;
+      Qby[1 * w + 1] = qy;
+    }
+    if (i == N) {
+      Qbx[(N + 1) * w + 1] = qx;
+      Qby[(N + 1) * w + 1] = qy;
+    }
+  }
+  if (j == M) {
+    Qbx[pos + 1] = qx;
+    Qby[pos + 1] = qy;
+    if (i == 2) {
+      Qbx[1 * w + M + 1] = qx;
+      Qby[1 * w + M + 1] = qy;
+    }
+    if (i == N) {
+      Qbx[(N + 1) * w + M + 1] = qx;
+      Qby[(N + 1) * w + M + 1] = qy;
+    }
+  }
+}
+
+// _bed_load on rows 3..N-2 (BedLoad with the j-sweep's range,
+// engine.cpp:292), cells of the row's wet segments of at least 3 cells.
+__global__ void k_bed_load(State S, Coef c) {
+  __shared__ int s_first[SEG], s_last[SEG];
+  __shared__ int s_n;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int i = blockIdx.y + 3;
+  if (threadIdx.x < SEG) {
+    s_first[threadIdx.x] = S.daui[i * SEG + threadIdx.x];
+    s_last[threadIdx.x] = S.cuoii[i * SEG + threadIdx.x];
+  }
+  if (threadIdx.x == 0) s_n = S.moci[i];
+  __syncthreads();
+  if (i >= S.N - 1 || j > S.M) return;
+  int first = 0, last = 0;
+  for (int k = 0; k < s_n; ++k)
+    if (s_first[k] <= j && j <= s_last[k]) {
+      first = s_first[k];
+      last = s_last[k];
+      break;
+    }
+  if (last - first < 2 || j < first || j > last) return;
+  const int w = S.W, pos = i * w + j, M = S.M, N = S.N;
+  const int* kh = S.khouot;
+  const double *Qbx = S.Qbx, *Qby = S.Qby, *FS = S.FS, *tu = S.tu, *tv = S.tv;
+  double p = 0, q = 0;
+  if (kh[pos - w] == 1) {
+    if (tu[pos] < 0) p = (-3 * Qbx[pos] + 4 * Qbx[pos + w] - Qbx[pos + 2 * w]) * c.r_dX2;
+  } else {
+    if (kh[pos + w] == 1) {
+      if (tu[pos] > 0) p = (3 * Qbx[pos] - 4 * Qbx[pos - w] + Qbx[pos - 2 * w]) * c.r_dX2;
+    } else {
+      p = (Qbx[pos + w] - Qbx[pos - w]) * c.r_dX2;
+    }
+  }
+  if (kh[pos - 1] == 1) {
+    if (tv[pos] < 0) q = (-3 * Qby[pos] + 4 * Qby[pos + 1] - Qby[pos + 2]) * c.r_dY2;
+  } else {
+    if (kh[pos + 1] == 1) {
+      if (tv[pos] > 0) q = (3 * Qby[pos] - 4 * Qby[pos - 1] + Qby[pos - 2]) * c.r_dY2;
+    } else {
+      q = (Qby[pos + 1] - Qby[pos - 1]) * c.r_dY2;
+    }
+  }
+  double tH = p + q;
+  p = FS[pos + w] - FS[pos];
+  if ((kh[pos + 2 * w] == 1 || kh[pos - w] == 1) && (i < N)) p = 0;
+  q = FS[pos] - FS[pos - w];
+  if ((i > 2) && (kh[pos - 2 * w] == 1 || kh[pos + w] == 1)) q = 0;
+  p = c.r_dXbp * (S.Htdu[pos] * S.Kx[pos] * p - S.Htdu[pos - w] * S.Kx[pos - w] * q);
+  tH = tH + p;
+  p = FS[pos + 1] - FS[pos];
+  if (((last < M) && (kh[pos - 1] == 1 || kh[pos + 2] == 1)) || (last == M && (kh[pos - 1] == 1))) p = 0;
+  q = FS[pos] - FS[pos - 1];
+  if (((first > 2) && (kh[pos - 2] == 1 || kh[pos + 1] == 1)) || (first == 2 && kh[pos + 1] == 1)) q = 0;
+  p = c.r_dYbp * (S.Htdv[pos] * S.Ky[pos] * p - S.Htdv[pos - 1] * S.Ky[pos - 1] * q);
+  tH = tH + p;
+  const double Hm = S.Hmoi[pos], fs = FS[pos], vth = S.VTH[pos];
+  const double cc = 18 * log(12 * Hm / c.Ks);
+  const double Uf = c.sqrt_g * fabs(vth) / cc;
+  const double om = 1 - fs, om2 = om * om;
+  const double wsm = c.wss * (om2 * om2);
+  double Zf = 0;
+  if (fs > 0.0) Zf = wsm / (0.4 * (Uf + 2 * wsm));
+  const double src = S.ketdinh ? source_chs(c, wsm, Zf, fs, S.Fw[pos], vth, Hm)
+                               : source_nchs(c, wsm, Zf, Uf, 1.0 / Hm, fs);
+  S.dH[pos] += c.dT / (1 - c.Dorong) * (src + tH);
+}
+
 __global__ void k_update_fs(State S) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int i = blockIdx.y + 1;
@@ -51,8 +185,8 @@ __global__ void k_update_fs(State S) {
   S.FS[g] = S.tFS[g];
 }
 
-void launch_sediment(const State& S, const Coef& c, double s_start, bool xdir, cudaStream_t st,
-                     Trace* tr) {
+void launch_sediment(const State& S, const Coef& c, double s_start, bool xdir, bool bed,
+                     cudaStream_t st, Trace* tr) {
   // first half: Find_VTH/hesoK over rows to N; second half: to N-1
   // (launch shape of engine.cpp:259-260 never reaches row N)
   const int i_hi = xdir ? S.N : S.N - 1;
@@ -61,7 +195,14 @@ void launch_sediment(const State& S, const Coef& c, double s_start, bool xdir, c
   launch_fs_sweep(S, c, xdir ? 0 : 1, s_start, st);
   if (tr) tr->kend(st, xdir ? KS_FS_X : KS_FS_Y);
   k_update_fs<<<dim3(cdiv(S.M, 128), S.N), 128, 0, st>>>(S);
-  if (tr) tr->mark(st, xdir ? PH_SEDIMENT_X : PH_SEDIMENT_Y, 3);
+  int launched = 3;
+  if (bed && S.N >= 5) {
+    // the bed change once per step, after the j-sweep (engine.cpp:290-293)
+    k_calc_qb<<<dim3(cdiv(S.M - 1, 128), S.N - 1), 128, 0, st>>>(S, c);
+    k_bed_load<<<dim3(cdiv(S.M - 1, 128), S.N - 4), 128, 0, st>>>(S, c);
+    launched += 2;
+  }
+  if (tr) tr->mark(st, xdir ? PH_SEDIMENT_X : PH_SEDIMENT_Y, launched);
 }
 
 }  // namespace hyd

@@ -107,8 +107,10 @@ typedef struct HydistOptions {
   double sediment_start;   /* -b: sediment sweeps from this t  main.cpp:82  */
   double bed_change_start; /* -B: erosion source and bed change from this t */
   int32_t ketdinh;         /* cohesive sediment (main.cpp:53 sets 1)        */
-  int32_t bed_change;      /* 1: apply the bed-change update each step (not
-                              implemented yet: hydist_create refuses 1)     */
+  int32_t bed_change;      /* 1: accumulate the bed change dH once per step
+                              from bed_change_start (Calculate_Qb/BedLoad,
+                              sediment_transport.cpp:352-537, which the
+                              reference never launches)                     */
   int32_t precision;       /* enum HydistPrecision                          */
   int32_t reserved;
 } HydistOptions;

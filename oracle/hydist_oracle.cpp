@@ -1198,6 +1198,115 @@ struct Sim {
     }
   }
 
+  // ------------------------------------------------------ bed change
+  // Calculate_Qb (sediment_transport.cpp:352-434) and _bed_load / BedLoad
+  // (:436-537, :664-673). The reference never launches them (its call is
+  // commented out, engine.cpp:290-293); its code is read as intended where it
+  // cannot be meant literally: the flux is computed where the speed is not
+  // zero (:385 tests !VTH and then divides by VTH), Toee starts from the
+  // coefficient Toe (:359 reads a shared copy before it is assigned), the
+  // corner copies take both components under their condition (:410-419
+  // lack braces), and the downwind test reads t_u[pos] > 0 (:479 indexes
+  // t_u with a boolean).
+  void calc_qb() {
+    const int w = W;
+    const double kq = 0.053 * std::sqrt((c.Sx - 1) * c.g) * std::pow(c.dm, 1.5);
+    const double dxr = std::pow(c.Dxr, -0.3);
+    for (int i = 2; i <= N; ++i)
+      for (int j = 2; j <= M; ++j) {
+        const int pos = id(i, j);
+        double qx = 0, qy = 0;
+        if (VTH[pos] != 0 && khouot[pos] == 0) {
+          double Toee = c.Toe, Tx = 0;
+          const double Tob = c.ro * Fw[pos] * (VTH[pos] * VTH[pos]);
+          if (Hmoi[pos] > c.ghtoe) Toee = c.Toe * (1 + c.hstoe * ((Hmoi[pos] - c.ghtoe)));
+          if (Tob > Toee) Tx = Tob / Toee - 1;
+          const double base = kq * std::pow(Tx, 2.1) * dxr;
+          qx = base * (tu[pos] + tu[pos - w]) * 0.5 / VTH[pos];
+          qy = base * (tv[pos] + tv[pos - 1]) * 0.5 / VTH[pos];
+        }
+        Qbx[pos] = qx;
+        Qby[pos] = qy;
+      }
+    // margins copy the nearest interior value (:402-431)
+    for (int j = 2; j <= M; ++j) {
+      Qbx[id(1, j)] = Qbx[id(2, j)];
+      Qby[id(1, j)] = Qby[id(2, j)];
+      Qbx[id(N + 1, j)] = Qbx[id(N, j)];
+      Qby[id(N + 1, j)] = Qby[id(N, j)];
+    }
+    for (int i = 2; i <= N; ++i) {
+      Qbx[id(i, 1)] = Qbx[id(i, 2)];
+      Qby[id(i, 1)] = Qby[id(i, 2)];
+      Qbx[id(i, M + 1)] = Qbx[id(i, M)];
+      Qby[id(i, M + 1)] = Qby[id(i, M)];
+    }
+    const int corner[4][4] = {{1, 1, 2, 2}, {N + 1, 1, N, 2}, {1, M + 1, 2, M}, {N + 1, M + 1, N, M}};
+    for (const auto& k : corner) {
+      Qbx[id(k[0], k[1])] = Qbx[id(k[2], k[3])];
+      Qby[id(k[0], k[1])] = Qby[id(k[2], k[3])];
+    }
+  }
+
+  // _bed_load for rows 3..N-2 (BedLoad's launch with the j-sweep's range,
+  // engine.cpp:292), cells of the row's wet segments of at least 3 cells.
+  void bed_load() {
+    const int w = W;
+    const double dX = c.dX, dY = c.dY;
+    for (int i = 3; i < N - 1; ++i)
+      for (int k = 0; k < moci[i]; ++k) {
+        const int first = daui[i * SEG + k], last = cuoii[i * SEG + k];
+        if (last - first < 2) continue;
+        for (int j = first; j <= last; ++j) {
+          const int pos = id(i, j);
+          double p = 0, q = 0;
+          if (khouot[pos - w] == 1) {
+            if (tu[pos] < 0) p = (-3 * Qbx[pos] + 4 * Qbx[pos + w] - Qbx[pos + 2 * w]) / (dX * 2);
+          } else {
+            if (khouot[pos + w] == 1) {
+              if (tu[pos] > 0) p = (3 * Qbx[pos] - 4 * Qbx[pos - w] + Qbx[pos - 2 * w]) / (dX * 2);
+            } else {
+              p = (Qbx[pos + w] - Qbx[pos - w]) / (dX * 2);
+            }
+          }
+          if (khouot[pos - 1] == 1) {
+            if (tv[pos] < 0) q = (-3 * Qby[pos] + 4 * Qby[pos + 1] - Qby[pos + 2]) / (dY * 2);
+          } else {
+            if (khouot[pos + 1] == 1) {
+              if (tv[pos] > 0) q = (3 * Qby[pos] - 4 * Qby[pos - 1] + Qby[pos - 2]) / (dY * 2);
+            } else {
+              q = (Qby[pos + 1] - Qby[pos - 1]) / (dY * 2);
+            }
+          }
+          double tH = p + q;
+          p = FS[pos + w] - FS[pos];
+          if ((khouot[pos + 2 * w] == 1 || khouot[pos - w] == 1) && (i < N)) p = 0;
+          q = FS[pos] - FS[pos - w];
+          if ((i > 2) && (khouot[pos - 2 * w] == 1 || khouot[pos + w] == 1)) q = 0;
+          p = 1 / (dX * dX) * (Htdu[pos] * Kx[pos] * p - Htdu[pos - w] * Kx[pos - w] * q);
+          tH = tH + p;
+          p = FS[pos + 1] - FS[pos];
+          if (((last < M) && (khouot[pos - 1] == 1 || khouot[pos + 2] == 1)) ||
+              (last == M && (khouot[pos - 1] == 1)))
+            p = 0;
+          q = FS[pos] - FS[pos - 1];
+          if (((first > 2) && (khouot[pos - 2] == 1 || khouot[pos + 1] == 1)) ||
+              (first == 2 && khouot[pos + 1] == 1))
+            q = 0;
+          p = 1 / ((dY * dY)) * (Htdv[pos] * Ky[pos] * p - Htdv[pos - 1] * Ky[pos - 1] * q);
+          tH = tH + p;
+          const double cc = 18 * std::log(12 * Hmoi[pos] / c.Ks);
+          const double Uf = std::sqrt(c.g) * std::fabs(VTH[pos]) / cc;
+          const double wsm = c.wss * std::pow((1 - FS[pos]), 4);
+          double Zf = 0;
+          if (FS[pos] > 0.0) Zf = wsm / (0.4 * (Uf + 2 * wsm));
+          const double S = o.ketdinh ? source_chs(wsm, Zf, FS[pos], Fw[pos], VTH[pos], Hmoi[pos])
+                                     : source_nchs(wsm, Zf, Uf, Hmoi[pos], FS[pos]);
+          dH[pos] += c.dT / (1 - c.Dorong) * (S + tH);
+        }
+      }
+  }
+
   // Update_FS, sediment_transport.cpp:654-663.
   void update_fs() {
     for (int i = 1; i <= N; ++i)
@@ -1303,6 +1412,11 @@ struct Sim {
       const double tt = t;
       for_lines(3, N - 1, [&](LineBuf& L, int i) { fsi_row(L, i, tt); });
       update_fs();
+      // the bed change once per step after the j-sweep (engine.cpp:290-293)
+      if (o.bed_change && t >= o.bed_change_start) {
+        calc_qb();
+        bed_load();
+      }
     }
   }
 };

@@ -268,3 +268,26 @@ def test_multiseg_mesh(hyd, oracle_mod):
     sim.sync()
     bad = _compare(sim, orc, ["u", "v", "z"], 1e-8)
     assert not bad, bad
+
+
+def test_bed_change(hyd, oracle_mod):
+    """The bed change (Calculate_Qb / BedLoad read as intended; the reference
+    never launches them) against the oracle's restatement: the flux and the
+    accumulated dH after the first step with it, and after 30 steps."""
+    b = S.make_channel(N=96, M=48, seed=20269000, dx=10.0, dt=2.0, hours=1.0, sediment=True,
+                       sediment_start=10.0)
+    b["options"] = dict(b["options"], bed_change=1, bed_change_start=20.0)
+    sim = hyd.Simulation(b)
+    orc = oracle_mod.OracleSim(b, nthreads=4)
+    sim.step(10)
+    orc.step(10)
+    sim.sync()
+    assert _max_rel(sim.download("dH"), orc.get("dH")) <= 1e-10
+    assert np.abs(orc.get("dH")).max() > 0 and np.abs(orc.get("Qbx")).max() > 0
+    bad = _compare(sim, orc, ["u", "v", "z", "FS", "Qbx", "Qby", "dH"], 1e-10)
+    assert not bad, bad
+    sim.step(20)
+    orc.step(20)
+    sim.sync()
+    bad = _compare(sim, orc, ["u", "v", "z", "FS", "dH"], 1e-8)
+    assert not bad, bad
