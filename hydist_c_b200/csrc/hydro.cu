@@ -108,78 +108,8 @@ __global__ void k_interp_fs_col(State S, Coef c) {
   }
 }
 
-// The reference's run scan (support_funcs.cpp:260-288): wet runs of a line
-// starting at index 2, bounded by lim (M for rows, N for columns).
-__device__ __forceinline__ int scan_line(const int* k0, int stride, int lim, int* dau, int* cuoi,
-                                         int* err) {
-  int nseg = 0, start = 2, end = 0;
-  while (start < lim) {
-    if (k0[start * stride] != 0) {
-      while (k0[start * stride] && start < lim) start++;
-    }
-    if (start + 1 == lim) start = lim;
-    if (k0[start * stride] == 0 && start + 1 < lim) {
-      if (nseg >= SEG) {
-        atomicExch(err, DEV_SEG_OVERFLOW);
-        return nseg;
-      }
-      dau[nseg] = start;
-      end = start;
-      while (k0[end * stride] == 0 && end < lim) end++;
-      if (k0[end * stride] != 0 && end <= lim) {
-        cuoi[nseg] = end - 1;
-        start = end;
-      } else {
-        cuoi[nseg] = lim;
-        start = lim;
-      }
-      nseg++;
-    }
-  }
-  return nseg;
-}
-
-// The same tables as scan_line, in a fixed-trip loop whose loads do not
-// depend on the scan state (so they pipeline). The reference's loop yields
-// the maximal wet runs [s, e] of [2, lim] with s <= lim-2 (a run starting
-// at lim-1 or lim is dropped by its `start + 1 == lim` test); e is capped at
-// lim.
-__device__ __forceinline__ int scan_runs(const int* k0, int stride, int lim, int* dau, int* cuoi,
-                                         int* err) {
-  int nseg = 0, s = 0;
-  bool in = false;
-#pragma unroll 8
-  for (int p = 2; p <= lim; ++p) {
-    const bool wet = k0[p * stride] == 0;
-    if (wet && !in) {
-      in = true;
-      s = p;
-    } else if (!wet && in) {
-      in = false;
-      if (s <= lim - 2) {
-        if (nseg < SEG) {
-          dau[nseg] = s;
-          cuoi[nseg] = p - 1;
-        }
-        ++nseg;
-      }
-    }
-  }
-  if (in && s <= lim - 2) {
-    if (nseg < SEG) {
-      dau[nseg] = s;
-      cuoi[nseg] = lim;
-    }
-    ++nseg;
-  }
-  if (nseg > SEG) {
-    atomicExch(err, DEV_SEG_OVERFLOW);
-    nseg = SEG;
-  }
-  return nseg;
-}
-
-// Parallel form of the same tables. A cell p of a line (positions 2..lim) is
+// The wet-segment tables of Find_Calculation_limits_* (support_funcs.cpp:
+// 238-343) in parallel form. A cell p of a line (positions 2..lim) is
 // the start of a recorded run when it is wet, p == 2 or p-1 is dry, and
 // p <= lim-2; it is the end of a recorded run when it is wet, p == lim or
 // p+1 is dry, and the run it ends starts at or before lim-2 (for p = lim-1
@@ -283,18 +213,6 @@ __global__ void k_runs_sort(State S, int* seg_cnt) {
   *ce = 0;
 }
 
-__global__ void k_scan_rows(State S) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
-  if (i > S.N) return;
-  S.moci[i] = scan_runs(S.khouot + i * S.W, 1, S.M, S.daui + i * SEG, S.cuoii + i * SEG, S.err);
-}
-
-__global__ void k_scan_cols(State S) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
-  if (j > S.M) return;
-  S.mocj[j] = scan_runs(S.khouot + j, S.W, S.N, S.dauj + j * SEG, S.cuoij + j * SEG, S.err);
-}
-
 __global__ void k_htuongdoi(State S) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int i = blockIdx.y + 1;
@@ -302,70 +220,6 @@ __global__ void k_htuongdoi(State S) {
   const int W = S.W, p = i * W + j;
   S.Htdu[p] = (S.h[p - 1] + S.h[p] + S.z[p + W] + S.z[p]) * 0.5;
   S.Htdv[p] = (S.h[p - W] + S.h[p] + S.z[p + 1] + S.z[p]) * 0.5;
-}
-
-// preprocess_data (support_funcs.cpp:482-601): discharge distribution
-// weights per boundary cell and the FS boundary scale. One thread: it runs
-// once per scenario.
-__global__ void k_preprocess(State S, Coef c) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const int W = S.W, M = S.M, N = S.N;
-  const double dX = c.dX, ND = c.NANGDAY, ros = c.ros;
-  double* hu = S.hi;
-  for (int k = 0; k < S.mocj[M]; ++k) {
-    double sum = 0;
-    for (int i = S.dauj[M * SEG + k]; i <= S.cuoij[M * SEG + k]; ++i) {
-      hu[i] = (S.h[i * W + M] + S.h[(i - 1) * W + M]) / 2.0 - ND;
-      sum += pow(hu[i], 5.0 / 3.0);
-    }
-    for (int i = S.dauj[M * SEG + k]; i <= S.cuoij[M * SEG + k]; ++i)
-      hu[i] = pow(hu[i], 2.0 / 3.0) / (sum * dX);
-  }
-  double* hd = hu + (N + 3);
-  for (int k = 0; k < S.mocj[2]; ++k) {
-    double sum = 0;
-    for (int i = S.dauj[2 * SEG + k]; i <= S.cuoij[2 * SEG + k]; ++i) {
-      hd[i] = (S.h[i * W + 1] + S.h[(i - 1) * W + 1]) / 2.0 - ND;
-      sum += pow(hd[i], 5.0 / 3.0);
-    }
-    for (int i = S.dauj[2 * SEG + k]; i <= S.cuoij[2 * SEG + k]; ++i)
-      hd[i] = pow(hd[i], 2.0 / 3.0) / (sum * dX);
-  }
-  double* hl = hd + (N + 3);
-  for (int k = 0; k < S.moci[2]; ++k) {
-    double sum = 0;
-    for (int j = S.daui[2 * SEG + k]; j <= S.cuoii[2 * SEG + k]; ++j) {
-      hl[j] = (S.h[1 * W + j] + S.h[1 * W + j - 1]) / 2.0 - ND;
-      sum += pow(hl[j], 5.0 / 3.0);
-    }
-    for (int j = S.daui[2 * SEG + k]; j <= S.cuoii[2 * SEG + k]; ++j)
-      hl[j] = pow(hl[j], 2.0 / 3.0) / (sum * dX);
-  }
-  double* hr = hl + (M + 3);
-  for (int k = 0; k < S.moci[N]; ++k) {
-    double sum = 0;
-    for (int j = S.daui[N * SEG + k]; j <= S.cuoii[N * SEG + k]; ++j) {
-      hr[j] = (S.h[N * W + j] + S.h[N * W + j - 1]) / 2.0 - ND;
-      sum += pow(hr[j], 5.0 / 3.0);
-    }
-    for (int j = S.daui[N * SEG + k]; j <= S.cuoii[N * SEG + k]; ++j)
-      hr[j] = pow(hr[j], 2.0 / 3.0) / (sum * dX);
-  }
-  const double* hb = S.htaiz_bd;
-  double mu = hb[2 * W + M], md = hb[2 * W + 2];
-  for (int i = 3; i < N; ++i) {
-    if (hb[i * W + M] > mu) mu = hb[i * W + M];
-    if (hb[i * W + 2] > md) md = hb[i * W + 2];
-  }
-  double ml = hb[2 * W + 2], mr = hb[N * W + 2];
-  for (int j = 3; j < M; ++j) {
-    if (hb[2 * W + j] > ml) ml = hb[2 * W + j];
-    if (hb[N * W + j] > mr) mr = hb[N * W + j];
-  }
-  S.hmax[0] = mu != 0 ? 1.0 / (ros * mu) : mu;
-  S.hmax[1] = md != 0 ? 1.0 / (ros * md) : md;
-  S.hmax[2] = ml != 0 ? 1.0 / (ros * ml) : ml;
-  S.hmax[3] = mr != 0 ? 1.0 / (ros * mr) : mr;
 }
 
 // preprocess_data with one CTA per side: the per-cell powers in parallel,
@@ -485,11 +339,9 @@ __global__ void k_boundary(State S) {
   }
 }
 
-// ---------------------------------------------------- ADI line sweeps
-// (per-cell assembly: assembly.cuh)
 // ------------------------------------------------------------ smoothing
-// _normalize (support_funcs.cpp:761-782): tmp <- smoothed value, interior.
-// The same smoothing into a complete array (su / sv): smoothed on the
+// _normalize / update_buffer (support_funcs.cpp:761-808) into a complete
+// array (su / sv): smoothed on the
 // interior [2,N]x[2,M], the unsmoothed value elsewhere, i.e. t_u / t_v as
 // they stand after update_buffer. Readers of the smoothed velocity use it
 // directly and the half-step commit writes it back to t_u / t_v, u / v.
@@ -522,40 +374,6 @@ __global__ void k_smooth_full(State S, Coef c, int isU) {
     }
   }
   out_arr[g] = out;
-}
-
-__global__ void k_smooth(State S, Coef c, int isU) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
-  const int i = blockIdx.y + 2;
-  if (i > S.N || j > S.M) return;
-  const int W = S.W, g = i * W + j;
-  const double* val = isU ? S.tu : S.tv;
-  const int close = isU ? W : 1, far = isU ? 1 : W;
-  const double vg = val[g];
-  double out = vg;
-  if (vg != 0) {
-    int count = 2;
-    double nb = val[g - close] + val[g + close];
-    if (S.khouot[g - far] == 0) {
-      nb += val[g - far];
-      count++;
-    }
-    if (S.khouot[g + far] == 0) {
-      nb += val[g + far];
-      count++;
-    }
-    out = out * c.heso + (1 - c.heso) * nb / count;
-  }
-  S.tmp[g] = out;
-}
-
-// update_buffer (support_funcs.cpp:784-800).
-__global__ void k_smooth_commit(State S, int isU) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
-  const int i = blockIdx.y + 2;
-  if (i > S.N || j > S.M) return;
-  const int g = i * S.W + j;
-  (isU ? S.tu : S.tv)[g] = S.tmp[g];
 }
 
 // ---------------------------------------------------- explicit updates
@@ -714,62 +532,6 @@ __global__ void k_margin_u(State S, Coef c) {
     else tu[(first - 1) * w + j] = 2 * tu[first * w + j] - tu[(first + 1) * w + j];
     if (br2) tu[last * w + j] = 0;
     else tu[last * w + j] = 2 * tu[(last - 1) * w + j] - tu[(last - 2) * w + j];
-  }
-}
-
-// update_h_moi (support_funcs.cpp:71-86) over [1,N]x[1,M].
-__global__ void k_update_h_moi(State S) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int i = blockIdx.y + 1;
-  if (i > S.N || j > S.M) return;
-  const int g = i * S.W + j;
-  if (S.khouot[g] == 0) S.Hmoi[g] = S.htaiz[g] + S.tz[g];
-}
-
-// update_uvz (support_funcs.cpp:732-759) over [0,N]x[0,M].
-__global__ void k_update_uvz(State S, Coef c) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = blockIdx.y;
-  if (i > S.N || j > S.M) return;
-  const int g = i * S.W + j;
-  S.z[g] = S.tz[g];
-  S.u[g] = S.tu[g] * (1 - c.kenhhepd);
-  S.v[g] = S.tv[g] * (1 - c.kenhhepng);
-}
-
-// Reset_states_vertical (support_funcs.cpp:142-188): one thread per column.
-__global__ void k_reset_vertical(State S, Coef c) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (j > S.M) return;
-  const int off = S.W, N = S.N;
-  double* tz = S.tz;
-  double* Hm = S.Hmoi;
-  int* kh = S.khouot;
-  for (int i = 2; i <= N; ++i) {
-    if (tz[i * off + j] > S.z[i * off + j]) {
-      if (kh[(i - 1) * off + j] == 1) {
-        tz[(i - 1) * off + j] = tz[i * off + j];
-        Hm[(i - 1) * off + j] = S.htaiz[(i - 1) * off + j] + tz[i * off + j];
-        kh[(i - 1) * off + j] = 0;
-        S.FS[(i - 1) * off + j] = S.FS[i * off + j];
-      }
-      if (kh[(i + 1) * off + j] == 1) {
-        tz[(i + 1) * off + j] = tz[i * off + j];
-        Hm[(i + 1) * off + j] = S.htaiz[(i + 1) * off + j] + tz[i * off + j];
-        kh[(i + 1) * off + j] = 0;
-        S.FS[(i + 1) * off + j] = S.FS[i * off + j];
-      }
-    }
-  }
-  for (int i = 2; i <= N; ++i) {
-    if ((kh[i * off + j] == 0) && (Hm[i * off + j] <= c.H_TINH)) {
-      S.tu[(i - 1) * off + j] = 0;
-      S.tu[i * off + j] = 0;
-      S.tv[i * off + j - 1] = 0;
-      S.tv[i * off + j] = 0;
-      kh[i * off + j] = 1;
-      S.FS[i * off + j] = 0;
-    }
   }
 }
 
