@@ -2,7 +2,7 @@
 """Benchmark of the Hydist ADI time step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64] [--workload sediment-2048x1024|channel-256x128]
+                    [--precision fp64|fp32] [--workload sediment-2048x1024|channel-256x128]
 
 A step is one full ADI step (two half-steps, with the concentration sweeps)
 of the 2048x1024 sediment workload: dx=dy=5 m, dt=2 s, seeded synthetic
@@ -39,7 +39,7 @@ sys.path.insert(0, str(ROOT))
 from hydist_c_b200 import replicas as R  # noqa: E402
 
 BYTES_PER_CELL_STEP = {  # algorithmic bytes per interior cell and full step
-    ("fp64", False): 168, ("fp64", True): 232}
+    ("fp64", False): 168, ("fp64", True): 232, ("fp32", False): 112, ("fp32", True): 152}
 # Algorithmic bytes per cell of one line-solver launch (FP64), each field the
 # kernel's formulas read counted once and each field it writes once:
 #   hydraulic sweeps: read u, v, z, H_moi, Htdu, Htdv, visco, Kx1 (Ky1),
@@ -47,8 +47,13 @@ BYTES_PER_CELL_STEP = {  # algorithmic bytes per interior cell and full step
 #   concentration sweeps: read FS, H_moi, VTH, Fw, t_u, t_v, Htdu, Htdv, Kx,
 #     Ky = 10 x 8 B; write tFS = 8 B                             -> 88 B
 # The line-solver scratch (3 doubles per unknown, L2-resident) is not counted.
-SWEEP_BYTES_PER_CELL = {"line_solve_hydro_x": 88, "line_solve_hydro_y": 88,
-                        "line_solve_conc_x": 88, "line_solve_conc_y": 88}
+# In the FP32 form z is read (8 B) and t_z written (8 B) in FP64, the other
+# fields are 4 B: hydraulic 8 + 8 x 4 + 8 + 4 = 52 B, concentration 11 x 4 = 44 B.
+SWEEP_BYTES_PER_CELL = {
+    "fp64": {"line_solve_hydro_x": 88, "line_solve_hydro_y": 88,
+             "line_solve_conc_x": 88, "line_solve_conc_y": 88},
+    "fp32": {"line_solve_hydro_x": 52, "line_solve_hydro_y": 52,
+             "line_solve_conc_x": 44, "line_solve_conc_y": 44}}
 
 
 def sweep_cells(name, N, M):
@@ -593,7 +598,7 @@ def run_ours(args):
     # the four line solvers as the top kernels)
     dom = max(sweeps, key=sweeps.get)
     dom_cells = sweep_cells(dom, N, M)
-    alg_bytes = SWEEP_BYTES_PER_CELL[dom] * dom_cells
+    alg_bytes = SWEEP_BYTES_PER_CELL[args.precision][dom] * dom_cells
     ach = alg_bytes / (sweeps[dom] * 1e-3) / 1e9
     step_bytes = BYTES_PER_CELL_STEP[(args.precision, sed)] * cells
     step_ms = ms / args.steps
@@ -607,7 +612,8 @@ def run_ours(args):
     if traffic_file.exists():
         try:
             tj = json.loads(traffic_file.read_text())
-            roof["traffic"] = tj.get(args.workload, {}).get(dom)
+            roof["traffic"] = tj.get(args.workload if args.precision == "fp64"
+                                     else args.workload + "-fp32", {}).get(dom)
         except Exception:
             pass
     e2e = measure_e2e(H, bundle, dev, prec, args) if rank == 0 and not args.no_e2e else None
@@ -694,7 +700,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--workload", default="sediment-2048x1024",
                     help="sediment-2048x1024 | channel-256x128 | " + TRIDIAG + " | " + ENSEMBLE +
                          " | " + SERVING)

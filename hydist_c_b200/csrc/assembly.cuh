@@ -16,25 +16,28 @@
 
 namespace hyd {
 
-// Per-cell coefficients of the preindex step.
-struct Pre {
-  double f1, f2, f3, f5, a2, c2, d2;
+// Per-cell coefficients of the preindex step, in the step's type R.
+template <class R>
+struct PreT {
+  R f1, f2, f3, f5, a2, c2, d2;
 };
+using Pre = PreT<double>;
 
 // _uzSolver_calculate_preindex (UVZSolver_multithread.cpp:210-278).
-__device__ __forceinline__ Pre pre_x(const State& S, const Coef& c, int i, int j) {
+template <class R>
+__device__ __forceinline__ PreT<R> pre_x(const StateT<R>& S, const CoefT<R>& c, int i, int j) {
   const int w = S.W;
   const int g = i * w + j;
-  const double* u = S.u;
-  const double* v = S.v;
-  const double* Hm = S.Hmoi;
-  Pre P;
-  double p = 0.0, q = 0.0;
-  const double vtb = (v[g - 1] + v[g] + v[g + w - 1] + v[g + w]) * 0.25;
-  const double uu = u[g], VI = S.visco[g], Hu = S.Htdu[g];
-  const double dT = c.dT;
-  const double rH = 1.0 / Hu;
-  const double visc = VI * c.dT_dXbp;
+  const R* u = S.u;
+  const R* v = S.v;
+  const R* Hm = S.Hmoi;
+  PreT<R> P;
+  R p = 0, q = 0;
+  const R vtb = (v[g - 1] + v[g] + v[g + w - 1] + v[g + w]) * R(0.25);
+  const R uu = u[g], VI = S.visco[g], Hu = S.Htdu[g];
+  const R dT = c.dT;
+  const R rH = R(1) / Hu;
+  const R visc = VI * c.dT_dXbp;
   P.f1 = c.dTchia2dX * uu + visc;
   P.f2 = -(2 + S.Kx1[g] * dT * sqrt(uu * uu + vtb * vtb) * rH + 2 * visc);
   P.f3 = visc - c.dTchia2dX * uu;
@@ -58,24 +61,25 @@ __device__ __forceinline__ Pre pre_x(const State& S, const Coef& c, int i, int j
          dT * (c.Windx - S.Tsxw[g]) * rH;
   P.c2 = c.dTchia2dX * Hu;
   P.a2 = -c.dTchia2dX * S.Htdu[g - w];
-  P.d2 = S.z[g] - c.dTchia2dY * (S.Htdv[g] * v[g] - S.Htdv[g - 1] * v[g - 1]);
+  P.d2 = R(S.z[g]) - c.dTchia2dY * (S.Htdv[g] * v[g] - S.Htdv[g - 1] * v[g - 1]);
   return P;
 }
 
 // _vzSolver_calculate_preindex (UVZSolver_multithread.cpp:142-208).
-__device__ __forceinline__ Pre pre_y(const State& S, const Coef& c, int i, int j) {
+template <class R>
+__device__ __forceinline__ PreT<R> pre_y(const StateT<R>& S, const CoefT<R>& c, int i, int j) {
   const int w = S.W;
   const int g = i * w + j;
-  const double* u = S.u;
-  const double* v = S.v;
-  const double* Hm = S.Hmoi;
-  Pre P;
-  double p = 0.0, q = 0.0;
-  const double utb = (u[g - w] + u[g] + u[g - w + 1] + u[g + 1]) * 0.25;
-  const double vv = v[g], VI = S.visco[g], Hv = S.Htdv[g];
-  const double dT = c.dT;
-  const double rH = 1.0 / Hv;
-  const double visc = VI * c.dT_dYbp;
+  const R* u = S.u;
+  const R* v = S.v;
+  const R* Hm = S.Hmoi;
+  PreT<R> P;
+  R p = 0, q = 0;
+  const R utb = (u[g - w] + u[g] + u[g - w + 1] + u[g + 1]) * R(0.25);
+  const R vv = v[g], VI = S.visco[g], Hv = S.Htdv[g];
+  const R dT = c.dT;
+  const R rH = R(1) / Hv;
+  const R visc = VI * c.dT_dYbp;
   P.f1 = c.dTchia2dY * vv + visc;
   P.f2 = -(2 + S.Ky1[g] * dT * sqrt(vv * vv + utb * utb) * rH + 2 * visc);
   P.f3 = visc - c.dTchia2dY * vv;
@@ -99,34 +103,37 @@ __device__ __forceinline__ Pre pre_y(const State& S, const Coef& c, int i, int j
          dT * (c.Windy - S.Tsyw[g]) * rH;
   P.c2 = c.dTchia2dY * Hv;
   P.a2 = -c.dTchia2dY * S.Htdv[g - 1];
-  P.d2 = S.z[g] - c.dTchia2dX * (S.Htdu[g] * u[g] - S.Htdu[g - w] * u[g - w]);
+  P.d2 = R(S.z[g]) - c.dTchia2dX * (S.Htdu[g] * u[g] - S.Htdu[g - w] * u[g - w]);
   return P;
 }
 
-struct Mom {
-  double a1, b1, c1, d1;
+template <class R>
+struct MomT {
+  R a1, b1, c1, d1;
 };
+using Mom = MomT<double>;
 
 // _calculate_abcd (UVZSolver_multithread.cpp:280-342) at position k of a
 // segment [first, last]; P = cell k, Pn = cell k+1 (read only when used).
-__device__ __forceinline__ Mom abcd(const Pre& P, const Pre& Pn, int k, int first, int last,
-                                    double f4, bool br1, bool br2) {
-  Mom m;
+template <class R>
+__device__ __forceinline__ MomT<R> abcd(const PreT<R>& P, const PreT<R>& Pn, int k, int first,
+                                       int last, R f4, bool br1, bool br2) {
+  MomT<R> m;
   if (last - 1 > first) {
     if (br1 && k == first) {
-      const double rc = P.f3 / Pn.c2;
+      const R rc = P.f3 / Pn.c2;
       m.a1 = f4;
       m.b1 = P.f2 - rc * Pn.a2;
       m.c1 = -f4 - rc;
       m.d1 = P.f5 - rc * Pn.d2;
     } else if (br2 && k == last - 1) {
-      const double ra = P.f1 / P.a2;
+      const R ra = P.f1 / P.a2;
       m.a1 = f4 - ra;
       m.b1 = P.f2 - ra * P.c2;
       m.c1 = -f4;
       m.d1 = P.f5 - ra * P.d2;
     } else {
-      const double ra = P.f1 / P.a2, rc = P.f3 / Pn.c2;
+      const R ra = P.f1 / P.a2, rc = P.f3 / Pn.c2;
       m.a1 = f4 - ra;
       m.c1 = -f4 - rc;
       m.b1 = P.f2 - ra * P.c2 - rc * Pn.a2;

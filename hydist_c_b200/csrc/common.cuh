@@ -17,52 +17,71 @@ namespace hyd {
 
 constexpr int SEG = HYDIST_SEGMENT_LIMIT;
 
-// Constant_Coeffs (engine.h:39-52), derived as Load_coeffs does.
-struct Coef {
-  double dX, dY, dT, dXbp, dYbp, dX2, dY2, dTchia2dX, dTchia2dY, HaiChiadT;
-  double NANGDAY, H_TINH, heso, mu_mn, kenhhepng, kenhhepd;
-  double NDnen, Tod, Toe, hstoe, ghtoe, Mbochat;
-  double ro, ros, dm, muy, d90, Dorong, Sx;
-  double CORIOLIS_FORCE, g, Ks, Windx, Windy, Ufr, Dxr, wss;
+// Constant_Coeffs (engine.h:39-52), derived as Load_coeffs does, in the
+// arithmetic type R of the step (double; float in the FP32 form).
+template <class R>
+struct CoefT {
+  R dX, dY, dT, dXbp, dYbp, dX2, dY2, dTchia2dX, dTchia2dY, HaiChiadT;
+  R NANGDAY, H_TINH, heso, mu_mn, kenhhepng, kenhhepd;
+  R NDnen, Tod, Toe, hstoe, ghtoe, Mbochat;
+  R ro, ros, dm, muy, d90, Dorong, Sx;
+  R CORIOLIS_FORCE, g, Ks, Windx, Windy, Ufr, Dxr, wss;
   // reciprocals and products of constants, so that the kernels multiply
   // where the reference divides by a constant (one rounding of difference)
-  double r_dX, r_dY, r_dX2, r_dY2, r_dXbp, r_dYbp, dT_dXbp, dT_dYbp, sqrt_g;
-  double Mb_ros, r_Tod, r_Ufr2, Dxr_m03;  // Mbochat/ros, 1/Tod, 1/Ufr^2, Dxr^-0.3
-  double qb_k;  // 0.053 sqrt((Sx-1) g) dm^1.5 of the bed-load flux
+  R r_dX, r_dY, r_dX2, r_dY2, r_dXbp, r_dYbp, dT_dXbp, dT_dYbp, sqrt_g;
+  R Mb_ros, r_Tod, r_Ufr2, Dxr_m03;  // Mbochat/ros, 1/Tod, 1/Ufr^2, Dxr^-0.3
+  R qb_k;  // 0.053 sqrt((Sx-1) g) dm^1.5 of the bed-load flux
+
+  template <class Q>
+  static CoefT from(const CoefT<Q>& q) {
+    CoefT c;
+    const Q* src = reinterpret_cast<const Q*>(&q);
+    R* dst = reinterpret_cast<R*>(&c);
+    for (size_t k = 0; k < sizeof(CoefT<Q>) / sizeof(Q); ++k) dst[k] = (R)src[k];
+    return c;
+  }
 };
+using Coef = CoefT<double>;
 
 // Device error codes recorded in State::err[0].
 enum DevErr { DEV_OK = 0, DEV_SEG_OVERFLOW = 1 };
 
-// Every device pointer of one scenario. Passed by value to kernels.
-struct State {
+// Every device pointer of one scenario. Passed by value to kernels. The
+// water level (z, t_z), the bed (h, htaiz, htaiz_bd, dH), the series and the
+// clock are FP64 in every form; the other fields have the type R of the step
+// (double in the plain form, float in the FP32 form).
+template <class R>
+struct StateT {
   int M, N, W, H;  // W = M+3, H = N+3
   int T;           // rows of the hourly series
   int bienQ[4];
   int ketdinh;
   int race_new;    // extraction at an open last end reads the new neighbour
   // static fields
-  const double *h, *hsnham, *visco, *Fw, *htaiz, *htaiz_bd, *Kx1, *Ky1, *Tsxw, *Tsyw;
+  const double *h, *hsnham, *htaiz, *htaiz_bd;
+  const R *visco, *Fw, *Kx1, *Ky1, *Tsxw, *Tsyw;
   // state
-  double *u, *v, *z, *tu, *tv, *tz, *Hmoi, *Htdu, *Htdv, *FS, *tFS, *VTH, *Kx, *Ky, *dH, *Qbx,
-      *Qby;
+  double *z, *tz, *dH;
+  R *u, *v, *tu, *tv, *Hmoi, *Htdu, *Htdv, *FS, *tFS, *VTH, *Kx, *Ky, *Qbx, *Qby;
   int* khouot;
   // boundary
-  double *ubt, *ubp, *vbt, *vbd, *hi, *hmax;  // hmax[4]: up, down, left, right
+  R *ubt, *ubp, *vbt, *vbd;
+  double *hi, *hmax;  // hmax[4]: up, down, left, right
   const double *bc[4], *CC[4];
   const int* btype;  // 4 x SEG
   // wet segments
   int *daui, *cuoii, *moci, *dauj, *cuoij, *mocj;
   // scratch
-  double* tmp;   // smoothing buffer, (N+3)*(M+3)
-  double *su, *sv;  // t_u / t_v after the smoothing of the current half-step
+  R* tmp;        // smoothing buffer, (N+3)*(M+3)
+  R *su, *sv;    // t_u / t_v after the smoothing of the current half-step
   int* err;      // [0]: DevErr
-  double* lscratch;  // partitioned line solver: one slot per resident CTA
-  int lslots;        // number of slots (CTAs of the persistent sweep grid)
-  int* colflag;      // per column: holds a cell dried during the run
-  int* segcnt;       // run-start / run-end counters of the segment scan
-  double* clock;     // [0]: simulated time, advanced on the device by k_tick
+  R* lscratch;   // partitioned line solver: one slot per resident CTA
+  int lslots;    // number of slots (CTAs of the persistent sweep grid)
+  int* colflag;  // per column: holds a cell dried during the run
+  int* segcnt;   // run-start / run-end counters of the segment scan
+  double* clock; // [0]: simulated time, advanced on the device by k_tick
 };
+using State = StateT<double>;
 
 __host__ __device__ inline int cdiv(int a, int b) { return (a + b - 1) / b; }
 

@@ -106,8 +106,14 @@ void derive(const HydistParams& p, Coef& c) {
 struct HydistHandle {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // S holds the FP64 form's state; in the FP32 form Sf holds it and S only
+  // the fields common to both (dimensions, water level, bed, mask, tables,
+  // series, clock), so that form-independent code reads S alone
   State S{};
   Coef c{};
+  bool fp32 = false;
+  StateT<float> Sf{};
+  CoefT<float> cf{};
   HydistOptions o{};
   double t = 0;
   std::vector<void*> allocs;
@@ -123,6 +129,13 @@ struct HydistHandle {
 };
 
 namespace {
+
+// The launchers of the handle's form: f(state, coefficients).
+template <class F>
+void on_state(HydistHandle* h, F&& f) {
+  if (h->fp32) f(h->Sf, h->cf);
+  else f(h->S, h->c);
+}
 
 template <class T>
 int dalloc(HydistHandle* h, T** p, size_t n) {
@@ -160,12 +173,14 @@ int check_horizon(HydistHandle* h, int nsteps) {
 // one full step (engine.cpp:65-295); the sediment gates (engine.cpp:149,
 // 258) are decided on the host, the time itself advances on the device
 void enqueue_step(HydistHandle* h, bool sed_x, bool sed_y, bool bed, Trace* tr) {
-  launch_half_x(h->S, h->c, h->stream, tr);
-  if (sed_x) launch_sediment(h->S, h->c, h->o.bed_change_start, true, false, h->stream, tr);
-  else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_X + 1], h->stream);
-  launch_half_y(h->S, h->c, h->stream, tr);
-  if (sed_y) launch_sediment(h->S, h->c, h->o.bed_change_start, false, bed, h->stream, tr);
-  else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_Y + 1], h->stream);
+  on_state(h, [&](auto& St, auto& Cf) {
+    launch_half_x(St, Cf, h->stream, tr);
+    if (sed_x) launch_sediment(St, Cf, h->o.bed_change_start, true, false, h->stream, tr);
+    else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_X + 1], h->stream);
+    launch_half_y(St, Cf, h->stream, tr);
+    if (sed_y) launch_sediment(St, Cf, h->o.bed_change_start, false, bed, h->stream, tr);
+    else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_Y + 1], h->stream);
+  });
 }
 
 // the bed change runs after the j-sweep of a step ending at t2 once both the
@@ -211,32 +226,73 @@ __global__ void k_mass_final(const double* part, int n, double* out) {
   if (threadIdx.x == 0) out[0] = sh[0];
 }
 
-double* field_ptr(HydistHandle* h, int f) {
-  State& S = h->S;
+// A field's device array and element size (8, or 4 for the FP32 form's
+// single-precision fields).
+struct FieldRef {
+  void* p = nullptr;
+  int esz = 8;
+};
+
+template <class R>
+FieldRef bulk_field(const StateT<R>& S, int f) {
+  auto r = [](const R* q) { return FieldRef{const_cast<R*>(q), (int)sizeof(R)}; };
   switch (f) {
-    case HYDIST_FIELD_U: return S.u;
-    case HYDIST_FIELD_V: return S.v;
-    case HYDIST_FIELD_Z: return S.z;
-    case HYDIST_FIELD_FS: return S.FS;
-    case HYDIST_FIELD_TFS: return S.tFS;
-    case HYDIST_FIELD_H_MOI: return S.Hmoi;
-    case HYDIST_FIELD_DH: return S.dH;
-    case HYDIST_FIELD_HTDU: return S.Htdu;
-    case HYDIST_FIELD_HTDV: return S.Htdv;
-    case HYDIST_FIELD_TU: return S.tu;
-    case HYDIST_FIELD_TV: return S.tv;
-    case HYDIST_FIELD_TZ: return S.tz;
-    case HYDIST_FIELD_KX1: return const_cast<double*>(S.Kx1);
-    case HYDIST_FIELD_KY1: return const_cast<double*>(S.Ky1);
-    case HYDIST_FIELD_VTH: return S.VTH;
-    case HYDIST_FIELD_KX: return S.Kx;
-    case HYDIST_FIELD_KY: return S.Ky;
-    case HYDIST_FIELD_H: return const_cast<double*>(S.h);
-    case HYDIST_FIELD_HTAIZ: return const_cast<double*>(S.htaiz);
-    case HYDIST_FIELD_QBX: return S.Qbx;
-    case HYDIST_FIELD_QBY: return S.Qby;
-    default: return nullptr;
+    case HYDIST_FIELD_U: return r(S.u);
+    case HYDIST_FIELD_V: return r(S.v);
+    case HYDIST_FIELD_FS: return r(S.FS);
+    case HYDIST_FIELD_TFS: return r(S.tFS);
+    case HYDIST_FIELD_H_MOI: return r(S.Hmoi);
+    case HYDIST_FIELD_HTDU: return r(S.Htdu);
+    case HYDIST_FIELD_HTDV: return r(S.Htdv);
+    case HYDIST_FIELD_TU: return r(S.tu);
+    case HYDIST_FIELD_TV: return r(S.tv);
+    case HYDIST_FIELD_KX1: return r(S.Kx1);
+    case HYDIST_FIELD_KY1: return r(S.Ky1);
+    case HYDIST_FIELD_VTH: return r(S.VTH);
+    case HYDIST_FIELD_KX: return r(S.Kx);
+    case HYDIST_FIELD_KY: return r(S.Ky);
+    case HYDIST_FIELD_QBX: return r(S.Qbx);
+    case HYDIST_FIELD_QBY: return r(S.Qby);
+    default: return FieldRef{};
   }
+}
+
+FieldRef field_ref(HydistHandle* h, int f) {
+  const State& S = h->S;
+  switch (f) {
+    case HYDIST_FIELD_Z: return FieldRef{S.z, 8};
+    case HYDIST_FIELD_TZ: return FieldRef{S.tz, 8};
+    case HYDIST_FIELD_DH: return FieldRef{S.dH, 8};
+    case HYDIST_FIELD_H: return FieldRef{const_cast<double*>(S.h), 8};
+    case HYDIST_FIELD_HTAIZ: return FieldRef{const_cast<double*>(S.htaiz), 8};
+    default: return h->fp32 ? bulk_field(h->Sf, f) : bulk_field(h->S, f);
+  }
+}
+
+// n values of a field to host FP64 / from host FP64 (synchronous)
+int field_to_host(HydistHandle* h, const FieldRef& r, double* host, size_t n) {
+  if (r.esz == 8) {
+    CK(cudaMemcpyAsync(host, r.p, n * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return HYDIST_OK;
+  }
+  std::vector<float> tmp(n);
+  CK(cudaMemcpyAsync(tmp.data(), r.p, n * 4, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (size_t k = 0; k < n; ++k) host[k] = tmp[k];
+  return HYDIST_OK;
+}
+
+int field_from_host(HydistHandle* h, const FieldRef& r, const double* host, size_t n) {
+  if (r.esz == 8) {
+    CK(cudaMemcpyAsync(r.p, host, n * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return HYDIST_OK;
+  }
+  std::vector<float> tmp(host, host + n);
+  CK(cudaMemcpyAsync(r.p, tmp.data(), n * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return HYDIST_OK;
 }
 
 }  // namespace
@@ -298,14 +354,14 @@ void hydist_bienq_from_boundary_type(const int32_t* bt, int32_t n, int32_t bienQ
   for (int k = 0; k < 4; ++k) bienQ[k] = (bt && k < n && bt[k] == 2) ? 1 : 0;
 }
 
+}  // extern "C"
+
 namespace {
 
 int check_params(const HydistParams* p, const HydistOptions* o) {
   if (!(p->dX > 0 && p->dY > 0 && p->dT > 0)) return fail(HYDIST_ERR_ARG, "dX, dY, dT must be > 0");
   if (o->precision != HYDIST_FP64 && o->precision != HYDIST_FP32_REFINE)
     return fail(HYDIST_ERR_ARG, "unknown precision");
-  if (o->precision == HYDIST_FP32_REFINE)
-    return fail(HYDIST_ERR_ARG, "precision HYDIST_FP32_REFINE is not implemented yet");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(HYDIST_ERR_NODEVICE, "no CUDA device");
@@ -322,6 +378,8 @@ int new_handle(const HydistParams* p, const HydistOptions* o, int device, int M,
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   derive(*p, h->c);
+  h->fp32 = o->precision == HYDIST_FP32_REFINE;
+  h->cf = CoefT<float>::from(h->c);
   h->o = *o;
   h->t = o->t_start;
   State& S = h->S;
@@ -338,12 +396,29 @@ int new_handle(const HydistParams* p, const HydistOptions* o, int device, int M,
 
 // The arrays only this library uses: smoothing buffers, boundary weights,
 // line-solver scratch, flags, counters, the device clock.
+// The FP64 / FP32 arrays only this library uses: smoothing buffers and the
+// line-solver scratch (3 values per unknown, 4 lines per slot, one slot per
+// CTA of the persistent sweep grid).
+template <class R>
+int bulk_private(HydistHandle* h, StateT<R>& B) {
+  const State& S = h->S;
+  const size_t n = (size_t)S.W * S.H;
+  TRY(dalloc(h, &B.tmp, n));
+  TRY(dalloc(h, &B.sv, n));
+  B.su = B.tmp;
+  int nsm = 0;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+  B.lslots = 2 * nsm;
+  const size_t U = (size_t)2 * std::max(S.M, S.N);
+  // at least 4 (max(M,N)+3) doubles: preprocess_data borrows it as FP64
+  TRY(dalloc(h, &B.lscratch, std::max((size_t)B.lslots * 3 * U * 4, 8 * U + 64)));
+  return HYDIST_OK;
+}
+
+// The arrays only this library uses: the above, the boundary weights,
+// flags, counters, the device clock.
 int private_arrays(HydistHandle* h) {
   State& S = h->S;
-  const size_t n = (size_t)S.W * S.H;
-  TRY(dalloc(h, &S.tmp, n));
-  TRY(dalloc(h, &S.sv, n));
-  S.su = S.tmp;
   TRY(dalloc(h, &S.hi, 2 * (S.M + S.N + 6)));
   TRY(dalloc(h, &S.hmax, 4));
   TRY(dalloc(h, &S.err, 4));
@@ -351,19 +426,98 @@ int private_arrays(HydistHandle* h) {
   TRY(dalloc(h, &S.segcnt, 2 * S.H + 2 * S.W));
   TRY(dalloc(h, &S.clock, 4));
   TRY(set_device_clock(h));
-  // partitioned line solver scratch: 3 doubles per unknown, 4 lines per
-  // slot, one slot per CTA of the persistent sweep grid
-  int nsm = 0;
-  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
-  S.lslots = 2 * nsm;
-  const size_t U = (size_t)2 * std::max(S.M, S.N);
-  TRY(dalloc(h, &S.lscratch, (size_t)S.lslots * 3 * U * 4));
   h->mass_blocks = 296;
   TRY(dalloc(h, &h->mass_part, h->mass_blocks + 1));
+  return h->fp32 ? bulk_private(h, h->Sf) : bulk_private(h, h->S);
+}
+
+// a device array of n values of type R from host FP64 (converted; synchronous)
+template <class R>
+int upload_new(HydistHandle* h, R** dst, const double* host, size_t n) {
+  TRY(dalloc(h, dst, n));
+  if (!host) return HYDIST_OK;
+  if (sizeof(R) == 8) {
+    CK(cudaMemcpyAsync(*dst, host, n * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  } else {
+    std::vector<R> tmp(host, host + n);
+    CK(cudaMemcpyAsync(*dst, tmp.data(), n * sizeof(R), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
   return HYDIST_OK;
 }
 
+// the fields of the step's type R: static inputs (ν, Fw), derived statics
+// (Kx1, Ky1, Tsxw, Tsyw), the velocity/depth/concentration state and the
+// boundary velocities
+template <class R>
+int bulk_arrays(HydistHandle* h, StateT<R>& B, const HydistScenario* sc) {
+  const State& S = h->S;
+  const size_t n = (size_t)S.W * S.H;
+  R* tmp;
+  TRY(upload_new(h, &tmp, sc->visco, n));
+  B.visco = tmp;
+  TRY(upload_new(h, &tmp, sc->Fw, n));
+  B.Fw = tmp;
+  const R** st_static[] = {&B.Kx1, &B.Ky1, &B.Tsxw, &B.Tsyw};
+  for (const R** q : st_static) {
+    TRY(dalloc(h, &tmp, n));
+    *q = tmp;
+  }
+  R** st[] = {&B.u, &B.v, &B.tu, &B.tv, &B.Hmoi, &B.Htdu, &B.Htdv, &B.VTH, &B.Kx, &B.Ky, &B.Qbx,
+              &B.Qby};
+  for (R** q : st) TRY(dalloc(h, q, n));
+  TRY(upload_new(h, &B.FS, sc->FS0, n));
+  TRY(upload_new(h, &B.tFS, sc->FS0, n));
+  TRY(dalloc(h, &B.ubt, S.W));
+  TRY(dalloc(h, &B.ubp, S.W));
+  TRY(dalloc(h, &B.vbt, S.H));
+  TRY(dalloc(h, &B.vbd, S.H));
+  return HYDIST_OK;
+}
+
+// the fields common to both forms, from S into the FP32 form's state
+void mirror_common(HydistHandle* h) {
+  const State& S = h->S;
+  StateT<float>& F = h->Sf;
+  F.M = S.M;
+  F.N = S.N;
+  F.W = S.W;
+  F.H = S.H;
+  F.T = S.T;
+  for (int k = 0; k < 4; ++k) F.bienQ[k] = S.bienQ[k];
+  F.ketdinh = S.ketdinh;
+  F.race_new = S.race_new;
+  F.h = S.h;
+  F.hsnham = S.hsnham;
+  F.htaiz = S.htaiz;
+  F.htaiz_bd = S.htaiz_bd;
+  F.z = S.z;
+  F.tz = S.tz;
+  F.dH = S.dH;
+  F.khouot = S.khouot;
+  F.hi = S.hi;
+  F.hmax = S.hmax;
+  for (int k = 0; k < 4; ++k) {
+    F.bc[k] = S.bc[k];
+    F.CC[k] = S.CC[k];
+  }
+  F.btype = S.btype;
+  F.daui = S.daui;
+  F.cuoii = S.cuoii;
+  F.moci = S.moci;
+  F.dauj = S.dauj;
+  F.cuoij = S.cuoij;
+  F.mocj = S.mocj;
+  F.err = S.err;
+  F.colflag = S.colflag;
+  F.segcnt = S.segcnt;
+  F.clock = S.clock;
+}
+
 }  // namespace
+
+extern "C" {
 
 int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistOptions* o,
                   int device, HydistHandle** out) {
@@ -382,67 +536,43 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistO
     State& S = h->S;
     const size_t n = (size_t)S.W * S.H;
     double* tmp;
-    // static inputs
-    TRY(dalloc(h, &tmp, n));
-    CK(cudaMemcpyAsync(tmp, sc->h, n * 8, cudaMemcpyHostToDevice, h->stream));
+    // FP64 in both forms: bed, water level, bed change, series
+    TRY(upload_new(h, &tmp, sc->h, n));
     S.h = tmp;
-    TRY(dalloc(h, &tmp, n));
-    CK(cudaMemcpyAsync(tmp, sc->hsnham, n * 8, cudaMemcpyHostToDevice, h->stream));
+    TRY(upload_new(h, &tmp, sc->hsnham, n));
     S.hsnham = tmp;
-    TRY(dalloc(h, &tmp, n));
-    CK(cudaMemcpyAsync(tmp, sc->visco, n * 8, cudaMemcpyHostToDevice, h->stream));
-    S.visco = tmp;
-    TRY(dalloc(h, &tmp, n));
-    CK(cudaMemcpyAsync(tmp, sc->Fw, n * 8, cudaMemcpyHostToDevice, h->stream));
-    S.Fw = tmp;
     const double* bcs[4] = {sc->bc_up, sc->bc_down, sc->bc_left, sc->bc_right};
     const double* ccs[4] = {sc->CC_up, sc->CC_down, sc->CC_left, sc->CC_right};
     for (int k = 0; k < 4; ++k) {
-      TRY(dalloc(h, &tmp, S.T));
-      if (bcs[k]) CK(cudaMemcpyAsync(tmp, bcs[k], S.T * 8, cudaMemcpyHostToDevice, h->stream));
+      TRY(upload_new(h, &tmp, bcs[k], S.T));
       S.bc[k] = tmp;
-      TRY(dalloc(h, &tmp, S.T));
-      if (ccs[k]) CK(cudaMemcpyAsync(tmp, ccs[k], S.T * 8, cudaMemcpyHostToDevice, h->stream));
+      TRY(upload_new(h, &tmp, ccs[k], S.T));
       S.CC[k] = tmp;
     }
     int* itmp;
     TRY(dalloc(h, &itmp, 4 * SEG));
     CK(cudaMemcpyAsync(itmp, sc->boundary_type, 4 * SEG * 4, cudaMemcpyHostToDevice, h->stream));
     S.btype = itmp;
-    // derived static fields
     TRY(dalloc(h, &tmp, n));
     S.htaiz = tmp;
     TRY(dalloc(h, &tmp, n));
     S.htaiz_bd = tmp;
-    TRY(dalloc(h, &tmp, n));
-    S.Kx1 = tmp;
-    TRY(dalloc(h, &tmp, n));
-    S.Ky1 = tmp;
-    TRY(dalloc(h, &tmp, n));
-    S.Tsxw = tmp;
-    TRY(dalloc(h, &tmp, n));
-    S.Tsyw = tmp;
-    // state
-    double** st[] = {&S.u, &S.v, &S.z, &S.tu, &S.tv, &S.tz, &S.Hmoi, &S.Htdu, &S.Htdv, &S.FS,
-                     &S.tFS, &S.VTH, &S.Kx, &S.Ky, &S.dH, &S.Qbx, &S.Qby};
-    for (double** q : st) TRY(dalloc(h, q, n));
+    TRY(dalloc(h, &S.z, n));
+    TRY(dalloc(h, &S.tz, n));
+    TRY(dalloc(h, &S.dH, n));
     TRY(dalloc(h, &S.khouot, n));
-    if (sc->FS0) {
-      CK(cudaMemcpyAsync(S.FS, sc->FS0, n * 8, cudaMemcpyHostToDevice, h->stream));
-      CK(cudaMemcpyAsync(S.tFS, sc->FS0, n * 8, cudaMemcpyHostToDevice, h->stream));
-    }
-    TRY(dalloc(h, &S.ubt, S.W));
-    TRY(dalloc(h, &S.ubp, S.W));
-    TRY(dalloc(h, &S.vbt, S.H));
-    TRY(dalloc(h, &S.vbd, S.H));
     TRY(dalloc(h, &S.daui, S.H * SEG));
     TRY(dalloc(h, &S.cuoii, S.H * SEG));
     TRY(dalloc(h, &S.moci, S.H));
     TRY(dalloc(h, &S.dauj, S.W * SEG));
     TRY(dalloc(h, &S.cuoij, S.W * SEG));
     TRY(dalloc(h, &S.mocj, S.W));
+    // the step's type: FP64, or FP32 in the FP32 form
+    if (h->fp32) TRY(bulk_arrays(h, h->Sf, sc));
+    else TRY(bulk_arrays(h, h->S, sc));
     TRY(private_arrays(h));
-    launch_init(S, h->c, h->stream);
+    if (h->fp32) mirror_common(h);
+    on_state(h, [&](auto& St, auto& Cf) { launch_init(St, Cf, h->stream); });
     CK(cudaGetLastError());
     TRY(check_device_err(h));
     return HYDIST_OK;
@@ -471,6 +601,8 @@ int hydist_create_external(const HydistExternal* e, const HydistParams* p, const
   for (const void* q : need)
     if (!q) return fail(HYDIST_ERR_ARG, "missing device array");
   TRY(check_params(p, o));
+  if (o->precision != HYDIST_FP64)
+    return fail(HYDIST_ERR_ARG, "caller-owned arrays are FP64: use HYDIST_FP64");
   HydistHandle* h = nullptr;
   int rc = new_handle(p, o, device, e->M, e->N, e->total_time, e->bienQ, &h);
   if (rc == HYDIST_OK) rc = [&]() -> int {
@@ -550,13 +682,17 @@ int hydist_half_step(HydistHandle* h, int32_t half) {
   const double t = h->t + 0.5 * h->c.dT;
   const bool sed = t >= h->o.sediment_start;
   if (half == 0) {
-    launch_half_x(h->S, h->c, h->stream, &h->trace);
-    if (sed) launch_sediment(h->S, h->c, h->o.bed_change_start, true, false, h->stream, &h->trace);
+    on_state(h, [&](auto& St, auto& Cf) {
+      launch_half_x(St, Cf, h->stream, &h->trace);
+      if (sed) launch_sediment(St, Cf, h->o.bed_change_start, true, false, h->stream, &h->trace);
+    });
   } else {
-    launch_half_y(h->S, h->c, h->stream, &h->trace);
-    if (sed)
-      launch_sediment(h->S, h->c, h->o.bed_change_start, false, bed_on(h, t), h->stream,
-                      &h->trace);
+    on_state(h, [&](auto& St, auto& Cf) {
+      launch_half_y(St, Cf, h->stream, &h->trace);
+      if (sed)
+        launch_sediment(St, Cf, h->o.bed_change_start, false, bed_on(h, t), h->stream,
+                        &h->trace);
+    });
   }
   h->t = t;
   h->next_half = 1 - half;
@@ -571,7 +707,7 @@ int hydist_update_boundary(HydistHandle* h, double t) {
   h->t = t;
   int rc = set_device_clock(h);
   if (rc == HYDIST_OK) {
-    launch_boundary(h->S, h->stream);
+    on_state(h, [&](auto& St, auto&) { launch_boundary(St, h->stream); });
     h->trace.launches += 1;
     rc = cudaGetLastError() == cudaSuccess ? HYDIST_OK : fail(HYDIST_ERR_CUDA, "boundary launch failed");
   }
@@ -874,7 +1010,7 @@ int hydist_checkpoint_save(HydistHandle* h, const char* path) {
   std::vector<double> buf(n);
   for (int fid : kCheckpointFields) {
     if (!ok) break;
-    ok = cudaMemcpy(buf.data(), field_ptr(h, fid), n * 8, cudaMemcpyDeviceToHost) == cudaSuccess &&
+    ok = field_to_host(h, field_ref(h, fid), buf.data(), n) == HYDIST_OK &&
          std::fwrite(buf.data(), 8, n, f) == n;
   }
   std::vector<int32_t> mask(n);
@@ -909,7 +1045,7 @@ int hydist_checkpoint_load(HydistHandle* h, const char* path) {
   CK(cudaStreamSynchronize(h->stream));
   for (int fid : kCheckpointFields) {
     ok = std::fread(buf.data(), 8, n, f) == n &&
-         cudaMemcpy(field_ptr(h, fid), buf.data(), n * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+         field_from_host(h, field_ref(h, fid), buf.data(), n) == HYDIST_OK;
     if (!ok) break;
   }
   ok = ok && std::fread(mask.data(), 4, n, f) == n &&
@@ -937,9 +1073,9 @@ int hydist_download(HydistHandle* h, int32_t field, void* host) {
   if (field == HYDIST_FIELD_KHOUOT) {
     CK(cudaMemcpyAsync(host, h->S.khouot, n * 4, cudaMemcpyDeviceToHost, h->stream));
   } else {
-    double* p = field_ptr(h, field);
-    if (!p) return fail(HYDIST_ERR_ARG, "unknown field");
-    CK(cudaMemcpyAsync(host, p, n * 8, cudaMemcpyDeviceToHost, h->stream));
+    const FieldRef r = field_ref(h, field);
+    if (!r.p) return fail(HYDIST_ERR_ARG, "unknown field");
+    return field_to_host(h, r, static_cast<double*>(host), n);
   }
   CK(cudaStreamSynchronize(h->stream));
   return HYDIST_OK;
@@ -954,9 +1090,9 @@ int hydist_upload(HydistHandle* h, int32_t field, const void* host) {
     launch_scan_segments(h->S, h->stream);
     CK(cudaGetLastError());
   } else {
-    double* p = field_ptr(h, field);
-    if (!p) return fail(HYDIST_ERR_ARG, "unknown field");
-    CK(cudaMemcpyAsync(p, host, n * 8, cudaMemcpyHostToDevice, h->stream));
+    const FieldRef r = field_ref(h, field);
+    if (!r.p) return fail(HYDIST_ERR_ARG, "unknown field");
+    return field_from_host(h, r, static_cast<const double*>(host), n);
   }
   CK(cudaStreamSynchronize(h->stream));
   return HYDIST_OK;

@@ -31,7 +31,8 @@
 namespace hyd {
 
 // ----------------------------------------------------------------- init
-__global__ void k_onetime_init(State S, Coef c) {
+template <class R>
+__global__ void k_onetime_init(StateT<R> S, CoefT<R> c) {
   const int W = S.W, H = S.H, N = S.N, M = S.M;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
@@ -53,8 +54,8 @@ __global__ void k_onetime_init(State S, Coef c) {
   if (i >= 1 && j >= 1 && i <= N && j <= M) {
     double* htaiz = const_cast<double*>(S.htaiz);
     double* htaiz_bd = const_cast<double*>(S.htaiz_bd);
-    double* Kx1 = const_cast<double*>(S.Kx1);
-    double* Ky1 = const_cast<double*>(S.Ky1);
+    R* Kx1 = const_cast<R*>(S.Kx1);
+    R* Ky1 = const_cast<R*>(S.Ky1);
     htaiz[p] = (S.h[(i - 1) * W + j - 1] + S.h[(i - 1) * W + j] + S.h[i * W + j - 1] + S.h[p]) * 0.25;
     htaiz_bd[p] = htaiz[p];
     if (S.h[i * W + j - 1] + S.h[p] != 0)
@@ -67,7 +68,8 @@ __global__ void k_onetime_init(State S, Coef c) {
 }
 
 // ------------------------------------------------------- segment tables
-__global__ void k_interp_fs_rows(State S, Coef c) {
+template <class R>
+__global__ void k_interp_fs_rows(StateT<R> S, CoefT<R> c) {
   // Interpolate_FS_ng at row N (offset N-1, sign -1) and row 2 (offset 2, +1)
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int which = blockIdx.y;
@@ -90,7 +92,8 @@ __global__ void k_interp_fs_rows(State S, Coef c) {
   }
 }
 
-__global__ void k_interp_fs_col(State S, Coef c) {
+template <class R>
+__global__ void k_interp_fs_col(StateT<R> S, CoefT<R> c) {
   // Interpolate_FS_d at column M (offset M-1, sign -1); rows 1..M-1 as the
   // reference loops them (support_funcs.cpp:227)
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -126,7 +129,8 @@ __device__ __forceinline__ void run_flags(bool wm1, bool w, bool wp1, bool wm2_l
   end = w && (p == lim || !wp1) && ok;
 }
 
-__global__ void k_runs_flags(State S, int* seg_cnt) {
+template <class R>
+__global__ void k_runs_flags(StateT<R> S, int* seg_cnt) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int i = blockIdx.y + 2;
   if (i > S.N || j > S.M) return;
@@ -180,7 +184,8 @@ __device__ __forceinline__ void sort_small(int* a, int n) {
 
 // One thread per line: order the claimed slots, set the counts, clear the
 // counters for the next scan.
-__global__ void k_runs_sort(State S, int* seg_cnt) {
+template <class R>
+__global__ void k_runs_sort(StateT<R> S, int* seg_cnt) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int H = S.H, W = S.W;
   const int nrow = S.N - 1, ncol = S.M - 1;
@@ -213,7 +218,8 @@ __global__ void k_runs_sort(State S, int* seg_cnt) {
   *ce = 0;
 }
 
-__global__ void k_htuongdoi(State S) {
+template <class R>
+__global__ void k_htuongdoi(StateT<R> S) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int i = blockIdx.y + 1;
   if (i > S.N || j > S.M) return;
@@ -227,7 +233,8 @@ __global__ void k_htuongdoi(State S) {
 // round as the reference's), the boundary-depth maximum by one thread.
 // side: 0 up (column M), 1 down (column 2, node column 1), 2 left (row 2,
 // node row 1), 3 right (row N).
-__global__ void k_preprocess_sides(State S, Coef c, double* p53) {
+template <class R>
+__global__ void k_preprocess_sides(StateT<R> S, CoefT<R> c, double* p53) {
   const int side = blockIdx.x;
   const int W = S.W, M = S.M, N = S.N;
   const double dX = c.dX, ND = c.NANGDAY, ros = c.ros;
@@ -286,11 +293,13 @@ __global__ void k_preprocess_sides(State S, Coef c, double* p53) {
 // ------------------------------------------------------------- boundary
 // The simulated time lives on the device so that a captured step replays
 // unchanged: advanced by t += dT/2 per half-step (engine.cpp:66, 176).
-__global__ void k_tick(State S, double half) { S.clock[0] += half; }
+template <class R>
+__global__ void k_tick(StateT<R> S, double half) { S.clock[0] += half; }
 
 // Update_Boundary_Value (support_funcs.cpp:682-728). t arrives through a
 // float parameter in the reference (engine.cpp:22), hence the rounding.
-__global__ void k_boundary(State S) {
+template <class R>
+__global__ void k_boundary(StateT<R> S) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int M = S.M, N = S.N, W = S.W;
   if (i > M && i > N) return;
@@ -312,7 +321,7 @@ __global__ void k_boundary(State S) {
     const int* dau = isU ? S.daui : S.dauj;
     const int* cuoi = isU ? S.cuoii : S.cuoij;
     const double* hiv = s == 0 ? hi_up : (s == 1 ? hi_down : (s == 2 ? hi_left : hi_right));
-    double* barr = s == 0 ? S.vbt : (s == 1 ? S.vbd : (s == 2 ? S.ubt : S.ubp));
+    R* barr = s == 0 ? S.vbt : (s == 1 ? S.vbd : (s == 2 ? S.ubt : S.ubp));
     if (moc[loc] <= 0) continue;
     if (!(dau[loc * SEG] <= i && i <= cuoi[loc * SEG])) continue;
     const int seg = 0;  // only segment 0 is matched (support_funcs.cpp:614-618)
@@ -345,23 +354,24 @@ __global__ void k_boundary(State S) {
 // interior [2,N]x[2,M], the unsmoothed value elsewhere, i.e. t_u / t_v as
 // they stand after update_buffer. Readers of the smoothed velocity use it
 // directly and the half-step commit writes it back to t_u / t_v, u / v.
-__global__ void k_smooth_full(State S, Coef c, int isU) {
+template <class R>
+__global__ void k_smooth_full(StateT<R> S, CoefT<R> c, int isU) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   if (i >= S.H || j >= S.W) return;
   const int W = S.W, g = i * W + j;
-  const double* val = isU ? S.tu : S.tv;
-  double* out_arr = isU ? S.su : S.sv;
-  const double vg = val[g];
-  double out = vg;
+  const R* val = isU ? S.tu : S.tv;
+  R* out_arr = isU ? S.su : S.sv;
+  const R vg = val[g];
+  R out = vg;
   if (i >= 2 && i <= S.N && j >= 2 && j <= S.M) {
     // every operand is loaded up front, one round of memory latency
     const int close = isU ? W : 1, far = isU ? 1 : W;
-    const double a = val[g - close], b = val[g + close], l = val[g - far], r = val[g + far];
+    const R a = val[g - close], b = val[g + close], l = val[g - far], r = val[g + far];
     const int kl = S.khouot[g - far], kr = S.khouot[g + far];
     if (vg != 0) {
       int count = 2;
-      double nb = a + b;
+      R nb = a + b;
       if (kl == 0) {
         nb += l;
         count++;
@@ -390,7 +400,8 @@ __device__ __forceinline__ bool find_seg(const int* dau, const int* cuoi, int n,
 }
 
 // vSolver driven by solveV (UVZSolver_multithread.cpp:607-663, 961-978).
-__global__ void k_solve_v(State S, Coef c) {
+template <class R>
+__global__ void k_solve_v(StateT<R> S, CoefT<R> c) {
   // the block's cells share one row: its segment table goes to shared memory
   __shared__ int s_first[SEG], s_last[SEG];
   __shared__ int s_n;
@@ -407,22 +418,22 @@ __global__ void k_solve_v(State S, Coef c) {
   if (!find_seg(s_first, s_last, s_n, col, first, last)) return;
   if (first >= last || col >= last || col < first) return;
   const int off = S.W, g = row * off + col;
-  const double* u = S.u;
-  const double* v = S.v;
-  const double* tu = S.su;  // t_u after its smoothing
-  const double* Hm = S.Hmoi;
+  const R* u = S.u;
+  const R* v = S.v;
+  const R* tu = S.su;  // t_u after its smoothing
+  const R* Hm = S.Hmoi;
   // every operand up front: one round of memory latency
-  const double u00 = u[g - off], u01 = u[g], u10 = u[g - off + 1], u11 = u[g + 1];
-  const double t00 = tu[g - off], t01 = tu[g], t10 = tu[g - off + 1], t11 = tu[g + 1];
-  const double vv = v[g], vl = v[g - 1], vr = v[g + 1];
-  const double vm1 = v[g - off], vm2 = v[g - 2 * off], vp1 = v[g + off], vp2 = v[g + 2 * off];
-  const double hm1 = Hm[g - off], hm2 = Hm[g - 2 * off], hp1 = Hm[g + off];
-  const double Hv = S.Htdv[g], Ky1 = S.Ky1[g], zc = S.z[g], zr = S.z[g + 1], vis = S.visco[g],
-               tsy = S.Tsyw[g];
-  double p, q = 0, tmp = 0;
-  const double utb = (u00 + u01 + u10 + u11) * 0.25;
-  const double t_utb = (t00 + t01 + t10 + t11) * 0.25;
-  const double rHv = 1.0 / Hv;
+  const R u00 = u[g - off], u01 = u[g], u10 = u[g - off + 1], u11 = u[g + 1];
+  const R t00 = tu[g - off], t01 = tu[g], t10 = tu[g - off + 1], t11 = tu[g + 1];
+  const R vv = v[g], vl = v[g - 1], vr = v[g + 1];
+  const R vm1 = v[g - off], vm2 = v[g - 2 * off], vp1 = v[g + off], vp2 = v[g + 2 * off];
+  const R hm1 = Hm[g - off], hm2 = Hm[g - 2 * off], hp1 = Hm[g + off];
+  const R Hv = S.Htdv[g], Ky1 = S.Ky1[g], vis = S.visco[g], tsy = S.Tsyw[g];
+  const R dz = R(S.z[g + 1] - S.z[g]);  // the level difference in FP64 first
+  R p, q = 0, tmp = 0;
+  const R utb = (u00 + u01 + u10 + u11) * R(0.25);
+  const R t_utb = (t00 + t01 + t10 + t11) * R(0.25);
+  const R rHv = R(1) / Hv;
   p = (vr - vl) * c.r_dY2;
   p = c.HaiChiadT + p + Ky1 * sqrt(utb * utb + vv * vv) * rHv;
   if (hm1 <= c.H_TINH) {
@@ -442,41 +453,42 @@ __global__ void k_solve_v(State S, Coef c) {
     }
   }
   q = c.HaiChiadT * vv - q - c.CORIOLIS_FORCE * t_utb;
-  q = (q - c.g * (zr - zc) * c.r_dY + vis * (tmp + (vr - 2 * vv + vl) * c.r_dYbp)) +
+  q = (q - c.g * dz * c.r_dY + vis * (tmp + (vr - 2 * vv + vl) * c.r_dYbp)) +
       (c.Windy - tsy) * rHv;
   S.tv[g] = q / p;
 }
 
 // uSolver driven by solveU (UVZSolver_multithread.cpp:724-795, 938-959);
 // dX and Windx are read from dY and Windy as the reference does (:731,734).
-__global__ void k_solve_u(State S, Coef c) {
+template <class R>
+__global__ void k_solve_u(StateT<R> S, CoefT<R> c) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int row = blockIdx.y + 1;
   if (row > S.N || col > S.M) return;
   const int off = S.W;
   const int ij = row * off + col, i1j = ij + off;
-  const double* u = S.u;
-  const double* v = S.v;
-  const double* tv = S.sv;  // t_v after its smoothing
-  const double* Hm = S.Hmoi;
+  const R* u = S.u;
+  const R* v = S.v;
+  const R* tv = S.sv;  // t_v after its smoothing
+  const R* Hm = S.Hmoi;
   // every operand is loaded before the segment lookup (all in bounds for
   // rows 1..N, columns 2..M), so both take one round of memory latency
-  const double v00 = v[ij - 1], v01 = v[ij], v10 = v[i1j - 1], v11 = v[i1j];
-  const double t00 = tv[ij - 1], t01 = tv[ij], t10 = tv[i1j - 1], t11 = tv[i1j];
-  const double uu = u[ij], ud = u[i1j], uup = u[ij - off];
-  const double ul1 = u[ij - 1], ul2 = u[ij - 2], ur1 = u[ij + 1], ur2 = u[ij + 2];
-  const double hl1 = Hm[ij - 1], hl2 = Hm[ij - 2], hr1 = Hm[ij + 1];
-  const double Hu = S.Htdu[ij], Kx1 = S.Kx1[ij], zc = S.z[ij], zd = S.z[i1j], vis = S.visco[ij],
-               tsx = S.Tsxw[ij];
+  const R v00 = v[ij - 1], v01 = v[ij], v10 = v[i1j - 1], v11 = v[i1j];
+  const R t00 = tv[ij - 1], t01 = tv[ij], t10 = tv[i1j - 1], t11 = tv[i1j];
+  const R uu = u[ij], ud = u[i1j], uup = u[ij - off];
+  const R ul1 = u[ij - 1], ul2 = u[ij - 2], ur1 = u[ij + 1], ur2 = u[ij + 2];
+  const R hl1 = Hm[ij - 1], hl2 = Hm[ij - 2], hr1 = Hm[ij + 1];
+  const R Hu = S.Htdu[ij], Kx1 = S.Kx1[ij], vis = S.visco[ij], tsx = S.Tsxw[ij];
+  const R dz = R(S.z[i1j] - S.z[ij]);  // the level difference in FP64 first
   int first, last;
   if (!find_seg(S.dauj + col * SEG, S.cuoij + col * SEG, S.mocj[col], row, first, last)) return;
   if (first > last || row < first - 1 || row >= last) return;
-  const double Windx = c.Windy;
+  const R Windx = c.Windy;
   // dX is read from dY: 1/(2dX) = r_dY2, 1/dX^2 = r_dYbp, 1/dX = r_dY
-  double p, q = 0, tmp = 0;
-  const double vtb = (v00 + v01 + v10 + v11) * 0.25;
-  const double t_vtb = (t00 + t01 + t10 + t11) * 0.25;
-  const double rHu = 1.0 / Hu;
+  R p, q = 0, tmp = 0;
+  const R vtb = (v00 + v01 + v10 + v11) * R(0.25);
+  const R t_vtb = (t00 + t01 + t10 + t11) * R(0.25);
+  const R rHu = R(1) / Hu;
   p = (ud - uup) * c.r_dY2;
   p = (c.HaiChiadT + p + Kx1 * sqrt(vtb * vtb + uu * uu) * rHu);
   if (hl1 <= c.H_TINH) {
@@ -496,17 +508,18 @@ __global__ void k_solve_u(State S, Coef c) {
     }
   }
   q = c.HaiChiadT * uu - q + c.CORIOLIS_FORCE * t_vtb;
-  q = (q - c.g * (zd - zc) * c.r_dY + vis * (tmp + (ud - 2 * uu + uup) * c.r_dYbp)) +
+  q = (q - c.g * dz * c.r_dY + vis * (tmp + (ud - 2 * uu + uup) * c.r_dYbp)) +
       (Windx - tsx) * rHu;
   S.tu[ij] = q / p;
 }
 
 // update_margin_elem_V (UVZSolver_multithread.cpp:1018-1060).
-__global__ void k_margin_v(State S, Coef c) {
+template <class R>
+__global__ void k_margin_v(StateT<R> S, CoefT<R> c) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   if (i > S.N) return;
   const int w = S.W, M = S.M;
-  double* tv = S.tv;
+  R* tv = S.tv;
   for (int k = 0; k < S.moci[i]; ++k) {
     const int first = S.daui[i * SEG + k], last = S.cuoii[i * SEG + k];
     const bool br1 = (first > 2) || ((first == 2) && (fabs((S.h[i * w + first - 1] + S.h[(i - 1) * w + first - 1]) * 0.5 - c.NANGDAY) < 1e-16));
@@ -519,11 +532,12 @@ __global__ void k_margin_v(State S, Coef c) {
 }
 
 // update_margin_elem_U (UVZSolver_multithread.cpp:980-1016).
-__global__ void k_margin_u(State S, Coef c) {
+template <class R>
+__global__ void k_margin_u(StateT<R> S, CoefT<R> c) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
   if (j > S.M) return;
   const int w = S.W, N = S.N;
-  double* tu = S.tu;
+  R* tu = S.tu;
   for (int k = 0; k < S.mocj[j]; ++k) {
     const int first = S.dauj[j * SEG + k], last = S.cuoij[j * SEG + k];
     const bool br1 = (first > 2) || ((first == 2) && (fabs((S.h[1 * w + j] + S.h[1 * w + j - 1]) * 0.5 - c.NANGDAY) < 1e-16));
@@ -541,7 +555,8 @@ __global__ void k_margin_u(State S, Coef c) {
 // [1,N]x[1,M] in one pass. Htuongdoi reads the committed z of the
 // neighbour: t_z where it was committed, z where it never is (row N+1,
 // column M+1).
-__global__ void k_commit_a(State S, Coef c) {
+template <class R>
+__global__ void k_commit_a(StateT<R> S, CoefT<R> c) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   if (i > S.N || j > S.M) return;
@@ -549,7 +564,7 @@ __global__ void k_commit_a(State S, Coef c) {
   const double tz = S.tz[g];
   if (i >= 1 && j >= 1 && S.khouot[g] == 0) S.Hmoi[g] = S.htaiz[g] + tz;
   // t_u, t_v after their smoothing (update_buffer) and the commit
-  const double tu = S.su[g], tv = S.sv[g];
+  const R tu = S.su[g], tv = S.sv[g];
   S.tu[g] = tu;
   S.tv[g] = tv;
   S.z[g] = tz;
@@ -566,7 +581,8 @@ __global__ void k_commit_a(State S, Coef c) {
 // Half-step B, before the wetting pass: update_h_moi, and a per-column flag
 // telling whether the column holds a cell dried during the run (khouot 1),
 // the only cells the wetting loop of Reset_states_vertical can change.
-__global__ void k_hmoi_flags(State S, int* colflag) {
+template <class R>
+__global__ void k_hmoi_flags(StateT<R> S, int* colflag) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int i = blockIdx.y + 1;
   if (i > S.N + 1 || j > S.M) return;
@@ -578,14 +594,15 @@ __global__ void k_hmoi_flags(State S, int* colflag) {
 
 // The wetting loop of Reset_states_vertical (support_funcs.cpp:160-175),
 // sequential along i, on flagged columns only.
-__global__ void k_wetting(State S, Coef c, int* colflag) {
+template <class R>
+__global__ void k_wetting(StateT<R> S, CoefT<R> c, int* colflag) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (j > S.M) return;
   if (!colflag[j]) return;
   colflag[j] = 0;
   const int off = S.W, N = S.N;
   double* tz = S.tz;
-  double* Hm = S.Hmoi;
+  R* Hm = S.Hmoi;
   int* kh = S.khouot;
   for (int i = 2; i <= N; ++i) {
     if (tz[i * off + j] > S.z[i * off + j]) {
@@ -609,7 +626,8 @@ __global__ void k_wetting(State S, Coef c, int* colflag) {
 // independent per cell), update_uvz and Htuongdoi. A drying cell (i,j)
 // zeroes t_u at (i-1,j),(i,j) and t_v at (i,j-1),(i,j); each cell here reads
 // its own test and those of (i+1,j) and (i,j+1).
-__global__ void k_commit_b(State S, Coef c) {
+template <class R>
+__global__ void k_commit_b(StateT<R> S, CoefT<R> c) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   if (i > S.N || j > S.M) return;
@@ -643,7 +661,8 @@ __global__ void k_commit_b(State S, Coef c) {
 
 // The drying cells' mask (khouot = 1), written after k_commit_b has read
 // every neighbour's test.
-__global__ void k_dry_mask(State S, Coef c) {
+template <class R>
+__global__ void k_dry_mask(StateT<R> S, CoefT<R> c) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int i = blockIdx.y + 2;
   if (i > S.N || j > S.M) return;
@@ -654,35 +673,41 @@ __global__ void k_dry_mask(State S, Coef c) {
 // ------------------------------------------------------------- launchers
 static inline dim3 grid2(int nx, int ny, int bx) { return dim3(cdiv(nx, bx), ny); }
 
-void launch_init(const State& S, const Coef& c, cudaStream_t st) {
+template <class R>
+void launch_init(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
   k_onetime_init<<<dim3(cdiv(S.W, 128), S.H), 128, 0, st>>>(S, c);
   launch_find_limits(S, c, st, nullptr);
   k_htuongdoi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
   // the per-side scratch of the powers: the line-solver scratch is free here
-  k_preprocess_sides<<<4, 256, 0, st>>>(S, c, S.lscratch);
+  k_preprocess_sides<<<4, 256, 0, st>>>(S, c, reinterpret_cast<double*>(S.lscratch));
 }
 
-void launch_preprocess(const State& S, const Coef& c, cudaStream_t st) {
-  k_preprocess_sides<<<4, 256, 0, st>>>(S, c, S.lscratch);
+template <class R>
+void launch_preprocess(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
+  k_preprocess_sides<<<4, 256, 0, st>>>(S, c, reinterpret_cast<double*>(S.lscratch));
 }
 
-void launch_boundary(const State& S, cudaStream_t st) {
+template <class R>
+void launch_boundary(const StateT<R>& S, cudaStream_t st) {
   k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
 }
 
-void launch_scan_segments(const State& S, cudaStream_t st) {
+template <class R>
+void launch_scan_segments(const StateT<R>& S, cudaStream_t st) {
   k_runs_flags<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, S.segcnt);
   k_runs_sort<<<cdiv(S.N + S.M - 2, 128), 128, 0, st>>>(S, S.segcnt);
 }
 
-void launch_find_limits(const State& S, const Coef& c, cudaStream_t st, Trace* tr) {
+template <class R>
+void launch_find_limits(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace* tr) {
   k_interp_fs_rows<<<dim3(cdiv(S.M, 128), 2), 128, 0, st>>>(S, c);
   k_interp_fs_col<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
   launch_scan_segments(S, st);
   if (tr) tr->launches += 4;
 }
 
-void launch_half_x(const State& S, const Coef& c, cudaStream_t st, Trace* tr) {
+template <class R>
+void launch_half_x(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace* tr) {
   k_tick<<<1, 1, 0, st>>>(S, 0.5 * c.dT);
   k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
   if (tr) tr->mark(st, PH_BOUNDARY_X, 2);
@@ -707,7 +732,8 @@ void launch_half_x(const State& S, const Coef& c, cudaStream_t st, Trace* tr) {
   if (tr) tr->mark(st, PH_COMMIT_X, 3);
 }
 
-void launch_half_y(const State& S, const Coef& c, cudaStream_t st, Trace* tr) {
+template <class R>
+void launch_half_y(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace* tr) {
   k_tick<<<1, 1, 0, st>>>(S, c.dT * 0.5);
   k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
   if (tr) tr->mark(st, PH_BOUNDARY_Y, 2);
@@ -729,5 +755,17 @@ void launch_half_y(const State& S, const Coef& c, cudaStream_t st, Trace* tr) {
   launch_find_limits(S, c, st, tr);
   if (tr) tr->mark(st, PH_COMMIT_Y, 4);
 }
+
+#define HYD_HYDRO_INST(R)                                                                  \
+  template void launch_init<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t);         \
+  template void launch_preprocess<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t);   \
+  template void launch_boundary<R>(const StateT<R>&, cudaStream_t);                      \
+  template void launch_scan_segments<R>(const StateT<R>&, cudaStream_t);                 \
+  template void launch_find_limits<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t,   \
+                                      Trace*);                                            \
+  template void launch_half_x<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t, Trace*); \
+  template void launch_half_y<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t, Trace*);
+HYD_HYDRO_INST(double)
+HYD_HYDRO_INST(float)
 
 }  // namespace hyd

@@ -45,36 +45,37 @@ struct LineSeg {
   SegD s[SEG];
 };
 
-// Shared-memory layout of one CTA.
-template <int P>
+// Shared-memory layout of one CTA (R: the generator's arithmetic type).
+template <class R, int P>
 struct LSShared {
   LineSeg seg[LPB];
-  double sep[4][P * LPB];   // separator rows a, b, c, d
-  double tri[6][P * LPB];   // yF vF wF yL vL wL per chunk
-  double red[4][P * LPB];   // reduced system during PCR
-  double xsep[P * LPB];     // separator solutions
-  double xlast[LPB][SEG];   // solution at each segment's last row
+  R sep[4][P * LPB];   // separator rows a, b, c, d
+  R tri[6][P * LPB];   // yF vF wF yL vL wL per chunk
+  R red[4][P * LPB];   // reduced system during PCR
+  R xsep[P * LPB];     // separator solutions
+  R xlast[LPB][SEG];   // solution at each segment's last row
 };
 
-// Reciprocal with one Newton correction of the hardware estimate is not
-// used: a plain FP64 division keeps the rounding of the reference's
+// A plain division: with FP64 it keeps the rounding of the reference's
 // formulas within one ulp.
-__device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+template <class R>
+__device__ __forceinline__ R rcp(R x) { return R(1) / x; }
 
 // Gen::MIN_BLOCKS: resident CTAs per SM the P = 128 solver is compiled for
 // (2 caps registers at 64 per thread).
 template <class Gen, int P>
 __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_line_solve(Gen G) {
+  using R = typename Gen::Real;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  LSShared<P>& sh = *reinterpret_cast<LSShared<P>*>(smem_raw);
+  LSShared<R, P>& sh = *reinterpret_cast<LSShared<R, P>*>(smem_raw);
   const int tid = threadIdx.x;
   const int l = tid % LPB, k = tid / LPB;
   const int cidx = k * LPB + l;
   const int U = G.unknowns_per_line();
-  double* scr = G.scratch + (size_t)blockIdx.x * 3 * (size_t)U * LPB;
-  double* sc_c = scr;
-  double* sc_y = scr + (size_t)U * LPB;
-  double* sc_v = scr + 2 * (size_t)U * LPB;
+  R* scr = G.scratch + (size_t)blockIdx.x * 3 * (size_t)U * LPB;
+  R* sc_c = scr;
+  R* sc_y = scr + (size_t)U * LPB;
+  R* sc_v = scr + 2 * (size_t)U * LPB;
   const int ncells = G.cells_per_line();
   const int upc = Gen::UPC;
   const int ngroups = cdiv(G.lines(), LPB);
@@ -97,16 +98,16 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
     {
       typename Gen::Walker W;
       W.init(G, LS, line, c0);
-      double cp = 0, yp = 0, vp = 0;
+      R cp = 0, yp = 0, vp = 0;
       // first interior row in terms of both separators, accumulated forward:
       // x_0 = sum_k P_k (y'_k + v'_k x_L) + P_L x_R, P_0 = 1, P_{k+1} = -c'_k P_k
-      double Pk = 1, fy = 0, fv = 0;
+      R Pk = 1, fy = 0, fv = 0;
       int s = 0;
       for (int c = c0; c < c1; ++c) {
         W.cell(G, LS, c);
 #pragma unroll
         for (int e = 0; e < Gen::UPC; ++e, ++s) {
-          double A, B, C, D;
+          R A, B, C, D;
           W.row(G, LS, e, A, B, C, D);
           if (s == nu - 1) {
             sh.sep[0][cidx] = A;
@@ -115,12 +116,12 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
             sh.sep[3][cidx] = D;
           } else {
             if (s == 0) {
-              const double m = rcp(B);
+              const R m = rcp(B);
               cp = C * m;
               yp = D * m;
               vp = -A * m;
             } else {
-              const double m = rcp(B - A * cp);
+              const R m = rcp(B - A * cp);
               yp = (D - A * yp) * m;
               vp = -A * vp * m;
               cp = C * m;
@@ -145,12 +146,12 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
     }
     __syncthreads();
     // ---- reduced (Schur complement) system of the separators
-    double ra, rb, rc, rd;
+    R ra, rb, rc, rd;
     {
-      const double as = sh.sep[0][cidx], bs = sh.sep[1][cidx], cs = sh.sep[2][cidx],
-                   ds = sh.sep[3][cidx];
-      const double yL = sh.tri[3][cidx], vL = sh.tri[4][cidx], wL = sh.tri[5][cidx];
-      double yF = 0, vF = 0, wF = 0;
+      const R as = sh.sep[0][cidx], bs = sh.sep[1][cidx], cs = sh.sep[2][cidx],
+              ds = sh.sep[3][cidx];
+      const R yL = sh.tri[3][cidx], vL = sh.tri[4][cidx], wL = sh.tri[5][cidx];
+      R yF = 0, vF = 0, wF = 0;
       if (k + 1 < P) {
         const int n1 = cidx + LPB;
         yF = sh.tri[0][n1];
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
       sh.red[2][cidx] = rc;
       sh.red[3][cidx] = rd;
       __syncthreads();
-      double am = 0, bm = 1, cm = 0, dm = 0, an = 0, bn = 1, cn = 0, dn = 0;
+      R am = 0, bm = 1, cm = 0, dm = 0, an = 0, bn = 1, cn = 0, dn = 0;
       if (k - st >= 0) {
         const int o = cidx - st * LPB;
         am = sh.red[0][o];
@@ -185,10 +186,10 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
         dn = sh.red[3][o];
       }
       __syncthreads();
-      const double k1 = ra / bm, k2 = rc / bn;
-      const double na = -am * k1, nc = -cn * k2;
-      const double nb = rb - cm * k1 - an * k2;
-      const double nd = rd - dm * k1 - dn * k2;
+      const R k1 = ra / bm, k2 = rc / bn;
+      const R na = -am * k1, nc = -cn * k2;
+      const R nb = rb - cm * k1 - an * k2;
+      const R nd = rd - dm * k1 - dn * k2;
       ra = na;
       rb = nb;
       rc = nc;
@@ -198,16 +199,16 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
     __syncthreads();
     // ---- pass C: back substitution and emission
     {
-      const double xr = sh.xsep[cidx];
-      const double xl = (k > 0) ? sh.xsep[cidx - LPB] : 0.0;
+      const R xr = sh.xsep[cidx];
+      const R xl = (k > 0) ? sh.xsep[cidx - LPB] : R(0);
       typename Gen::Emitter E;
       E.init(G, LS, line);
       E.emit(G, LS, sh.xlast[l], q0 + nu - 1, xr);
-      double xn = xr;
+      R xn = xr;
 #pragma unroll 4
       for (int t = nu - 2; t >= 0; --t) {
         const size_t o = (size_t)(q0 + t) * LPB + l;
-        const double x = sc_y[o] + sc_v[o] * xl - sc_c[o] * xn;
+        const R x = sc_y[o] + sc_v[o] * xl - sc_c[o] * xn;
         E.emit(G, LS, sh.xlast[l], q0 + t, x);
         xn = x;
       }

@@ -16,32 +16,33 @@ namespace hyd {
 
 // Find_VTH (rows/columns 2..) and hesoK (1..) over one grid: both read the
 // committed velocities of the same cells.
-__global__ void k_vth_heso(State S, Coef c, int i_hi) {
+template <class R>
+__global__ void k_vth_heso(StateT<R> S, CoefT<R> c, int i_hi) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int i = blockIdx.y + 1;
   if (i > i_hi || j > S.M) return;
   const int W = S.W, p = i * W + j;
-  const double tu = S.tu[p], tv = S.tv[p];
+  const R tu = S.tu[p], tv = S.tv[p];
   if (i >= 2 && j >= 2) {
     if ((S.htaiz[p] > c.NANGDAY) && (S.Hmoi[p] > c.H_TINH)) {
-      const double ut = (tu + S.tu[p - W]) * 0.5;
-      const double vt = (tv + S.tv[p - 1]) * 0.5;
+      const R ut = (tu + S.tu[p - W]) * R(0.5);
+      const R vt = (tv + S.tv[p - 1]) * R(0.5);
       S.VTH[p] = sqrt(ut * ut + vt * vt);
     } else {
       S.VTH[p] = 0;
     }
   }
   const double hp = S.h[p];
-  const double Hu = S.Htdu[p], Hv = S.Htdv[p];
+  const R Hu = S.Htdu[p], Hv = S.Htdv[p];
   if (Hu > 0) {
-    const double Cz = 18 * log(12 * Hu / c.Ks);
-    const double k = 5.93 * c.sqrt_g * (S.h[p - 1] + hp) * 0.25 * fabs(tu) / Cz;
-    S.Kx[p] = fmin(100.0, fmax(5.0, k));
+    const R Cz = 18 * log(12 * Hu / c.Ks);
+    const R k = R(5.93) * c.sqrt_g * R(S.h[p - 1] + hp) * R(0.25) * fabs(tu) / Cz;
+    S.Kx[p] = fmin(R(100), fmax(R(5), k));
   }
   if (Hv > 0) {
-    const double Cz = 18 * log(12 * Hv / c.Ks);
-    const double k = 5.93 * c.sqrt_g * (S.h[p - W] + hp) * 0.25 * fabs(tv) / Cz;
-    S.Ky[p] = fmin(100.0, fmax(5.0, k));
+    const R Cz = 18 * log(12 * Hv / c.Ks);
+    const R k = R(5.93) * c.sqrt_g * R(S.h[p - W] + hp) * R(0.25) * fabs(tv) / Cz;
+    S.Ky[p] = fmin(R(100), fmax(R(5), k));
   }
 }
 
@@ -52,25 +53,26 @@ __global__ void k_vth_heso(State S, Coef c, int i_hi) {
 // the VTH it tests to be zero), Toee starting from the coefficient Toe
 // (:359), both components in the corner copies (:410-419), t_u[pos] > 0 in
 // the downwind test (:479).
-__global__ void k_calc_qb(State S, Coef c) {
+template <class R>
+__global__ void k_calc_qb(StateT<R> S, CoefT<R> c) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int i = blockIdx.y + 2;
   if (i > S.N || j > S.M) return;
   const int w = S.W, pos = i * w + j, N = S.N, M = S.M;
-  double qx = 0, qy = 0;
-  const double vth = S.VTH[pos];
+  R qx = 0, qy = 0;
+  const R vth = S.VTH[pos];
   if (vth != 0 && S.khouot[pos] == 0) {
-    double Toee = c.Toe, Tx = 0;
-    const double Hm = S.Hmoi[pos];
-    const double Tob = c.ro * S.Fw[pos] * (vth * vth);
+    R Toee = c.Toe, Tx = 0;
+    const R Hm = S.Hmoi[pos];
+    const R Tob = c.ro * S.Fw[pos] * (vth * vth);
     if (Hm > c.ghtoe) Toee = c.Toe * (1 + c.hstoe * ((Hm - c.ghtoe)));
     if (Tob > Toee) Tx = Tob / Toee - 1;
-    const double base = c.qb_k * pow(Tx, 2.1) * c.Dxr_m03;
-    qx = base * (S.tu[pos] + S.tu[pos - w]) * 0.5 / vth;
-    qy = base * (S.tv[pos] + S.tv[pos - 1]) * 0.5 / vth;
+    const R base = c.qb_k * pow(Tx, R(2.1)) * c.Dxr_m03;
+    qx = base * (S.tu[pos] + S.tu[pos - w]) * R(0.5) / vth;
+    qy = base * (S.tv[pos] + S.tv[pos - 1]) * R(0.5) / vth;
   }
-  double* Qbx = S.Qbx;
-  double* Qby = S.Qby;
+  R* Qbx = S.Qbx;
+  R* Qby = S.Qby;
   Qbx[pos] = qx;
   Qby[pos] = qy;
   // margins and corners copy the nearest interior value (:402-431)
@@ -110,7 +112,8 @@ __global__ void k_calc_qb(State S, Coef c) {
 
 // _bed_load on rows 3..N-2 (BedLoad with the j-sweep's range,
 // engine.cpp:292), cells of the row's wet segments of at least 3 cells.
-__global__ void k_bed_load(State S, Coef c) {
+template <class R>
+__global__ void k_bed_load(StateT<R> S, CoefT<R> c) {
   __shared__ int s_first[SEG], s_last[SEG];
   __shared__ int s_n;
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
@@ -132,8 +135,8 @@ __global__ void k_bed_load(State S, Coef c) {
   if (last - first < 2 || j < first || j > last) return;
   const int w = S.W, pos = i * w + j, M = S.M, N = S.N;
   const int* kh = S.khouot;
-  const double *Qbx = S.Qbx, *Qby = S.Qby, *FS = S.FS, *tu = S.tu, *tv = S.tv;
-  double p = 0, q = 0;
+  const R *Qbx = S.Qbx, *Qby = S.Qby, *FS = S.FS, *tu = S.tu, *tv = S.tv;
+  R p = 0, q = 0;
   if (kh[pos - w] == 1) {
     if (tu[pos] < 0) p = (-3 * Qbx[pos] + 4 * Qbx[pos + w] - Qbx[pos + 2 * w]) * c.r_dX2;
   } else {
@@ -152,7 +155,7 @@ __global__ void k_bed_load(State S, Coef c) {
       q = (Qby[pos + 1] - Qby[pos - 1]) * c.r_dY2;
     }
   }
-  double tH = p + q;
+  R tH = p + q;
   p = FS[pos + w] - FS[pos];
   if ((kh[pos + 2 * w] == 1 || kh[pos - w] == 1) && (i < N)) p = 0;
   q = FS[pos] - FS[pos - w];
@@ -165,19 +168,20 @@ __global__ void k_bed_load(State S, Coef c) {
   if (((first > 2) && (kh[pos - 2] == 1 || kh[pos + 1] == 1)) || (first == 2 && kh[pos + 1] == 1)) q = 0;
   p = c.r_dYbp * (S.Htdv[pos] * S.Ky[pos] * p - S.Htdv[pos - 1] * S.Ky[pos - 1] * q);
   tH = tH + p;
-  const double Hm = S.Hmoi[pos], fs = FS[pos], vth = S.VTH[pos];
-  const double cc = 18 * log(12 * Hm / c.Ks);
-  const double Uf = c.sqrt_g * fabs(vth) / cc;
-  const double om = 1 - fs, om2 = om * om;
-  const double wsm = c.wss * (om2 * om2);
-  double Zf = 0;
-  if (fs > 0.0) Zf = wsm / (0.4 * (Uf + 2 * wsm));
-  const double src = S.ketdinh ? source_chs(c, wsm, Zf, fs, S.Fw[pos], vth, Hm)
-                               : source_nchs(c, wsm, Zf, Uf, 1.0 / Hm, fs);
-  S.dH[pos] += c.dT / (1 - c.Dorong) * (src + tH);
+  const R Hm = S.Hmoi[pos], fs = FS[pos], vth = S.VTH[pos];
+  const R cc = 18 * log(12 * Hm / c.Ks);
+  const R Uf = c.sqrt_g * fabs(vth) / cc;
+  const R om = 1 - fs, om2 = om * om;
+  const R wsm = c.wss * (om2 * om2);
+  R Zf = 0;
+  if (fs > R(0)) Zf = wsm / (R(0.4) * (Uf + 2 * wsm));
+  const R src = S.ketdinh ? source_chs(c, wsm, Zf, fs, S.Fw[pos], vth, Hm)
+                          : source_nchs(c, wsm, Zf, Uf, R(1) / Hm, fs);
+  S.dH[pos] += double(c.dT / (1 - c.Dorong) * (src + tH));
 }
 
-__global__ void k_update_fs(State S) {
+template <class R>
+__global__ void k_update_fs(StateT<R> S) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int i = blockIdx.y + 1;
   if (i > S.N || j > S.M) return;
@@ -185,7 +189,8 @@ __global__ void k_update_fs(State S) {
   S.FS[g] = S.tFS[g];
 }
 
-void launch_sediment(const State& S, const Coef& c, double s_start, bool xdir, bool bed,
+template <class R>
+void launch_sediment(const StateT<R>& S, const CoefT<R>& c, double s_start, bool xdir, bool bed,
                      cudaStream_t st, Trace* tr) {
   // first half: Find_VTH/hesoK over rows to N; second half: to N-1
   // (launch shape of engine.cpp:259-260 never reaches row N)
@@ -204,5 +209,10 @@ void launch_sediment(const State& S, const Coef& c, double s_start, bool xdir, b
   }
   if (tr) tr->mark(st, xdir ? PH_SEDIMENT_X : PH_SEDIMENT_Y, launched);
 }
+
+template void launch_sediment<double>(const StateT<double>&, const CoefT<double>&, double, bool,
+                                      bool, cudaStream_t, Trace*);
+template void launch_sediment<float>(const StateT<float>&, const CoefT<float>&, double, bool, bool,
+                                     cudaStream_t, Trace*);
 
 }  // namespace hyd

@@ -12,29 +12,30 @@
 namespace hyd {
 
 // source_chs (sediment_transport.cpp:11-38)
-__device__ __forceinline__ double source_chs(const Coef& c, double wsm, double Zf, double fs,
-                                             double fw, double vth, double h_moi) {
-  double toee = c.Toe;
-  double S = 0;
-  const double tob = c.ro * fw * (vth * vth);
+template <class R>
+__device__ __forceinline__ R source_chs(const CoefT<R>& c, R wsm, R Zf, R fs, R fw, R vth,
+                                        R h_moi) {
+  R toee = c.Toe;
+  R S = 0;
+  const R tob = c.ro * fw * (vth * vth);
   if (h_moi > c.ghtoe) toee = toee * (1 + c.hstoe * ((h_moi - c.ghtoe)));
   if (tob > toee) {
     S = c.Mb_ros * (tob - toee) / toee;
   } else if (tob < c.Tod) {
-    const double Pd = 1 - tob * c.r_Tod;
-    const double beta = 1 + (Zf / (1.25 + 4.75 * (Pd * Pd * sqrt(Pd))));
-    const double Cb = beta * fs;
+    const R Pd = 1 - tob * c.r_Tod;
+    const R beta = 1 + (Zf / (R(1.25) + R(4.75) * (Pd * Pd * sqrt(Pd))));
+    const R Cb = beta * fs;
     S = -wsm * Cb * Pd;
   }
   return S;
 }
 
 // source_nchs (sediment_transport.cpp:41-49)
-__device__ __forceinline__ double source_nchs(const Coef& c, double wsm, double Zf, double Uf,
-                                              double r_hmoi, double fs) {
-  const double gamac = 0.434 + 5.975 * Zf + 2.888 * Zf * Zf;
-  const double Tx = fmax(0.0, (Uf * Uf - c.Ufr * c.Ufr) * c.r_Ufr2);
-  const double Cac = 0.015 * c.dm * (Tx * sqrt(Tx)) * c.Dxr_m03 * (20.0 * r_hmoi);
+template <class R>
+__device__ __forceinline__ R source_nchs(const CoefT<R>& c, R wsm, R Zf, R Uf, R r_hmoi, R fs) {
+  const R gamac = R(0.434) + R(5.975) * Zf + R(2.888) * Zf * Zf;
+  const R Tx = fmax(R(0), (Uf * Uf - c.Ufr * c.Ufr) * c.r_Ufr2);
+  const R Cac = R(0.015) * c.dm * (Tx * sqrt(Tx)) * c.Dxr_m03 * (R(20) * r_hmoi);
   return wsm * (Cac - gamac * fs);
 }
 
@@ -44,50 +45,50 @@ __device__ __forceinline__ double source_nchs(const Coef& c, double wsm, double 
 // velocity and Htd*K product of this cell (x: tu, Htdu*Kx at pos; y: tv,
 // Htdv*Ky at pos), vel_p / hk_p those of the cell before it (pos-W in x,
 // pos-1 in y).
-__device__ __forceinline__ void fs_cell(const State& S, const Coef& c, bool xdir, int i, int j,
-                                        double vel_c, double hk_c, double vel_p, double hk_p,
-                                        double tt, double s_start, double& A, double& B,
-                                        double& Cc, double& D) {
+template <class R>
+__device__ __forceinline__ void fs_cell(const StateT<R>& S, const CoefT<R>& c, bool xdir, int i,
+                                        int j, R vel_c, R hk_c, R vel_p, R hk_p, double tt,
+                                        double s_start, R& A, R& B, R& Cc, R& D) {
   const int w = S.W, pos = i * w + j;
-  const double* Hm = S.Hmoi;
-  const double* FS = S.FS;
-  const double H_TINH = c.H_TINH;
-  const double Hc = Hm[pos], fs = FS[pos], vth = S.VTH[pos];
-  const double rH = 1.0 / Hc;
-  const double cc = 18 * log(12 * Hc / c.Ks);
-  const double Uf = c.sqrt_g * fabs(vth) / cc;
-  const double om = 1 - fs, om2 = om * om;
-  const double wsm = c.wss * (om2 * om2);
-  double Zf = 0, Sx;
-  if (fs > 0.00001) Zf = wsm / (0.4 * (Uf + 2 * wsm));
+  const R* Hm = S.Hmoi;
+  const R* FS = S.FS;
+  const R H_TINH = c.H_TINH;
+  const R Hc = Hm[pos], fs = FS[pos], vth = S.VTH[pos];
+  const R rH = R(1) / Hc;
+  const R cc = 18 * log(12 * Hc / c.Ks);
+  const R Uf = c.sqrt_g * fabs(vth) / cc;
+  const R om = 1 - fs, om2 = om * om;
+  const R wsm = c.wss * (om2 * om2);
+  R Zf = 0, Sx;
+  if (fs > R(0.00001)) Zf = wsm / (R(0.4) * (Uf + 2 * wsm));
   // the i-sweep evaluates gamav before Zf (:247), the j-sweep after it (:109)
-  const double gamav = xdir ? 0.98 : 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;
+  const R gamav = xdir ? R(0.98) : R(0.98) - R(0.198) * Zf + R(0.032) * Zf * Zf;
   if (S.ketdinh)
     Sx = source_chs(c, wsm, Zf, fs, S.Fw[pos], vth, Hc);
   else
     Sx = source_nchs(c, wsm, Zf, Uf, rH, fs);
   if (tt < s_start) Sx = 0;
   // along-line terms
-  const double r_d2 = xdir ? c.r_dX2 : c.r_dY2;      // 1 / (2 d)
-  const double r_dd = (xdir ? c.r_dXbp : c.r_dYbp) * rH;  // 1 / (H_moi d^2)
-  const double adv = gamav * 0.5 * (vel_c + vel_p) * r_d2;
+  const R r_d2 = xdir ? c.r_dX2 : c.r_dY2;      // 1 / (2 d)
+  const R r_dd = (xdir ? c.r_dXbp : c.r_dYbp) * rH;  // 1 / (H_moi d^2)
+  const R adv = gamav * R(0.5) * (vel_c + vel_p) * r_d2;
   A = -adv - hk_p * r_dd;
   Cc = adv - hk_c * r_dd;
   B = c.HaiChiadT + (hk_c + hk_p) * r_dd;
   // cross-line terms
   const int s = xdir ? 1 : w;  // stride across the sweep
-  const double* vx = xdir ? S.tv : S.tu;
-  const double* hx = xdir ? S.Htdv : S.Htdu;
-  const double* kx = xdir ? S.Ky : S.Kx;
-  const double hm1 = Hm[pos - s], hp1 = Hm[pos + s], hm2 = Hm[pos - 2 * s], hp2 = Hm[pos + 2 * s];
-  const double fm = FS[pos - s], fp = FS[pos + s];
-  double p = 0, q = 0;
+  const R* vx = xdir ? S.tv : S.tu;
+  const R* hx = xdir ? S.Htdv : S.Htdu;
+  const R* kx = xdir ? S.Ky : S.Kx;
+  const R hm1 = Hm[pos - s], hp1 = Hm[pos + s], hm2 = Hm[pos - 2 * s], hp2 = Hm[pos + 2 * s];
+  const R fm = FS[pos - s], fp = FS[pos + s];
+  R p = 0, q = 0;
   if ((hm1 > H_TINH) && (hp2 > H_TINH)) p = (fp - fs);
   if ((hm2 > H_TINH) && (hp1 > H_TINH)) q = (fs - fm);
   p = (rH * (xdir ? c.r_dYbp : c.r_dXbp)) * (hx[pos] * kx[pos] * p - hx[pos - s] * kx[pos - s] * q);
   if ((hm2 > H_TINH) && (hp2 > H_TINH)) {
     q = (fp - fm) * (xdir ? c.r_dY2 : c.r_dX2);
-    q = (vx[pos] + vx[pos - s]) * 0.5 * q * gamav;
+    q = (vx[pos] + vx[pos - s]) * R(0.5) * q * gamav;
   } else {
     q = 0;
   }

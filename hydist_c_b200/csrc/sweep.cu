@@ -21,16 +21,17 @@ int line_chunks(int ncells, int min_cells) {
   return P;
 }
 
-template <int DIR>
+template <int DIR, class R>
 struct HydroGen {
+  using Real = R;
   static constexpr int UPC = 2;
   // x sweeps (columns, 4 adjacent per warp) run faster with two CTAs per SM
   // despite the register cap; y sweeps (rows) slower
   static constexpr int MIN_BLOCKS = DIR == 0 ? 2 : 1;
-  State S;
-  Coef c;
-  double* scratch;
-  double f4;
+  StateT<R> S;
+  CoefT<R> c;
+  R* scratch;
+  R f4;
 
   __device__ int lines() const { return DIR == 0 ? S.M - 1 : S.N - 1; }
   __device__ int cells_per_line() const { return DIR == 0 ? S.N - 1 : S.M - 1; }
@@ -38,10 +39,10 @@ struct HydroGen {
   __device__ int end_pos() const { return DIR == 0 ? S.N : S.M; }
   // field index of position p on line position lp
   __device__ int at(int lp, int p) const { return DIR == 0 ? p * S.W + lp : lp * S.W + p; }
-  __device__ Pre pre(int lp, int p) const {
+  __device__ PreT<R> pre(int lp, int p) const {
     return DIR == 0 ? pre_x(S, c, p, lp) : pre_y(S, c, lp, p);
   }
-  __device__ double* vel() const { return DIR == 0 ? S.tu : S.tv; }
+  __device__ R* vel() const { return DIR == 0 ? S.tu : S.tv; }
   // the VZ extraction reaches columns j <= N only (UVZSolver_multithread.cpp:851)
   __device__ bool extract_ok(int p) const { return DIR == 0 ? true : p <= S.N; }
 
@@ -95,8 +96,8 @@ struct HydroGen {
   struct Walker {
     int lp, si, pos, prev;
     bool in;
-    Pre Pc, Pn;
-    Mom Mi;
+    PreT<R> Pc, Pn;
+    MomT<R> Mi;
     __device__ void init(const HydroGen& G, const LineSeg& LS, int line, int c0) {
       lp = line + 2;
       si = 0;
@@ -117,11 +118,11 @@ struct HydroGen {
       if (pos + 1 <= d.last) Pn = G.pre(lp, pos + 1);
       else Pn = Pc;
       if (pos <= d.last - 1 || pos == d.first) Mi = abcd(Pc, Pn, pos, d.first, d.last, G.f4, d.br1, d.br2);
-      else Mi = Mom{0, 0, 0, 0};
+      else Mi = MomT<R>{0, 0, 0, 0};
       prev = pos;
     }
-    __device__ void row(const HydroGen& G, const LineSeg& LS, int e, double& A, double& B,
-                        double& C, double& D) const {
+    __device__ void row(const HydroGen& G, const LineSeg& LS, int e, R& A, R& B, R& C,
+                        R& D) const {
       const int r = 2 * pos + e;
       if (!in) {
         A = 0; B = 1; C = 0; D = 0;
@@ -134,7 +135,7 @@ struct HydroGen {
       }
       const bool even = (r & 1) == 0;
       if ((bool)d.ran == even) {
-        const Pre& P = d.ran ? Pc : Pn;
+        const PreT<R>& P = d.ran ? Pc : Pn;
         A = P.a2; B = 1; C = P.c2; D = P.d2;
       } else {
         A = Mi.a1; B = Mi.b1; C = Mi.c1; D = Mi.d1;
@@ -142,24 +143,24 @@ struct HydroGen {
       if (r == d.off) {
         if (d.ran) {
           if (d.qfirst) {
-            const double ub = DIR == 0 ? G.S.ubt[lp] : G.S.vbd[lp];
+            const R ub = DIR == 0 ? G.S.ubt[lp] : G.S.vbd[lp];
             D = Pc.d2 - Pc.a2 * ub;
           } else {
             D = Pc.d2;
           }
         } else {
-          const double TZ_l = G.S.tz[G.at(lp, d.first)];
+          const R TZ_l = R(G.S.tz[G.at(lp, d.first)]);
           D = Mi.d1 - Mi.a1 * TZ_l;
         }
         A = 0;  // the system starts here
       }
       if (r == d.rend) {
-        const Pre& PL = (pos == d.last) ? Pc : Pn;
+        const PreT<R>& PL = (pos == d.last) ? Pc : Pn;
         if (d.last_kind == 1) {
-          const double ub = DIR == 0 ? G.S.ubp[lp] : G.S.vbt[lp];
+          const R ub = DIR == 0 ? G.S.ubp[lp] : G.S.vbt[lp];
           A = PL.a2; B = 1; D = PL.d2 - PL.c2 * ub;
         } else if (d.last_kind == 2) {
-          const double TZ_r = G.S.tz[G.at(lp, d.last)];
+          const R TZ_r = R(G.S.tz[G.at(lp, d.last)]);
           A = Mi.a1; B = Mi.b1; D = Mi.d1 - Mi.c1 * TZ_r;
         } else {
           A = PL.a2; B = 1; D = PL.d2;
@@ -176,15 +177,14 @@ struct HydroGen {
       lp = line + 2;
       si = LS.nseg - 1;
     }
-    __device__ void emit(const HydroGen& G, const LineSeg& LS, double* xlast, int q,
-                         double x) {
+    __device__ void emit(const HydroGen& G, const LineSeg& LS, R* xlast, int q, R x) {
       const int r = q + 4, pos = r >> 1;
       while (si >= 0 && LS.s[si].first > pos) --si;
       if (si < 0) return;
       const SegD& d = LS.s[si];
       if (pos > d.last || r < d.off || r > d.rend) return;
       if (r == d.rend) xlast[si] = x;
-      double* vel = G.vel();
+      R* vel = G.vel();
       if (d.ran) {
         const int i = r >> 1;
         if (i < d.last && G.extract_ok(i)) {
@@ -206,10 +206,10 @@ struct HydroGen {
   };
 
   // Segment ends (_uzSolver_extract_solution :558-601 / _vzSolver_ :488-536).
-  __device__ void fixup(const LineSeg& LS, const double* xlast, int line, int s) const {
+  __device__ void fixup(const LineSeg& LS, const R* xlast, int line, int s) const {
     const SegD& d = LS.s[s];
     const int lp = line + 2, first = d.first, last = d.last;
-    double* vel = vel_ptr();
+    R* vel = vel_ptr();
     double* tz = S.tz;
     if (first < last && extract_ok(first)) {
       if (d.br1) {
@@ -217,12 +217,12 @@ struct HydroGen {
       } else if (d.xq_first && first == 2) {
         vel[at(lp, first - 1)] = DIR == 0 ? S.ubt[lp] : S.vbd[lp];
       } else {
-        const Pre Pf = pre(lp, first);
+        const PreT<R> Pf = pre(lp, first);
         vel[at(lp, first - 1)] = (Pf.d2 - tz[at(lp, first)] - Pf.c2 * vel[at(lp, first)]) / Pf.a2;
       }
     }
     if (!extract_ok(last)) return;
-    const double xl = (d.rend >= d.off) ? xlast[s] : 0.0;
+    const R xl = (d.rend >= d.off) ? xlast[s] : R(0);
     if (d.br2) {
       vel[at(lp, last)] = 0;
       tz[at(lp, last)] = xl;
@@ -230,16 +230,16 @@ struct HydroGen {
       vel[at(lp, last)] = DIR == 0 ? S.ubp[lp] : S.vbt[lp];
       tz[at(lp, last)] = xl;
     } else {
-      const Pre Pl = pre(lp, last);
+      const PreT<R> Pl = pre(lp, last);
       vel[at(lp, last)] = (Pl.d2 - Pl.a2 * vel[at(lp, last - 1)] - tz[at(lp, last)]) / Pl.c2;
     }
   }
-  __device__ double* vel_ptr() const { return DIR == 0 ? S.tu : S.tv; }
+  __device__ R* vel_ptr() const { return DIR == 0 ? S.tu : S.tv; }
 };
 
 template <class Gen, int P>
 static void launch_gen(const Gen& G, cudaStream_t st, int grid) {
-  const size_t smem = sizeof(LSShared<P>);
+  const size_t smem = sizeof(LSShared<typename Gen::Real, P>);
   static bool attr[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -259,9 +259,9 @@ static void launch_any(const Gen& G, int P, cudaStream_t st, int grid) {
   else launch_gen<Gen, 16>(G, st, grid);
 }
 
-template <int DIR>
-static void launch_dir(const State& S, const Coef& c, cudaStream_t st, int grid, int P) {
-  HydroGen<DIR> G;
+template <int DIR, class R>
+static void launch_dir(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, int grid, int P) {
+  HydroGen<DIR, R> G;
   G.S = S;
   G.c = c;
   G.scratch = S.lscratch;
@@ -274,20 +274,21 @@ static void launch_dir(const State& S, const Coef& c, cudaStream_t st, int grid,
 // wet segment of at least three cells (Scan_FSj / Scan_FSi,
 // sediment_transport.cpp:51-164, 204-313; extraction :167-201, 316-349).
 // DIR 0: columns j = 3..M-1 along i; DIR 1: rows i = 3..N-1 along j.
-template <int DIR>
+template <int DIR, class R>
 struct FSGen {
+  using Real = R;
   static constexpr int UPC = 1;
   static constexpr int MIN_BLOCKS = DIR == 0 ? 2 : 1;
-  State S;
-  Coef c;
-  double* scratch;
+  StateT<R> S;
+  CoefT<R> c;
+  R* scratch;
   double s_start;
 
   __device__ int lines() const { return DIR == 0 ? S.M - 3 : S.N - 3; }
   __device__ int cells_per_line() const { return DIR == 0 ? S.N - 1 : S.M - 1; }
   __device__ int unknowns_per_line() const { return cells_per_line(); }
   __device__ int at(int lp, int p) const { return DIR == 0 ? p * S.W + lp : lp * S.W + p; }
-  __device__ const double* vel() const { return DIR == 0 ? S.tu : S.tv; }
+  __device__ const R* vel() const { return DIR == 0 ? S.tu : S.tv; }
 
   __device__ void load_segment(LineSeg& LS, int line, int s) const {
     const bool ok = line < lines();
@@ -324,7 +325,7 @@ struct FSGen {
   }
 
   // sweep-direction diffusivity product Htd*K of cell g
-  __device__ double hk(int g) const {
+  __device__ R hk(int g) const {
     return DIR == 0 ? S.Htdu[g] * S.Kx[g] : S.Htdv[g] * S.Ky[g];
   }
 
@@ -334,8 +335,8 @@ struct FSGen {
     int lp, si, pos;
     bool in;
     double tt;             // simulated time of the sweep
-    double vel_c, hk_c;    // this cell
-    double vel_p, hk_p;    // the cell before it along the line
+    R vel_c, hk_c;         // this cell
+    R vel_p, hk_p;         // the cell before it along the line
     __device__ void init(const FSGen& G, const LineSeg& LS, int line, int c0) {
       lp = line + 3;
       si = 0;
@@ -355,8 +356,8 @@ struct FSGen {
       vel_c = G.vel()[g];
       hk_c = G.hk(g);
     }
-    __device__ void row(const FSGen& G, const LineSeg& LS, int e, double& A, double& B,
-                        double& C, double& D) const {
+    __device__ void row(const FSGen& G, const LineSeg& LS, int e, R& A, R& B, R& C,
+                        R& D) const {
       if (!in) {
         A = 0; B = 1; C = 0; D = 0;
         return;
@@ -364,7 +365,7 @@ struct FSGen {
       const SegD& d = LS.s[si];
       const int i = DIR == 0 ? pos : lp, j = DIR == 0 ? lp : pos;
       fs_cell(G.S, G.c, DIR == 0, i, j, vel_c, hk_c, vel_p, hk_p, tt, G.s_start, A, B, C, D);
-      const double* vel = G.vel();
+      const R* vel = G.vel();
       if (pos == d.first + 1) {
         // the velocity at the segment's first cell is the previous cell's
         if (d.br1 || vel_p == 0) B = B + A;
@@ -387,7 +388,7 @@ struct FSGen {
       lp = line + 3;
       si = LS.nseg - 1;
     }
-    __device__ void emit(const FSGen& G, const LineSeg& LS, double* xlast, int q, double x) {
+    __device__ void emit(const FSGen& G, const LineSeg& LS, R* xlast, int q, R x) {
       const int pos = q + 2;
       while (si >= 0 && LS.s[si].first > pos) --si;
       if (si < 0) return;
@@ -397,12 +398,12 @@ struct FSGen {
     }
   };
 
-  __device__ void fixup(const LineSeg& LS, const double* xlast, int line, int s) const {
+  __device__ void fixup(const LineSeg& LS, const R* xlast, int line, int s) const {
     const SegD& d = LS.s[s];
     if (d.rend < d.off) return;
     const int lp = line + 3;
-    const double* v = vel();
-    double* tFS = S.tFS;
+    const R* v = vel();
+    R* tFS = S.tFS;
     tFS[at(lp, d.first)] = (d.br1 || v[at(lp, d.first)] == 0) ? tFS[at(lp, d.first + 1)]
                                                                : S.FS[at(lp, d.first)];
     tFS[at(lp, d.last)] = (d.br2 || v[at(lp, d.last)] == 0) ? tFS[at(lp, d.last - 1)]
@@ -410,28 +411,38 @@ struct FSGen {
   }
 };
 
-void launch_fs_sweep(const State& S, const Coef& c, int dir, double s_start, cudaStream_t st) {
+template <class R>
+void launch_fs_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, double s_start,
+                     cudaStream_t st) {
   const int ncells = dir == 0 ? S.N - 1 : S.M - 1;
   const int lines = dir == 0 ? S.M - 3 : S.N - 3;
   if (lines <= 0) return;
   const int grid = min(cdiv(lines, LPB), S.lslots);
   const int P = line_chunks(ncells, 4);
   if (dir == 0) {
-    FSGen<0> G{S, c, S.lscratch, s_start};
+    FSGen<0, R> G{S, c, S.lscratch, s_start};
     launch_any(G, P, st, grid);
   } else {
-    FSGen<1> G{S, c, S.lscratch, s_start};
+    FSGen<1, R> G{S, c, S.lscratch, s_start};
     launch_any(G, P, st, grid);
   }
 }
 
-void launch_sweep(const State& S, const Coef& c, int dir, cudaStream_t st) {
+template <class R>
+void launch_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t st) {
   const int ncells = dir == 0 ? S.N - 1 : S.M - 1;
   const int lines = dir == 0 ? S.M - 1 : S.N - 1;
   const int grid = min(cdiv(lines, LPB), S.lslots);
   const int P = line_chunks(ncells, 4);
-  if (dir == 0) launch_dir<0>(S, c, st, grid, P);
-  else launch_dir<1>(S, c, st, grid, P);
+  if (dir == 0) launch_dir<0, R>(S, c, st, grid, P);
+  else launch_dir<1, R>(S, c, st, grid, P);
 }
+
+template void launch_sweep<double>(const StateT<double>&, const CoefT<double>&, int, cudaStream_t);
+template void launch_sweep<float>(const StateT<float>&, const CoefT<float>&, int, cudaStream_t);
+template void launch_fs_sweep<double>(const StateT<double>&, const CoefT<double>&, int, double,
+                                      cudaStream_t);
+template void launch_fs_sweep<float>(const StateT<float>&, const CoefT<float>&, int, double,
+                                     cudaStream_t);
 
 }  // namespace hyd

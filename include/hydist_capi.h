@@ -76,8 +76,11 @@ enum HydistField {
 /* Precision of the time step. */
 enum HydistPrecision {
   HYDIST_FP64 = 0,       /* plain FP64 form: reproduces the reference       */
-  HYDIST_FP32_REFINE = 1 /* FP32 bulk, FP64 z/bed state + FP64 refinement
-                            (not implemented yet: hydist_create refuses it) */
+  HYDIST_FP32_REFINE = 1 /* FP32 fields, assembly and solves; FP64 water
+                            level, bed, series and mass accumulation (the
+                            FP64-residual refinement pass of the line
+                            solves is not in yet); FP64 only for
+                            hydist_create_external */
 };
 
 /* Physical and numerical constants: the inputs of Load_coeffs
