@@ -2,7 +2,7 @@
 """Benchmark of the Hydist ADI time step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64|fp32] [--workload sediment-2048x1024|channel-256x128]
+                    [--precision fp64|fp32|fp32-refine] [--workload sediment-2048x1024|channel-256x128]
 
 A step is one full ADI step (two half-steps, with the concentration sweeps)
 of the 2048x1024 sediment workload: dx=dy=5 m, dt=2 s, seeded synthetic
@@ -536,7 +536,7 @@ def run_ours(args):
     rank, local, ws = R.init("nccl")
     dev = local
     torch.cuda.set_device(dev)
-    prec = H.FP64 if args.precision == "fp64" else H.FP32_REFINE
+    prec = {"fp64": H.FP64, "fp32": H.FP32, "fp32-refine": H.FP32_REFINE}[args.precision]
     bundle, spin = workload(args.workload, rank)
     if args.sed0 and bundle["options"]["sediment_start"] < 1e11:
         # sediment sweeps from the first step: the same per-step work without
@@ -598,9 +598,10 @@ def run_ours(args):
     # the four line solvers as the top kernels)
     dom = max(sweeps, key=sweeps.get)
     dom_cells = sweep_cells(dom, N, M)
-    alg_bytes = SWEEP_BYTES_PER_CELL[args.precision][dom] * dom_cells
+    pkey = "fp64" if args.precision == "fp64" else "fp32"
+    alg_bytes = SWEEP_BYTES_PER_CELL[pkey][dom] * dom_cells
     ach = alg_bytes / (sweeps[dom] * 1e-3) / 1e9
-    step_bytes = BYTES_PER_CELL_STEP[(args.precision, sed)] * cells
+    step_bytes = BYTES_PER_CELL_STEP[(pkey, sed)] * cells
     step_ms = ms / args.steps
     roof = {"bound": "hbm", "kernel": dom, "kernel_ms": round(sweeps[dom], 4),
             "bytes_per_launch": alg_bytes, "achieved": ach, "peak": hbm, "unit": "GB/s",
@@ -613,7 +614,7 @@ def run_ours(args):
         try:
             tj = json.loads(traffic_file.read_text())
             roof["traffic"] = tj.get(args.workload if args.precision == "fp64"
-                                     else args.workload + "-fp32", {}).get(dom)
+                                     else args.workload + "-" + args.precision, {}).get(dom)
         except Exception:
             pass
     e2e = measure_e2e(H, bundle, dev, prec, args) if rank == 0 and not args.no_e2e else None
@@ -631,7 +632,8 @@ def run_ours(args):
             "metric": "ADI cell-steps/s", "value": value, "unit": "cell-steps/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64-refine",
+            "vs_baseline": None, "dtype": {"fp64": "f64", "fp32": "f32 (f64 z, bed, mass)",
+                      "fp32-refine": "f32 + f64-residual refinement (f64 z, bed, mass)"}[args.precision],
             "data": "synthetic (seeded bathymetry, Manning, boundaries)",
             "config": {"workload": args.workload, "N": bundle["meta"]["N"],
                        "M": bundle["meta"]["M"], "cells": cells, "dx": 5.0, "dt": 2.0,
@@ -700,7 +702,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "fp32-refine"])
     ap.add_argument("--workload", default="sediment-2048x1024",
                     help="sediment-2048x1024 | channel-256x128 | " + TRIDIAG + " | " + ENSEMBLE +
                          " | " + SERVING)

@@ -23,9 +23,9 @@ import ctypes as C
 import numpy as np
 
 from . import capi, scenario
-from .capi import FIELDS, FP32_REFINE, FP64, HydistError
+from .capi import FIELDS, FP32, FP32_REFINE, FP64, HydistError
 
-__all__ = ["Simulation", "Ensemble", "Server", "gtsv_batched", "HydistError", "scenario", "FP64", "FP32_REFINE",
+__all__ = ["Simulation", "Ensemble", "Server", "gtsv_batched", "HydistError", "scenario", "FP64", "FP32", "FP32_REFINE",
            "FIELDS", "library"]
 
 

@@ -29,6 +29,7 @@ FIELDS = {
 
 FP64 = 0
 FP32_REFINE = 1
+FP32 = 2
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)

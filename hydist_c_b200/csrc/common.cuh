@@ -57,6 +57,7 @@ struct StateT {
   int bienQ[4];
   int ketdinh;
   int race_new;    // extraction at an open last end reads the new neighbour
+  int refine;      // line solves refined once with an FP64 residual
   // static fields
   const double *h, *hsnham, *htaiz, *htaiz_bd;
   const R *visco, *Fw, *Kx1, *Ky1, *Tsxw, *Tsyw;

@@ -360,7 +360,8 @@ namespace {
 
 int check_params(const HydistParams* p, const HydistOptions* o) {
   if (!(p->dX > 0 && p->dY > 0 && p->dT > 0)) return fail(HYDIST_ERR_ARG, "dX, dY, dT must be > 0");
-  if (o->precision != HYDIST_FP64 && o->precision != HYDIST_FP32_REFINE)
+  if (o->precision != HYDIST_FP64 && o->precision != HYDIST_FP32_REFINE &&
+      o->precision != HYDIST_FP32)
     return fail(HYDIST_ERR_ARG, "unknown precision");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -378,7 +379,7 @@ int new_handle(const HydistParams* p, const HydistOptions* o, int device, int M,
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   derive(*p, h->c);
-  h->fp32 = o->precision == HYDIST_FP32_REFINE;
+  h->fp32 = o->precision == HYDIST_FP32_REFINE || o->precision == HYDIST_FP32;
   h->cf = CoefT<float>::from(h->c);
   h->o = *o;
   h->t = o->t_start;
@@ -391,6 +392,7 @@ int new_handle(const HydistParams* p, const HydistOptions* o, int device, int M,
   for (int k = 0; k < 4; ++k) S.bienQ[k] = bienQ[k] ? 1 : 0;
   S.ketdinh = o->ketdinh ? 1 : 0;
   S.race_new = 1;
+  S.refine = o->precision == HYDIST_FP32_REFINE ? 1 : 0;
   return HYDIST_OK;
 }
 
@@ -410,8 +412,10 @@ int bulk_private(HydistHandle* h, StateT<R>& B) {
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
   B.lslots = 2 * nsm;
   const size_t U = (size_t)2 * std::max(S.M, S.N);
-  // at least 4 (max(M,N)+3) doubles: preprocess_data borrows it as FP64
-  TRY(dalloc(h, &B.lscratch, std::max((size_t)B.lslots * 3 * U * 4, 8 * U + 64)));
+  // at least 4 (max(M,N)+3) doubles: preprocess_data borrows it as FP64;
+  // the FP32 form keeps 7 values per unknown (its refinement stores the rows)
+  const size_t arrays = S.refine ? 7 : 3;
+  TRY(dalloc(h, &B.lscratch, std::max((size_t)B.lslots * arrays * U * 4, 8 * U + 64)));
   return HYDIST_OK;
 }
 
@@ -488,6 +492,7 @@ void mirror_common(HydistHandle* h) {
   for (int k = 0; k < 4; ++k) F.bienQ[k] = S.bienQ[k];
   F.ketdinh = S.ketdinh;
   F.race_new = S.race_new;
+  F.refine = S.refine;
   F.h = S.h;
   F.hsnham = S.hsnham;
   F.htaiz = S.htaiz;

@@ -53,7 +53,7 @@ struct LSShared {
   R tri[6][P * LPB];   // yF vF wF yL vL wL per chunk
   R red[4][P * LPB];   // reduced system during PCR
   R xsep[P * LPB];     // separator solutions
-  R xlast[LPB][SEG];   // solution at each segment's last row
+  double xlast[LPB][SEG];  // solution at each segment's last row
 };
 
 // A plain division: with FP64 it keeps the rounding of the reference's
@@ -72,10 +72,13 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
   const int l = tid % LPB, k = tid / LPB;
   const int cidx = k * LPB + l;
   const int U = G.unknowns_per_line();
-  R* scr = G.scratch + (size_t)blockIdx.x * 3 * (size_t)U * LPB;
+  // scratch slot of this CTA: c', y', v' per unknown, and with refinement
+  // also the rows A, B, C, D (Gen::SCRATCH_ARRAYS arrays of U x LPB)
+  const size_t UL = (size_t)U * LPB;
+  R* scr = G.scratch + (size_t)blockIdx.x * Gen::SCRATCH_ARRAYS * UL;
   R* sc_c = scr;
-  R* sc_y = scr + (size_t)U * LPB;
-  R* sc_v = scr + 2 * (size_t)U * LPB;
+  R* sc_y = scr + UL;
+  R* sc_v = scr + 2 * UL;
   const int ncells = G.cells_per_line();
   const int upc = Gen::UPC;
   const int ngroups = cdiv(G.lines(), LPB);
@@ -109,6 +112,13 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
         for (int e = 0; e < Gen::UPC; ++e, ++s) {
           R A, B, C, D;
           W.row(G, LS, e, A, B, C, D);
+          if constexpr (Gen::REFINE) {
+            const size_t o = (size_t)(q0 + s) * LPB + l;
+            scr[3 * UL + o] = A;
+            scr[4 * UL + o] = B;
+            scr[5 * UL + o] = C;
+            scr[6 * UL + o] = D;
+          }
           if (s == nu - 1) {
             sh.sep[0][cidx] = A;
             sh.sep[1][cidx] = B;
@@ -198,7 +208,7 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
     sh.xsep[cidx] = rd / rb;
     __syncthreads();
     // ---- pass C: back substitution and emission
-    {
+    if constexpr (!Gen::REFINE) {
       const R xr = sh.xsep[cidx];
       const R xl = (k > 0) ? sh.xsep[cidx - LPB] : R(0);
       typename Gen::Emitter E;
@@ -211,6 +221,122 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
         const R x = sc_y[o] + sc_v[o] * xl - sc_c[o] * xn;
         E.emit(G, LS, sh.xlast[l], q0 + t, x);
         xn = x;
+      }
+    } else {
+      // the first solution x goes over y'; then one refinement pass:
+      // r = D - A x_{-1} - B x - C x_{+1} in FP64 with the stored rows,
+      // A d = r with the same elimination (c', v', the reduced matrix),
+      // x + d emitted
+      R* sA = scr + 3 * UL;
+      R* sB = scr + 4 * UL;
+      R* sC = scr + 5 * UL;
+      R* sD = scr + 6 * UL;
+      {
+        const R xr = sh.xsep[cidx];
+        const R xl = (k > 0) ? sh.xsep[cidx - LPB] : R(0);
+        sc_y[(size_t)(q0 + nu - 1) * LPB + l] = xr;
+        R xn = xr;
+        for (int t = nu - 2; t >= 0; --t) {
+          const size_t o = (size_t)(q0 + t) * LPB + l;
+          const R x = sc_y[o] + sc_v[o] * xl - sc_c[o] * xn;
+          sc_y[o] = x;
+          xn = x;
+        }
+      }
+      __syncthreads();
+      // residual in FP64 (over D)
+      for (int t = 0; t < nu; ++t) {
+        const int q = q0 + t;
+        const size_t o = (size_t)q * LPB + l;
+        const double xm = q > 0 ? (double)sc_y[o - LPB] : 0.0;
+        const double xp = q + 1 < U ? (double)sc_y[o + LPB] : 0.0;
+        const double r = (double)sD[o] - (double)sA[o] * xm - (double)sB[o] * (double)sc_y[o] -
+                         (double)sC[o] * xp;
+        sD[o] = (R)r;
+      }
+      __syncthreads();
+      // forward elimination of the residual (y'' over D)
+      R fy = 0, yL = 0, Pk = 1, cp = 0;
+      for (int t = 0; t < nu - 1; ++t) {
+        const size_t o = (size_t)(q0 + t) * LPB + l;
+        const R A = sA[o], B = sB[o];
+        const R m = rcp(t == 0 ? B : B - A * cp);
+        const R y = (sD[o] - (t == 0 ? R(0) : A * yL)) * m;
+        sD[o] = y;
+        cp = sc_c[o];
+        fy += Pk * y;
+        Pk *= -cp;
+        yL = y;
+      }
+      sh.tri[0][cidx] = fy;
+      sh.tri[3][cidx] = yL;
+      __syncthreads();
+      R ra2, rb2, rc2, rd2;
+      {
+        const R as = sh.sep[0][cidx], bs = sh.sep[1][cidx], cs = sh.sep[2][cidx];
+        const R ds = sD[(size_t)(q0 + nu - 1) * LPB + l];
+        const R vL = sh.tri[4][cidx], wL = sh.tri[5][cidx];
+        R yF = 0, vF = 0, wF = 0;
+        if (k + 1 < P) {
+          const int n1 = cidx + LPB;
+          yF = sh.tri[0][n1];
+          vF = sh.tri[1][n1];
+          wF = sh.tri[2][n1];
+        }
+        ra2 = as * vL;
+        rb2 = bs + as * wL + cs * vF;
+        rc2 = cs * wF;
+        rd2 = ds - as * yL - cs * yF;
+      }
+      for (int st = 1; st < P; st <<= 1) {
+        sh.red[0][cidx] = ra2;
+        sh.red[1][cidx] = rb2;
+        sh.red[2][cidx] = rc2;
+        sh.red[3][cidx] = rd2;
+        __syncthreads();
+        R am = 0, bm = 1, cm = 0, dm = 0, an = 0, bn = 1, cn = 0, dn = 0;
+        if (k - st >= 0) {
+          const int o = cidx - st * LPB;
+          am = sh.red[0][o];
+          bm = sh.red[1][o];
+          cm = sh.red[2][o];
+          dm = sh.red[3][o];
+        }
+        if (k + st < P) {
+          const int o = cidx + st * LPB;
+          an = sh.red[0][o];
+          bn = sh.red[1][o];
+          cn = sh.red[2][o];
+          dn = sh.red[3][o];
+        }
+        __syncthreads();
+        const R k1 = ra2 / bm, k2 = rc2 / bn;
+        const R na = -am * k1, nc = -cn * k2;
+        const R nb = rb2 - cm * k1 - an * k2;
+        const R nd = rd2 - dm * k1 - dn * k2;
+        ra2 = na;
+        rb2 = nb;
+        rc2 = nc;
+        rd2 = nd;
+      }
+      sh.xsep[cidx] = rd2 / rb2;
+      __syncthreads();
+      {
+        const R dr = sh.xsep[cidx];
+        const R dl = (k > 0) ? sh.xsep[cidx - LPB] : R(0);
+        typename Gen::Emitter E;
+        E.init(G, LS, line);
+        {
+          const size_t o = (size_t)(q0 + nu - 1) * LPB + l;
+          E.emit(G, LS, sh.xlast[l], q0 + nu - 1, (double)sc_y[o] + (double)dr);
+        }
+        R dn = dr;
+        for (int t = nu - 2; t >= 0; --t) {
+          const size_t o = (size_t)(q0 + t) * LPB + l;
+          const R d = sD[o] + sc_v[o] * dl - sc_c[o] * dn;
+          E.emit(G, LS, sh.xlast[l], q0 + t, (double)sc_y[o] + (double)d);
+          dn = d;
+        }
       }
     }
     __syncthreads();

@@ -21,9 +21,12 @@ int line_chunks(int ncells, int min_cells) {
   return P;
 }
 
-template <int DIR, class R>
+// REF: refine each line solve once with an FP64 residual (FP32 forms)
+template <int DIR, class R, bool REF = false>
 struct HydroGen {
   using Real = R;
+  static constexpr bool REFINE = REF;
+  static constexpr int SCRATCH_ARRAYS = REFINE ? 7 : 3;
   static constexpr int UPC = 2;
   // x sweeps (columns, 4 adjacent per warp) run faster with two CTAs per SM
   // despite the register cap; y sweeps (rows) slower
@@ -177,7 +180,7 @@ struct HydroGen {
       lp = line + 2;
       si = LS.nseg - 1;
     }
-    __device__ void emit(const HydroGen& G, const LineSeg& LS, R* xlast, int q, R x) {
+    __device__ void emit(const HydroGen& G, const LineSeg& LS, double* xlast, int q, double x) {
       const int r = q + 4, pos = r >> 1;
       while (si >= 0 && LS.s[si].first > pos) --si;
       if (si < 0) return;
@@ -206,7 +209,7 @@ struct HydroGen {
   };
 
   // Segment ends (_uzSolver_extract_solution :558-601 / _vzSolver_ :488-536).
-  __device__ void fixup(const LineSeg& LS, const R* xlast, int line, int s) const {
+  __device__ void fixup(const LineSeg& LS, const double* xlast, int line, int s) const {
     const SegD& d = LS.s[s];
     const int lp = line + 2, first = d.first, last = d.last;
     R* vel = vel_ptr();
@@ -222,7 +225,7 @@ struct HydroGen {
       }
     }
     if (!extract_ok(last)) return;
-    const R xl = (d.rend >= d.off) ? xlast[s] : R(0);
+    const double xl = (d.rend >= d.off) ? xlast[s] : 0.0;
     if (d.br2) {
       vel[at(lp, last)] = 0;
       tz[at(lp, last)] = xl;
@@ -259,9 +262,9 @@ static void launch_any(const Gen& G, int P, cudaStream_t st, int grid) {
   else launch_gen<Gen, 16>(G, st, grid);
 }
 
-template <int DIR, class R>
+template <int DIR, class R, bool REF>
 static void launch_dir(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, int grid, int P) {
-  HydroGen<DIR, R> G;
+  HydroGen<DIR, R, REF> G;
   G.S = S;
   G.c = c;
   G.scratch = S.lscratch;
@@ -274,9 +277,11 @@ static void launch_dir(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, i
 // wet segment of at least three cells (Scan_FSj / Scan_FSi,
 // sediment_transport.cpp:51-164, 204-313; extraction :167-201, 316-349).
 // DIR 0: columns j = 3..M-1 along i; DIR 1: rows i = 3..N-1 along j.
-template <int DIR, class R>
+template <int DIR, class R, bool REF = false>
 struct FSGen {
   using Real = R;
+  static constexpr bool REFINE = REF;
+  static constexpr int SCRATCH_ARRAYS = REFINE ? 7 : 3;
   static constexpr int UPC = 1;
   static constexpr int MIN_BLOCKS = DIR == 0 ? 2 : 1;
   StateT<R> S;
@@ -388,7 +393,7 @@ struct FSGen {
       lp = line + 3;
       si = LS.nseg - 1;
     }
-    __device__ void emit(const FSGen& G, const LineSeg& LS, R* xlast, int q, R x) {
+    __device__ void emit(const FSGen& G, const LineSeg& LS, double* xlast, int q, double x) {
       const int pos = q + 2;
       while (si >= 0 && LS.s[si].first > pos) --si;
       if (si < 0) return;
@@ -398,7 +403,7 @@ struct FSGen {
     }
   };
 
-  __device__ void fixup(const LineSeg& LS, const R* xlast, int line, int s) const {
+  __device__ void fixup(const LineSeg& LS, const double* xlast, int line, int s) const {
     const SegD& d = LS.s[s];
     if (d.rend < d.off) return;
     const int lp = line + 3;
@@ -420,11 +425,21 @@ void launch_fs_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, double s_st
   const int grid = min(cdiv(lines, LPB), S.lslots);
   const int P = line_chunks(ncells, 4);
   if (dir == 0) {
-    FSGen<0, R> G{S, c, S.lscratch, s_start};
-    launch_any(G, P, st, grid);
+    if (S.refine) {
+      FSGen<0, R, true> G{S, c, S.lscratch, s_start};
+      launch_any(G, P, st, grid);
+    } else {
+      FSGen<0, R, false> G{S, c, S.lscratch, s_start};
+      launch_any(G, P, st, grid);
+    }
   } else {
-    FSGen<1, R> G{S, c, S.lscratch, s_start};
-    launch_any(G, P, st, grid);
+    if (S.refine) {
+      FSGen<1, R, true> G{S, c, S.lscratch, s_start};
+      launch_any(G, P, st, grid);
+    } else {
+      FSGen<1, R, false> G{S, c, S.lscratch, s_start};
+      launch_any(G, P, st, grid);
+    }
   }
 }
 
@@ -434,8 +449,13 @@ void launch_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t s
   const int lines = dir == 0 ? S.M - 1 : S.N - 1;
   const int grid = min(cdiv(lines, LPB), S.lslots);
   const int P = line_chunks(ncells, 4);
-  if (dir == 0) launch_dir<0, R>(S, c, st, grid, P);
-  else launch_dir<1, R>(S, c, st, grid, P);
+  if (S.refine) {
+    if (dir == 0) launch_dir<0, R, true>(S, c, st, grid, P);
+    else launch_dir<1, R, true>(S, c, st, grid, P);
+  } else {
+    if (dir == 0) launch_dir<0, R, false>(S, c, st, grid, P);
+    else launch_dir<1, R, false>(S, c, st, grid, P);
+  }
 }
 
 template void launch_sweep<double>(const StateT<double>&, const CoefT<double>&, int, cudaStream_t);

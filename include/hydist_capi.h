@@ -76,11 +76,12 @@ enum HydistField {
 /* Precision of the time step. */
 enum HydistPrecision {
   HYDIST_FP64 = 0,       /* plain FP64 form: reproduces the reference       */
-  HYDIST_FP32_REFINE = 1 /* FP32 fields, assembly and solves; FP64 water
-                            level, bed, series and mass accumulation (the
-                            FP64-residual refinement pass of the line
-                            solves is not in yet); FP64 only for
-                            hydist_create_external */
+  HYDIST_FP32_REFINE = 1, /* FP32 fields, assembly and solves, each line
+                             solve refined once with a residual computed in
+                             FP64; FP64 water level, bed, series and mass
+                             accumulation                                  */
+  HYDIST_FP32 = 2         /* the same without the refinement pass          */
+  /* hydist_create_external takes HYDIST_FP64 only */
 };
 
 /* Physical and numerical constants: the inputs of Load_coeffs

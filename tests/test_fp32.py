@@ -1,5 +1,5 @@
-"""The FP32 form (HYDIST_FP32_REFINE): FP32 fields, assembly and solves, FP64
-water level, bed and mass. After one simulated hour of the 256x128 channel it
+"""The FP32 forms (HYDIST_FP32_REFINE, and HYDIST_FP32 without the refinement
+pass): FP32 fields, assembly and solves, FP64 water level, bed and mass. After one simulated hour of the 256x128 channel it
 must stay within the stated tolerances of the FP64 form (which is itself
 pinned to the oracle within 1e-6 over the same hour): max |dz| <= 1e-4 m,
 relative difference of the water volume <= 1e-6, relative L2 of u and v
@@ -16,10 +16,11 @@ def _rel_l2(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-def test_fp32_one_hour_channel(hyd):
+@pytest.mark.parametrize("form", ["FP32_REFINE", "FP32"])
+def test_fp32_one_hour_channel(hyd, form):
     b = S.config0()
     s64 = hyd.Simulation(b, precision=hyd.FP64)
-    s32 = hyd.Simulation(b, precision=hyd.FP32_REFINE)
+    s32 = hyd.Simulation(b, precision=getattr(hyd, form))
     s64.step(1800)
     s32.step(1800)
     z64, z32 = s64.download("z"), s32.download("z")
@@ -34,11 +35,12 @@ def test_fp32_one_hour_channel(hyd):
     s32.close()
 
 
-def test_fp32_sediment(hyd):
+@pytest.mark.parametrize("form", ["FP32_REFINE", "FP32"])
+def test_fp32_sediment(hyd, form):
     b = S.make_channel(N=128, M=64, seed=20260500, dx=10.0, dt=2.0, hours=1.0, sediment=True,
                        sediment_start=20.0)
     s64 = hyd.Simulation(b, precision=hyd.FP64)
-    s32 = hyd.Simulation(b, precision=hyd.FP32_REFINE)
+    s32 = hyd.Simulation(b, precision=getattr(hyd, form))
     s64.step(300)
     s32.step(300)
     assert _rel_l2(s32.download("FS"), s64.download("FS")) <= 1e-3
