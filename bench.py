@@ -183,7 +183,8 @@ def run_ensemble(args):
     nmem = 64
     bundles = [S.config3_member(k, seed=replica_seed(20263000, rank)) for k in range(nmem)]
     cells = sum(b["meta"]["cells"] for b in bundles)
-    sims = [H.Simulation(b, device=dev.index) for b in bundles]
+    prec = {"fp64": H.FP64, "fp32": H.FP32, "fp32-refine": H.FP32_REFINE}[args.precision]
+    sims = [H.Simulation(b, device=dev.index, precision=prec) for b in bundles]
     ens = H.Ensemble(sims)
     spin = int(round(300.0 / 2.0))  # to t = 300 s, where the sediment sweeps start
     ens.step(spin)
@@ -209,7 +210,7 @@ def run_ensemble(args):
     launches = sims[0].kernel_launches - l0
     value = ws * cells * args.steps / (ms_max * 1e-3)
     hbm, peak_kind = _peaks()
-    step_bytes = BYTES_PER_CELL_STEP[("fp64", True)] * cells
+    step_bytes = BYTES_PER_CELL_STEP[("fp64" if args.precision == "fp64" else "fp32", True)] * cells
     ach = step_bytes / (ms / args.steps * 1e-3) / 1e9
     mass = [m.mass() for m in sims[:4]]
     ens.close()
@@ -237,7 +238,7 @@ def run_ensemble(args):
                                options=dict(b["options"], sediment_start=0.0, bed_change_start=0.0)))
         torch.cuda.synchronize(dev)
         t0 = _t.perf_counter()
-        ms2 = [H.Simulation(b, device=dev.index) for b in pinned]
+        ms2 = [H.Simulation(b, device=dev.index, precision=prec) for b in pinned]
         en2 = H.Ensemble(ms2)
         for _ in range(args.steps):
             en2.step(1)
@@ -259,8 +260,11 @@ def run_ensemble(args):
             "metric": "ADI cell-steps/s", "value": value, "unit": "cell-steps/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded per member)",
+            "vs_baseline": None, "dtype": {"fp64": "f64", "fp32": "f32 (f64 z, bed, mass)",
+                                            "fp32-refine": "f32 + f64-residual refinement"}[args.precision],
+            "data": "synthetic (seeded per member)",
             "config": {"workload": ENSEMBLE, "members": nmem, "N": 1024, "M": 512, "cells": cells,
+                       "precision": args.precision,
                        "sediment": True, "cuda_graph": "one graph launch per step for all members",
                        "l2": "inputs larger than L2", "parallelism": f"replicas x{ws}"},
             "p50_step_ms": float(np.percentile(per, 50)), "p99_step_ms": float(np.percentile(per, 99)),

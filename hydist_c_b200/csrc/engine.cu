@@ -1057,7 +1057,7 @@ int hydist_checkpoint_load(HydistHandle* h, const char* path) {
        cudaMemcpy(h->S.khouot, mask.data(), n * 4, cudaMemcpyHostToDevice) == cudaSuccess;
   std::fclose(f);
   if (!ok) return fail(HYDIST_ERR_ARG, std::string("truncated or unreadable checkpoint: ") + path);
-  launch_scan_segments(h->S, h->stream);
+  on_state(h, [&](auto& St, auto& Cf) { launch_scan_segments(St, Cf, false, h->stream); });
   CK(cudaGetLastError());
   h->t = hd.t;
   TRY(set_device_clock(h));
@@ -1092,7 +1092,7 @@ int hydist_upload(HydistHandle* h, int32_t field, const void* host) {
   const size_t n = (size_t)h->S.W * h->S.H;
   if (field == HYDIST_FIELD_KHOUOT) {
     CK(cudaMemcpyAsync(h->S.khouot, host, n * 4, cudaMemcpyHostToDevice, h->stream));
-    launch_scan_segments(h->S, h->stream);
+    on_state(h, [&](auto& St, auto& Cf) { launch_scan_segments(St, Cf, false, h->stream); });
     CK(cudaGetLastError());
   } else {
     const FieldRef r = field_ref(h, field);

@@ -15,7 +15,7 @@
 //   k_solve_v/k_solve_u [solveV/vSolver, solveU/uSolver, :607-795, 938-978]
 //   k_margin_v/k_margin_u [update_margin_elem_V/U, :980-1060]
 //   k_commit_a          [update_h_moi + update_uvz + Htuongdoi, :71-86, 732-759, 346-362]
-//   k_hmoi_flags, k_wetting, k_commit_b, k_dry_mask
+//   k_smooth_full (with H_moi), k_wetting, k_commit_b, k_runs_flags (drying)
 //                       [update_h_moi + Reset_states_vertical + update_uvz +
 //                        Htuongdoi, support_funcs.cpp:71-86, 142-188, 732-759]
 //
@@ -129,19 +129,38 @@ __device__ __forceinline__ void run_flags(bool wm1, bool w, bool wp1, bool wm2_l
   end = w && (p == lim || !wp1) && ok;
 }
 
+// With dry != 0 the drying pass of Reset_states_vertical
+// (support_funcs.cpp:177-186) is applied on the fly: a wet cell of rows
+// 2..N, columns 1..M whose depth is at most H_TINH reads as dried (1) and
+// is written so. Reading a neighbour's mask while its thread writes it is
+// safe: the write turns 0 into 1 exactly when this test gives 1.
 template <class R>
-__global__ void k_runs_flags(StateT<R> S, int* seg_cnt) {
+__global__ void k_runs_flags(StateT<R> S, CoefT<R> c, int* seg_cnt, int dry) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int i = blockIdx.y + 2;
   if (i > S.N || j > S.M) return;
   const int W = S.W, H = S.H, g = i * W + j;
-  const int* K = S.khouot;
-  const bool w = K[g] == 0;
+  int* K = S.khouot;
+  auto mask = [&](int q, int qi, int qj) -> int {
+    const int k = K[q];
+    if (dry && k == 0 && qi >= 2 && qi <= S.N && qj >= 1 && qj <= S.M && S.Hmoi[q] <= c.H_TINH)
+      return 1;
+    return k;
+  };
+  if (dry) {
+    const int k0 = mask(g, i, j);
+    if (k0 != K[g]) K[g] = k0;
+    if (j == 2) {  // column 1 is outside this grid
+      const int k1 = mask(g - 1, i, 1);
+      if (k1 != K[g - 1]) K[g - 1] = k1;
+    }
+  }
+  const bool w = mask(g, i, j) == 0;
   if (!w) return;
   // row i, position j, lim M
   {
-    const bool wm1 = K[g - 1] == 0, wp1 = K[g + 1] == 0;
-    const bool wm2 = K[g - 2] == 0;
+    const bool wm1 = mask(g - 1, i, j - 1) == 0, wp1 = mask(g + 1, i, j + 1) == 0;
+    const bool wm2 = mask(g - 2, i, j - 2) == 0;
     bool st, en;
     run_flags(wm1, w, wp1, wm2, j, S.M, st, en);
     if (st) {
@@ -155,8 +174,8 @@ __global__ void k_runs_flags(StateT<R> S, int* seg_cnt) {
   }
   // column j, position i, lim N
   {
-    const bool wm1 = K[g - W] == 0, wp1 = K[g + W] == 0;
-    const bool wm2 = K[g - 2 * W] == 0;
+    const bool wm1 = mask(g - W, i - 1, j) == 0, wp1 = mask(g + W, i + 1, j) == 0;
+    const bool wm2 = mask(g - 2 * W, i - 2, j) == 0;
     bool st, en;
     run_flags(wm1, w, wp1, wm2, i, S.N, st, en);
     if (st) {
@@ -354,12 +373,20 @@ __global__ void k_boundary(StateT<R> S) {
 // interior [2,N]x[2,M], the unsmoothed value elsewhere, i.e. t_u / t_v as
 // they stand after update_buffer. Readers of the smoothed velocity use it
 // directly and the half-step commit writes it back to t_u / t_v, u / v.
+// hmoi != 0 (the last smoothing of half-step B) also does update_h_moi and
+// the column flags of the wetting pass (k_hmoi_flags' work, after the explicit
+// u update that reads H_moi).
 template <class R>
-__global__ void k_smooth_full(StateT<R> S, CoefT<R> c, int isU) {
+__global__ void k_smooth_full(StateT<R> S, CoefT<R> c, int isU, int hmoi) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   if (i >= S.H || j >= S.W) return;
   const int W = S.W, g = i * W + j;
+  if (hmoi && i >= 1 && i <= S.N + 1 && j >= 1 && j <= S.M) {
+    const int kh = S.khouot[g];
+    if (i <= S.N && kh == 0) S.Hmoi[g] = S.htaiz[g] + S.tz[g];
+    if (kh == 1) S.colflag[j] = 1;
+  }
   const R* val = isU ? S.tu : S.tv;
   R* out_arr = isU ? S.su : S.sv;
   const R vg = val[g];
@@ -578,20 +605,6 @@ __global__ void k_commit_a(StateT<R> S, CoefT<R> c) {
   }
 }
 
-// Half-step B, before the wetting pass: update_h_moi, and a per-column flag
-// telling whether the column holds a cell dried during the run (khouot 1),
-// the only cells the wetting loop of Reset_states_vertical can change.
-template <class R>
-__global__ void k_hmoi_flags(StateT<R> S, int* colflag) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int i = blockIdx.y + 1;
-  if (i > S.N + 1 || j > S.M) return;
-  const int g = i * S.W + j;
-  const int kh = S.khouot[g];
-  if (i <= S.N && kh == 0) S.Hmoi[g] = S.htaiz[g] + S.tz[g];
-  if (kh == 1) colflag[j] = 1;
-}
-
 // The wetting loop of Reset_states_vertical (support_funcs.cpp:160-175),
 // sequential along i, on flagged columns only.
 template <class R>
@@ -646,7 +659,7 @@ __global__ void k_commit_b(StateT<R> S, CoefT<R> c) {
   if (d0 || dright) tv = 0;
   S.tu[g] = tu;
   S.tv[g] = tv;
-  if (d0) S.FS[g] = 0;  // khouot is set by k_dry_mask after this pass
+  if (d0) S.FS[g] = 0;  // khouot is set by the segment scan after this pass
   const double tz = S.tz[g];
   S.z[g] = tz;
   S.u[g] = tu * (1 - c.kenhhepd);
@@ -661,22 +674,13 @@ __global__ void k_commit_b(StateT<R> S, CoefT<R> c) {
 
 // The drying cells' mask (khouot = 1), written after k_commit_b has read
 // every neighbour's test.
-template <class R>
-__global__ void k_dry_mask(StateT<R> S, CoefT<R> c) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int i = blockIdx.y + 2;
-  if (i > S.N || j > S.M) return;
-  const int g = i * S.W + j;
-  if (S.khouot[g] == 0 && S.Hmoi[g] <= c.H_TINH) S.khouot[g] = 1;
-}
-
 // ------------------------------------------------------------- launchers
 static inline dim3 grid2(int nx, int ny, int bx) { return dim3(cdiv(nx, bx), ny); }
 
 template <class R>
 void launch_init(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
   k_onetime_init<<<dim3(cdiv(S.W, 128), S.H), 128, 0, st>>>(S, c);
-  launch_find_limits(S, c, st, nullptr);
+  launch_find_limits(S, c, false, st, nullptr);
   k_htuongdoi<<<grid2(S.M, S.N, 128), 128, 0, st>>>(S);
   // the per-side scratch of the powers: the line-solver scratch is free here
   k_preprocess_sides<<<4, 256, 0, st>>>(S, c, reinterpret_cast<double*>(S.lscratch));
@@ -693,16 +697,17 @@ void launch_boundary(const StateT<R>& S, cudaStream_t st) {
 }
 
 template <class R>
-void launch_scan_segments(const StateT<R>& S, cudaStream_t st) {
-  k_runs_flags<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, S.segcnt);
+void launch_scan_segments(const StateT<R>& S, const CoefT<R>& c, bool dry, cudaStream_t st) {
+  k_runs_flags<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, S.segcnt, dry ? 1 : 0);
   k_runs_sort<<<cdiv(S.N + S.M - 2, 128), 128, 0, st>>>(S, S.segcnt);
 }
 
 template <class R>
-void launch_find_limits(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace* tr) {
+void launch_find_limits(const StateT<R>& S, const CoefT<R>& c, bool dry, cudaStream_t st,
+                        Trace* tr) {
   k_interp_fs_rows<<<dim3(cdiv(S.M, 128), 2), 128, 0, st>>>(S, c);
   k_interp_fs_col<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
-  launch_scan_segments(S, st);
+  launch_scan_segments(S, c, dry, st);
   if (tr) tr->launches += 4;
 }
 
@@ -718,10 +723,10 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace
   // smoothing of t_u into su, explicit v from it, margins, smoothing of t_v
   // into sv; k_commit_a writes both back (Normalize/update_buffer pairs,
   // engine.cpp:109-124)
-  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 1);
+  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 1, 0);
   k_solve_v<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c);
   k_margin_v<<<cdiv(S.N - 1, 128), 128, 0, st>>>(S, c);
-  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 0);
+  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 0, 0);
   if (tr) tr->mark(st, PH_EXPLICIT_V, 4);
   // update_h_moi + update_uvz + Htuongdoi; the wet/dry mask does not change
   // in this half-step, so the segment tables are not rescanned, only the
@@ -741,27 +746,28 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace
   launch_sweep(S, c, 1, st);
   if (tr) tr->kend(st, KS_SWEEP_Y);
   if (tr) tr->mark(st, PH_SWEEP_Y, 1);
-  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 0);
+  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 0, 0);
   k_solve_u<<<grid2(S.M - 1, S.N, 128), 128, 0, st>>>(S, c);
   k_margin_u<<<cdiv(S.M - 1, 128), 128, 0, st>>>(S, c);
-  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 1);
+  // with update_h_moi and the wetting pass's column flags
+  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 1, 1);
   if (tr) tr->mark(st, PH_EXPLICIT_U, 4);
   // update_h_moi, Reset_states_vertical (wetting on flagged columns, drying
   // per cell), update_uvz, Htuongdoi, then the segment tables
-  k_hmoi_flags<<<grid2(S.M, S.N + 1, 128), 128, 0, st>>>(S, S.colflag);
   k_wetting<<<cdiv(S.M, 128), 128, 0, st>>>(S, c, S.colflag);
   k_commit_b<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c);
-  k_dry_mask<<<grid2(S.M, S.N - 1, 128), 128, 0, st>>>(S, c);
-  launch_find_limits(S, c, st, tr);
-  if (tr) tr->mark(st, PH_COMMIT_Y, 4);
+  // the drying mask is written by the segment scan (k_runs_flags, dry)
+  launch_find_limits(S, c, true, st, tr);
+  if (tr) tr->mark(st, PH_COMMIT_Y, 2);
 }
 
 #define HYD_HYDRO_INST(R)                                                                  \
   template void launch_init<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t);         \
   template void launch_preprocess<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t);   \
   template void launch_boundary<R>(const StateT<R>&, cudaStream_t);                      \
-  template void launch_scan_segments<R>(const StateT<R>&, cudaStream_t);                 \
-  template void launch_find_limits<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t,   \
+  template void launch_scan_segments<R>(const StateT<R>&, const CoefT<R>&, bool,         \
+                                        cudaStream_t);                                    \
+  template void launch_find_limits<R>(const StateT<R>&, const CoefT<R>&, bool, cudaStream_t, \
                                       Trace*);                                            \
   template void launch_half_x<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t, Trace*); \
   template void launch_half_y<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t, Trace*);

@@ -21,12 +21,14 @@ void launch_preprocess(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st);
 // Update_Boundary_Value (support_funcs.cpp:603-728) at the device clock's time
 template <class R>
 void launch_boundary(const StateT<R>& S, cudaStream_t st);
-// segment tables only (from khouot)
+// segment tables only (from khouot; dry: with the drying pass of
+// Reset_states_vertical applied to the mask first)
 template <class R>
-void launch_scan_segments(const StateT<R>& S, cudaStream_t st);
+void launch_scan_segments(const StateT<R>& S, const CoefT<R>& c, bool dry, cudaStream_t st);
 // segment tables + boundary concentration interpolation
 template <class R>
-void launch_find_limits(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace* tr);
+void launch_find_limits(const StateT<R>& S, const CoefT<R>& c, bool dry, cudaStream_t st,
+                        Trace* tr);
 // hydraulic half-step A: t += dT/2, boundary, x sweep, explicit v, commit
 template <class R>
 void launch_half_x(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace* tr);
