@@ -174,10 +174,10 @@ int check_horizon(HydistHandle* h, int nsteps) {
 // 258) are decided on the host, the time itself advances on the device
 void enqueue_step(HydistHandle* h, bool sed_x, bool sed_y, bool bed, Trace* tr) {
   on_state(h, [&](auto& St, auto& Cf) {
-    launch_half_x(St, Cf, h->stream, tr);
+    launch_half_x(St, Cf, sed_x, h->stream, tr);
     if (sed_x) launch_sediment(St, Cf, h->o.bed_change_start, true, false, h->stream, tr);
     else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_X + 1], h->stream);
-    launch_half_y(St, Cf, h->stream, tr);
+    launch_half_y(St, Cf, sed_y, h->stream, tr);
     if (sed_y) launch_sediment(St, Cf, h->o.bed_change_start, false, bed, h->stream, tr);
     else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_Y + 1], h->stream);
   });
@@ -688,12 +688,12 @@ int hydist_half_step(HydistHandle* h, int32_t half) {
   const bool sed = t >= h->o.sediment_start;
   if (half == 0) {
     on_state(h, [&](auto& St, auto& Cf) {
-      launch_half_x(St, Cf, h->stream, &h->trace);
+      launch_half_x(St, Cf, sed, h->stream, &h->trace);
       if (sed) launch_sediment(St, Cf, h->o.bed_change_start, true, false, h->stream, &h->trace);
     });
   } else {
     on_state(h, [&](auto& St, auto& Cf) {
-      launch_half_y(St, Cf, h->stream, &h->trace);
+      launch_half_y(St, Cf, sed, h->stream, &h->trace);
       if (sed)
         launch_sediment(St, Cf, h->o.bed_change_start, false, bed_on(h, t), h->stream,
                         &h->trace);

@@ -14,10 +14,13 @@
 //   k_smooth_full       [Normalize/_normalize/update_buffer, :761-808]
 //   k_solve_v/k_solve_u [solveV/vSolver, solveU/uSolver, :607-795, 938-978]
 //   k_margin_v/k_margin_u [update_margin_elem_V/U, :980-1060]
-//   k_commit_a          [update_h_moi + update_uvz + Htuongdoi, :71-86, 732-759, 346-362]
+//   k_commit_a          [update_h_moi + update_uvz + Htuongdoi, :71-86, 732-759, 346-362;
+//                        before a concentration step also Find_VTH + hesoK,
+//                        sediment_transport.cpp:575-602, 539-573]
 //   k_smooth_full (with H_moi), k_wetting, k_commit_b, k_runs_flags (drying)
 //                       [update_h_moi + Reset_states_vertical + update_uvz +
-//                        Htuongdoi, support_funcs.cpp:71-86, 142-188, 732-759]
+//                        Htuongdoi, support_funcs.cpp:71-86, 142-188, 732-759;
+//                        Find_VTH + hesoK as in k_commit_a]
 //
 // Formulas keep the reference's structure; nvcc may fuse a multiply and an
 // add into one FMA, which the CPU oracle does not, so results agree to
@@ -577,19 +580,61 @@ __global__ void k_margin_u(StateT<R> S, CoefT<R> c) {
 }
 
 // ------------------------------------------------------ fused commits
+// Find_VTH (sediment_transport.cpp:575-602) and hesoK (:539-573) of cell
+// (i, j) from the committed values the commit holds: tu, tv of the cell,
+// tu_up = t_u(i-1, j), tv_left = t_v(i, j-1), H_moi, the bed depths h of the
+// cell, of (i, j-1) and of (i-1, j), and the new Htdu, Htdv. Rows 1..vth_hi
+// (the sediment launch shape: N after half-step A, N-1 after B), VTH from
+// row and column 2.
+template <class R>
+__device__ __forceinline__ void vth_heso_cell(const StateT<R>& S, const CoefT<R>& c, int i, int j,
+                                              int g, R tu, R tv, R tu_up, R tv_left, R Hm,
+                                              double hp, double hl, double hup, R Hu, R Hv) {
+  if (i >= 2 && j >= 2) {
+    if ((S.htaiz[g] > c.NANGDAY) && (Hm > c.H_TINH)) {
+      const R ut = (tu + tu_up) * R(0.5);
+      const R vt = (tv + tv_left) * R(0.5);
+      S.VTH[g] = sqrt(ut * ut + vt * vt);
+    } else {
+      S.VTH[g] = 0;
+    }
+  }
+  if (Hu > 0) {
+    const R Cz = 18 * log(12 * Hu / c.Ks);
+    const R k = R(5.93) * c.sqrt_g * R(hl + hp) * R(0.25) * fabs(tu) / Cz;
+    S.Kx[g] = fmin(R(100), fmax(R(5), k));
+  }
+  if (Hv > 0) {
+    const R Cz = 18 * log(12 * Hv / c.Ks);
+    const R k = R(5.93) * c.sqrt_g * R(hup + hp) * R(0.25) * fabs(tv) / Cz;
+    S.Ky[g] = fmin(R(100), fmax(R(5), k));
+  }
+}
+
 // Half-step A commit: update_h_moi (support_funcs.cpp:71-86) on [1,N]x[1,M],
 // update_uvz (:732-759) on [0,N]x[0,M] and Htuongdoi (:346-362) on
 // [1,N]x[1,M] in one pass. Htuongdoi reads the committed z of the
 // neighbour: t_z where it was committed, z where it never is (row N+1,
-// column M+1).
+// column M+1). With vth_hi > 0 (the concentration step follows) also
+// Find_VTH + hesoK on rows 1..vth_hi: nothing between this commit and the
+// concentration sweep changes what they read.
 template <class R>
-__global__ void k_commit_a(StateT<R> S, CoefT<R> c) {
+__global__ void k_commit_a(StateT<R> S, CoefT<R> c, int vth_hi) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   if (i > S.N || j > S.M) return;
   const int W = S.W, g = i * W + j;
   const double tz = S.tz[g];
-  if (i >= 1 && j >= 1 && S.khouot[g] == 0) S.Hmoi[g] = S.htaiz[g] + tz;
+  R Hm = 0;
+  const bool vth = i >= 1 && j >= 1 && i <= vth_hi;
+  if (i >= 1 && j >= 1) {
+    if (S.khouot[g] == 0) {
+      Hm = S.htaiz[g] + tz;
+      S.Hmoi[g] = Hm;
+    } else if (vth) {
+      Hm = S.Hmoi[g];
+    }
+  }
   // t_u, t_v after their smoothing (update_buffer) and the commit
   const R tu = S.su[g], tv = S.sv[g];
   S.tu[g] = tu;
@@ -600,8 +645,13 @@ __global__ void k_commit_a(StateT<R> S, CoefT<R> c) {
   if (i >= 1 && j >= 1) {
     const double zd = (i + 1 <= S.N) ? S.tz[g + W] : S.z[g + W];
     const double zr = (j + 1 <= S.M) ? S.tz[g + 1] : S.z[g + 1];
-    S.Htdu[g] = (S.h[g - 1] + S.h[g] + zd + tz) * 0.5;
-    S.Htdv[g] = (S.h[g - W] + S.h[g] + zr + tz) * 0.5;
+    const double hp = S.h[g], hl = S.h[g - 1], hup = S.h[g - W];
+    const R Hu = (hl + hp + zd + tz) * 0.5;
+    const R Hv = (hup + hp + zr + tz) * 0.5;
+    S.Htdu[g] = Hu;
+    S.Htdv[g] = Hv;
+    // the committed t_u(i-1, j), t_v(i, j-1) are the smoothed values there
+    if (vth) vth_heso_cell(S, c, i, j, g, tu, tv, S.su[g - W], S.sv[g - 1], Hm, hp, hl, hup, Hu, Hv);
   }
 }
 
@@ -639,8 +689,13 @@ __global__ void k_wetting(StateT<R> S, CoefT<R> c, int* colflag) {
 // independent per cell), update_uvz and Htuongdoi. A drying cell (i,j)
 // zeroes t_u at (i-1,j),(i,j) and t_v at (i,j-1),(i,j); each cell here reads
 // its own test and those of (i+1,j) and (i,j+1).
+//
+// With vth_hi > 0 also Find_VTH + hesoK on rows 1..vth_hi, as in
+// k_commit_a: the segment scan and the boundary interpolation that follow
+// change none of their operands. The committed t_u(i-1, j) and t_v(i, j-1)
+// are rebuilt here from the same drying tests their own threads make.
 template <class R>
-__global__ void k_commit_b(StateT<R> S, CoefT<R> c) {
+__global__ void k_commit_b(StateT<R> S, CoefT<R> c, int vth_hi) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   if (i > S.N || j > S.M) return;
@@ -667,8 +722,18 @@ __global__ void k_commit_b(StateT<R> S, CoefT<R> c) {
   if (i >= 1 && j >= 1) {
     const double zd = (i + 1 <= S.N) ? S.tz[g + W] : S.z[g + W];
     const double zr = (j + 1 <= S.M) ? S.tz[g + 1] : S.z[g + 1];
-    S.Htdu[g] = (S.h[g - 1] + S.h[g] + zd + tz) * 0.5;
-    S.Htdv[g] = (S.h[g - W] + S.h[g] + zr + tz) * 0.5;
+    const double hp = S.h[g], hl = S.h[g - 1], hup = S.h[g - W];
+    const R Hu = (hl + hp + zd + tz) * 0.5;
+    const R Hv = (hup + hp + zr + tz) * 0.5;
+    S.Htdu[g] = Hu;
+    S.Htdv[g] = Hv;
+    if (i <= vth_hi) {
+      // t_u(i-1, j) is zeroed when (i-1, j) or (i, j) dries, t_v(i, j-1)
+      // when (i, j-1) or (i, j) does
+      const R tu_up = (dries(i - 1, j) || d0) ? R(0) : S.su[g - W];
+      const R tv_left = (dries(i, j - 1) || d0) ? R(0) : S.sv[g - 1];
+      vth_heso_cell(S, c, i, j, g, R(tu), R(tv), tu_up, tv_left, S.Hmoi[g], hp, hl, hup, Hu, Hv);
+    }
   }
 }
 
@@ -712,7 +777,7 @@ void launch_find_limits(const StateT<R>& S, const CoefT<R>& c, bool dry, cudaStr
 }
 
 template <class R>
-void launch_half_x(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace* tr) {
+void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr) {
   k_tick<<<1, 1, 0, st>>>(S, 0.5 * c.dT);
   k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
   if (tr) tr->mark(st, PH_BOUNDARY_X, 2);
@@ -731,14 +796,15 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace
   // update_h_moi + update_uvz + Htuongdoi; the wet/dry mask does not change
   // in this half-step, so the segment tables are not rescanned, only the
   // boundary concentration is interpolated (support_funcs.cpp:255-258, 311)
-  k_commit_a<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c);
+  // with sed, also Find_VTH + hesoK of the concentration step (rows to N)
+  k_commit_a<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c, sed ? S.N : 0);
   k_interp_fs_rows<<<dim3(cdiv(S.M, 128), 2), 128, 0, st>>>(S, c);
   k_interp_fs_col<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
   if (tr) tr->mark(st, PH_COMMIT_X, 3);
 }
 
 template <class R>
-void launch_half_y(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace* tr) {
+void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr) {
   k_tick<<<1, 1, 0, st>>>(S, c.dT * 0.5);
   k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
   if (tr) tr->mark(st, PH_BOUNDARY_Y, 2);
@@ -755,7 +821,9 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace
   // update_h_moi, Reset_states_vertical (wetting on flagged columns, drying
   // per cell), update_uvz, Htuongdoi, then the segment tables
   k_wetting<<<cdiv(S.M, 128), 128, 0, st>>>(S, c, S.colflag);
-  k_commit_b<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c);
+  // with sed, also Find_VTH + hesoK (rows to N-1: the launch shape of
+  // engine.cpp:259-260 never reaches row N)
+  k_commit_b<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c, sed ? S.N - 1 : 0);
   // the drying mask is written by the segment scan (k_runs_flags, dry)
   launch_find_limits(S, c, true, st, tr);
   if (tr) tr->mark(st, PH_COMMIT_Y, 2);
@@ -769,8 +837,8 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace
                                         cudaStream_t);                                    \
   template void launch_find_limits<R>(const StateT<R>&, const CoefT<R>&, bool, cudaStream_t, \
                                       Trace*);                                            \
-  template void launch_half_x<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t, Trace*); \
-  template void launch_half_y<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t, Trace*);
+  template void launch_half_x<R>(const StateT<R>&, const CoefT<R>&, bool, cudaStream_t, Trace*); \
+  template void launch_half_y<R>(const StateT<R>&, const CoefT<R>&, bool, cudaStream_t, Trace*);
 HYD_HYDRO_INST(double)
 HYD_HYDRO_INST(float)
 

@@ -29,13 +29,15 @@ void launch_scan_segments(const StateT<R>& S, const CoefT<R>& c, bool dry, cudaS
 template <class R>
 void launch_find_limits(const StateT<R>& S, const CoefT<R>& c, bool dry, cudaStream_t st,
                         Trace* tr);
-// hydraulic half-step A: t += dT/2, boundary, x sweep, explicit v, commit
+// hydraulic half-step A: t += dT/2, boundary, x sweep, explicit v, commit;
+// sed: a concentration step follows (the commit computes its speeds and
+// diffusivities, Find_VTH + hesoK)
 template <class R>
-void launch_half_x(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace* tr);
+void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr);
 // hydraulic half-step B: t += dT/2, boundary, y sweep, explicit u, wet/dry,
-// commit
+// commit; sed as above
 template <class R>
-void launch_half_y(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, Trace* tr);
+void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr);
 // partitioned hydraulic line sweep: dir 0 = x (columns), 1 = y (rows)
 template <class R>
 void launch_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t st);
@@ -43,8 +45,8 @@ void launch_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t s
 // the erosion source is on from s_start
 template <class R>
 void launch_fs_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, double s_start, cudaStream_t st);
-// concentration step: xdir = the i-sweep after half-step A; bed: the bed
-// change after the j-sweep
+// concentration step (after a half-step launched with sed): xdir = the
+// i-sweep after half-step A; bed: the bed change after the j-sweep
 template <class R>
 void launch_sediment(const StateT<R>& S, const CoefT<R>& c, double s_start, bool xdir, bool bed,
                      cudaStream_t st, Trace* tr);

@@ -1,7 +1,8 @@
 // sediment.cu -- suspended-sediment concentration step on the GPU.
 //
 // Kernels (reference kernel each one replaces in brackets):
-//   k_vth_heso     [Find_VTH + hesoK, sediment_transport.cpp:575-602, 539-573]
+//   Find_VTH + hesoK [sediment_transport.cpp:575-602, 539-573] run in the
+//                  hydraulic commits (hydro.cu: k_commit_a, k_commit_b)
 //   the sweeps     [Scan_FSj/Scan_FSi + tridiagSolver + FSj/FSi_extract_
 //                   solution, :51-349, 604-651]: the partitioned line solver
 //                   with FSGen (sweep.cu), cell rows in sediment_cell.cuh
@@ -13,38 +14,6 @@
 #include "sediment_cell.cuh"
 
 namespace hyd {
-
-// Find_VTH (rows/columns 2..) and hesoK (1..) over one grid: both read the
-// committed velocities of the same cells.
-template <class R>
-__global__ void k_vth_heso(StateT<R> S, CoefT<R> c, int i_hi) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int i = blockIdx.y + 1;
-  if (i > i_hi || j > S.M) return;
-  const int W = S.W, p = i * W + j;
-  const R tu = S.tu[p], tv = S.tv[p];
-  if (i >= 2 && j >= 2) {
-    if ((S.htaiz[p] > c.NANGDAY) && (S.Hmoi[p] > c.H_TINH)) {
-      const R ut = (tu + S.tu[p - W]) * R(0.5);
-      const R vt = (tv + S.tv[p - 1]) * R(0.5);
-      S.VTH[p] = sqrt(ut * ut + vt * vt);
-    } else {
-      S.VTH[p] = 0;
-    }
-  }
-  const double hp = S.h[p];
-  const R Hu = S.Htdu[p], Hv = S.Htdv[p];
-  if (Hu > 0) {
-    const R Cz = 18 * log(12 * Hu / c.Ks);
-    const R k = R(5.93) * c.sqrt_g * R(S.h[p - 1] + hp) * R(0.25) * fabs(tu) / Cz;
-    S.Kx[p] = fmin(R(100), fmax(R(5), k));
-  }
-  if (Hv > 0) {
-    const R Cz = 18 * log(12 * Hv / c.Ks);
-    const R k = R(5.93) * c.sqrt_g * R(S.h[p - W] + hp) * R(0.25) * fabs(tv) / Cz;
-    S.Ky[p] = fmin(R(100), fmax(R(5), k));
-  }
-}
 
 // ---- bed change: Calculate_Qb (sediment_transport.cpp:352-434) and
 // _bed_load / BedLoad (:436-537, :664-673), which the reference never
@@ -192,15 +161,12 @@ __global__ void k_update_fs(StateT<R> S) {
 template <class R>
 void launch_sediment(const StateT<R>& S, const CoefT<R>& c, double s_start, bool xdir, bool bed,
                      cudaStream_t st, Trace* tr) {
-  // first half: Find_VTH/hesoK over rows to N; second half: to N-1
-  // (launch shape of engine.cpp:259-260 never reaches row N)
-  const int i_hi = xdir ? S.N : S.N - 1;
-  k_vth_heso<<<dim3(cdiv(S.M, 128), i_hi), 128, 0, st>>>(S, c, i_hi);
+  // Find_VTH + hesoK ran in the half-step's commit (k_commit_a/k_commit_b)
   if (tr) tr->kbegin(st, xdir ? KS_FS_X : KS_FS_Y);
   launch_fs_sweep(S, c, xdir ? 0 : 1, s_start, st);
   if (tr) tr->kend(st, xdir ? KS_FS_X : KS_FS_Y);
   k_update_fs<<<dim3(cdiv(S.M, 128), S.N), 128, 0, st>>>(S);
-  int launched = 3;
+  int launched = 2;
   if (bed && S.N >= 5) {
     // the bed change once per step, after the j-sweep (engine.cpp:290-293)
     k_calc_qb<<<dim3(cdiv(S.M - 1, 128), S.N - 1), 128, 0, st>>>(S, c);
