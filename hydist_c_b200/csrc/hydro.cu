@@ -372,34 +372,73 @@ __global__ void k_boundary(StateT<R> S) {
 
 // ------------------------------------------------------------ smoothing
 // _normalize / update_buffer (support_funcs.cpp:761-808) into a complete
-// array (su / sv): smoothed on the
-// interior [2,N]x[2,M], the unsmoothed value elsewhere, i.e. t_u / t_v as
-// they stand after update_buffer. Readers of the smoothed velocity use it
-// directly and the half-step commit writes it back to t_u / t_v, u / v.
-// hmoi != 0 (the last smoothing of half-step B) also does update_h_moi and
-// the column flags of the wetting pass (k_hmoi_flags' work, after the explicit
-// u update that reads H_moi).
+// array (su / sv): smoothed on the interior [2,N]x[2,M], the unsmoothed
+// value elsewhere, i.e. t_u / t_v as they stand after update_buffer.
+// Readers of the smoothed velocity use it directly and the half-step commit
+// writes it back to t_u / t_v, u / v. hmoi != 0 (the last smoothing of
+// half-step B, after the explicit u update that reads H_moi) also does
+// update_h_moi and flags the columns the wetting pass must visit.
+// One thread smooths SMOOTH_ROWS consecutive rows of a column: the column's
+// values and mask over those rows and the two around them are loaded once
+// and shared between the rows, every operand before any arithmetic.
+constexpr int SMOOTH_ROWS = 4;
+
 template <class R>
 __global__ void k_smooth_full(StateT<R> S, CoefT<R> c, int isU, int hmoi) {
+  constexpr int RB = SMOOTH_ROWS;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = blockIdx.y;
-  if (i >= S.H || j >= S.W) return;
-  const int W = S.W, g = i * W + j;
-  if (hmoi && i >= 1 && i <= S.N + 1 && j >= 1 && j <= S.M) {
-    const int kh = S.khouot[g];
-    if (i <= S.N && kh == 0) S.Hmoi[g] = S.htaiz[g] + S.tz[g];
-    if (kh == 1) S.colflag[j] = 1;
-  }
+  const int i0 = blockIdx.y * RB;
+  if (j >= S.W) return;
+  const int W = S.W, H = S.H, N = S.N, M = S.M;
   const R* val = isU ? S.tu : S.tv;
   R* out_arr = isU ? S.su : S.sv;
-  const R vg = val[g];
-  R out = vg;
-  if (i >= 2 && i <= S.N && j >= 2 && j <= S.M) {
-    // every operand is loaded up front, one round of memory latency
-    const int close = isU ? W : 1, far = isU ? 1 : W;
-    const R a = val[g - close], b = val[g + close], l = val[g - far], r = val[g + far];
-    const int kl = S.khouot[g - far], kr = S.khouot[g + far];
-    if (vg != 0) {
+  const bool jin = j >= 2 && j <= M;
+  // column j over rows i0-1 .. i0+RB (clamped to the array; the clamped
+  // values are never used)
+  R col[RB + 2];
+  int kcol[RB + 2];
+#pragma unroll
+  for (int r = 0; r < RB + 2; ++r) {
+    const int i = min(max(i0 - 1 + r, 0), H - 1);
+    col[r] = val[i * W + j];
+    kcol[r] = S.khouot[i * W + j];
+  }
+  // the row neighbours (j-1, j+1) of each row, interior cells only
+  R sa[RB], sb[RB];
+  int ka[RB], kb[RB];
+#pragma unroll
+  for (int r = 0; r < RB; ++r) {
+    const int i = i0 + r;
+    sa[r] = sb[r] = 0;
+    ka[r] = kb[r] = 0;
+    if (i >= 2 && i <= N && jin) {
+      const int g = i * W + j;
+      sa[r] = val[g - 1];
+      sb[r] = val[g + 1];
+      if (isU) {
+        ka[r] = S.khouot[g - 1];
+        kb[r] = S.khouot[g + 1];
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < RB; ++r) {
+    const int i = i0 + r;
+    if (i >= H) break;
+    const int g = i * W + j;
+    if (hmoi && i >= 1 && i <= N + 1 && j >= 1 && j <= M) {
+      const int kh = kcol[r + 1];
+      if (i <= N && kh == 0) S.Hmoi[g] = S.htaiz[g] + S.tz[g];
+      if (kh == 1) S.colflag[j] = 1;
+    }
+    const R vg = col[r + 1];
+    R out = vg;
+    if (i >= 2 && i <= N && jin && vg != 0) {
+      // u: the close neighbours are the rows above and below, the far ones
+      // (counted where wet) the columns; v the other way round
+      const R a = isU ? col[r] : sa[r], b = isU ? col[r + 2] : sb[r];
+      const R l = isU ? sa[r] : col[r], rr = isU ? sb[r] : col[r + 2];
+      const int kl = isU ? ka[r] : kcol[r], kr = isU ? kb[r] : kcol[r + 2];
       int count = 2;
       R nb = a + b;
       if (kl == 0) {
@@ -407,13 +446,13 @@ __global__ void k_smooth_full(StateT<R> S, CoefT<R> c, int isU, int hmoi) {
         count++;
       }
       if (kr == 0) {
-        nb += r;
+        nb += rr;
         count++;
       }
       out = out * c.heso + (1 - c.heso) * nb / count;
     }
+    out_arr[g] = out;
   }
-  out_arr[g] = out;
 }
 
 // ---------------------------------------------------- explicit updates
@@ -788,10 +827,10 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   // smoothing of t_u into su, explicit v from it, margins, smoothing of t_v
   // into sv; k_commit_a writes both back (Normalize/update_buffer pairs,
   // engine.cpp:109-124)
-  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 1, 0);
+  k_smooth_full<<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c, 1, 0);
   k_solve_v<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c);
   k_margin_v<<<cdiv(S.N - 1, 128), 128, 0, st>>>(S, c);
-  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 0, 0);
+  k_smooth_full<<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c, 0, 0);
   if (tr) tr->mark(st, PH_EXPLICIT_V, 4);
   // update_h_moi + update_uvz + Htuongdoi; the wet/dry mask does not change
   // in this half-step, so the segment tables are not rescanned, only the
@@ -812,11 +851,11 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   launch_sweep(S, c, 1, st);
   if (tr) tr->kend(st, KS_SWEEP_Y);
   if (tr) tr->mark(st, PH_SWEEP_Y, 1);
-  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 0, 0);
+  k_smooth_full<<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c, 0, 0);
   k_solve_u<<<grid2(S.M - 1, S.N, 128), 128, 0, st>>>(S, c);
   k_margin_u<<<cdiv(S.M - 1, 128), 128, 0, st>>>(S, c);
   // with update_h_moi and the wetting pass's column flags
-  k_smooth_full<<<grid2(S.W, S.H, 128), 128, 0, st>>>(S, c, 1, 1);
+  k_smooth_full<<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c, 1, 1);
   if (tr) tr->mark(st, PH_EXPLICIT_U, 4);
   // update_h_moi, Reset_states_vertical (wetting on flagged columns, drying
   // per cell), update_uvz, Htuongdoi, then the segment tables
