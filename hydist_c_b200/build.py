@@ -18,8 +18,10 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "libhydist_b200.so"
-SOURCES = ["engine.cu", "hydro.cu", "sweep.cu", "sediment.cu", "tridiag.cu", "compat.cu", "server.cu"]
-HEADERS = ["common.cuh", "hydro.cuh", "assembly.cuh", "linesolve.cuh", "partsolve.cuh", "sediment_cell.cuh"]
+SOURCES = ["engine.cu", "hydro.cu", "sweep.cu", "sediment.cu", "tridiag.cu", "compat.cu", "server.cu",
+           "uvz_compat.cu"]
+HEADERS = ["common.cuh", "hydro.cuh", "assembly.cuh", "linesolve.cuh", "partsolve.cuh", "sediment_cell.cuh",
+           "explicit.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-Xptxas", "-v"]
@@ -42,8 +44,8 @@ def _stale(out: Path, deps) -> bool:
 def build(force: bool = False, verbose: bool = False) -> Path:
     OBJ.mkdir(exist_ok=True)
     nvcc = _nvcc()
-    hdrs = [CSRC / h for h in HEADERS] + [ROOT / "include" / "hydist_capi.h",
-                                            ROOT / "include" / "hydist_compat.h"]
+    hdrs = [CSRC / h for h in HEADERS] + [ROOT / "include" / h for h in (
+        "hydist_capi.h", "hydist_compat.h", "hydist_uvz_compat.h", "hydist_gtsv_device.cuh")]
     objs = []
     logs = []
     for s in SOURCES:

@@ -29,6 +29,7 @@
 
 #include "assembly.cuh"
 #include "common.cuh"
+#include "explicit.cuh"
 #include "hydro.cuh"
 
 namespace hyd {
@@ -468,7 +469,8 @@ __device__ __forceinline__ bool find_seg(const int* dau, const int* cuoi, int n,
   return false;
 }
 
-// vSolver driven by solveV (UVZSolver_multithread.cpp:607-663, 961-978).
+// vSolver driven by solveV (UVZSolver_multithread.cpp:607-663, 961-978);
+// the cell's arithmetic is v_new (explicit.cuh).
 template <class R>
 __global__ void k_solve_v(StateT<R> S, CoefT<R> c) {
   // the block's cells share one row: its segment table goes to shared memory
@@ -486,136 +488,45 @@ __global__ void k_solve_v(StateT<R> S, CoefT<R> c) {
   int first, last;
   if (!find_seg(s_first, s_last, s_n, col, first, last)) return;
   if (first >= last || col >= last || col < first) return;
-  const int off = S.W, g = row * off + col;
-  const R* u = S.u;
-  const R* v = S.v;
-  const R* tu = S.su;  // t_u after its smoothing
-  const R* Hm = S.Hmoi;
+  const int g = row * S.W + col;
   // every operand up front: one round of memory latency
-  const R u00 = u[g - off], u01 = u[g], u10 = u[g - off + 1], u11 = u[g + 1];
-  const R t00 = tu[g - off], t01 = tu[g], t10 = tu[g - off + 1], t11 = tu[g + 1];
-  const R vv = v[g], vl = v[g - 1], vr = v[g + 1];
-  const R vm1 = v[g - off], vm2 = v[g - 2 * off], vp1 = v[g + off], vp2 = v[g + 2 * off];
-  const R hm1 = Hm[g - off], hm2 = Hm[g - 2 * off], hp1 = Hm[g + off];
-  const R Hv = S.Htdv[g], Ky1 = S.Ky1[g], vis = S.visco[g], tsy = S.Tsyw[g];
-  const R dz = R(S.z[g + 1] - S.z[g]);  // the level difference in FP64 first
-  R p, q = 0, tmp = 0;
-  const R utb = (u00 + u01 + u10 + u11) * R(0.25);
-  const R t_utb = (t00 + t01 + t10 + t11) * R(0.25);
-  const R rHv = R(1) / Hv;
-  p = (vr - vl) * c.r_dY2;
-  p = c.HaiChiadT + p + Ky1 * sqrt(utb * utb + vv * vv) * rHv;
-  if (hm1 <= c.H_TINH) {
-    if (utb < 0) {
-      q = t_utb * (-3 * vv + 4 * vp1 - vp2) * c.r_dX2;
-      tmp = (vv - 2 * vp1 + vp2) * c.r_dXbp;
-    }
-  } else {
-    if (hp1 <= c.H_TINH) {
-      if ((hm2 > c.H_TINH) && (utb > 0)) {
-        q = t_utb * (3 * vv - 4 * vm1 + vm2) * c.r_dX2;
-        tmp = (vv - 2 * vm1 + vm2) * c.r_dXbp;
-      }
-    } else {
-      q = t_utb * (vp1 - vm1) * c.r_dX2;
-      tmp = (vp1 - 2 * vv + vm1) * c.r_dXbp;
-    }
-  }
-  q = c.HaiChiadT * vv - q - c.CORIOLIS_FORCE * t_utb;
-  q = (q - c.g * dz * c.r_dY + vis * (tmp + (vr - 2 * vv + vl) * c.r_dYbp)) +
-      (c.Windy - tsy) * rHv;
-  S.tv[g] = q / p;
+  const VOps<R> o = v_ops(S, S.su, g);  // t_u after its smoothing
+  S.tv[g] = v_new(o, c);
 }
 
 // uSolver driven by solveU (UVZSolver_multithread.cpp:724-795, 938-959);
-// dX and Windx are read from dY and Windy as the reference does (:731,734).
+// the cell's arithmetic is u_new (explicit.cuh).
 template <class R>
 __global__ void k_solve_u(StateT<R> S, CoefT<R> c) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int row = blockIdx.y + 1;
   if (row > S.N || col > S.M) return;
-  const int off = S.W;
-  const int ij = row * off + col, i1j = ij + off;
-  const R* u = S.u;
-  const R* v = S.v;
-  const R* tv = S.sv;  // t_v after its smoothing
-  const R* Hm = S.Hmoi;
+  const int ij = row * S.W + col;
   // every operand is loaded before the segment lookup (all in bounds for
   // rows 1..N, columns 2..M), so both take one round of memory latency
-  const R v00 = v[ij - 1], v01 = v[ij], v10 = v[i1j - 1], v11 = v[i1j];
-  const R t00 = tv[ij - 1], t01 = tv[ij], t10 = tv[i1j - 1], t11 = tv[i1j];
-  const R uu = u[ij], ud = u[i1j], uup = u[ij - off];
-  const R ul1 = u[ij - 1], ul2 = u[ij - 2], ur1 = u[ij + 1], ur2 = u[ij + 2];
-  const R hl1 = Hm[ij - 1], hl2 = Hm[ij - 2], hr1 = Hm[ij + 1];
-  const R Hu = S.Htdu[ij], Kx1 = S.Kx1[ij], vis = S.visco[ij], tsx = S.Tsxw[ij];
-  const R dz = R(S.z[i1j] - S.z[ij]);  // the level difference in FP64 first
+  const UOps<R> o = u_ops(S, S.sv, ij);  // t_v after its smoothing
   int first, last;
   if (!find_seg(S.dauj + col * SEG, S.cuoij + col * SEG, S.mocj[col], row, first, last)) return;
   if (first > last || row < first - 1 || row >= last) return;
-  const R Windx = c.Windy;
-  // dX is read from dY: 1/(2dX) = r_dY2, 1/dX^2 = r_dYbp, 1/dX = r_dY
-  R p, q = 0, tmp = 0;
-  const R vtb = (v00 + v01 + v10 + v11) * R(0.25);
-  const R t_vtb = (t00 + t01 + t10 + t11) * R(0.25);
-  const R rHu = R(1) / Hu;
-  p = (ud - uup) * c.r_dY2;
-  p = (c.HaiChiadT + p + Kx1 * sqrt(vtb * vtb + uu * uu) * rHu);
-  if (hl1 <= c.H_TINH) {
-    if (vtb < 0) {
-      q = t_vtb * (-3 * uu + 4 * ur1 - ur2) * c.r_dY2;
-      tmp = (uu - 2 * ur1 + ur2) * c.r_dYbp;
-    }
-  } else {
-    if (hr1 <= c.H_TINH) {
-      if ((hl2 > c.H_TINH) && (vtb > 0)) {
-        q = t_vtb * (3 * uu - 4 * ul1 + ul2) * c.r_dY2;
-        tmp = (uu - 2 * ul1 + ul2) * c.r_dYbp;
-      }
-    } else {
-      q = t_vtb * (ur1 - ul1) * c.r_dY2;
-      tmp = (ur1 - 2 * uu + ul1) * c.r_dYbp;
-    }
-  }
-  q = c.HaiChiadT * uu - q + c.CORIOLIS_FORCE * t_vtb;
-  q = (q - c.g * dz * c.r_dY + vis * (tmp + (ud - 2 * uu + uup) * c.r_dYbp)) +
-      (Windx - tsx) * rHu;
-  S.tu[ij] = q / p;
+  S.tu[ij] = u_new(o, c);
 }
 
-// update_margin_elem_V (UVZSolver_multithread.cpp:1018-1060).
+// update_margin_elem_V (UVZSolver_multithread.cpp:1018-1060), one row per
+// thread.
 template <class R>
 __global__ void k_margin_v(StateT<R> S, CoefT<R> c) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   if (i > S.N) return;
-  const int w = S.W, M = S.M;
-  R* tv = S.tv;
-  for (int k = 0; k < S.moci[i]; ++k) {
-    const int first = S.daui[i * SEG + k], last = S.cuoii[i * SEG + k];
-    const bool br1 = (first > 2) || ((first == 2) && (fabs((S.h[i * w + first - 1] + S.h[(i - 1) * w + first - 1]) * 0.5 - c.NANGDAY) < 1e-16));
-    const bool br2 = (last < M) || ((last == M) && (fabs((S.h[i * w + last] + S.h[(i - 1) * w + last]) * 0.5 - c.NANGDAY) < 1e-16));
-    if (br1) tv[i * w + first - 1] = 0;
-    else tv[i * w + first - 1] = 2 * tv[i * w + first] - tv[i * w + first + 1];
-    if (br2) tv[i * w + last] = 0;
-    else tv[i * w + last] = 2 * tv[i * w + last - 1] - tv[i * w + last - 2];
-  }
+  margin_v(S, (double)c.NANGDAY, i);
 }
 
-// update_margin_elem_U (UVZSolver_multithread.cpp:980-1016).
+// update_margin_elem_U (UVZSolver_multithread.cpp:980-1016), one column per
+// thread.
 template <class R>
 __global__ void k_margin_u(StateT<R> S, CoefT<R> c) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
   if (j > S.M) return;
-  const int w = S.W, N = S.N;
-  R* tu = S.tu;
-  for (int k = 0; k < S.mocj[j]; ++k) {
-    const int first = S.dauj[j * SEG + k], last = S.cuoij[j * SEG + k];
-    const bool br1 = (first > 2) || ((first == 2) && (fabs((S.h[1 * w + j] + S.h[1 * w + j - 1]) * 0.5 - c.NANGDAY) < 1e-16));
-    const bool br2 = (last < N) || ((last == N) && (fabs((S.h[N * w + j] + S.h[N * w + j - 1]) * 0.5 - c.NANGDAY) < 1e-16));
-    if (br1) tu[(first - 1) * w + j] = 0;
-    else tu[(first - 1) * w + j] = 2 * tu[first * w + j] - tu[(first + 1) * w + j];
-    if (br2) tu[last * w + j] = 0;
-    else tu[last * w + j] = 2 * tu[(last - 1) * w + j] - tu[(last - 2) * w + j];
-  }
+  margin_u(S, (double)c.NANGDAY, j);
 }
 
 // ------------------------------------------------------ fused commits

@@ -12,7 +12,12 @@ tree is present, the reference driver.
   tridiag() on batched systems, and ``oracle/_ref/hydist_ref_main_b200``:
   the reference's own main.cpp, loader.cpp and set-up kernels linked against
   this repository's library in place of the reference's engine.cpp (the
-  drop-in check of tests/test_compat.py). Outputs go to oracle/_ref/ only.
+  drop-in check of tests/test_compat.py), and
+  ``oracle/_ref/hydist_ref_driver_uvz_b200``: the driver with the reference's
+  own engine.cpp, support_funcs.cpp, loader.cpp and sediment_transport.cpp
+  but this library's UVZSolver kernels in place of UVZSolver_multithread.cpp
+  and gtsv.cpp (the kernel-level drop-in check of tests/test_uvz_compat.py).
+  Outputs go to oracle/_ref/ only.
 """
 from __future__ import annotations
 
@@ -31,6 +36,8 @@ REF_TRIDIAG = REF_OUT / "hydist_ref_tridiag"
 # the reference's own main.cpp + loader.cpp + set-up kernels, linked against
 # this repository's library in place of engine.cpp (the drop-in check)
 REF_MAIN_B200 = REF_OUT / "hydist_ref_main_b200"
+# the driver on the reference's engine with this library's UVZSolver kernels
+REF_DRIVER_UVZ = REF_OUT / "hydist_ref_driver_uvz_b200"
 PRODUCT_DIR = HERE.parent / "hydist_c_b200"
 REF_SOURCES = ["engine.cpp", "support_funcs.cpp", "UVZSolver_multithread.cpp", "loader.cpp",
                "sediment_transport.cpp", "gtsv.cpp"]
@@ -79,6 +86,8 @@ def build_reference(src="/root/reference", force=False):
     if not force and not _stale(REF_DRIVER, deps) and not _stale(REF_TRIDIAG, deps):
         if not REF_MAIN_B200.exists():
             build_reference_main_on_library(src)
+        if not REF_DRIVER_UVZ.exists():
+            build_reference_engine_on_library_kernels(src)
         return REF_DRIVER
     objs = []
     for s in REF_SOURCES:
@@ -96,7 +105,28 @@ def build_reference(src="/root/reference", force=False):
     _run(["nvcc", *ARCH, str(objdir / "UVZSolver_multithread.o"), str(objdir / "support_funcs.o"),
           str(objdir / "gtsv.o"), str(t_o), "-o", str(REF_TRIDIAG)])
     build_reference_main_on_library(src)
+    build_reference_engine_on_library_kernels(src)
     return REF_DRIVER
+
+
+def build_reference_engine_on_library_kernels(src="/root/reference"):
+    """Link ref_driver.cu and the reference's engine.cpp, support_funcs.cpp,
+    loader.cpp and sediment_transport.cpp (objects from build_reference) with
+    libhydist_b200.so for the UVZSolver kernels (include/hydist_uvz_compat.h):
+    the reference's engine launches this library's kernels unchanged."""
+    src = Path(src)
+    lib = PRODUCT_DIR / "libhydist_b200.so"
+    objdir = REF_OUT / "obj"
+    names = ["ref_driver.o", "engine.o", "support_funcs.o", "loader.o", "sediment_transport.o"]
+    objs = [objdir / n for n in names]
+    if not lib.exists() or not all(o.exists() for o in objs):
+        return None
+    # -cudart shared: the engine's launches of the library's kernels pass
+    # their configuration through the CUDA runtime, which must be the
+    # library's (the shared one), not a static copy in the executable
+    _run(["nvcc", *ARCH, "-cudart", "shared", *map(str, objs), f"-L{PRODUCT_DIR}", "-lhydist_b200",
+          "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/../../hydist_c_b200", "-o", str(REF_DRIVER_UVZ)])
+    return REF_DRIVER_UVZ
 
 
 def build_reference_main_on_library(src="/root/reference"):
