@@ -3,12 +3,16 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--precision fp64|fp32|fp32-refine] [--workload sediment-2048x1024|channel-256x128]
+                    [--eager]
 
 A step is one full ADI step (two half-steps, with the concentration sweeps)
 of the 2048x1024 sediment workload: dx=dy=5 m, dt=2 s, seeded synthetic
 bathymetry, sediment from t=600 s. The state is spun up to t=600 s before
 timing so that every timed step runs the sediment sweeps. value is
-cell-steps/s (N*M interior cells x steps / device seconds), whole job.
+cell-steps/s (N*M interior cells x steps / device seconds), whole job. Each
+step is one replay of the step's CUDA graph (hydist_step_graph), the path the
+ensembles and the server take; --eager launches the kernels one by one
+(hydist_step).
 
 Multi-GPU: scenarios are independent, so N GPUs run N replicas with no
 data-path collective (weak scaling); the time is the max over ranks.
@@ -685,7 +689,7 @@ def measure_e2e(H, bundle, dev, prec, args):
     sim.sync()
     t1 = time.perf_counter()
     for _ in range(args.steps):
-        sim.step(1)
+        (sim.step_graph if args.graph else sim.step)(1)
         sim.mass()
     t2 = time.perf_counter()
     outs = [sim.download(f) for f in ("u", "v", "z", "FS")]
@@ -716,13 +720,16 @@ def main():
                     help="steps per request and scheduling round (" + SERVING + ")")
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"],
                     help="arithmetic of the " + TRIDIAG + " workload")
-    ap.add_argument("--graph", action="store_true")
+    ap.add_argument("--eager", action="store_true",
+                    help="launch each step's kernels one by one instead of replaying the "
+                         "step's CUDA graph (hydist_step instead of hydist_step_graph)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--sed0", action="store_true",
                     help="sediment sweeps from t=0 instead of a spin-up to t=600 s")
     args = ap.parse_args()
+    args.graph = not args.eager
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
