@@ -625,6 +625,9 @@ def run_ours(args):
                                      else args.workload + "-" + args.precision, {}).get(dom)
         except Exception:
             pass
+    acc = None
+    if prec != H.FP64 and rank == 0:
+        acc = accuracy_vs_fp64(H, sim, bundle, dev, spin + max(args.warmup, 3) + 2 * args.steps)
     e2e = measure_e2e(H, bundle, dev, prec, args) if rank == 0 and not args.no_e2e else None
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -658,9 +661,31 @@ def run_ours(args):
             "gpu_launches": launches,
             "clocks": clk,
         }
+        if acc is not None:
+            line["accuracy_vs_fp64"] = acc
         print(json.dumps(line), flush=True)
     sim.close()
     R.finish(ws)
+
+
+def accuracy_vs_fp64(H, sim, bundle, dev, nsteps):
+    """Errors of an FP32 form after nsteps steps against the FP64 form (whose
+    steps match the FP64 CPU oracle to 1e-10 per step) run from the same
+    start: max |dz| in metres, relative L2 of u, v and the concentration, and
+    the relative difference of the water volume (mass)."""
+    ref = H.Simulation(bundle, device=dev, precision=H.FP64)
+    ref.step(nsteps)
+    out = {"steps": nsteps}
+    got = {f: sim.download(f) for f in ("z", "u", "v", "FS")}
+    want = {f: ref.download(f) for f in ("z", "u", "v", "FS")}
+    out["max_abs_dz_m"] = float(np.abs(got["z"] - want["z"]).max())
+    for f in ("u", "v", "FS"):
+        den = float(np.linalg.norm(want[f]))
+        out[f"rel_l2_{f}"] = float(np.linalg.norm(got[f] - want[f]) / den) if den > 0 else 0.0
+    m_ref = ref.mass()
+    out["rel_volume_diff"] = float(abs(sim.mass() - m_ref) / abs(m_ref))
+    ref.close()
+    return out
 
 
 def measure_e2e(H, bundle, dev, prec, args):
