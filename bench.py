@@ -708,6 +708,9 @@ def measure_e2e(H, bundle, dev, prec, args):
         b["options"] = dict(bundle["options"], sediment_start=0.0, bed_change_start=0.0)
     h2d = sum(a.nbytes for a in pinned.values())
     n = (sc["N"] + 3) * (sc["M"] + 3)
+    # pinned host buffers for the results, as for the inputs
+    outs = {f: torch.empty((sc["N"] + 3, sc["M"] + 3), dtype=torch.float64).pin_memory().numpy()
+            for f in ("u", "v", "z", "FS")}
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     sim = H.Simulation(b, device=dev, precision=prec)
@@ -717,7 +720,8 @@ def measure_e2e(H, bundle, dev, prec, args):
         (sim.step_graph if args.graph else sim.step)(1)
         sim.mass()
     t2 = time.perf_counter()
-    outs = [sim.download(f) for f in ("u", "v", "z", "FS")]
+    for f, o in outs.items():
+        sim.download(f, out=o)
     dt = time.perf_counter() - t0
     sim.close()
     steps = args.steps

@@ -139,9 +139,16 @@ class Simulation:
         return int(self._lib.hydist_stream(self._h) or 0)
 
     # -- fields
-    def download(self, name: str) -> np.ndarray:
+    def download(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
+        """A field as a (N+3, M+3) array; `out` (C-contiguous, of that shape
+        and the field's dtype, e.g. in pinned memory) receives it if given."""
         f = FIELDS[name]
-        out = np.empty(self.shape, dtype=np.int32 if name == "khouot" else np.float64)
+        dt = np.int32 if name == "khouot" else np.float64
+        if out is None:
+            out = np.empty(self.shape, dtype=dt)
+        elif out.shape != self.shape or out.dtype != dt or not out.flags.c_contiguous:
+            raise ValueError(f"{name}: out must be a C-contiguous {dt.__name__} array of shape "
+                             f"{self.shape}")
         capi.check(self._lib, self._lib.hydist_download(self._h, f, out.ctypes.data),
                    "hydist_download")
         return out
