@@ -91,12 +91,13 @@ enum Phase {
   PH_BOUNDARY_X = 0,  // Update_Boundary_Value, first half
   PH_SWEEP_X,         // x sweep: assembly + tridiagonal solve + extraction
   PH_EXPLICIT_V,      // smoothing of u, explicit v, margins, smoothing of v
-  PH_COMMIT_X,        // H_moi, commit, segment tables, total depths
-  PH_SEDIMENT_X,      // speed, diffusivity, concentration i-sweep, commit
+  PH_COMMIT_X,        // H_moi, commit, total depths (and, before a concentration
+                      // step, the speed and diffusivities)
+  PH_SEDIMENT_X,      // concentration i-sweep, commit
   PH_BOUNDARY_Y,
   PH_SWEEP_Y,
   PH_EXPLICIT_U,
-  PH_COMMIT_Y,        // + wetting/drying
+  PH_COMMIT_Y,        // + wetting/drying, segment tables
   PH_SEDIMENT_Y,
   PH_COUNT
 };
