@@ -73,7 +73,8 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
   const int cidx = k * LPB + l;
   const int U = G.unknowns_per_line();
   // scratch slot of this CTA: c', y', v' per unknown, and with refinement
-  // also the rows A, B, C, D (Gen::SCRATCH_ARRAYS arrays of U x LPB)
+  // also the rows A, B, C, D and the pivot reciprocals (Gen::SCRATCH_ARRAYS
+  // arrays of U x LPB)
   const size_t UL = (size_t)U * LPB;
   R* scr = G.scratch + (size_t)blockIdx.x * Gen::SCRATCH_ARRAYS * UL;
   R* sc_c = scr;
@@ -125,18 +126,21 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
             sh.sep[2][cidx] = C;
             sh.sep[3][cidx] = D;
           } else {
+            R m;
             if (s == 0) {
-              const R m = rcp(B);
+              m = rcp(B);
               cp = C * m;
               yp = D * m;
               vp = -A * m;
             } else {
-              const R m = rcp(B - A * cp);
+              m = rcp(B - A * cp);
               yp = (D - A * yp) * m;
               vp = -A * vp * m;
               cp = C * m;
             }
             const size_t o = (size_t)(q0 + s) * LPB + l;
+            // the refinement's correction reuses the pivot reciprocals
+            if constexpr (Gen::REFINE) scr[7 * UL + o] = m;
             sc_c[o] = cp;
             sc_y[o] = yp;
             sc_v[o] = vp;
@@ -225,43 +229,54 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
     } else {
       // the first solution x goes over y'; then one refinement pass:
       // r = D - A x_{-1} - B x - C x_{+1} in FP64 with the stored rows,
-      // A d = r with the same elimination (c', v', the reduced matrix),
-      // x + d emitted
+      // A d = r with the same elimination (c', the stored pivot reciprocals,
+      // v', the reduced matrix), x + d emitted
       R* sA = scr + 3 * UL;
       R* sB = scr + 4 * UL;
       R* sC = scr + 5 * UL;
       R* sD = scr + 6 * UL;
+      const R* sM = scr + 7 * UL;
+      auto resid = [&](size_t o, R xm, R x, R xp) {
+        return (R)((double)sD[o] - (double)sA[o] * (double)xm - (double)sB[o] * (double)x -
+                   (double)sC[o] * (double)xp);
+      };
+      R x_before_sep = 0;  // x of the chunk's last interior unknown
       {
+        // back substitution; each interior unknown's residual as soon as the
+        // unknown before it is known (the separator's needs the next chunk)
         const R xr = sh.xsep[cidx];
         const R xl = (k > 0) ? sh.xsep[cidx - LPB] : R(0);
         sc_y[(size_t)(q0 + nu - 1) * LPB + l] = xr;
-        R xn = xr;
+        R x1 = xr, x2 = 0;  // x_{t+1}, x_{t+2}
         for (int t = nu - 2; t >= 0; --t) {
           const size_t o = (size_t)(q0 + t) * LPB + l;
-          const R x = sc_y[o] + sc_v[o] * xl - sc_c[o] * xn;
+          const R x = sc_y[o] + sc_v[o] * xl - sc_c[o] * x1;
           sc_y[o] = x;
-          xn = x;
+          if (t == nu - 2) x_before_sep = x;
+          else sD[o + LPB] = resid(o + LPB, x, x1, x2);
+          x2 = x1;
+          x1 = x;
         }
+        // the first unknown: its left neighbour is the previous separator
+        // (none at the line's start)
+        const size_t o0 = (size_t)q0 * LPB + l;
+        if (nu >= 2) sD[o0] = resid(o0, q0 > 0 ? xl : R(0), x1, x2);
       }
       __syncthreads();
-      // residual in FP64 (over D)
-      for (int t = 0; t < nu; ++t) {
-        const int q = q0 + t;
+      {
+        // the separator row: its right neighbour is the next chunk's first
+        // unknown (none at the line's end)
+        const int q = q0 + nu - 1;
         const size_t o = (size_t)q * LPB + l;
-        const double xm = q > 0 ? (double)sc_y[o - LPB] : 0.0;
-        const double xp = q + 1 < U ? (double)sc_y[o + LPB] : 0.0;
-        const double r = (double)sD[o] - (double)sA[o] * xm - (double)sB[o] * (double)sc_y[o] -
-                         (double)sC[o] * xp;
-        sD[o] = (R)r;
+        const R xm = nu >= 2 ? x_before_sep : (q > 0 ? sc_y[o - LPB] : R(0));
+        const R xp = q + 1 < U ? sc_y[o + LPB] : R(0);
+        sD[o] = resid(o, xm, sc_y[o], xp);
       }
-      __syncthreads();
       // forward elimination of the residual (y'' over D)
       R fy = 0, yL = 0, Pk = 1, cp = 0;
       for (int t = 0; t < nu - 1; ++t) {
         const size_t o = (size_t)(q0 + t) * LPB + l;
-        const R A = sA[o], B = sB[o];
-        const R m = rcp(t == 0 ? B : B - A * cp);
-        const R y = (sD[o] - (t == 0 ? R(0) : A * yL)) * m;
+        const R y = (sD[o] - (t == 0 ? R(0) : sA[o] * yL)) * sM[o];
         sD[o] = y;
         cp = sc_c[o];
         fy += Pk * y;

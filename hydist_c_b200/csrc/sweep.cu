@@ -26,7 +26,7 @@ template <int DIR, class R, bool REF = false>
 struct HydroGen {
   using Real = R;
   static constexpr bool REFINE = REF;
-  static constexpr int SCRATCH_ARRAYS = REFINE ? 7 : 3;
+  static constexpr int SCRATCH_ARRAYS = REFINE ? 8 : 3;
   static constexpr int UPC = 2;
   // x sweeps (columns, 4 adjacent per warp) run faster with two CTAs per SM
   // despite the register cap; y sweeps (rows) slower
@@ -281,7 +281,7 @@ template <int DIR, class R, bool REF = false>
 struct FSGen {
   using Real = R;
   static constexpr bool REFINE = REF;
-  static constexpr int SCRATCH_ARRAYS = REFINE ? 7 : 3;
+  static constexpr int SCRATCH_ARRAYS = REFINE ? 8 : 3;
   static constexpr int UPC = 1;
   static constexpr int MIN_BLOCKS = DIR == 0 ? 2 : 1;
   StateT<R> S;
