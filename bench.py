@@ -408,13 +408,20 @@ def run_tridiag(args):
     x = torch.empty_like(t[1])
     stream = torch.cuda.current_stream(dev)
     table = (C.c_int32 * capi.GTSV_BANDS)()
-    capi.check(lib, lib.hydist_gtsv_autotune(dt_code, C.c_void_p(stream.cuda_stream), table),
-               "hydist_gtsv_autotune")
+    if args.gtsv_algo:
+        # one solver for every band (the library hands a band it cannot take
+        # to a more general one)
+        for k in range(capi.GTSV_BANDS):
+            table[k] = args.gtsv_algo
+    else:
+        capi.check(lib, lib.hydist_gtsv_autotune(dt_code, C.c_void_p(stream.cuda_stream), table),
+                   "hydist_gtsv_autotune")
 
     def solve(xo, tt, oo, ll):
         st = lib.hydist_gtsv_batched(tt[0].data_ptr(), tt[1].data_ptr(), tt[2].data_ptr(),
                                      tt[3].data_ptr(), xo.data_ptr(), oo.data_ptr(), ll.data_ptr(),
-                                     len(ln), dt_code, capi.GTSV_AUTO, C.c_void_p(stream.cuda_stream))
+                                     len(ln), dt_code, args.gtsv_algo or capi.GTSV_AUTO,
+                                     C.c_void_p(stream.cuda_stream))
         capi.check(lib, st, "hydist_gtsv_batched")
 
     for _ in range(max(args.warmup, 3)):
@@ -485,7 +492,7 @@ def run_tridiag(args):
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": args.dtype, "data": "synthetic (seeded)",
             "config": {"workload": TRIDIAG, "systems": len(ln), "unknowns": n,
-                       "lengths": "log-uniform [16, 4096]", "algo": "auto",
+                       "lengths": "log-uniform [16, 4096]", "algo": args.gtsv_algo or "auto",
                        "autotuned": dict(zip([str(v) for v in bands], list(table))),
                        "l2": "inputs larger than L2", "parallelism": f"replicas x{ws}"},
             "p50_step_ms": float(np.percentile(per, 50)), "p99_step_ms": float(np.percentile(per, 99)),
@@ -749,6 +756,9 @@ def main():
                     help="steps per request and scheduling round (" + SERVING + ")")
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"],
                     help="arithmetic of the " + TRIDIAG + " workload")
+    ap.add_argument("--gtsv-algo", type=int, default=0,
+                    help="solver of every band of the " + TRIDIAG + " workload (enum "
+                         "HydistGtsvAlgo; 0: the autotuned one per band)")
     ap.add_argument("--eager", action="store_true",
                     help="launch each step's kernels one by one instead of replaying the "
                          "step's CUDA graph (hydist_step instead of hydist_step_graph)")

@@ -1,5 +1,6 @@
 // partsolve.cuh -- partition-method solve of one tridiagonal system held in
-// shared memory, by a CTA or by a warp.
+// shared memory by a warp, and the reduced-system work space of the CTA
+// solver (tridiag.cu).
 //
 // Rows r = 0..n-1: A_r x_{r-1} + B_r x_r + C_r x_{r+1} = D_r, A_0 = C_{n-1} = 0.
 // The system is cut into chunks of S unknowns (the last chunk takes the
@@ -134,67 +135,6 @@ struct PartCtaShared {
   T red[4][NT];
   T xsep[NT];
 };
-
-// CTA-wide solve (all NT threads call it; the rows are in shared memory).
-template <class T, int NT>
-__device__ void part_solve_cta(T* rA, T* rB, T* rC, T* rD, const PartGeom& g,
-                               PartCtaShared<T, NT>& sh, int n) {
-  const int k = threadIdx.x, P = g.nchunk, S = g.S;
-  const int q0 = k * S;
-  const int nu = k < P ? ((k == P - 1) ? n - q0 : S) : 0;
-  T sep[4] = {0, 1, 0, 0}, tri[6] = {0, 0, 1, 0, 0, 0};
-  if (k < P) part_forward(rA, rB, rC, rD, q0, nu, S, sep, tri);
-  sh.tri[0][k] = tri[0];
-  sh.tri[1][k] = tri[1];
-  sh.tri[2][k] = tri[2];
-  __syncthreads();
-  T ra = 0, rb = 1, rc = 0, rd = 0;
-  if (k < P) {
-    T yF = 0, vF = 0, wF = 0;
-    if (k + 1 < P) {
-      yF = sh.tri[0][k + 1];
-      vF = sh.tri[1][k + 1];
-      wF = sh.tri[2][k + 1];
-    }
-    ra = sep[0] * tri[4];
-    rb = sep[1] + sep[0] * tri[5] + sep[2] * vF;
-    rc = sep[2] * wF;
-    rd = sep[3] - sep[0] * tri[3] - sep[2] * yF;
-  }
-  for (int st = 1; st < P; st <<= 1) {
-    sh.red[0][k] = ra;
-    sh.red[1][k] = rb;
-    sh.red[2][k] = rc;
-    sh.red[3][k] = rd;
-    __syncthreads();
-    T am = 0, bm = 1, cm = 0, dm = 0, an = 0, bn = 1, cn = 0, dn = 0;
-    if (k < P && k - st >= 0) {
-      am = sh.red[0][k - st];
-      bm = sh.red[1][k - st];
-      cm = sh.red[2][k - st];
-      dm = sh.red[3][k - st];
-    }
-    if (k + st < P) {
-      an = sh.red[0][k + st];
-      bn = sh.red[1][k + st];
-      cn = sh.red[2][k + st];
-      dn = sh.red[3][k + st];
-    }
-    __syncthreads();
-    const T k1 = ra / bm, k2 = rc / bn;
-    const T na = -am * k1, nc = -cn * k2;
-    const T nb = rb - cm * k1 - an * k2;
-    const T nd = rd - dm * k1 - dn * k2;
-    ra = na;
-    rb = nb;
-    rc = nc;
-    rd = nd;
-  }
-  sh.xsep[k] = rd / rb;
-  __syncthreads();
-  if (k < P) part_back(rA, rC, rD, q0, nu, S, k > 0 ? sh.xsep[k - 1] : T(0), sh.xsep[k]);
-  __syncthreads();
-}
 
 // Warp-wide solve (all 32 lanes call it; the rows are in the warp's slice of
 // shared memory). The reduced system is solved with shuffles.

@@ -13,9 +13,11 @@
 //   warp        one warp per system staged in shared memory, partition
 //               method with a shuffle PCR of the 32 chunk separators
 //               (systems up to GT_WARP_MAX rows);
-//   CTA         one 256-thread CTA per system staged in shared memory,
-//               partition method with a shared-memory PCR (systems up to the
-//               shared memory of one CTA, about 6000 FP64 / 12000 FP32 rows).
+//   CTA         one CTA of 256 or 512 threads per system, its rows staged
+//               in shared memory by TMA bulk copies (the next system's while
+//               one is solved, where two fit), partition method with a
+//               shared-memory PCR (systems up to the shared memory of one
+//               CTA, about 6000 FP64 / 12000 FP32 rows).
 // A classification kernel files each system under its length band on the
 // device; the bands' solvers then run over their lists. The autotuner times
 // the feasible solvers per band on synthetic diagonally dominant batches and
@@ -118,31 +120,248 @@ __device__ __forceinline__ void gt_load(const T* dl, const T* d, const T* du, co
   __pipeline_wait_prior(0);
 }
 
-// one system per CTA of NT threads (the tile size of the partition)
-template <class T, int NT>
-__global__ void __launch_bounds__(NT) k_gtsv_cta(const T* __restrict__ dl, const T* __restrict__ d,
-                                                 const T* __restrict__ du, const T* __restrict__ b,
-                                                 T* __restrict__ x, const int* __restrict__ off,
-                                                 const int* __restrict__ len,
-                                                 const int* __restrict__ list,
-                                                 const int* __restrict__ count) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  auto& sh = *reinterpret_cast<PartCtaShared<T, NT>*>(smem_raw);
-  T* rows = reinterpret_cast<T*>(smem_raw + sizeof(PartCtaShared<T, NT>));
+// ------------------------------------------ bulk-staged partition solver
+// One system per CTA of NT threads. Thread 0 stages the system's rows with
+// TMA bulk copies (cp.async.bulk, completion counted on an mbarrier) into an
+// unpadded layout; the few rows at either end that are not 16-byte aligned
+// in global memory are read with plain loads. With NBUF = 2 the next
+// system's rows are fetched while the current one is solved. The chunk
+// length S is odd, so the threads' walks over their chunks (a stride of S
+// rows between threads) fall on distinct shared-memory banks.
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// the index of row 0 of a system at offset o within an array's region: the
+// region starts 16-byte aligned and the rows from a0 (o rounded up to 16
+// bytes) on land 16-byte aligned
+template <class T>
+__device__ __forceinline__ int bulk_pad(int o) {
+  constexpr int E = 16 / sizeof(T);
+  const int d = (E - o % E) % E;  // a0 - o
+  return (E - d) % E;
+}
+
+// elements of one array's region for systems of up to nmax rows
+template <class T>
+__host__ __device__ inline int bulk_region(int nmax) {
+  constexpr int E = 16 / sizeof(T);
+  return (nmax + 2 * E + E - 1) / E * E;
+}
+
+// the odd chunk length of a system of n rows on NT threads (at least 3)
+__device__ __forceinline__ int bulk_chunk(int n, int NT) {
+  int S = (n + NT - 1) / NT;
+  if (S < 3) S = 3;
+  return S | 1;
+}
+
+// waits of the staging barrier before a CTA gives a system up (each try
+// suspends the thread for a while; a stalled copy is reported, not waited
+// for without end)
+constexpr long GT_WAIT_TRIES = 1L << 22;
+
+template <class T, int NT, int NBUF>
+__global__ void __launch_bounds__(NT) k_gtsv_bulk(const T* __restrict__ dl, const T* __restrict__ d,
+                                                  const T* __restrict__ du, const T* __restrict__ b,
+                                                  T* __restrict__ x, const int* __restrict__ off,
+                                                  const int* __restrict__ len,
+                                                  const int* __restrict__ list,
+                                                  const int* __restrict__ count, int region,
+                                                  int* __restrict__ stalled) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);  // NBUF barriers
+  auto& sh = *reinterpret_cast<PartCtaShared<T, NT>*>(smem_raw + 128);
+  T* bufs = reinterpret_cast<T*>(smem_raw + 128 + (sizeof(PartCtaShared<T, NT>) + 127) / 128 * 128);
+  constexpr int E = 16 / sizeof(T);
+  const int tid = threadIdx.x;
   const int cnt = *count;
-  for (int i = blockIdx.x; i < cnt; i += gridDim.x) {
-    const int s = list[i];
-    const int o = off[s], n = len[s];
-    const PartGeom g = part_geom(n, NT);
-    T* rA = rows;
-    T* rB = rA + g.stride;
-    T* rC = rB + g.stride;
-    T* rD = rC + g.stride;
-    gt_load(dl, d, du, b, o, n, g.S, rA, rB, rC, rD, (int)threadIdx.x, NT);
+  const T* src[4] = {dl, d, du, b};
+  // thread 0: the bulk copies of system list[i] into buffer k
+  auto issue = [&](int i, int k) {
+    const int sys = list[i];
+    const int o = off[sys], n = len[sys];
+    const int a0 = (o + E - 1) / E * E, a1 = (o + n) / E * E;
+    T* base = bufs + (size_t)k * 4 * region + bulk_pad<T>(o);
+    if (a1 > a0) {
+      const unsigned bytes = (unsigned)((a1 - a0) * sizeof(T));
+      mbar_arrive_expect(&bar[k], 4 * bytes);
+      for (int a = 0; a < 4; ++a) bulk_g2s(base + (size_t)a * region + (a0 - o), src[a] + a0, bytes, &bar[k]);
+    } else {
+      mbar_arrive_expect(&bar[k], 0);
+    }
+  };
+  if (tid == 0) {
+    for (int k = 0; k < NBUF; ++k) mbar_init(&bar[k], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0 && (int)blockIdx.x < cnt) issue(blockIdx.x, 0);
+  unsigned phase = 0;  // bit k: the parity of buffer k's next completion
+  int it = 0;
+  for (int i = blockIdx.x; i < cnt; i += gridDim.x, ++it) {
+    const int k = NBUF == 2 ? (it & 1) : 0;
+    const int sys = list[i];
+    const int o = off[sys], n = len[sys];
+    // wait for the rows (bounded)
+    bool ok = false;
+    for (long t = 0; t < GT_WAIT_TRIES && !ok; ++t) ok = mbar_try_wait(&bar[k], (phase >> k) & 1u);
+    phase ^= 1u << k;
+    const int inext = i + gridDim.x;
+    if (NBUF == 2 && tid == 0 && inext < cnt) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(inext, k ^ 1);
+    }
+    T* rA = bufs + (size_t)k * 4 * region + bulk_pad<T>(o);
+    T* rB = rA + region;
+    T* rC = rB + region;
+    T* rD = rC + region;
+    // the rows outside the aligned bulk part
+    const int a0 = (o + E - 1) / E * E, a1 = (o + n) / E * E;
+    const int head = min(a0 - o, n), tail0 = max(a1 - o, head);
+    for (int q = tid; q < head + (n - tail0); q += NT) {
+      const int r = q < head ? q : tail0 + (q - head);
+      rA[r] = dl[o + r];
+      rB[r] = d[o + r];
+      rC[r] = du[o + r];
+      rD[r] = b[o + r];
+    }
     __syncthreads();
-    part_solve_cta<T, NT>(rA, rB, rC, rD, g, sh, n);
-    for (PartStrideIdx it(threadIdx.x, NT, g.S); it.q < n; it.next(NT)) x[o + it.q] = rD[it.idx()];
+    if (!__syncthreads_and(ok)) {
+      // a copy that never completed: record it and leave the system
+      if (tid == 0) atomicExch(stalled, 1);
+      continue;
+    }
+    // ---- partition solve in place: forward per chunk, separators by PCR
+    const int S = bulk_chunk(n, NT), P = max(1, n / S);
+    const int q0 = tid * S;
+    const int nu = tid < P ? (tid == P - 1 ? n - q0 : S) : 0;
+    T sep[4] = {0, 1, 0, 0};
+    T cp = 0, yp = 0, vp = 0, Pk = 1, fy = 0, fv = 0;
+    for (int s = 0; s < nu; ++s) {
+      const int q = q0 + s;
+      const T A = q > 0 ? rA[q] : T(0), B = rB[q], C = q + 1 < n ? rC[q] : T(0), Dv = rD[q];
+      if (s == nu - 1) {
+        sep[0] = A;
+        sep[1] = B;
+        sep[2] = C;
+        sep[3] = Dv;
+      } else {
+        if (s == 0) {
+          const T m = T(1) / B;
+          cp = C * m;
+          yp = Dv * m;
+          vp = -A * m;
+        } else {
+          const T m = T(1) / (B - A * cp);
+          yp = (Dv - A * yp) * m;
+          vp = -A * vp * m;
+          cp = C * m;
+        }
+        rC[q] = cp;
+        rD[q] = yp;
+        rA[q] = vp;
+        fy += Pk * yp;
+        fv += Pk * vp;
+        Pk *= -cp;
+      }
+    }
+    sh.tri[0][tid] = fy;
+    sh.tri[1][tid] = fv;
+    sh.tri[2][tid] = Pk;
     __syncthreads();
+    T ra = 0, rb = 1, rc = 0, rd = 0;
+    if (tid < P) {
+      T yF = 0, vF = 0, wF = 0;
+      if (tid + 1 < P) {
+        yF = sh.tri[0][tid + 1];
+        vF = sh.tri[1][tid + 1];
+        wF = sh.tri[2][tid + 1];
+      }
+      ra = sep[0] * vp;
+      rb = sep[1] - sep[0] * cp + sep[2] * vF;
+      rc = sep[2] * wF;
+      rd = sep[3] - sep[0] * yp - sep[2] * yF;
+    }
+    for (int st = 1; st < P; st <<= 1) {
+      sh.red[0][tid] = ra;
+      sh.red[1][tid] = rb;
+      sh.red[2][tid] = rc;
+      sh.red[3][tid] = rd;
+      __syncthreads();
+      T am = 0, bm = 1, cm = 0, dm = 0, an = 0, bn = 1, cn = 0, dn = 0;
+      if (tid < P && tid - st >= 0) {
+        am = sh.red[0][tid - st];
+        bm = sh.red[1][tid - st];
+        cm = sh.red[2][tid - st];
+        dm = sh.red[3][tid - st];
+      }
+      if (tid + st < P) {
+        an = sh.red[0][tid + st];
+        bn = sh.red[1][tid + st];
+        cn = sh.red[2][tid + st];
+        dn = sh.red[3][tid + st];
+      }
+      __syncthreads();
+      const T k1 = ra / bm, k2 = rc / bn;
+      const T na = -am * k1, nc = -cn * k2;
+      const T nb = rb - cm * k1 - an * k2;
+      const T nd = rd - dm * k1 - dn * k2;
+      ra = na;
+      rb = nb;
+      rc = nc;
+      rd = nd;
+    }
+    sh.xsep[tid] = rd / rb;
+    __syncthreads();
+    if (tid < P) {
+      const T xl = tid > 0 ? sh.xsep[tid - 1] : T(0), xr = sh.xsep[tid];
+      rD[q0 + nu - 1] = xr;
+      T xn = xr;
+      for (int t = nu - 2; t >= 0; --t) {
+        const int q = q0 + t;
+        const T xq = rD[q] + rA[q] * xl - rC[q] * xn;
+        rD[q] = xq;
+        xn = xq;
+      }
+    }
+    __syncthreads();
+    for (int q = tid; q < n; q += NT) x[o + q] = rD[q];
+    __syncthreads();  // the buffer is free
+    if (NBUF == 1 && tid == 0 && inext < cnt) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(inext, 0);
+    }
   }
 }
 
@@ -252,10 +471,12 @@ DevInfo* dev_info(int dev) {
   return &D;
 }
 
-// shared memory for systems of up to nmax rows (monotonic in nmax)
+// shared memory of the bulk-staged CTA solver for systems of up to nmax
+// rows with nbuf row buffers (monotonic in nmax)
 template <class T, int NT>
-size_t cta_smem(int nmax) {
-  return sizeof(hyd::PartCtaShared<T, NT>) + 4 * sizeof(T) * (size_t)hyd::part_stride_bound(nmax, NT);
+size_t cta_smem(int nmax, int nbuf = 1) {
+  return 128 + (sizeof(hyd::PartCtaShared<T, NT>) + 127) / 128 * 128 +
+         (size_t)nbuf * 4 * hyd::bulk_region<T>(nmax) * sizeof(T);
 }
 
 template <class T>
@@ -303,37 +524,66 @@ int default_algo(int band, const Caps& c) {
   return HYDIST_GTSV_THOMAS;
 }
 
-template <class T, int NT>
-int launch_cta(int nmax, const T* dl, const T* d, const T* du, const T* b, T* x, const int* off,
-               const int* len, const int* list, const int* count, int nsys_band, const DevInfo& D,
-               cudaStream_t st) {
-  const size_t smem = cta_smem<T, NT>(nmax);
+template <class T, int NT, int NBUF>
+int launch_bulk(int nmax, const T* dl, const T* d, const T* du, const T* b, T* x, const int* off,
+                const int* len, const int* list, const int* count, int* stalled, int nsys_band,
+                const DevInfo& D, cudaStream_t st) {
+  const size_t smem = cta_smem<T, NT>(nmax, NBUF);
   static bool attr[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr[dev]) {
-    cudaFuncSetAttribute(hyd::k_gtsv_cta<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, D.optin);
+    cudaFuncSetAttribute(hyd::k_gtsv_bulk<T, NT, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         D.optin);
     attr[dev] = true;
   }
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hyd::k_gtsv_cta<T, NT>, NT, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hyd::k_gtsv_bulk<T, NT, NBUF>, NT, smem);
   if (per_sm < 1) return HYDIST_ERR_CUDA;
   const int grid = std::min(nsys_band, per_sm * D.nsm);
-  hyd::k_gtsv_cta<T, NT><<<grid, NT, smem, st>>>(dl, d, du, b, x, off, len, list, count);
+  hyd::k_gtsv_bulk<T, NT, NBUF><<<grid, NT, smem, st>>>(dl, d, du, b, x, off, len, list, count,
+                                                         hyd::bulk_region<T>(nmax), stalled);
   return HYDIST_OK;
+}
+
+// CTAs of the bulk-staged solver resident per SM with nbuf row buffers
+template <class T, int NT>
+int bulk_per_sm(int nmax, int nbuf, const DevInfo& D) {
+  const size_t smem = cta_smem<T, NT>(nmax, nbuf);
+  if (smem > (size_t)D.optin) return 0;
+  int per_sm = 0;
+  if (nbuf == 2) {
+    cudaFuncSetAttribute(hyd::k_gtsv_bulk<T, NT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, D.optin);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hyd::k_gtsv_bulk<T, NT, 2>, NT, smem);
+  } else {
+    cudaFuncSetAttribute(hyd::k_gtsv_bulk<T, NT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, D.optin);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hyd::k_gtsv_bulk<T, NT, 1>, NT, smem);
+  }
+  return per_sm;
+}
+
+// the CTA solver: the next system's rows are staged while one is solved
+// where the second buffer costs no resident CTA
+template <class T, int NT>
+int launch_cta(int nmax, const T* dl, const T* d, const T* du, const T* b, T* x, const int* off,
+               const int* len, const int* list, const int* count, int* stalled, int nsys_band,
+               const DevInfo& D, cudaStream_t st) {
+  if (bulk_per_sm<T, NT>(nmax, 2, D) >= std::max(1, bulk_per_sm<T, NT>(nmax, 1, D)))
+    return launch_bulk<T, NT, 2>(nmax, dl, d, du, b, x, off, len, list, count, stalled, nsys_band, D, st);
+  return launch_bulk<T, NT, 1>(nmax, dl, d, du, b, x, off, len, list, count, stalled, nsys_band, D, st);
 }
 
 template <class T>
 int launch_band(int algo, int band, const T* dl, const T* d, const T* du, const T* b, T* x, T* w,
-                const int* off, const int* len, const int* list, const int* count, int nsys_band,
-                const DevInfo& D, cudaStream_t st) {
+                const int* off, const int* len, const int* list, const int* count, int* stalled,
+                int nsys_band, const DevInfo& D, cudaStream_t st) {
   if (nsys_band <= 0) return HYDIST_OK;
   const int hi = hyd::gt_band_hi(band);
   int rc = HYDIST_OK;
   if (algo == HYDIST_GTSV_PARTITION) {
-    rc = launch_cta<T, 256>(hi, dl, d, du, b, x, off, len, list, count, nsys_band, D, st);
+    rc = launch_cta<T, 256>(hi, dl, d, du, b, x, off, len, list, count, stalled, nsys_band, D, st);
   } else if (algo == HYDIST_GTSV_PARTITION_512) {
-    rc = launch_cta<T, 512>(hi, dl, d, du, b, x, off, len, list, count, nsys_band, D, st);
+    rc = launch_cta<T, 512>(hi, dl, d, du, b, x, off, len, list, count, stalled, nsys_band, D, st);
   } else if (algo == HYDIST_GTSV_WARP) {
     const int nmax = std::min(hi, hyd::GT_WARP_MAX);
     const int slice = hyd::part_stride_bound(nmax, 32);
@@ -376,8 +626,12 @@ int ensure_scratch(DevScratch& s, size_t w_bytes, size_t nsys) {
     if (cudaMalloc(&s.lists, (size_t)GT_NB * nsys * sizeof(int)) != cudaSuccess) return HYDIST_ERR_OOM;
     s.lists_cap = nsys;
   }
-  if (!s.counts && cudaMalloc(&s.counts, (GT_NB + 2) * sizeof(int)) != cudaSuccess)
-    return HYDIST_ERR_OOM;
+  // band sizes, packed extent, offset check, and a flag that stays set
+  // until read: a CTA solver gave a system up (its staging never completed)
+  if (!s.counts) {
+    if (cudaMalloc(&s.counts, (GT_NB + 3) * sizeof(int)) != cudaSuccess) return HYDIST_ERR_OOM;
+    if (cudaMemset(s.counts, 0, (GT_NB + 3) * sizeof(int)) != cudaSuccess) return HYDIST_ERR_CUDA;
+  }
   return HYDIST_OK;
 }
 
@@ -390,12 +644,28 @@ int solve_batch(const T* dl, const T* d, const T* du, const T* b, T* x, const in
   if (cudaMemsetAsync(D.scr.counts, 0, (GT_NB + 2) * sizeof(int), st) != cudaSuccess)
     return HYDIST_ERR_CUDA;
   hyd::k_gt_classify<<<(nsys + 255) / 256, 256, 0, st>>>(off, len, nsys, D.scr.lists, D.scr.counts);
-  // band sizes, packed extent and the offset check in one synchronisation
-  int counts[GT_NB + 2];
+  // band sizes, packed extent, the offset check and the stall flag in one
+  // synchronisation
+  int counts[GT_NB + 3];
   if (cudaMemcpyAsync(counts, D.scr.counts, sizeof(counts), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return HYDIST_ERR_CUDA;
+  if (counts[GT_NB + 2]) {
+    cudaMemsetAsync(D.scr.counts + GT_NB + 2, 0, sizeof(int), st);
+    return HYDIST_ERR_TIMEOUT;
+  }
   if (counts[GT_NB + 1]) return HYDIST_ERR_ARG;
+  // the CTA solvers stage rows with bulk copies, which need 16-byte aligned
+  // arrays; misaligned ones go to Thomas
+  int tab[GT_NB];
+  const bool aligned =
+      (((uintptr_t)dl | (uintptr_t)d | (uintptr_t)du | (uintptr_t)b) & 15) == 0;
+  for (int bnd = 0; bnd < GT_NB; ++bnd)
+    tab[bnd] = (!aligned && (table[bnd] == HYDIST_GTSV_PARTITION ||
+                             table[bnd] == HYDIST_GTSV_PARTITION_512))
+                   ? HYDIST_GTSV_THOMAS
+                   : table[bnd];
+  table = tab;
   bool thomas = false;
   for (int bnd = 0; bnd < GT_NB; ++bnd) thomas |= counts[bnd] > 0 && table[bnd] == HYDIST_GTSV_THOMAS;
   if (thomas) {
@@ -404,7 +674,8 @@ int solve_batch(const T* dl, const T* d, const T* du, const T* b, T* x, const in
   }
   for (int bnd = 0; bnd < GT_NB; ++bnd) {
     rc = launch_band<T>(table[bnd], bnd, dl, d, du, b, x, (T*)D.scr.w, off, len,
-                        D.scr.lists + (size_t)bnd * nsys, D.scr.counts + bnd, counts[bnd], D, st);
+                        D.scr.lists + (size_t)bnd * nsys, D.scr.counts + bnd,
+                        D.scr.counts + GT_NB + 2, counts[bnd], D, st);
     if (rc != HYDIST_OK) return rc;
   }
   return HYDIST_OK;
@@ -558,6 +829,9 @@ extern "C" int hydist_gtsv_batched(const void* dl, const void* d, const void* du
                             (float*)x, offsets, lengths, nsys, table, *D, st);
   }
   if (rc == HYDIST_ERR_ARG) hyd::set_last_error("hydist_gtsv_batched: a system has a negative offset");
+  else if (rc == HYDIST_ERR_TIMEOUT)
+    hyd::set_last_error("hydist_gtsv_batched: a previous batch gave a system up (its rows never "
+                        "arrived in shared memory); this batch was not solved");
   else if (rc != HYDIST_OK) hyd::set_last_error("hydist_gtsv_batched: a CUDA call failed");
   return rc;
 }
