@@ -413,9 +413,9 @@ int bulk_private(HydistHandle* h, StateT<R>& B) {
   B.lslots = 2 * nsm;
   const size_t U = (size_t)2 * std::max(S.M, S.N);
   // at least 4 (max(M,N)+3) doubles: preprocess_data borrows it as FP64;
-  // the refined FP32 form keeps 8 values per unknown (its refinement stores
-  // the rows and the pivot reciprocals)
-  const size_t arrays = S.refine ? 8 : 3;
+  // the refined FP32 form keeps 7 values per unknown (its refinement stores
+  // the rows)
+  const size_t arrays = S.refine ? 7 : 3;
   TRY(dalloc(h, &B.lscratch, std::max((size_t)B.lslots * arrays * U * 4, 8 * U + 64)));
   return HYDIST_OK;
 }

@@ -61,6 +61,16 @@ struct LSShared {
 template <class R>
 __device__ __forceinline__ R rcp(R x) { return R(1) / x; }
 
+// PCR levels for P separators per line
+constexpr int pcr_levels(int P) { return P <= 1 ? 0 : 1 + pcr_levels(P / 2); }
+
+// dynamic shared memory of one CTA: LSShared, and with refinement the PCR
+// multipliers
+template <class R, int P>
+constexpr size_t line_smem(bool refine) {
+  return sizeof(LSShared<R, P>) + (refine ? (size_t)2 * pcr_levels(P) * P * LPB * sizeof(R) : 0);
+}
+
 // Gen::MIN_BLOCKS: resident CTAs per SM the P = 128 solver is compiled for
 // (2 caps registers at 64 per thread).
 template <class Gen, int P>
@@ -68,13 +78,15 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
   using R = typename Gen::Real;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   LSShared<R, P>& sh = *reinterpret_cast<LSShared<R, P>*>(smem_raw);
+  // with refinement: the PCR multipliers, 2 per level per thread
+  constexpr int PL = P * LPB;
+  R* pm = reinterpret_cast<R*>(smem_raw + sizeof(LSShared<R, P>));
   const int tid = threadIdx.x;
   const int l = tid % LPB, k = tid / LPB;
   const int cidx = k * LPB + l;
   const int U = G.unknowns_per_line();
   // scratch slot of this CTA: c', y', v' per unknown, and with refinement
-  // also the rows A, B, C, D and the pivot reciprocals (Gen::SCRATCH_ARRAYS
-  // arrays of U x LPB)
+  // also the rows A, B, C, D (Gen::SCRATCH_ARRAYS arrays of U x LPB)
   const size_t UL = (size_t)U * LPB;
   R* scr = G.scratch + (size_t)blockIdx.x * Gen::SCRATCH_ARRAYS * UL;
   R* sc_c = scr;
@@ -113,13 +125,6 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
         for (int e = 0; e < Gen::UPC; ++e, ++s) {
           R A, B, C, D;
           W.row(G, LS, e, A, B, C, D);
-          if constexpr (Gen::REFINE) {
-            const size_t o = (size_t)(q0 + s) * LPB + l;
-            scr[3 * UL + o] = A;
-            scr[4 * UL + o] = B;
-            scr[5 * UL + o] = C;
-            scr[6 * UL + o] = D;
-          }
           if (s == nu - 1) {
             sh.sep[0][cidx] = A;
             sh.sep[1][cidx] = B;
@@ -139,8 +144,13 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
               cp = C * m;
             }
             const size_t o = (size_t)(q0 + s) * LPB + l;
-            // the refinement's correction reuses the pivot reciprocals
-            if constexpr (Gen::REFINE) scr[7 * UL + o] = m;
+            if constexpr (Gen::REFINE) {
+              // the interior rows, for the residual
+              scr[3 * UL + o] = A;
+              scr[4 * UL + o] = B;
+              scr[5 * UL + o] = C;
+              scr[6 * UL + o] = D;
+            }
             sc_c[o] = cp;
             sc_y[o] = yp;
             sc_v[o] = vp;
@@ -177,8 +187,9 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
       rc = cs * wF;
       rd = ds - as * yL - cs * yF;
     }
-    // parallel cyclic reduction
-    for (int st = 1; st < P; st <<= 1) {
+    // parallel cyclic reduction (the refinement keeps each level's
+    // multipliers for its correction)
+    for (int st = 1, lvl = 0; st < P; st <<= 1, ++lvl) {
       sh.red[0][cidx] = ra;
       sh.red[1][cidx] = rb;
       sh.red[2][cidx] = rc;
@@ -201,6 +212,10 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
       }
       __syncthreads();
       const R k1 = ra / bm, k2 = rc / bn;
+      if constexpr (Gen::REFINE) {
+        pm[(2 * lvl) * PL + cidx] = k1;
+        pm[(2 * lvl + 1) * PL + cidx] = k2;
+      }
       const R na = -am * k1, nc = -cn * k2;
       const R nb = rb - cm * k1 - an * k2;
       const R nd = rd - dm * k1 - dn * k2;
@@ -227,131 +242,100 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
         xn = x;
       }
     } else {
-      // the first solution x goes over y'; then one refinement pass:
-      // r = D - A x_{-1} - B x - C x_{+1} in FP64 with the stored rows,
-      // A d = r with the same elimination (c', the stored pivot reciprocals,
-      // v', the reduced matrix), x + d emitted
+      // one refinement pass. The back substitution stores x over y' and, as
+      // soon as x_{t-1..t+1} are known, takes row t's residual
+      // r = D - A x_{t-1} - B x_t - C x_{t+1} in FP64 from the stored rows
+      // and eliminates the correction system A d = r backward through it:
+      // d_t = h_t - a_t d_{t-1} - w_t d_R (d_R the chunk's separator), the
+      // (a, h, w) over the rows' A, D, C. The separators' correction solves
+      // the same Schur complement as pass A, so the reduction reuses pass
+      // A's PCR multipliers; the chunk interiors are then substituted
+      // forward and x + d is emitted in FP64.
       R* sA = scr + 3 * UL;
       R* sB = scr + 4 * UL;
       R* sC = scr + 5 * UL;
       R* sD = scr + 6 * UL;
-      const R* sM = scr + 7 * UL;
-      auto resid = [&](size_t o, R xm, R x, R xp) {
-        return (R)((double)sD[o] - (double)sA[o] * (double)xm - (double)sB[o] * (double)x -
-                   (double)sC[o] * (double)xp);
-      };
+      const R xr = sh.xsep[cidx];
+      const R xl = (k > 0) ? sh.xsep[cidx - LPB] : R(0);
       R x_before_sep = 0;  // x of the chunk's last interior unknown
+      R ha = 0, hy = 0, hw = -1;  // (a, h, w) of the row below the one eliminated
+      R gy = 0, gw = 0, Q = 1;    // d of the last interior unknown: gy - gw d_R + Q d_L
+      auto eliminate = [&](size_t o, R xm, R x, R xp) {
+        const R A = sA[o], B = sB[o], C = sC[o];
+        const R r = (R)((double)sD[o] - (double)A * (double)xm - (double)B * (double)x -
+                        (double)C * (double)xp);
+        const R m = rcp(B - C * ha);
+        ha = A * m;
+        hy = (r - C * hy) * m;
+        hw = -C * hw * m;
+        sA[o] = ha;
+        sD[o] = hy;
+        sC[o] = hw;
+        gy += Q * hy;
+        gw += Q * hw;
+        Q *= -ha;
+      };
       {
-        // back substitution; each interior unknown's residual as soon as the
-        // unknown before it is known (the separator's needs the next chunk)
-        const R xr = sh.xsep[cidx];
-        const R xl = (k > 0) ? sh.xsep[cidx - LPB] : R(0);
-        sc_y[(size_t)(q0 + nu - 1) * LPB + l] = xr;
         R x1 = xr, x2 = 0;  // x_{t+1}, x_{t+2}
         for (int t = nu - 2; t >= 0; --t) {
           const size_t o = (size_t)(q0 + t) * LPB + l;
           const R x = sc_y[o] + sc_v[o] * xl - sc_c[o] * x1;
           sc_y[o] = x;
           if (t == nu - 2) x_before_sep = x;
-          else sD[o + LPB] = resid(o + LPB, x, x1, x2);
+          else eliminate(o + LPB, x, x1, x2);
           x2 = x1;
           x1 = x;
         }
         // the first unknown: its left neighbour is the previous separator
         // (none at the line's start)
-        const size_t o0 = (size_t)q0 * LPB + l;
-        if (nu >= 2) sD[o0] = resid(o0, q0 > 0 ? xl : R(0), x1, x2);
+        if (nu >= 2) eliminate((size_t)q0 * LPB + l, q0 > 0 ? xl : R(0), x1, x2);
       }
+      // the first interior unknown's constant term, for the previous chunk
+      sh.tri[0][cidx] = hy;
       __syncthreads();
-      {
+      R rd2 = 0;
+      if (nu >= 1) {
         // the separator row: its right neighbour is the next chunk's first
         // unknown (none at the line's end)
         const int q = q0 + nu - 1;
         const size_t o = (size_t)q * LPB + l;
         const R xm = nu >= 2 ? x_before_sep : (q > 0 ? sc_y[o - LPB] : R(0));
         const R xp = q + 1 < U ? sc_y[o + LPB] : R(0);
-        sD[o] = resid(o, xm, sc_y[o], xp);
+        const R as = sh.sep[0][cidx], bs = sh.sep[1][cidx], cs = sh.sep[2][cidx],
+                ds = sh.sep[3][cidx];
+        const R rs = (R)((double)ds - (double)as * (double)xm - (double)bs * (double)xr -
+                         (double)cs * (double)xp);
+        const R hF = (k + 1 < P) ? sh.tri[0][cidx + LPB] : R(0);
+        rd2 = rs - as * gy - cs * hF;
       }
-      // forward elimination of the residual (y'' over D)
-      R fy = 0, yL = 0, Pk = 1, cp = 0;
-      for (int t = 0; t < nu - 1; ++t) {
-        const size_t o = (size_t)(q0 + t) * LPB + l;
-        const R y = (sD[o] - (t == 0 ? R(0) : sA[o] * yL)) * sM[o];
-        sD[o] = y;
-        cp = sc_c[o];
-        fy += Pk * y;
-        Pk *= -cp;
-        yL = y;
-      }
-      sh.tri[0][cidx] = fy;
-      sh.tri[3][cidx] = yL;
-      __syncthreads();
-      R ra2, rb2, rc2, rd2;
+      // the reduction with pass A's multipliers (one barrier per level: the
+      // levels alternate between two buffers)
       {
-        const R as = sh.sep[0][cidx], bs = sh.sep[1][cidx], cs = sh.sep[2][cidx];
-        const R ds = sD[(size_t)(q0 + nu - 1) * LPB + l];
-        const R vL = sh.tri[4][cidx], wL = sh.tri[5][cidx];
-        R yF = 0, vF = 0, wF = 0;
-        if (k + 1 < P) {
-          const int n1 = cidx + LPB;
-          yF = sh.tri[0][n1];
-          vF = sh.tri[1][n1];
-          wF = sh.tri[2][n1];
+        int lvl = 0;
+        for (int st = 1; st < P; st <<= 1, ++lvl) {
+          R* buf = sh.red[lvl & 1];
+          buf[cidx] = rd2;
+          __syncthreads();
+          const R dm = (k - st >= 0) ? buf[cidx - st * LPB] : R(0);
+          const R dn = (k + st < P) ? buf[cidx + st * LPB] : R(0);
+          rd2 = rd2 - dm * pm[(2 * lvl) * PL + cidx] - dn * pm[(2 * lvl + 1) * PL + cidx];
         }
-        ra2 = as * vL;
-        rb2 = bs + as * wL + cs * vF;
-        rc2 = cs * wF;
-        rd2 = ds - as * yL - cs * yF;
       }
-      for (int st = 1; st < P; st <<= 1) {
-        sh.red[0][cidx] = ra2;
-        sh.red[1][cidx] = rb2;
-        sh.red[2][cidx] = rc2;
-        sh.red[3][cidx] = rd2;
-        __syncthreads();
-        R am = 0, bm = 1, cm = 0, dm = 0, an = 0, bn = 1, cn = 0, dn = 0;
-        if (k - st >= 0) {
-          const int o = cidx - st * LPB;
-          am = sh.red[0][o];
-          bm = sh.red[1][o];
-          cm = sh.red[2][o];
-          dm = sh.red[3][o];
-        }
-        if (k + st < P) {
-          const int o = cidx + st * LPB;
-          an = sh.red[0][o];
-          bn = sh.red[1][o];
-          cn = sh.red[2][o];
-          dn = sh.red[3][o];
-        }
-        __syncthreads();
-        const R k1 = ra2 / bm, k2 = rc2 / bn;
-        const R na = -am * k1, nc = -cn * k2;
-        const R nb = rb2 - cm * k1 - an * k2;
-        const R nd = rd2 - dm * k1 - dn * k2;
-        ra2 = na;
-        rb2 = nb;
-        rc2 = nc;
-        rd2 = nd;
-      }
-      sh.xsep[cidx] = rd2 / rb2;
+      const R dr = rd2 / rb;
+      sh.xsep[cidx] = dr;
       __syncthreads();
       {
-        const R dr = sh.xsep[cidx];
         const R dl = (k > 0) ? sh.xsep[cidx - LPB] : R(0);
         typename Gen::Emitter E;
-        E.init(G, LS, line);
-        {
-          const size_t o = (size_t)(q0 + nu - 1) * LPB + l;
-          E.emit(G, LS, sh.xlast[l], q0 + nu - 1, (double)sc_y[o] + (double)dr);
-        }
-        R dn = dr;
-        for (int t = nu - 2; t >= 0; --t) {
+        E.init_fwd(G, LS, line);
+        R dp = dl;
+        for (int t = 0; t <= nu - 2; ++t) {
           const size_t o = (size_t)(q0 + t) * LPB + l;
-          const R d = sD[o] + sc_v[o] * dl - sc_c[o] * dn;
-          E.emit(G, LS, sh.xlast[l], q0 + t, (double)sc_y[o] + (double)d);
-          dn = d;
+          const R d = sD[o] - sA[o] * dp - sC[o] * dr;
+          E.template emit<true>(G, LS, sh.xlast[l], q0 + t, (double)sc_y[o] + (double)d);
+          dp = d;
         }
+        if (nu >= 1) E.template emit<true>(G, LS, sh.xlast[l], q0 + nu - 1, (double)xr + (double)dr);
       }
     }
     __syncthreads();

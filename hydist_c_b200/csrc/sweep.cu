@@ -26,11 +26,12 @@ template <int DIR, class R, bool REF = false>
 struct HydroGen {
   using Real = R;
   static constexpr bool REFINE = REF;
-  static constexpr int SCRATCH_ARRAYS = REFINE ? 8 : 3;
+  static constexpr int SCRATCH_ARRAYS = REFINE ? 7 : 3;
   static constexpr int UPC = 2;
   // x sweeps (columns, 4 adjacent per warp) run faster with two CTAs per SM
-  // despite the register cap; y sweeps (rows) slower
-  static constexpr int MIN_BLOCKS = DIR == 0 ? 2 : 1;
+  // despite the register cap, and so do the FP32 y sweeps; the FP64 and the
+  // refined FP32 y sweeps slower
+  static constexpr int MIN_BLOCKS = (DIR == 0 || (sizeof(R) == 4 && !REF)) ? 2 : 1;
   StateT<R> S;
   CoefT<R> c;
   R* scratch;
@@ -174,15 +175,25 @@ struct HydroGen {
   };
 
   // Writes each solved unknown to t_z / t_u (t_v) as the extraction does.
+  // FWD: the unknowns come in increasing order (init_fwd), else decreasing.
   struct Emitter {
     int lp, si;
     __device__ void init(const HydroGen& G, const LineSeg& LS, int line) {
       lp = line + 2;
       si = LS.nseg - 1;
     }
+    __device__ void init_fwd(const HydroGen& G, const LineSeg& LS, int line) {
+      lp = line + 2;
+      si = -1;
+    }
+    template <bool FWD = false>
     __device__ void emit(const HydroGen& G, const LineSeg& LS, double* xlast, int q, double x) {
       const int r = q + 4, pos = r >> 1;
-      while (si >= 0 && LS.s[si].first > pos) --si;
+      if constexpr (FWD) {
+        while (si + 1 < LS.nseg && LS.s[si + 1].first <= pos) ++si;
+      } else {
+        while (si >= 0 && LS.s[si].first > pos) --si;
+      }
       if (si < 0) return;
       const SegD& d = LS.s[si];
       if (pos > d.last || r < d.off || r > d.rend) return;
@@ -242,7 +253,7 @@ struct HydroGen {
 
 template <class Gen, int P>
 static void launch_gen(const Gen& G, cudaStream_t st, int grid) {
-  const size_t smem = sizeof(LSShared<typename Gen::Real, P>);
+  const size_t smem = line_smem<typename Gen::Real, P>(Gen::REFINE);
   static bool attr[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -281,9 +292,10 @@ template <int DIR, class R, bool REF = false>
 struct FSGen {
   using Real = R;
   static constexpr bool REFINE = REF;
-  static constexpr int SCRATCH_ARRAYS = REFINE ? 8 : 3;
+  static constexpr int SCRATCH_ARRAYS = REFINE ? 7 : 3;
   static constexpr int UPC = 1;
-  static constexpr int MIN_BLOCKS = DIR == 0 ? 2 : 1;
+  // two CTAs per SM but for the FP64 y sweep
+  static constexpr int MIN_BLOCKS = (DIR == 0 || sizeof(R) == 4) ? 2 : 1;
   StateT<R> S;
   CoefT<R> c;
   R* scratch;
@@ -387,15 +399,25 @@ struct FSGen {
     }
   };
 
+  // FWD: the unknowns come in increasing order (init_fwd), else decreasing.
   struct Emitter {
     int lp, si;
     __device__ void init(const FSGen& G, const LineSeg& LS, int line) {
       lp = line + 3;
       si = LS.nseg - 1;
     }
+    __device__ void init_fwd(const FSGen& G, const LineSeg& LS, int line) {
+      lp = line + 3;
+      si = -1;
+    }
+    template <bool FWD = false>
     __device__ void emit(const FSGen& G, const LineSeg& LS, double* xlast, int q, double x) {
       const int pos = q + 2;
-      while (si >= 0 && LS.s[si].first > pos) --si;
+      if constexpr (FWD) {
+        while (si + 1 < LS.nseg && LS.s[si + 1].first <= pos) ++si;
+      } else {
+        while (si >= 0 && LS.s[si].first > pos) --si;
+      }
       if (si < 0) return;
       const SegD& d = LS.s[si];
       if (pos < d.off || pos > d.rend) return;
