@@ -114,7 +114,8 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
     {
       typename Gen::Walker W;
       W.init(G, LS, line, c0);
-      R cp = 0, yp = 0, vp = 0;
+      // (with no interior row, the unknown left of the separator is x_L)
+      R cp = 0, yp = 0, vp = 1;
       // first interior row in terms of both separators, accumulated forward:
       // x_0 = sum_k P_k (y'_k + v'_k x_L) + P_L x_R, P_0 = 1, P_{k+1} = -c'_k P_k
       R Pk = 1, fy = 0, fv = 0;

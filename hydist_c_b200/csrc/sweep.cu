@@ -14,10 +14,14 @@
 
 namespace hyd {
 
-// chunks per line: as many as keep at least `min_cells` cells per chunk
+// chunks per line: as many as keep at least `min_cells` cells per chunk (of
+// 128, 64, 32, 16, 4 or 1), so that no chunk of a short line is empty or
+// holds its separator alone
 int line_chunks(int ncells, int min_cells) {
   int P = 128;
-  while (P > 16 && ncells < P * min_cells) P >>= 1;
+  while (P > 1 && ncells < P * min_cells) P >>= 1;
+  if (P == 8) P = 4;
+  if (P == 2) P = 1;
   return P;
 }
 
@@ -270,7 +274,9 @@ static void launch_any(const Gen& G, int P, cudaStream_t st, int grid) {
   if (P == 128) launch_gen<Gen, 128>(G, st, grid);
   else if (P == 64) launch_gen<Gen, 64>(G, st, grid);
   else if (P == 32) launch_gen<Gen, 32>(G, st, grid);
-  else launch_gen<Gen, 16>(G, st, grid);
+  else if (P == 16) launch_gen<Gen, 16>(G, st, grid);
+  else if (P == 4) launch_gen<Gen, 4>(G, st, grid);
+  else launch_gen<Gen, 1>(G, st, grid);
 }
 
 template <int DIR, class R, bool REF>

@@ -291,3 +291,21 @@ def test_bed_change(hyd, oracle_mod):
     sim.sync()
     bad = _compare(sim, orc, ["u", "v", "z", "FS", "dH"], 1e-8)
     assert not bad, bad
+
+
+@pytest.mark.parametrize("N,M,inflow", [(8, 8, 5.0), (10, 9, 5.0), (20, 12, 50.0), (40, 24, 200.0)])
+def test_short_lines_match_oracle(hyd, oracle_mod, N, M, inflow):
+    """Meshes whose lines are shorter than 64 cells take fewer chunks per
+    line (4 or 1), so that every chunk of the partitioned solver holds at
+    least four cells; the hydraulic and concentration sweeps agree with the
+    oracle there as on long lines."""
+    b = S.make_channel(N=N, M=M, seed=20267000 + N, dx=10.0, dt=2.0, hours=1.0, sediment=True,
+                       sediment_start=4.0, n_bumps=2, inflow=inflow)
+    sim = hyd.Simulation(b)
+    orc = oracle_mod.OracleSim(b)
+    sim.step(10)
+    orc.step(10)
+    sim.sync()
+    assert np.abs(orc.get("FS") - orc.get("FS").flat[0]).max() > 0
+    bad = _compare(sim, orc, ["u", "v", "z", "t_u", "t_v", "t_z", "FS"], 1e-10)
+    assert not bad, bad
