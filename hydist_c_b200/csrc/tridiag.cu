@@ -27,7 +27,9 @@
 
 #include <climits>
 #include <cmath>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -524,21 +526,34 @@ int default_algo(int band, const Caps& c) {
   return HYDIST_GTSV_THOMAS;
 }
 
+// Resident CTAs per SM of `kernel` with NT threads and `smem` bytes of
+// dynamic shared memory on the current device, its shared-memory limit
+// raised to the opt-in maximum; queried once per (device, kernel, smem),
+// since a batched solve launches the same few configurations every call.
+template <class K>
+int resident_ctas(K kernel, int nt, size_t smem, int optin) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, const void*, size_t>, int> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, (const void*)kernel, smem);
+  std::lock_guard<std::mutex> lk(mu);
+  const auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int per_sm = 0;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, nt, smem) != cudaSuccess)
+    return 0;
+  cache[key] = per_sm;
+  return per_sm;
+}
+
 template <class T, int NT, int NBUF>
 int launch_bulk(int nmax, const T* dl, const T* d, const T* du, const T* b, T* x, const int* off,
                 const int* len, const int* list, const int* count, int* stalled, int nsys_band,
                 const DevInfo& D, cudaStream_t st) {
   const size_t smem = cta_smem<T, NT>(nmax, NBUF);
-  static bool attr[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!attr[dev]) {
-    cudaFuncSetAttribute(hyd::k_gtsv_bulk<T, NT, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         D.optin);
-    attr[dev] = true;
-  }
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hyd::k_gtsv_bulk<T, NT, NBUF>, NT, smem);
+  const int per_sm = resident_ctas(hyd::k_gtsv_bulk<T, NT, NBUF>, NT, smem, D.optin);
   if (per_sm < 1) return HYDIST_ERR_CUDA;
   const int grid = std::min(nsys_band, per_sm * D.nsm);
   hyd::k_gtsv_bulk<T, NT, NBUF><<<grid, NT, smem, st>>>(dl, d, du, b, x, off, len, list, count,
@@ -551,15 +566,8 @@ template <class T, int NT>
 int bulk_per_sm(int nmax, int nbuf, const DevInfo& D) {
   const size_t smem = cta_smem<T, NT>(nmax, nbuf);
   if (smem > (size_t)D.optin) return 0;
-  int per_sm = 0;
-  if (nbuf == 2) {
-    cudaFuncSetAttribute(hyd::k_gtsv_bulk<T, NT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, D.optin);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hyd::k_gtsv_bulk<T, NT, 2>, NT, smem);
-  } else {
-    cudaFuncSetAttribute(hyd::k_gtsv_bulk<T, NT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, D.optin);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hyd::k_gtsv_bulk<T, NT, 1>, NT, smem);
-  }
-  return per_sm;
+  return nbuf == 2 ? resident_ctas(hyd::k_gtsv_bulk<T, NT, 2>, NT, smem, D.optin)
+                   : resident_ctas(hyd::k_gtsv_bulk<T, NT, 1>, NT, smem, D.optin);
 }
 
 // the CTA solver: the next system's rows are staged while one is solved
@@ -588,16 +596,7 @@ int launch_band(int algo, int band, const T* dl, const T* d, const T* du, const 
     const int nmax = std::min(hi, hyd::GT_WARP_MAX);
     const int slice = hyd::part_stride_bound(nmax, 32);
     const size_t smem = warp_smem<T>(nmax);
-    static bool attr[64][2] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!attr[dev][sizeof(T) == 4]) {
-      cudaFuncSetAttribute(hyd::k_gtsv_warp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, D.optin);
-      attr[dev][sizeof(T) == 4] = true;
-    }
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hyd::k_gtsv_warp<T>, hyd::GT_WARPS * 32,
-                                                  smem);
+    const int per_sm = resident_ctas(hyd::k_gtsv_warp<T>, hyd::GT_WARPS * 32, smem, D.optin);
     if (per_sm < 1) return HYDIST_ERR_CUDA;
     const int grid = std::min((nsys_band + hyd::GT_WARPS - 1) / hyd::GT_WARPS, per_sm * D.nsm);
     hyd::k_gtsv_warp<T><<<grid, hyd::GT_WARPS * 32, smem, st>>>(dl, d, du, b, x, off, len, list,
