@@ -254,7 +254,8 @@ EXPORTED_SYMBOLS = [
     "hydist_server_status", "hydist_server_counts", "hydist_server_handle",
     "hydist_server_release", "hydist_checkpoint_save", "hydist_checkpoint_load",
 ]
-GTSV_AUTO, GTSV_THOMAS, GTSV_PARTITION, GTSV_WARP, GTSV_PARTITION_512 = 0, 1, 2, 3, 4
+GTSV_AUTO, GTSV_THOMAS, GTSV_PARTITION, GTSV_WARP, GTSV_PARTITION_512, GTSV_PARTITION_128 = \
+    0, 1, 2, 3, 4, 5
 GTSV_BANDS = 7
 
 PHASES = ["boundary_x", "sweep_x", "explicit_v", "commit_x", "sediment_x",

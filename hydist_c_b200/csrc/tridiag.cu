@@ -499,12 +499,12 @@ int cta_max_rows(const DevInfo& D) {
 }
 
 struct Caps {
-  int cta256, cta512;  // longest systems of the two CTA tiles
+  int cta128, cta256, cta512;  // longest systems of the three CTA tiles
 };
 
 template <class T>
 Caps caps_of(const DevInfo& D) {
-  return Caps{cta_max_rows<T, 256>(D), cta_max_rows<T, 512>(D)};
+  return Caps{cta_max_rows<T, 128>(D), cta_max_rows<T, 256>(D), cta_max_rows<T, 512>(D)};
 }
 
 bool feasible(int algo, int band, const Caps& c) {
@@ -513,6 +513,7 @@ bool feasible(int algo, int band, const Caps& c) {
   if (algo == HYDIST_GTSV_WARP) return hi <= hyd::GT_WARP_MAX;
   if (algo == HYDIST_GTSV_PARTITION) return hi <= c.cta256;
   if (algo == HYDIST_GTSV_PARTITION_512) return hi <= c.cta512;
+  if (algo == HYDIST_GTSV_PARTITION_128) return hi <= c.cta128;
   return false;
 }
 
@@ -588,7 +589,9 @@ int launch_band(int algo, int band, const T* dl, const T* d, const T* du, const 
   if (nsys_band <= 0) return HYDIST_OK;
   const int hi = hyd::gt_band_hi(band);
   int rc = HYDIST_OK;
-  if (algo == HYDIST_GTSV_PARTITION) {
+  if (algo == HYDIST_GTSV_PARTITION_128) {
+    rc = launch_cta<T, 128>(hi, dl, d, du, b, x, off, len, list, count, stalled, nsys_band, D, st);
+  } else if (algo == HYDIST_GTSV_PARTITION) {
     rc = launch_cta<T, 256>(hi, dl, d, du, b, x, off, len, list, count, stalled, nsys_band, D, st);
   } else if (algo == HYDIST_GTSV_PARTITION_512) {
     rc = launch_cta<T, 512>(hi, dl, d, du, b, x, off, len, list, count, stalled, nsys_band, D, st);
@@ -661,7 +664,8 @@ int solve_batch(const T* dl, const T* d, const T* du, const T* b, T* x, const in
       (((uintptr_t)dl | (uintptr_t)d | (uintptr_t)du | (uintptr_t)b) & 15) == 0;
   for (int bnd = 0; bnd < GT_NB; ++bnd)
     tab[bnd] = (!aligned && (table[bnd] == HYDIST_GTSV_PARTITION ||
-                             table[bnd] == HYDIST_GTSV_PARTITION_512))
+                             table[bnd] == HYDIST_GTSV_PARTITION_512 ||
+                             table[bnd] == HYDIST_GTSV_PARTITION_128))
                    ? HYDIST_GTSV_THOMAS
                    : table[bnd];
   table = tab;
@@ -684,9 +688,9 @@ template <class T>
 int autotune(DevInfo& D, int dtype, cudaStream_t st) {
   const Caps caps = caps_of<T>(D);
   for (int bnd = 0; bnd < GT_NB; ++bnd) {
-    int cands[4], nc = 0;
+    int cands[5], nc = 0;
     for (int a : {HYDIST_GTSV_THOMAS, HYDIST_GTSV_PARTITION, HYDIST_GTSV_PARTITION_512,
-                  HYDIST_GTSV_WARP})
+                  HYDIST_GTSV_WARP, HYDIST_GTSV_PARTITION_128})
       if (feasible(a, bnd, caps)) cands[nc++] = a;
     if (nc == 1) {
       D.table[dtype][bnd] = cands[0];
@@ -796,7 +800,7 @@ extern "C" int hydist_gtsv_batched(const void* dl, const void* d, const void* du
     hyd::set_last_error("hydist_gtsv_batched: dtype must be 0 (FP64) or 1 (FP32)");
     return HYDIST_ERR_ARG;
   }
-  if (algo < HYDIST_GTSV_AUTO || algo > HYDIST_GTSV_PARTITION_512) {
+  if (algo < HYDIST_GTSV_AUTO || algo > HYDIST_GTSV_PARTITION_128) {
     hyd::set_last_error("hydist_gtsv_batched: unknown algo");
     return HYDIST_ERR_ARG;
   }
@@ -814,6 +818,7 @@ extern "C" int hydist_gtsv_batched(const void* dl, const void* d, const void* du
     if (a == HYDIST_GTSV_AUTO) a = D->table[dtype][bnd] ? D->table[dtype][bnd] : default_algo(bnd, caps);
     // a solver that cannot take the band's lengths hands it to the next
     // more general one: warp -> 512-thread tile -> 256-thread tile -> Thomas
+    if (a == HYDIST_GTSV_PARTITION_128 && !feasible(a, bnd, caps)) a = HYDIST_GTSV_PARTITION;
     if (a == HYDIST_GTSV_WARP && !feasible(a, bnd, caps)) a = HYDIST_GTSV_PARTITION_512;
     if (a == HYDIST_GTSV_PARTITION_512 && !feasible(a, bnd, caps)) a = HYDIST_GTSV_PARTITION;
     if (a == HYDIST_GTSV_PARTITION && !feasible(a, bnd, caps)) a = HYDIST_GTSV_THOMAS;

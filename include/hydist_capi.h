@@ -328,7 +328,10 @@ int hydist_kernel_launches(HydistHandle* h, int64_t* count);
  *   PARTITION_512  PARTITION with 512-thread tiles (more warps per system,
  *              less shared memory left for long systems).
  * A solver that cannot take a band's lengths passes it on (WARP ->
- * PARTITION_512 -> PARTITION -> THOMAS). Systems of length 0 are skipped.
+ * PARTITION_512 -> PARTITION -> THOMAS; PARTITION_128 -> PARTITION).
+ * PARTITION_128, PARTITION and PARTITION_512 are the same CTA partition
+ * solver on 128, 256 or 512 threads per system: fewer threads give each
+ * thread a longer chunk and the separators a shorter reduction. Systems of length 0 are skipped.
  * No pivoting: the systems are expected to be diagonally dominant, as the
  * ADI sweeps' are.
  * stream is a cudaStream_t (NULL = default stream). Scratch is allocated by
@@ -340,7 +343,8 @@ enum HydistGtsvAlgo {
   HYDIST_GTSV_THOMAS = 1,
   HYDIST_GTSV_PARTITION = 2,
   HYDIST_GTSV_WARP = 3,
-  HYDIST_GTSV_PARTITION_512 = 4
+  HYDIST_GTSV_PARTITION_512 = 4,
+  HYDIST_GTSV_PARTITION_128 = 5
 };
 int hydist_gtsv_batched(const void* dl, const void* d, const void* du,
                         const void* b, void* x, const int32_t* offsets,

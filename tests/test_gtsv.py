@@ -14,7 +14,7 @@ from hydist_c_b200 import capi
 EDGE_LENGTHS = [0, 1, 2, 3, 4, 31, 32, 33, 127, 128, 129, 511, 512, 513, 2047, 2048, 2049,
                 4095, 4096, 4097, 6144, 6145, 9000]
 ALGOS = [capi.GTSV_AUTO, capi.GTSV_THOMAS, capi.GTSV_PARTITION, capi.GTSV_WARP,
-         capi.GTSV_PARTITION_512]
+         capi.GTSV_PARTITION_512, capi.GTSV_PARTITION_128]
 
 
 def _batch(seed, nsys=600):
@@ -76,7 +76,7 @@ def test_autotune_then_auto(hyd, oracle_mod, dtype):
     capi.check(lib, st, "hydist_gtsv_autotune")
     table = list(table)
     assert all(v in (capi.GTSV_THOMAS, capi.GTSV_PARTITION, capi.GTSV_WARP,
-                    capi.GTSV_PARTITION_512) for v in table), table
+                    capi.GTSV_PARTITION_512, capi.GTSV_PARTITION_128) for v in table), table
     assert table[-1] == capi.GTSV_THOMAS  # the open band fits no shared memory
     a, d, c, b, off, ln = _batch(13, nsys=300)
     ref = oracle_mod.thomas_batched(a, d, c, b, off, ln)
