@@ -732,9 +732,9 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
   if (tr) tr->mark(st, PH_BOUNDARY_X, 2);
   if (tr) tr->kbegin(st, KS_SWEEP_X);
-  launch_sweep(S, c, 0, st);
+  const int nx = launch_sweep(S, c, 0, st);
   if (tr) tr->kend(st, KS_SWEEP_X);
-  if (tr) tr->mark(st, PH_SWEEP_X, 1);
+  if (tr) tr->mark(st, PH_SWEEP_X, nx);
   // smoothing of t_u into su, explicit v from it, margins, smoothing of t_v
   // into sv; k_commit_a writes both back (Normalize/update_buffer pairs,
   // engine.cpp:109-124)
@@ -759,9 +759,9 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
   if (tr) tr->mark(st, PH_BOUNDARY_Y, 2);
   if (tr) tr->kbegin(st, KS_SWEEP_Y);
-  launch_sweep(S, c, 1, st);
+  const int ny = launch_sweep(S, c, 1, st);
   if (tr) tr->kend(st, KS_SWEEP_Y);
-  if (tr) tr->mark(st, PH_SWEEP_Y, 1);
+  if (tr) tr->mark(st, PH_SWEEP_Y, ny);
   k_smooth_full<<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c, 0, 0);
   k_solve_u<<<grid2(S.M - 1, S.N, 128), 128, 0, st>>>(S, c);
   k_margin_u<<<cdiv(S.M - 1, 128), 128, 0, st>>>(S, c);

@@ -40,11 +40,11 @@ template <class R>
 void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr);
 // partitioned hydraulic line sweep: dir 0 = x (columns), 1 = y (rows)
 template <class R>
-void launch_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t st);
+int launch_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t st);
 // partitioned concentration line sweep: dir 0 = i-sweep (columns), 1 = rows;
 // the erosion source is on from s_start
 template <class R>
-void launch_fs_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, double s_start, cudaStream_t st);
+int launch_fs_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, double s_start, cudaStream_t st);
 // concentration step (after a half-step launched with sed): xdir = the
 // i-sweep after half-step A; bed: the bed change after the j-sweep
 template <class R>

@@ -1,10 +1,10 @@
 // linesolve.cuh -- partitioned tridiagonal line solver for the ADI sweeps.
 //
-// One CTA solves LPB = 4 adjacent lines at a time (a persistent loop walks
-// the line groups). Each line is split into P chunks of consecutive cells;
-// thread (chunk k, line l) = threadIdx.x = k*LPB + l, so a warp covers 8
-// chunks x 4 adjacent lines and every global access of the x sweep reads
-// 4 adjacent columns (one 32-byte sector).
+// One CTA solves L adjacent lines at a time (LPB = 4; a persistent loop
+// walks the line groups). Each line is split into P chunks of consecutive
+// cells; thread (chunk k, line l) = threadIdx.x = k*L + l, so with L = 4 a
+// warp covers 8 chunks x 4 adjacent lines and every global access of the x
+// sweep reads 4 adjacent columns (one 32-byte sector).
 //
 // The line's tridiagonal system (all wet segments of the line, identity rows
 // between them) is solved by the partition method:
@@ -46,14 +46,14 @@ struct LineSeg {
 };
 
 // Shared-memory layout of one CTA (R: the generator's arithmetic type).
-template <class R, int P>
+template <class R, int P, int L = LPB>
 struct LSShared {
-  LineSeg seg[LPB];
-  R sep[4][P * LPB];   // separator rows a, b, c, d
-  R tri[6][P * LPB];   // yF vF wF yL vL wL per chunk
-  R red[4][P * LPB];   // reduced system during PCR
-  R xsep[P * LPB];     // separator solutions
-  double xlast[LPB][SEG];  // solution at each segment's last row
+  LineSeg seg[L];
+  R sep[4][P * L];   // separator rows a, b, c, d
+  R tri[6][P * L];   // yF vF wF yL vL wL per chunk
+  R red[4][P * L];   // reduced system during PCR
+  R xsep[P * L];     // separator solutions
+  double xlast[L][SEG];  // solution at each segment's last row
 };
 
 // A plain division: with FP64 it keeps the rounding of the reference's
@@ -66,42 +66,43 @@ constexpr int pcr_levels(int P) { return P <= 1 ? 0 : 1 + pcr_levels(P / 2); }
 
 // dynamic shared memory of one CTA: LSShared, and with refinement the PCR
 // multipliers
-template <class R, int P>
+template <class R, int P, int L = LPB>
 constexpr size_t line_smem(bool refine) {
-  return sizeof(LSShared<R, P>) + (refine ? (size_t)2 * pcr_levels(P) * P * LPB * sizeof(R) : 0);
+  return sizeof(LSShared<R, P, L>) + (refine ? (size_t)2 * pcr_levels(P) * P * L * sizeof(R) : 0);
 }
 
 // Gen::MIN_BLOCKS: resident CTAs per SM the P = 128 solver is compiled for
 // (2 caps registers at 64 per thread).
-template <class Gen, int P>
-__global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_line_solve(Gen G) {
+// The launch solves line groups 0 .. ngroups-1 of L lines from line0 on.
+template <class Gen, int P, int L = LPB>
+__global__ void __launch_bounds__(L * P, (P == 128 && L == LPB) ? Gen::MIN_BLOCKS : 1)
+    k_line_solve(Gen G, int line0, int ngroups) {
   using R = typename Gen::Real;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  LSShared<R, P>& sh = *reinterpret_cast<LSShared<R, P>*>(smem_raw);
+  LSShared<R, P, L>& sh = *reinterpret_cast<LSShared<R, P, L>*>(smem_raw);
   // with refinement: the PCR multipliers, 2 per level per thread
-  constexpr int PL = P * LPB;
-  R* pm = reinterpret_cast<R*>(smem_raw + sizeof(LSShared<R, P>));
+  constexpr int PL = P * L;
+  R* pm = reinterpret_cast<R*>(smem_raw + sizeof(LSShared<R, P, L>));
   const int tid = threadIdx.x;
-  const int l = tid % LPB, k = tid / LPB;
-  const int cidx = k * LPB + l;
+  const int l = tid % L, k = tid / L;
+  const int cidx = k * L + l;
   const int U = G.unknowns_per_line();
   // scratch slot of this CTA: c', y', v' per unknown, and with refinement
-  // also the rows A, B, C, D (Gen::SCRATCH_ARRAYS arrays of U x LPB)
-  const size_t UL = (size_t)U * LPB;
+  // also the rows A, B, C, D (Gen::SCRATCH_ARRAYS arrays of U x L)
+  const size_t UL = (size_t)U * L;
   R* scr = G.scratch + (size_t)blockIdx.x * Gen::SCRATCH_ARRAYS * UL;
   R* sc_c = scr;
   R* sc_y = scr + UL;
   R* sc_v = scr + 2 * UL;
   const int ncells = G.cells_per_line();
   const int upc = Gen::UPC;
-  const int ngroups = cdiv(G.lines(), LPB);
 
   for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
-    const int line = grp * LPB + l;
+    const int line = line0 + grp * L + l;
     // ---- segment descriptors of the group's lines
-    for (int e = tid; e < LPB * (SEG + 1); e += blockDim.x) {
+    for (int e = tid; e < L * (SEG + 1); e += blockDim.x) {
       const int ll = e / (SEG + 1), s = e % (SEG + 1);
-      G.load_segment(sh.seg[ll], grp * LPB + ll, s);
+      G.load_segment(sh.seg[ll], line0 + grp * L + ll, s);
     }
     __syncthreads();
     const LineSeg& LS = sh.seg[l];
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
               vp = -A * vp * m;
               cp = C * m;
             }
-            const size_t o = (size_t)(q0 + s) * LPB + l;
+            const size_t o = (size_t)(q0 + s) * L + l;
             if constexpr (Gen::REFINE) {
               // the interior rows, for the residual
               scr[3 * UL + o] = A;
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
       const R yL = sh.tri[3][cidx], vL = sh.tri[4][cidx], wL = sh.tri[5][cidx];
       R yF = 0, vF = 0, wF = 0;
       if (k + 1 < P) {
-        const int n1 = cidx + LPB;
+        const int n1 = cidx + L;
         yF = sh.tri[0][n1];
         vF = sh.tri[1][n1];
         wF = sh.tri[2][n1];
@@ -198,14 +199,14 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
       __syncthreads();
       R am = 0, bm = 1, cm = 0, dm = 0, an = 0, bn = 1, cn = 0, dn = 0;
       if (k - st >= 0) {
-        const int o = cidx - st * LPB;
+        const int o = cidx - st * L;
         am = sh.red[0][o];
         bm = sh.red[1][o];
         cm = sh.red[2][o];
         dm = sh.red[3][o];
       }
       if (k + st < P) {
-        const int o = cidx + st * LPB;
+        const int o = cidx + st * L;
         an = sh.red[0][o];
         bn = sh.red[1][o];
         cn = sh.red[2][o];
@@ -230,14 +231,14 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
     // ---- pass C: back substitution and emission
     if constexpr (!Gen::REFINE) {
       const R xr = sh.xsep[cidx];
-      const R xl = (k > 0) ? sh.xsep[cidx - LPB] : R(0);
+      const R xl = (k > 0) ? sh.xsep[cidx - L] : R(0);
       typename Gen::Emitter E;
       E.init(G, LS, line);
       E.emit(G, LS, sh.xlast[l], q0 + nu - 1, xr);
       R xn = xr;
 #pragma unroll 4
       for (int t = nu - 2; t >= 0; --t) {
-        const size_t o = (size_t)(q0 + t) * LPB + l;
+        const size_t o = (size_t)(q0 + t) * L + l;
         const R x = sc_y[o] + sc_v[o] * xl - sc_c[o] * xn;
         E.emit(G, LS, sh.xlast[l], q0 + t, x);
         xn = x;
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
       R* sC = scr + 5 * UL;
       R* sD = scr + 6 * UL;
       const R xr = sh.xsep[cidx];
-      const R xl = (k > 0) ? sh.xsep[cidx - LPB] : R(0);
+      const R xl = (k > 0) ? sh.xsep[cidx - L] : R(0);
       R x_before_sep = 0;  // x of the chunk's last interior unknown
       R ha = 0, hy = 0, hw = -1;  // (a, h, w) of the row below the one eliminated
       R gy = 0, gw = 0, Q = 1;    // d of the last interior unknown: gy - gw d_R + Q d_L
@@ -279,17 +280,17 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
       {
         R x1 = xr, x2 = 0;  // x_{t+1}, x_{t+2}
         for (int t = nu - 2; t >= 0; --t) {
-          const size_t o = (size_t)(q0 + t) * LPB + l;
+          const size_t o = (size_t)(q0 + t) * L + l;
           const R x = sc_y[o] + sc_v[o] * xl - sc_c[o] * x1;
           sc_y[o] = x;
           if (t == nu - 2) x_before_sep = x;
-          else eliminate(o + LPB, x, x1, x2);
+          else eliminate(o + L, x, x1, x2);
           x2 = x1;
           x1 = x;
         }
         // the first unknown: its left neighbour is the previous separator
         // (none at the line's start)
-        if (nu >= 2) eliminate((size_t)q0 * LPB + l, q0 > 0 ? xl : R(0), x1, x2);
+        if (nu >= 2) eliminate((size_t)q0 * L + l, q0 > 0 ? xl : R(0), x1, x2);
       }
       // the first interior unknown's constant term, for the previous chunk
       sh.tri[0][cidx] = hy;
@@ -299,14 +300,14 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
         // the separator row: its right neighbour is the next chunk's first
         // unknown (none at the line's end)
         const int q = q0 + nu - 1;
-        const size_t o = (size_t)q * LPB + l;
-        const R xm = nu >= 2 ? x_before_sep : (q > 0 ? sc_y[o - LPB] : R(0));
-        const R xp = q + 1 < U ? sc_y[o + LPB] : R(0);
+        const size_t o = (size_t)q * L + l;
+        const R xm = nu >= 2 ? x_before_sep : (q > 0 ? sc_y[o - L] : R(0));
+        const R xp = q + 1 < U ? sc_y[o + L] : R(0);
         const R as = sh.sep[0][cidx], bs = sh.sep[1][cidx], cs = sh.sep[2][cidx],
                 ds = sh.sep[3][cidx];
         const R rs = (R)((double)ds - (double)as * (double)xm - (double)bs * (double)xr -
                          (double)cs * (double)xp);
-        const R hF = (k + 1 < P) ? sh.tri[0][cidx + LPB] : R(0);
+        const R hF = (k + 1 < P) ? sh.tri[0][cidx + L] : R(0);
         rd2 = rs - as * gy - cs * hF;
       }
       // the reduction with pass A's multipliers (one barrier per level: the
@@ -317,8 +318,8 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
           R* buf = sh.red[lvl & 1];
           buf[cidx] = rd2;
           __syncthreads();
-          const R dm = (k - st >= 0) ? buf[cidx - st * LPB] : R(0);
-          const R dn = (k + st < P) ? buf[cidx + st * LPB] : R(0);
+          const R dm = (k - st >= 0) ? buf[cidx - st * L] : R(0);
+          const R dn = (k + st < P) ? buf[cidx + st * L] : R(0);
           rd2 = rd2 - dm * pm[(2 * lvl) * PL + cidx] - dn * pm[(2 * lvl + 1) * PL + cidx];
         }
       }
@@ -326,12 +327,12 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
       sh.xsep[cidx] = dr;
       __syncthreads();
       {
-        const R dl = (k > 0) ? sh.xsep[cidx - LPB] : R(0);
+        const R dl = (k > 0) ? sh.xsep[cidx - L] : R(0);
         typename Gen::Emitter E;
         E.init_fwd(G, LS, line);
         R dp = dl;
         for (int t = 0; t <= nu - 2; ++t) {
-          const size_t o = (size_t)(q0 + t) * LPB + l;
+          const size_t o = (size_t)(q0 + t) * L + l;
           const R d = sD[o] - sA[o] * dp - sC[o] * dr;
           E.template emit<true>(G, LS, sh.xlast[l], q0 + t, (double)sc_y[o] + (double)d);
           dp = d;
@@ -341,9 +342,9 @@ __global__ void __launch_bounds__(LPB * P, P == 128 ? Gen::MIN_BLOCKS : 1) k_lin
     }
     __syncthreads();
     // ---- per-segment end fix-ups
-    for (int e = tid; e < LPB * SEG; e += blockDim.x) {
+    for (int e = tid; e < L * SEG; e += blockDim.x) {
       const int ll = e / SEG, s = e % SEG;
-      if (s < sh.seg[ll].nseg) G.fixup(sh.seg[ll], sh.xlast[ll], grp * LPB + ll, s);
+      if (s < sh.seg[ll].nseg) G.fixup(sh.seg[ll], sh.xlast[ll], line0 + grp * L + ll, s);
     }
     __syncthreads();
   }

@@ -163,10 +163,10 @@ void launch_sediment(const StateT<R>& S, const CoefT<R>& c, double s_start, bool
                      cudaStream_t st, Trace* tr) {
   // Find_VTH + hesoK ran in the half-step's commit (k_commit_a/k_commit_b)
   if (tr) tr->kbegin(st, xdir ? KS_FS_X : KS_FS_Y);
-  launch_fs_sweep(S, c, xdir ? 0 : 1, s_start, st);
+  const int nfs = launch_fs_sweep(S, c, xdir ? 0 : 1, s_start, st);
   if (tr) tr->kend(st, xdir ? KS_FS_X : KS_FS_Y);
   k_update_fs<<<dim3(cdiv(S.M, 128), S.N), 128, 0, st>>>(S);
-  int launched = 2;
+  int launched = nfs + 1;
   if (bed && S.N >= 5) {
     // the bed change once per step, after the j-sweep (engine.cpp:290-293)
     k_calc_qb<<<dim3(cdiv(S.M - 1, 128), S.N - 1), 128, 0, st>>>(S, c);

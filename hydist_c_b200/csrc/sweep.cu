@@ -32,6 +32,7 @@ struct HydroGen {
   static constexpr bool REFINE = REF;
   static constexpr int SCRATCH_ARRAYS = REFINE ? 7 : 3;
   static constexpr int UPC = 2;
+  static constexpr int DIRECTION = DIR;
   // x sweeps (columns, 4 adjacent per warp) run faster with two CTAs per SM
   // despite the register cap, and so do the FP32 y sweeps; the FP64 and the
   // refined FP32 y sweeps slower
@@ -255,38 +256,90 @@ struct HydroGen {
   __device__ R* vel_ptr() const { return DIR == 0 ? S.tu : S.tv; }
 };
 
-template <class Gen, int P>
-static void launch_gen(const Gen& G, cudaStream_t st, int grid) {
-  const size_t smem = line_smem<typename Gen::Real, P>(Gen::REFINE);
+// the kernel's shared-memory limit, raised once per device
+template <class Gen, int P, int L>
+static size_t prepare(int dev) {
+  const size_t smem = line_smem<typename Gen::Real, P, L>(Gen::REFINE);
   static bool attr[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
   if (dev < 64 && !attr[dev]) {
-    cudaFuncSetAttribute(k_line_solve<Gen, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_line_solve<Gen, P, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     attr[dev] = true;
   }
-  k_line_solve<Gen, P><<<grid, LPB * P, smem, st>>>(G);
+  return smem;
+}
+
+template <class Gen, int P, int L = LPB>
+static void launch_gen(const Gen& G, cudaStream_t st, int grid, int line0, int ngroups) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const size_t smem = prepare<Gen, P, L>(dev);
+  k_line_solve<Gen, P, L><<<grid, L * P, smem, st>>>(G, line0, ngroups);
 }
 
 template <class Gen>
-static void launch_any(const Gen& G, int P, cudaStream_t st, int grid) {
-  if (P == 128) launch_gen<Gen, 128>(G, st, grid);
-  else if (P == 64) launch_gen<Gen, 64>(G, st, grid);
-  else if (P == 32) launch_gen<Gen, 32>(G, st, grid);
-  else if (P == 16) launch_gen<Gen, 16>(G, st, grid);
-  else if (P == 4) launch_gen<Gen, 4>(G, st, grid);
-  else launch_gen<Gen, 1>(G, st, grid);
+static void launch_any(const Gen& G, int P, cudaStream_t st, int grid, int line0, int ngroups) {
+  if (P == 128) launch_gen<Gen, 128>(G, st, grid, line0, ngroups);
+  else if (P == 64) launch_gen<Gen, 64>(G, st, grid, line0, ngroups);
+  else if (P == 32) launch_gen<Gen, 32>(G, st, grid, line0, ngroups);
+  else if (P == 16) launch_gen<Gen, 16>(G, st, grid, line0, ngroups);
+  else if (P == 4) launch_gen<Gen, 4>(G, st, grid, line0, ngroups);
+  else launch_gen<Gen, 1>(G, st, grid, line0, ngroups);
+}
+
+// CTAs of the 128-chunk solver resident on the device at once (queried once
+// per device)
+template <class Gen>
+static int resident_slots() {
+  static int slots[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 64) return 0;
+  if (!slots[dev]) {
+    const size_t smem = prepare<Gen, 128, LPB>(dev);
+    int per_sm = 0, nsm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_line_solve<Gen, 128, LPB>, LPB * 128,
+                                                  smem);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    slots[dev] = per_sm * nsm;
+  }
+  return slots[dev];
+}
+
+// Launches a sweep over `lines` lines and returns the number of launches.
+// In a row sweep whose last round of 4-line groups would leave more than
+// half of the resident CTAs idle (2047 rows on 148 one-CTA SMs: 68 of 512
+// groups), that remainder runs as a second launch of 2-line groups with 256
+// chunks per line, half the chain per thread, on every SM.
+template <class Gen>
+static int launch_lines(const Gen& G, int P, int lines, int lslots, cudaStream_t st) {
+  const int groups = cdiv(lines, LPB);
+  if constexpr (Gen::DIRECTION == 1) {
+    if (P == 128) {
+      const int slots = std::min(resident_slots<Gen>(), lslots);
+      const int full = slots > 0 ? groups / slots : 0;
+      const int rem = groups - full * slots;
+      if (full >= 1 && rem > 0 && 2 * rem <= slots) {
+        launch_gen<Gen, 128>(G, st, slots, 0, full * slots);
+        const int line0 = full * slots * LPB;
+        const int g2 = cdiv(lines - line0, 2);
+        launch_gen<Gen, 256, 2>(G, st, std::min(g2, lslots), line0, g2);
+        return 2;
+      }
+    }
+  }
+  launch_any(G, P, st, std::min(groups, lslots), 0, groups);
+  return 1;
 }
 
 template <int DIR, class R, bool REF>
-static void launch_dir(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, int grid, int P) {
+static int launch_dir(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, int lines, int P) {
   HydroGen<DIR, R, REF> G;
   G.S = S;
   G.c = c;
   G.scratch = S.lscratch;
   G.f4 = DIR == 0 ? 2 * c.g * c.dTchia2dX : 2 * c.g * c.dTchia2dY;
-  launch_any(G, P, st, grid);
+  return launch_lines(G, P, lines, S.lslots, st);
 }
 
 // ---------------------------------------------------------------------
@@ -300,6 +353,7 @@ struct FSGen {
   static constexpr bool REFINE = REF;
   static constexpr int SCRATCH_ARRAYS = REFINE ? 7 : 3;
   static constexpr int UPC = 1;
+  static constexpr int DIRECTION = DIR;
   // two CTAs per SM but for the FP64 y sweep
   static constexpr int MIN_BLOCKS = (DIR == 0 || sizeof(R) == 4) ? 2 : 1;
   StateT<R> S;
@@ -445,52 +499,38 @@ struct FSGen {
 };
 
 template <class R>
-void launch_fs_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, double s_start,
-                     cudaStream_t st) {
+int launch_fs_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, double s_start,
+                    cudaStream_t st) {
   const int ncells = dir == 0 ? S.N - 1 : S.M - 1;
   const int lines = dir == 0 ? S.M - 3 : S.N - 3;
-  if (lines <= 0) return;
-  const int grid = min(cdiv(lines, LPB), S.lslots);
+  if (lines <= 0) return 0;
   const int P = line_chunks(ncells, 4);
   if (dir == 0) {
-    if (S.refine) {
-      FSGen<0, R, true> G{S, c, S.lscratch, s_start};
-      launch_any(G, P, st, grid);
-    } else {
-      FSGen<0, R, false> G{S, c, S.lscratch, s_start};
-      launch_any(G, P, st, grid);
-    }
-  } else {
-    if (S.refine) {
-      FSGen<1, R, true> G{S, c, S.lscratch, s_start};
-      launch_any(G, P, st, grid);
-    } else {
-      FSGen<1, R, false> G{S, c, S.lscratch, s_start};
-      launch_any(G, P, st, grid);
-    }
+    if (S.refine) return launch_lines(FSGen<0, R, true>{S, c, S.lscratch, s_start}, P, lines, S.lslots, st);
+    return launch_lines(FSGen<0, R, false>{S, c, S.lscratch, s_start}, P, lines, S.lslots, st);
   }
+  if (S.refine) return launch_lines(FSGen<1, R, true>{S, c, S.lscratch, s_start}, P, lines, S.lslots, st);
+  return launch_lines(FSGen<1, R, false>{S, c, S.lscratch, s_start}, P, lines, S.lslots, st);
 }
 
 template <class R>
-void launch_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t st) {
+int launch_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t st) {
   const int ncells = dir == 0 ? S.N - 1 : S.M - 1;
   const int lines = dir == 0 ? S.M - 1 : S.N - 1;
-  const int grid = min(cdiv(lines, LPB), S.lslots);
   const int P = line_chunks(ncells, 4);
   if (S.refine) {
-    if (dir == 0) launch_dir<0, R, true>(S, c, st, grid, P);
-    else launch_dir<1, R, true>(S, c, st, grid, P);
-  } else {
-    if (dir == 0) launch_dir<0, R, false>(S, c, st, grid, P);
-    else launch_dir<1, R, false>(S, c, st, grid, P);
+    if (dir == 0) return launch_dir<0, R, true>(S, c, st, lines, P);
+    return launch_dir<1, R, true>(S, c, st, lines, P);
   }
+  if (dir == 0) return launch_dir<0, R, false>(S, c, st, lines, P);
+  return launch_dir<1, R, false>(S, c, st, lines, P);
 }
 
-template void launch_sweep<double>(const StateT<double>&, const CoefT<double>&, int, cudaStream_t);
-template void launch_sweep<float>(const StateT<float>&, const CoefT<float>&, int, cudaStream_t);
-template void launch_fs_sweep<double>(const StateT<double>&, const CoefT<double>&, int, double,
-                                      cudaStream_t);
-template void launch_fs_sweep<float>(const StateT<float>&, const CoefT<float>&, int, double,
+template int launch_sweep<double>(const StateT<double>&, const CoefT<double>&, int, cudaStream_t);
+template int launch_sweep<float>(const StateT<float>&, const CoefT<float>&, int, cudaStream_t);
+template int launch_fs_sweep<double>(const StateT<double>&, const CoefT<double>&, int, double,
                                      cudaStream_t);
+template int launch_fs_sweep<float>(const StateT<float>&, const CoefT<float>&, int, double,
+                                    cudaStream_t);
 
 }  // namespace hyd
