@@ -130,6 +130,9 @@ struct HydistHandle {
   char* chunk = nullptr;
   size_t chunk_size = 0, chunk_used = 0;
   double* mass_part = nullptr;  // per-block partial sums
+  unsigned* mass_done = nullptr;  // blocks finished, reset by the last one
+  double* mass_host = nullptr;    // the result, in mapped pinned host memory
+  double* mass_host_dev = nullptr;
   int mass_blocks = 0;
   // one captured step per sediment phase: [bed*4 + sed_x*2 + sed_y]
   cudaGraphExec_t graph[8] = {};
@@ -253,14 +256,18 @@ int set_device_clock(HydistHandle* h) {
   return HYDIST_OK;
 }
 
-__global__ void k_mass_partial(State S, double* part) {
-  // sum over wet cells of H_moi-independent volume (htaiz + z), FP64
+// Volume of the wet cells, sum of (htaiz + z) over rows 2..N and columns
+// 2..M where khouot == 0, FP64. Each block sums whole rows into part[]; the
+// last block to finish adds the partial sums in block order (the same
+// result every call) and writes it to mapped host memory.
+__global__ void k_mass(State S, double* part, unsigned* done, double* out) {
   __shared__ double sh[256];
+  __shared__ bool last;
   double acc = 0;
-  const int n = S.W * S.H;
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
-    const int i = g / S.W, j = g - i * S.W;
-    if (i >= 2 && i <= S.N && j >= 2 && j <= S.M && S.khouot[g] == 0) acc += S.htaiz[g] + S.z[g];
+  for (int i = blockIdx.x + 2; i <= S.N; i += gridDim.x) {
+    const int row = i * S.W;
+    for (int j = threadIdx.x + 2; j <= S.M; j += blockDim.x)
+      if (S.khouot[row + j] == 0) acc += S.htaiz[row + j] + S.z[row + j];
   }
   sh[threadIdx.x] = acc;
   __syncthreads();
@@ -268,20 +275,27 @@ __global__ void k_mass_partial(State S, double* part) {
     if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
     __syncthreads();
   }
-  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
-}
-
-__global__ void k_mass_final(const double* part, int n, double* out) {
-  __shared__ double sh[256];
-  double acc = 0;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) acc += part[k];
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = sh[0];
+    __threadfence();
+    last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  acc = 0;
+  for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) acc += part[k];
   sh[threadIdx.x] = acc;
   __syncthreads();
   for (int s = 128; s > 0; s >>= 1) {
     if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
     __syncthreads();
   }
-  if (threadIdx.x == 0) out[0] = sh[0];
+  if (threadIdx.x == 0) {
+    *out = sh[0];
+    __threadfence_system();
+    *done = 0;
+  }
 }
 
 // A field's device array and element size (8, or 4 for the FP32 form's
@@ -491,6 +505,11 @@ int private_arrays(HydistHandle* h) {
   TRY(set_device_clock(h));
   h->mass_blocks = 296;
   TRY(dalloc(h, &h->mass_part, h->mass_blocks + 1));
+  TRY(dalloc(h, &h->mass_done, 1));
+  if (!h->planning && !h->mass_host) {
+    CK(cudaHostAlloc((void**)&h->mass_host, sizeof(double), cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer((void**)&h->mass_host_dev, h->mass_host, 0));
+  }
   return h->fp32 ? bulk_private(h, h->Sf) : bulk_private(h, h->S);
 }
 
@@ -808,6 +827,7 @@ int hydist_destroy(HydistHandle* h) {
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   for (void* p : h->allocs) cudaFree(p);
+  if (h->mass_host) cudaFreeHost(h->mass_host);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return HYDIST_OK;
@@ -1184,12 +1204,10 @@ int hydist_upload(HydistHandle* h, int32_t field, const void* host) {
 int hydist_mass(HydistHandle* h, double* volume) {
   if (!h || !volume) return fail(HYDIST_ERR_ARG, "null argument");
   CK(cudaSetDevice(h->device));
-  k_mass_partial<<<h->mass_blocks, 256, 0, h->stream>>>(h->S, h->mass_part);
-  k_mass_final<<<1, 256, 0, h->stream>>>(h->mass_part, h->mass_blocks, h->mass_part + h->mass_blocks);
-  double v = 0;
-  CK(cudaMemcpyAsync(&v, h->mass_part + h->mass_blocks, 8, cudaMemcpyDeviceToHost, h->stream));
+  k_mass<<<h->mass_blocks, 256, 0, h->stream>>>(h->S, h->mass_part, h->mass_done, h->mass_host_dev);
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(h->stream));
-  *volume = v * h->c.dX * h->c.dY;
+  *volume = *(volatile double*)h->mass_host * h->c.dX * h->c.dY;
   return HYDIST_OK;
 }
 
