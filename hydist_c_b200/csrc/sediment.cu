@@ -149,13 +149,21 @@ __global__ void k_bed_load(StateT<R> S, CoefT<R> c) {
   S.dH[pos] += double(c.dT / (1 - c.Dorong) * (src + tH));
 }
 
+constexpr int FS_ROWS = 8;
+
 template <class R>
 __global__ void k_update_fs(StateT<R> S) {
+  // FS = tFS on rows 1..N, columns 1..M; FS_ROWS rows per thread, every
+  // load before the first store
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int i = blockIdx.y + 1;
-  if (i > S.N || j > S.M) return;
-  const int g = i * S.W + j;
-  S.FS[g] = S.tFS[g];
+  const int i0 = blockIdx.y * FS_ROWS + 1;
+  if (j > S.M) return;
+  R v[FS_ROWS];
+#pragma unroll
+  for (int r = 0; r < FS_ROWS; ++r) v[r] = i0 + r <= S.N ? S.tFS[(i0 + r) * S.W + j] : R(0);
+#pragma unroll
+  for (int r = 0; r < FS_ROWS; ++r)
+    if (i0 + r <= S.N) S.FS[(i0 + r) * S.W + j] = v[r];
 }
 
 template <class R>
@@ -165,7 +173,7 @@ void launch_sediment(const StateT<R>& S, const CoefT<R>& c, double s_start, bool
   if (tr) tr->kbegin(st, xdir ? KS_FS_X : KS_FS_Y);
   const int nfs = launch_fs_sweep(S, c, xdir ? 0 : 1, s_start, st);
   if (tr) tr->kend(st, xdir ? KS_FS_X : KS_FS_Y);
-  k_update_fs<<<dim3(cdiv(S.M, 128), S.N), 128, 0, st>>>(S);
+  k_update_fs<<<dim3(cdiv(S.M, 128), cdiv(S.N, FS_ROWS)), 128, 0, st>>>(S);
   int launched = nfs + 1;
   if (bed && S.N >= 5) {
     // the bed change once per step, after the j-sweep (engine.cpp:290-293)
