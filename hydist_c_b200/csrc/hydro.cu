@@ -539,9 +539,10 @@ __global__ void k_margin_u(StateT<R> S, CoefT<R> c) {
 template <class R>
 __device__ __forceinline__ void vth_heso_cell(const StateT<R>& S, const CoefT<R>& c, int i, int j,
                                               int g, R tu, R tv, R tu_up, R tv_left, R Hm,
-                                              double hp, double hl, double hup, R Hu, R Hv) {
+                                              double ht, double hp, double hl, double hup, R Hu,
+                                              R Hv) {
   if (i >= 2 && j >= 2) {
-    if ((S.htaiz[g] > c.NANGDAY) && (Hm > c.H_TINH)) {
+    if ((ht > c.NANGDAY) && (Hm > c.H_TINH)) {
       const R ut = (tu + tu_up) * R(0.5);
       const R vt = (tv + tv_left) * R(0.5);
       S.VTH[g] = sqrt(ut * ut + vt * vt);
@@ -574,34 +575,41 @@ __global__ void k_commit_a(StateT<R> S, CoefT<R> c, int vth_hi) {
   const int i = blockIdx.y;
   if (i > S.N || j > S.M) return;
   const int W = S.W, g = i * W + j;
+  const bool in = i >= 1 && j >= 1;
+  const bool vth = in && i <= vth_hi;
+  // every operand before the first store (one round of memory latency);
+  // nothing this kernel stores is read by another of its threads
   const double tz = S.tz[g];
+  const int kh = S.khouot[g];
+  const double ht = S.htaiz[g];
+  const R hm_old = S.Hmoi[g];
+  const R tu = S.su[g], tv = S.sv[g];  // t_u, t_v after their smoothing
+  const double zd = (i + 1 <= S.N) ? S.tz[g + W] : S.z[g + W];
+  const double zr = (j + 1 <= S.M) ? S.tz[g + 1] : S.z[g + 1];
+  const double hp = S.h[g];
+  const double hl = in ? S.h[g - 1] : 0.0, hup = in ? S.h[g - W] : 0.0;
+  // the committed t_u(i-1, j), t_v(i, j-1) are the smoothed values there
+  const R tu_up = vth ? S.su[g - W] : R(0), tv_left = vth ? S.sv[g - 1] : R(0);
   R Hm = 0;
-  const bool vth = i >= 1 && j >= 1 && i <= vth_hi;
-  if (i >= 1 && j >= 1) {
-    if (S.khouot[g] == 0) {
-      Hm = S.htaiz[g] + tz;
+  if (in) {
+    if (kh == 0) {
+      Hm = ht + tz;
       S.Hmoi[g] = Hm;
     } else if (vth) {
-      Hm = S.Hmoi[g];
+      Hm = hm_old;
     }
   }
-  // t_u, t_v after their smoothing (update_buffer) and the commit
-  const R tu = S.su[g], tv = S.sv[g];
   S.tu[g] = tu;
   S.tv[g] = tv;
   S.z[g] = tz;
   S.u[g] = tu * (1 - c.kenhhepd);
   S.v[g] = tv * (1 - c.kenhhepng);
-  if (i >= 1 && j >= 1) {
-    const double zd = (i + 1 <= S.N) ? S.tz[g + W] : S.z[g + W];
-    const double zr = (j + 1 <= S.M) ? S.tz[g + 1] : S.z[g + 1];
-    const double hp = S.h[g], hl = S.h[g - 1], hup = S.h[g - W];
+  if (in) {
     const R Hu = (hl + hp + zd + tz) * 0.5;
     const R Hv = (hup + hp + zr + tz) * 0.5;
     S.Htdu[g] = Hu;
     S.Htdv[g] = Hv;
-    // the committed t_u(i-1, j), t_v(i, j-1) are the smoothed values there
-    if (vth) vth_heso_cell(S, c, i, j, g, tu, tv, S.su[g - W], S.sv[g - 1], Hm, hp, hl, hup, Hu, Hv);
+    if (vth) vth_heso_cell(S, c, i, j, g, tu, tv, tu_up, tv_left, Hm, ht, hp, hl, hup, Hu, Hv);
   }
 }
 
@@ -650,39 +658,53 @@ __global__ void k_commit_b(StateT<R> S, CoefT<R> c, int vth_hi) {
   const int i = blockIdx.y;
   if (i > S.N || j > S.M) return;
   const int W = S.W, g = i * W + j;
-  auto dries = [&](int ii, int jj) -> bool {
-    if (ii < 2 || ii > S.N || jj < 1 || jj > S.M) return false;
-    const int q = ii * W + jj;
-    return S.khouot[q] == 0 && S.Hmoi[q] <= c.H_TINH;
-  };
-  const bool d0 = dries(i, j);
-  const bool ddown = dries(i + 1, j);
-  const bool dright = dries(i, j + 1);
+  const bool in = i >= 1 && j >= 1;
+  const bool vth = in && i <= vth_hi;
+  // every operand before the first store (one round of memory latency);
+  // nothing this kernel stores is read by another of its threads. A cell
+  // dries when it is wet with H_moi at most H_TINH (rows 2..N, columns 1..M).
+  auto in_dry = [&](int ii, int jj) { return ii >= 2 && ii <= S.N && jj >= 1 && jj <= S.M; };
+  const bool c0 = in_dry(i, j), cd = in_dry(i + 1, j), cr = in_dry(i, j + 1);
+  const bool cu = vth && in_dry(i - 1, j), cl = vth && in_dry(i, j - 1);
+  const int k0 = c0 ? S.khouot[g] : 1, kd = cd ? S.khouot[g + W] : 1, kr = cr ? S.khouot[g + 1] : 1;
+  const int ku = cu ? S.khouot[g - W] : 1, kl = cl ? S.khouot[g - 1] : 1;
+  const R h0 = c0 ? S.Hmoi[g] : R(0), hd = cd ? S.Hmoi[g + W] : R(0), hr = cr ? S.Hmoi[g + 1] : R(0);
+  const R hu = cu ? S.Hmoi[g - W] : R(0), hl_ = cl ? S.Hmoi[g - 1] : R(0);
+  const double su = S.su[g], sv = S.sv[g];
+  const double tz = S.tz[g];
+  const double zd = (i + 1 <= S.N) ? S.tz[g + W] : S.z[g + W];
+  const double zr = (j + 1 <= S.M) ? S.tz[g + 1] : S.z[g + 1];
+  const double hp = S.h[g];
+  const double hl = in ? S.h[g - 1] : 0.0, hup = in ? S.h[g - W] : 0.0;
+  const double ht = vth ? S.htaiz[g] : 0.0;
+  const R hm = vth ? S.Hmoi[g] : R(0);
+  const R su_up = vth ? S.su[g - W] : R(0), sv_left = vth ? S.sv[g - 1] : R(0);
+  const bool d0 = c0 && k0 == 0 && h0 <= c.H_TINH;
+  const bool ddown = cd && kd == 0 && hd <= c.H_TINH;
+  const bool dright = cr && kr == 0 && hr <= c.H_TINH;
   // t_u, t_v after their smoothing, zeroed by the drying pass
-  double tu = S.su[g], tv = S.sv[g];
+  double tu = su, tv = sv;
   if (d0 || ddown) tu = 0;
   if (d0 || dright) tv = 0;
   S.tu[g] = tu;
   S.tv[g] = tv;
   if (d0) S.FS[g] = 0;  // khouot is set by the segment scan after this pass
-  const double tz = S.tz[g];
   S.z[g] = tz;
   S.u[g] = tu * (1 - c.kenhhepd);
   S.v[g] = tv * (1 - c.kenhhepng);
-  if (i >= 1 && j >= 1) {
-    const double zd = (i + 1 <= S.N) ? S.tz[g + W] : S.z[g + W];
-    const double zr = (j + 1 <= S.M) ? S.tz[g + 1] : S.z[g + 1];
-    const double hp = S.h[g], hl = S.h[g - 1], hup = S.h[g - W];
+  if (in) {
     const R Hu = (hl + hp + zd + tz) * 0.5;
     const R Hv = (hup + hp + zr + tz) * 0.5;
     S.Htdu[g] = Hu;
     S.Htdv[g] = Hv;
-    if (i <= vth_hi) {
+    if (vth) {
       // t_u(i-1, j) is zeroed when (i-1, j) or (i, j) dries, t_v(i, j-1)
       // when (i, j-1) or (i, j) does
-      const R tu_up = (dries(i - 1, j) || d0) ? R(0) : S.su[g - W];
-      const R tv_left = (dries(i, j - 1) || d0) ? R(0) : S.sv[g - 1];
-      vth_heso_cell(S, c, i, j, g, R(tu), R(tv), tu_up, tv_left, S.Hmoi[g], hp, hl, hup, Hu, Hv);
+      const bool dup = cu && ku == 0 && hu <= c.H_TINH;
+      const bool dleft = cl && kl == 0 && hl_ <= c.H_TINH;
+      const R tu_up = (dup || d0) ? R(0) : su_up;
+      const R tv_left = (dleft || d0) ? R(0) : sv_left;
+      vth_heso_cell(S, c, i, j, g, R(tu), R(tv), tu_up, tv_left, hm, ht, hp, hl, hup, Hu, Hv);
     }
   }
 }
