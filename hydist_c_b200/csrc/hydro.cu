@@ -145,26 +145,37 @@ __global__ void k_runs_flags(StateT<R> S, CoefT<R> c, int* seg_cnt, int dry) {
   if (i > S.N || j > S.M) return;
   const int W = S.W, H = S.H, g = i * W + j;
   int* K = S.khouot;
-  auto mask = [&](int q, int qi, int qj) -> int {
-    const int k = K[q];
-    if (dry && k == 0 && qi >= 2 && qi <= S.N && qj >= 1 && qj <= S.M && S.Hmoi[q] <= c.H_TINH)
+  // every operand first (one round of memory latency): the masks, and with
+  // dry the depths, of the cell and of its neighbours the run tests read
+  // (all inside the array for rows 2..N, columns 2..M)
+  const int qs[7] = {g, g - 1, g + 1, g - 2, g - W, g + W, g - 2 * W};
+  int kk[7];
+  R hh[7];
+#pragma unroll
+  for (int n = 0; n < 7; ++n) {
+    kk[n] = K[qs[n]];
+    hh[n] = dry ? S.Hmoi[qs[n]] : R(0);
+  }
+  auto mask = [&](int n, int qi, int qj) -> int {
+    const int k = kk[n];
+    if (dry && k == 0 && qi >= 2 && qi <= S.N && qj >= 1 && qj <= S.M && hh[n] <= c.H_TINH)
       return 1;
     return k;
   };
   if (dry) {
-    const int k0 = mask(g, i, j);
-    if (k0 != K[g]) K[g] = k0;
+    const int k0 = mask(0, i, j);
+    if (k0 != kk[0]) K[g] = k0;
     if (j == 2) {  // column 1 is outside this grid
-      const int k1 = mask(g - 1, i, 1);
-      if (k1 != K[g - 1]) K[g - 1] = k1;
+      const int k1 = mask(1, i, 1);
+      if (k1 != kk[1]) K[g - 1] = k1;
     }
   }
-  const bool w = mask(g, i, j) == 0;
+  const bool w = mask(0, i, j) == 0;
   if (!w) return;
   // row i, position j, lim M
   {
-    const bool wm1 = mask(g - 1, i, j - 1) == 0, wp1 = mask(g + 1, i, j + 1) == 0;
-    const bool wm2 = mask(g - 2, i, j - 2) == 0;
+    const bool wm1 = mask(1, i, j - 1) == 0, wp1 = mask(2, i, j + 1) == 0;
+    const bool wm2 = mask(3, i, j - 2) == 0;
     bool st, en;
     run_flags(wm1, w, wp1, wm2, j, S.M, st, en);
     if (st) {
@@ -178,8 +189,8 @@ __global__ void k_runs_flags(StateT<R> S, CoefT<R> c, int* seg_cnt, int dry) {
   }
   // column j, position i, lim N
   {
-    const bool wm1 = mask(g - W, i - 1, j) == 0, wp1 = mask(g + W, i + 1, j) == 0;
-    const bool wm2 = mask(g - 2 * W, i - 2, j) == 0;
+    const bool wm1 = mask(4, i - 1, j) == 0, wp1 = mask(5, i + 1, j) == 0;
+    const bool wm2 = mask(6, i - 2, j) == 0;
     bool st, en;
     run_flags(wm1, w, wp1, wm2, i, S.N, st, en);
     if (st) {
