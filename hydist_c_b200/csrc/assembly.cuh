@@ -78,25 +78,29 @@ __device__ __forceinline__ PreT<R> pre_y(const StateT<R>& S, const CoefT<R>& c, 
   const R utb = (u[g - w] + u[g] + u[g - w + 1] + u[g + 1]) * R(0.25);
   const R vv = v[g], VI = S.visco[g], Hv = S.Htdv[g];
   const R dT = c.dT;
+  // the cross-line stencil (rows i-2..i+2, inside the array for rows 2..N)
+  // loaded before the upwind tests choose from it
+  const R vm1 = v[g - w], vm2 = v[g - 2 * w], vp1 = v[g + w], vp2 = v[g + 2 * w];
+  const R hm1 = Hm[g - w], hp1 = Hm[g + w], hm2 = Hm[g - 2 * w];
   const R rH = R(1) / Hv;
   const R visc = VI * c.dT_dYbp;
   P.f1 = c.dTchia2dY * vv + visc;
   P.f2 = -(2 + S.Ky1[g] * dT * sqrt(vv * vv + utb * utb) * rH + 2 * visc);
   P.f3 = visc - c.dTchia2dY * vv;
-  if (Hm[g - w] <= c.H_TINH) {
+  if (hm1 <= c.H_TINH) {
     if (utb < 0) {
-      q = utb * (-3 * vv + 4 * v[g + w] - v[g + 2 * w]) * c.r_dX2;
-      p = (vv - 2 * v[g + w] + v[g + 2 * w]) * c.r_dXbp;
+      q = utb * (-3 * vv + 4 * vp1 - vp2) * c.r_dX2;
+      p = (vv - 2 * vp1 + vp2) * c.r_dXbp;
     }
   } else {
-    if (Hm[g + w] <= c.H_TINH) {
-      if ((Hm[g - 2 * w] > c.H_TINH) && (utb > 0)) {
-        q = utb * (3 * vv - 4 * v[g - w] + v[g - 2 * w]) * c.r_dX2;
-        p = (vv - 2 * v[g - w] + v[g - 2 * w]) * c.r_dXbp;
+    if (hp1 <= c.H_TINH) {
+      if ((hm2 > c.H_TINH) && (utb > 0)) {
+        q = utb * (3 * vv - 4 * vm1 + vm2) * c.r_dX2;
+        p = (vv - 2 * vm1 + vm2) * c.r_dXbp;
       }
     } else {
-      q = utb * (v[g + w] - v[g - w]) * c.r_dX2;
-      p = (v[g + w] - 2 * vv + v[g - w]) * c.r_dXbp;
+      q = utb * (vp1 - vm1) * c.r_dX2;
+      p = (vp1 - 2 * vv + vm1) * c.r_dXbp;
     }
   }
   P.f5 = -2 * vv + dT * q + dT * c.CORIOLIS_FORCE * utb - dT * VI * p -
