@@ -82,13 +82,14 @@ __device__ __forceinline__ void fs_cell(const StateT<R>& S, const CoefT<R>& c, b
   const R* kx = xdir ? S.Ky : S.Kx;
   const R hm1 = Hm[pos - s], hp1 = Hm[pos + s], hm2 = Hm[pos - 2 * s], hp2 = Hm[pos + 2 * s];
   const R fm = FS[pos - s], fp = FS[pos + s];
+  const R vxc = vx[pos], vxm = vx[pos - s];  // before the tests that use them
   R p = 0, q = 0;
   if ((hm1 > H_TINH) && (hp2 > H_TINH)) p = (fp - fs);
   if ((hm2 > H_TINH) && (hp1 > H_TINH)) q = (fs - fm);
   p = (rH * (xdir ? c.r_dYbp : c.r_dXbp)) * (hx[pos] * kx[pos] * p - hx[pos - s] * kx[pos - s] * q);
   if ((hm2 > H_TINH) && (hp2 > H_TINH)) {
     q = (fp - fm) * (xdir ? c.r_dY2 : c.r_dX2);
-    q = (vx[pos] + vx[pos - s]) * R(0.5) * q * gamav;
+    q = (vxc + vxm) * R(0.5) * q * gamav;
   } else {
     q = 0;
   }
