@@ -7,7 +7,8 @@
 //   k_runs_flags/sort   [Find_Calculation_limits_Horizontal/Vertical, :238-343]
 //   k_htuongdoi         [Htuongdoi, :346-362] (set-up; per step in the commits)
 //   k_preprocess_sides  [preprocess_data, :482-601]
-//   k_tick, k_boundary  [Update_Boundary_Value/Boundary_value/FS_boundary, :603-728]
+//   k_boundary          [Update_Boundary_Value/Boundary_value/FS_boundary, :603-728;
+//                        it also advances the device clock]
 //   the line sweeps     [UZSolver_*/VZSolver_* + tridiagSolver,
 //                        UVZSolver_multithread.cpp:19-139, 142-603, 798-933]:
 //                        sweep.cu on the partitioned solver of linesolve.cuh
@@ -327,17 +328,25 @@ __global__ void k_preprocess_sides(StateT<R> S, CoefT<R> c, double* p53) {
 // ------------------------------------------------------------- boundary
 // The simulated time lives on the device so that a captured step replays
 // unchanged: advanced by t += dT/2 per half-step (engine.cpp:66, 176).
+// Update_Boundary_Value (support_funcs.cpp:682-728) at the device clock
+// advanced by `half` (a half-step's time, or 0). t arrives through a float
+// parameter in the reference (engine.cpp:22), hence the rounding. With half
+// != 0 the last block to finish stores the advanced clock (clock[1] counts
+// the blocks), after every block has read the old one.
 template <class R>
-__global__ void k_tick(StateT<R> S, double half) { S.clock[0] += half; }
-
-// Update_Boundary_Value (support_funcs.cpp:682-728). t arrives through a
-// float parameter in the reference (engine.cpp:22), hence the rounding.
-template <class R>
-__global__ void k_boundary(StateT<R> S) {
+__global__ void k_boundary(StateT<R> S, double half) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int M = S.M, N = S.N, W = S.W;
+  const double t_new = S.clock[0] + half;
+  if (half != 0) {
+    __syncthreads();  // every thread of the block has read the clock
+    if (threadIdx.x == 0 && atomicAdd(&S.clock[1], 1.0) == (double)(gridDim.x - 1)) {
+      S.clock[0] = t_new;
+      S.clock[1] = 0;
+    }
+  }
   if (i > M && i > N) return;
-  const double t = (double)(float)S.clock[0];
+  const double t = (double)(float)t_new;
   // the host refuses steps past the series; the clamp keeps reads in bounds
   const int t1 = min(max((int)(t / 3600), 0), S.T - 2);
   const double t2h = (t - (double)(3600.0f * (float)t1)) / 3600.0f;
@@ -741,7 +750,7 @@ void launch_preprocess(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
 
 template <class R>
 void launch_boundary(const StateT<R>& S, cudaStream_t st) {
-  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
+  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, 0.0);
 }
 
 template <class R>
@@ -761,9 +770,8 @@ void launch_find_limits(const StateT<R>& S, const CoefT<R>& c, bool dry, cudaStr
 
 template <class R>
 void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr) {
-  k_tick<<<1, 1, 0, st>>>(S, 0.5 * c.dT);
-  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
-  if (tr) tr->mark(st, PH_BOUNDARY_X, 2);
+  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, 0.5 * c.dT);
+  if (tr) tr->mark(st, PH_BOUNDARY_X, 1);
   if (tr) tr->kbegin(st, KS_SWEEP_X);
   const int nx = launch_sweep(S, c, 0, st);
   if (tr) tr->kend(st, KS_SWEEP_X);
@@ -788,9 +796,8 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
 
 template <class R>
 void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr) {
-  k_tick<<<1, 1, 0, st>>>(S, c.dT * 0.5);
-  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S);
-  if (tr) tr->mark(st, PH_BOUNDARY_Y, 2);
+  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, c.dT * 0.5);
+  if (tr) tr->mark(st, PH_BOUNDARY_Y, 1);
   if (tr) tr->kbegin(st, KS_SWEEP_Y);
   const int ny = launch_sweep(S, c, 1, st);
   if (tr) tr->kend(st, KS_SWEEP_Y);
