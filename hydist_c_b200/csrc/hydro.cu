@@ -404,8 +404,10 @@ __global__ void k_boundary(StateT<R> S, double half) {
 // and shared between the rows, every operand before any arithmetic.
 constexpr int SMOOTH_ROWS = 4;
 
-template <class R>
-__global__ void k_smooth_full(StateT<R> S, CoefT<R> c, int isU, int hmoi) {
+// isU: t_u (else t_v); hmoi: with update_h_moi and the column flags. Both
+// are template parameters: each launch compiles to its own variant.
+template <class R, int isU, int hmoi>
+__global__ void k_smooth_full(StateT<R> S, CoefT<R> c) {
   constexpr int RB = SMOOTH_ROWS;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i0 = blockIdx.y * RB;
@@ -779,10 +781,10 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   // smoothing of t_u into su, explicit v from it, margins, smoothing of t_v
   // into sv; k_commit_a writes both back (Normalize/update_buffer pairs,
   // engine.cpp:109-124)
-  k_smooth_full<<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c, 1, 0);
+  k_smooth_full<R, 1, 0><<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c);
   k_solve_v<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c);
   k_margin_v<<<cdiv(S.N - 1, 128), 128, 0, st>>>(S, c);
-  k_smooth_full<<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c, 0, 0);
+  k_smooth_full<R, 0, 0><<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c);
   if (tr) tr->mark(st, PH_EXPLICIT_V, 4);
   // update_h_moi + update_uvz + Htuongdoi; the wet/dry mask does not change
   // in this half-step, so the segment tables are not rescanned, only the
@@ -802,11 +804,11 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   const int ny = launch_sweep(S, c, 1, st);
   if (tr) tr->kend(st, KS_SWEEP_Y);
   if (tr) tr->mark(st, PH_SWEEP_Y, ny);
-  k_smooth_full<<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c, 0, 0);
+  k_smooth_full<R, 0, 0><<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c);
   k_solve_u<<<grid2(S.M - 1, S.N, 128), 128, 0, st>>>(S, c);
   k_margin_u<<<cdiv(S.M - 1, 128), 128, 0, st>>>(S, c);
   // with update_h_moi and the wetting pass's column flags
-  k_smooth_full<<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c, 1, 1);
+  k_smooth_full<R, 1, 1><<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c);
   if (tr) tr->mark(st, PH_EXPLICIT_U, 4);
   // update_h_moi, Reset_states_vertical (wetting on flagged columns, drying
   // per cell), update_uvz, Htuongdoi, then the segment tables
