@@ -355,24 +355,43 @@ __global__ void k_boundary(StateT<R> S, double half) {
   const double* hi_down = hi_up + (N + 3);
   const double* hi_left = hi_down + (N + 3);
   const double* hi_right = hi_left + (M + 3);
+  // every operand of the four sides first (one round of memory latency);
+  // the indexed ones only where the index lies in their array
+  int mo[4], d0[4], c0[4], bt[4];
+  double bv0[4], bv1[4], cv0[4], cv1[4], hv[4], hb[4], hx[4];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const bool isU = s >= 2;
+    const int loc = s == 0 ? M : (s == 3 ? N : 2);
+    const int* moc = isU ? S.moci : S.mocj;
+    const int* dau = isU ? S.daui : S.dauj;
+    const int* cuoi = isU ? S.cuoii : S.cuoij;
+    const double* hiv = s == 0 ? hi_up : (s == 1 ? hi_down : (s == 2 ? hi_left : hi_right));
+    const int hlen = s < 2 ? N + 3 : M + 3;
+    const int ii = isU ? loc : i, jj = isU ? i : loc;
+    mo[s] = moc[loc];
+    d0[s] = dau[loc * SEG];  // only segment 0 is matched (support_funcs.cpp:614-618)
+    c0[s] = cuoi[loc * SEG];
+    bt[s] = S.btype[s * SEG];
+    bv0[s] = S.bc[s][t1];
+    bv1[s] = S.bc[s][t1 + 1];
+    cv0[s] = S.CC[s][t1];
+    cv1[s] = S.CC[s][t1 + 1];
+    hv[s] = i < hlen ? hiv[i] : 0.0;
+    hb[s] = (ii < S.H && jj < W) ? S.htaiz_bd[ii * W + jj] : 0.0;
+    hx[s] = S.hmax[s];
+  }
 #pragma unroll
   for (int s = 0; s < 4; ++s) {
     const bool isU = s >= 2;
     const int loc = s == 0 ? M : (s == 3 ? N : 2);
     const int ext = s == 0 ? M + 1 : (s == 3 ? N + 1 : 1);
-    const int* moc = isU ? S.moci : S.mocj;
-    const int* dau = isU ? S.daui : S.dauj;
-    const int* cuoi = isU ? S.cuoii : S.cuoij;
-    const double* hiv = s == 0 ? hi_up : (s == 1 ? hi_down : (s == 2 ? hi_left : hi_right));
     R* barr = s == 0 ? S.vbt : (s == 1 ? S.vbd : (s == 2 ? S.ubt : S.ubp));
-    if (moc[loc] <= 0) continue;
-    if (!(dau[loc * SEG] <= i && i <= cuoi[loc * SEG])) continue;
-    const int seg = 0;  // only segment 0 is matched (support_funcs.cpp:614-618)
-    const int bt = S.btype[s * SEG + seg];
-    const double* B = S.bc[s];
-    const double val = B[seg * S.T + t1] * (1.0f - t2h) + B[seg * S.T + t1 + 1] * t2h;
-    if (bt == 2) {
-      barr[i] = val * hiv[i];
+    if (mo[s] <= 0) continue;
+    if (!(d0[s] <= i && i <= c0[s])) continue;
+    const double val = bv0[s] * (1.0f - t2h) + bv1[s] * t2h;
+    if (bt[s] == 2) {
+      barr[i] = val * hv[s];
     } else {
       if (isU) {
         S.tz[loc * W + i] = val;
@@ -382,12 +401,11 @@ __global__ void k_boundary(StateT<R> S, double half) {
         S.tz[i * W + ext] = val;
       }
     }
-    if (bt != 2) continue;
-    const double* Cs = S.CC[s];
-    const double cv = Cs[seg * S.T + t1] * (1.0 - t2f) + Cs[seg * S.T + t1 + 1] * t2f;
+    if (bt[s] != 2) continue;
+    const double cv = cv0[s] * (1.0 - t2f) + cv1[s] * t2f;
     const int ii = isU ? loc : i;
     const int jj = isU ? i : loc;
-    S.FS[ii * W + jj] = cv * S.htaiz_bd[ii * W + jj] * S.hmax[s];
+    S.FS[ii * W + jj] = cv * hb[s] * hx[s];
   }
 }
 
