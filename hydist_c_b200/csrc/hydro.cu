@@ -518,19 +518,23 @@ __global__ void k_solve_v(StateT<R> S, CoefT<R> c) {
   __shared__ int s_n;
   const int col = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int row = blockIdx.y + 2;
+  const bool ok = row <= S.N && col <= S.M;
+  const int g = row * S.W + col;
+  // every operand, in bounds for rows 2..N and columns 2..M, is loaded
+  // with the segment table, before the lookup that decides whether the
+  // cell is updated: one round of memory latency
+  VOps<R> o;
+  if (ok) o = v_ops(S, S.su, g);  // t_u after its smoothing
   if (threadIdx.x < SEG) {
     s_first[threadIdx.x] = S.daui[row * SEG + threadIdx.x];
     s_last[threadIdx.x] = S.cuoii[row * SEG + threadIdx.x];
   }
   if (threadIdx.x == 0) s_n = S.moci[row];
   __syncthreads();
-  if (row > S.N || col > S.M) return;
+  if (!ok) return;
   int first, last;
   if (!find_seg(s_first, s_last, s_n, col, first, last)) return;
   if (first >= last || col >= last || col < first) return;
-  const int g = row * S.W + col;
-  // every operand up front: one round of memory latency
-  const VOps<R> o = v_ops(S, S.su, g);  // t_u after its smoothing
   S.tv[g] = v_new(o, c);
 }
 
