@@ -686,6 +686,12 @@ def run_ours(args):
     acc = None
     if prec != H.FP64 and rank == 0:
         acc = accuracy_vs_fp64(H, sim, bundle, dev, spin + max(args.warmup, 3) + 2 * args.steps)
+    forms = None
+    if prec == H.FP64 and rank == 0 and not args.no_forms and sed:
+        forms = measure_forms(H, sim, bundle, dev, args, ms_max / args.steps)
+    # the handle is released before the end-to-end run (its device memory
+    # goes back to the library's pool, as between two requests of a server)
+    sim.close()
     e2e = measure_e2e(H, bundle, dev, prec, args) if rank == 0 and not args.no_e2e else None
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -721,9 +727,78 @@ def run_ours(args):
         }
         if acc is not None:
             line["accuracy_vs_fp64"] = acc
+        if forms is not None:
+            line["forms"] = forms
         print(json.dumps(line), flush=True)
-    sim.close()
     R.finish(ws)
+
+
+# the state that carries from one step to the next (uploaded to start the
+# other forms and the oracle from the FP64 form's state)
+CARRY_FIELDS = ["u", "v", "z", "t_u", "t_v", "t_z", "H_moi", "Htdu", "Htdv", "FS", "tFS", "dH"]
+
+
+def measure_forms(H, sim, bundle, dev, args, fp64_ms, window=10):
+    """The FP32 and FP32 + FP64-residual refinement forms on the benchmarked
+    workload, started from the FP64 form's current state: each form's device
+    time per step (graph replay, CUDA events over args.steps steps, after a
+    window of `window` steps) and its ratio to the FP64 form's, and the
+    errors of every form after the window against the FP64 CPU oracle run
+    from the same state: max |dz| (m), relative L2 of u, v, the
+    concentration and the bed change dH, wet/dry cells that differ, and
+    the relative difference of the water volume."""
+    import torch
+    from oracle import oracle as O
+    start = {f: sim.download(f) for f in CARRY_FIELDS + ["khouot"]}
+    t0 = sim.t
+    orc = O.OracleSim(bundle, nthreads=os.cpu_count() or 1)
+    orc.load_state(start)
+    orc.t = t0
+    tw = time.perf_counter()
+    orc.step(window)
+    tw = time.perf_counter() - tw
+    want = {f: orc.get(f) for f in ("z", "u", "v", "FS", "dH", "khouot")}
+    k = want["khouot"]
+    ht = orc.get("htaiz")
+    N, M = bundle["meta"]["N"], bundle["meta"]["M"]
+    sl = (slice(2, N + 1), slice(2, M + 1))
+    p = H.capi.params_from_dict(bundle.get("params", {}))
+    vol_ref = float(np.sum(np.where(k[sl] == 0, ht[sl] + want["z"][sl], 0.0))) * p.dX * p.dY
+    orc.close()
+    out = {"window_steps": window, "oracle_s": round(tw, 2),
+           "start_t_s": t0, "oracle_threads": os.cpu_count() or 1}
+    for name, prec in (("fp64", H.FP64), ("fp32", H.FP32), ("fp32-refine", H.FP32_REFINE)):
+        f = H.Simulation(bundle, device=dev, precision=prec)
+        for fld, a in start.items():
+            f.upload(fld, a)
+        f.t = t0
+        f.step_graph(window)
+        f.sync()
+        got = {fld: f.download(fld) for fld in ("z", "u", "v", "FS", "dH", "khouot")}
+        err = {"max_abs_dz_m": float(np.abs(got["z"] - want["z"]).max())}
+        for fld in ("u", "v", "FS", "dH"):
+            den = float(np.linalg.norm(want[fld]))
+            err[f"rel_l2_{fld}"] = float(np.linalg.norm(got[fld] - want[fld]) / den) if den else 0.0
+        err["mask_cells_differing"] = int((got["khouot"] != want["khouot"]).sum())
+        err["rel_volume_diff"] = float(abs(f.mass() - vol_ref) / abs(vol_ref))
+        entry = {"errors_vs_oracle": err}
+        if name != "fp64":
+            stream = torch.cuda.ExternalStream(f.stream, device=dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f.step_graph(3)
+            torch.cuda.synchronize(dev)
+            e0.record(stream)
+            f.step_graph(args.steps)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ms = e0.elapsed_time(e1) / args.steps
+            entry.update(ms_per_step=ms, value=bundle["meta"]["cells"] / (ms * 1e-3),
+                         vs_fp64=fp64_ms / ms)
+        else:
+            entry["ms_per_step"] = fp64_ms
+        out[name] = entry
+        f.close()
+    return out
 
 
 def accuracy_vs_fp64(H, sim, bundle, dev, nsteps):
@@ -774,6 +849,7 @@ def measure_e2e(H, bundle, dev, prec, args):
     sim = H.Simulation(b, device=dev, precision=prec)
     sim.sync()
     t1 = time.perf_counter()
+    create = {k: round(v, 3) for k, v in sim.create_phases().items()}
     for _ in range(args.steps):
         (sim.step_graph if args.graph else sim.step)(1)
         sim.mass()
@@ -787,7 +863,7 @@ def measure_e2e(H, bundle, dev, prec, args):
     return {"value": cells * steps / dt, "unit": "cell-steps/s",
             "h2d_bytes_per_step": h2d / steps,
             "d2h_bytes_per_step": (8 * args.steps + 4 * 8 * n) / steps,
-            "wall_s": dt, "create_s": t1 - t0, "steps_s": t2 - t1,
+            "wall_s": dt, "create_s": t1 - t0, "create_phases_ms": create, "steps_s": t2 - t1,
             "download_s": dt - (t2 - t0), "steps": steps}
 
 
@@ -815,6 +891,8 @@ def main():
                          "step's CUDA graph (hydist_step instead of hydist_step_graph)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the FP32 forms and their errors against the oracle")
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--sed0", action="store_true",
                     help="sediment sweeps from t=0 instead of a spin-up to t=600 s")

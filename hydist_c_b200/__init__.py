@@ -170,6 +170,12 @@ class Simulation:
         capi.check(self._lib, self._lib.hydist_checkpoint_load(self._h, str(path).encode()),
                    "hydist_checkpoint_load")
 
+    def create_phases(self) -> dict:
+        """Host time of this handle's creation by part (ms)."""
+        ms = (C.c_double * 4)()
+        capi.check(self._lib, self._lib.hydist_create_phases(self._h, ms), "hydist_create_phases")
+        return dict(zip(("alloc_ms", "inputs_ms", "setup_ms", "total_ms"), list(ms)))
+
     def mass(self) -> float:
         v = C.c_double()
         capi.check(self._lib, self._lib.hydist_mass(self._h, C.byref(v)), "hydist_mass")

@@ -47,7 +47,9 @@ class HydistOptions(C.Structure):
     _fields_ = [("t_start", C.c_double), ("sediment_start", C.c_double),
                 ("bed_change_start", C.c_double), ("ketdinh", C.c_int32),
                 ("bed_change", C.c_int32), ("precision", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("kenhhepd", C.c_int32), ("kenhhepng", C.c_int32),
+                ("channel_wave", C.c_int32), ("reset_horizontal", C.c_int32),
+                ("bed_feedback", C.c_int32), ("reserved", C.c_int32)]
 
 
 class HydistScenario(C.Structure):
@@ -56,7 +58,7 @@ class HydistScenario(C.Structure):
                 ("h", _dp), ("hsnham", _dp), ("visco", _dp), ("Fw", _dp),
                 ("bc_up", _dp), ("bc_down", _dp), ("bc_left", _dp), ("bc_right", _dp),
                 ("CC_up", _dp), ("CC_down", _dp), ("CC_left", _dp), ("CC_right", _dp),
-                ("boundary_type", _ip), ("bienQ", C.c_int32 * 4), ("FS0", _dp)]
+                ("boundary_type", _ip), ("bienQ", C.c_int32 * 4), ("FS0", _dp), ("z0", _dp)]
 
 
 _vp = C.c_void_p
@@ -118,8 +120,9 @@ class ScenarioStruct:
                   "CC_up", "CC_down", "CC_left", "CC_right"):
             self.arrays[k] = np.ascontiguousarray(sc[k], dtype=np.float64)
         self.arrays["boundary_type"] = np.ascontiguousarray(sc["boundary_type"], dtype=np.int32)
-        fs0 = sc.get("FS0")
-        self.arrays["FS0"] = None if fs0 is None else np.ascontiguousarray(fs0, dtype=np.float64)
+        for k in ("FS0", "z0"):
+            a = sc.get(k)
+            self.arrays[k] = None if a is None else np.ascontiguousarray(a, dtype=np.float64)
         s = HydistScenario()
         s.M, s.N, s.total_time = int(sc["M"]), int(sc["N"]), int(sc["total_time"])
         s.n_boundary_type = int(self.arrays["boundary_type"].size)
@@ -130,6 +133,7 @@ class ScenarioStruct:
         for k in range(4):
             s.bienQ[k] = int(sc["bienQ"][k])
         s.FS0 = _ptr(self.arrays["FS0"])
+        s.z0 = _ptr(self.arrays["z0"])
         self.struct = s
 
 
@@ -197,6 +201,7 @@ def _declare(lib):
     lib.hydist_step_traced.argtypes = [vp, C.POINTER(C.c_float)]
     lib.hydist_step_traced_sweeps.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
     lib.hydist_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
+    lib.hydist_create_phases.argtypes = [vp, C.POINTER(C.c_double)]
     lib.hydist_gtsv_batched.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32,
                                         C.c_int32, vp]
     lib.hydist_gtsv_batched_noalloc.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int32,
@@ -253,6 +258,7 @@ EXPORTED_SYMBOLS = [
     "hydist_server_destroy", "hydist_server_submit", "hydist_server_round",
     "hydist_server_status", "hydist_server_counts", "hydist_server_handle",
     "hydist_server_release", "hydist_checkpoint_save", "hydist_checkpoint_load",
+    "hydist_create_phases",
 ]
 GTSV_AUTO, GTSV_THOMAS, GTSV_PARTITION, GTSV_WARP, GTSV_PARTITION_512, GTSV_PARTITION_128 = \
     0, 1, 2, 3, 4, 5

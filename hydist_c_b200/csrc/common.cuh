@@ -43,8 +43,17 @@ struct CoefT {
 };
 using Coef = CoefT<double>;
 
-// Device error codes recorded in State::err[0].
-enum DevErr { DEV_OK = 0, DEV_SEG_OVERFLOW = 1 };
+// Device error flags recorded (or-ed) in State::err[0]: a line with more
+// wet segments than the tables hold; a non-finite value committed to the
+// state (NaN/Inf canary of the commits).
+enum DevErr { DEV_OK = 0, DEV_SEG_OVERFLOW = 1, DEV_NONFINITE = 2 };
+
+// Records a non-finite committed value (the store of the flag runs only
+// when one is found).
+template <class T>
+__device__ __forceinline__ void canary(int* err, T a, T b, T c) {
+  if (!(isfinite(a) && isfinite(b) && isfinite(c))) atomicOr(err, DEV_NONFINITE);
+}
 
 // Every device pointer of one scenario. Passed by value to kernels. The
 // water level (z, t_z), the bed (h, htaiz, htaiz_bd, dH), the series and the
@@ -58,6 +67,16 @@ struct StateT {
   int ketdinh;
   int race_new;    // extraction at an open last end reads the new neighbour
   int refine;      // line solves refined once with an FP64 residual
+  // boundary update: 0 the hourly series (Update_Boundary_Value); in the
+  // narrow-channel mode 1 none (update_boundary_at_t, engine.cpp:24-30) or
+  // 2 the standing wave of boundary_up/down/left/right
+  int chan;
+  // line ranges of the hydraulic sweeps: columns x_lo..x_hi (x sweep), rows
+  // y_lo..N (y sweep); 3..M-1 / 3..N in the narrow-channel mode
+  int x_lo, x_hi, y_lo;
+  int reset_h;     // Reset_states_horizontal in the first half-step
+  int bed_fb;      // the bed change feeds back into h, htaiz, Kx1, Ky1
+  const double *h0, *htaiz0;  // the initial bed (with bed_fb)
   // static fields
   const double *h, *hsnham, *htaiz, *htaiz_bd;
   const R *visco, *Fw, *Kx1, *Ky1, *Tsxw, *Tsyw;
@@ -79,6 +98,7 @@ struct StateT {
   R* lscratch;   // partitioned line solver: one slot per resident CTA
   int lslots;    // number of slots (CTAs of the persistent sweep grid)
   int* colflag;  // per column: holds a cell dried during the run
+  int* rowflag;  // per row: the same (wetting along rows)
   int* segcnt;   // run-start / run-end counters of the segment scan
   double* clock; // [0]: simulated time, advanced on the device by k_tick
 };

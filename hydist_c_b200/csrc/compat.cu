@@ -143,8 +143,12 @@ HydistExternal external_of(const Argument_Pointers& a, int total_time, const int
 // reads become HydistOptions.
 HydistHandle* adopt(const Argument_Pointers& a, const Constant_Coeffs& c, double dT,
                     double NANGDAY, int total_time, double t_start, double sediment_start,
-                    double bed_change_start, bool ketdinh) {
-  if (c.kenhhepd != 0 || c.kenhhepng != 0) compat_fail("the narrow-channel mode is not supported");
+                    double bed_change_start, bool ketdinh, bool kenhhepd = false,
+                    bool kenhhepng = false) {
+  // update_uvz's coefficients (support_funcs.cpp:745-758); Load_coeffs sets
+  // both to 0 (loader.cpp:18-19) whatever the options
+  if (c.kenhhepd != 0 || c.kenhhepng != 0)
+    compat_fail("Constant_Coeffs kenhhepd/kenhhepng other than 0 are not supported");
   int bienQ[4] = {0, 0, 0, 0};
   CC(cudaMemcpy(bienQ, a.bienQ, sizeof(bienQ), cudaMemcpyDeviceToHost));
   const HydistExternal e = external_of(a, total_time, bienQ);
@@ -155,6 +159,8 @@ HydistHandle* adopt(const Argument_Pointers& a, const Constant_Coeffs& c, double
   o.sediment_start = sediment_start;
   o.bed_change_start = bed_change_start;
   o.ketdinh = ketdinh ? 1 : 0;
+  o.kenhhepd = kenhhepd ? 1 : 0;
+  o.kenhhepng = kenhhepng ? 1 : 0;
   HydistHandle* h = nullptr;
   HC(hydist_create_external(&e, &p, &o, -1, &h));
   return h;
@@ -210,12 +216,15 @@ void Hydraulic_Calculation(double dT, double NANGDAY, Argument_Pointers* d_arg_p
                            Argument_Pointers h_arg_ptr, Options ops) {
   (void)d_arg_ptr;
   (void)d_arr_ptr;
-  if (ops.channel) compat_fail("the narrow-channel mode is not supported");
   CC(cudaDeviceSynchronize());
   Constant_Coeffs c;
   CC(cudaMemcpy(&c, coeffs, sizeof(c), cudaMemcpyDeviceToHost));
+  // the narrow-channel mode (ops.channel = kenhhepd xor kenhhepng) is the
+  // handle's: no boundary update and the sweeps' index ranges of
+  // engine.cpp:77-80, 190-193
   HydistHandle* h = adopt(h_arg_ptr, c, dT, NANGDAY, ops.total_time, ops.t_start,
-                          ops.sediment_start, ops.bed_change_start, ops.ketdinh);
+                          ops.sediment_start, ops.bed_change_start, ops.ketdinh, ops.kenhhepd,
+                          ops.kenhhepng);
   double t = ops.t_start;
   const int Tmax = (int)ops.Tmax;  // the reference compares with int(Tmax)
   while (t < Tmax) {

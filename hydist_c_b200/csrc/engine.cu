@@ -8,10 +8,13 @@
 //                (the reference synchronises after each, engine.cpp:13-19)
 // hydist_step_graph  the same step captured once into a CUDA graph per
 //                sediment phase and replayed
+#include <chrono>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -141,9 +144,41 @@ struct HydistHandle {
   cudaEvent_t ev[PH_COUNT + 1] = {};
   cudaEvent_t kev[2 * KS_COUNT] = {};
   int next_half = 0;  // 1 while the second half of a step is pending
+  // host time of hydist_create by part (ms): device allocation and zeroing,
+  // input copies, set-up kernels, total
+  double create_ms[4] = {};
 };
 
 namespace {
+
+using Clock = std::chrono::steady_clock;
+double ms_since(Clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+}
+
+// One memory pool per device for the handles' arrays, keeping what destroyed
+// handles release (release threshold unlimited): a create after a destroy
+// reuses device pages that are already mapped instead of asking the driver
+// for new ones, which on a GPU's first use of the memory costs tens of ms
+// per GB. The pool's memory goes back to the driver at process exit.
+cudaMemPool_t handle_pool(int dev) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
 
 // The launchers of the handle's form: f(state, coefficients).
 template <class F>
@@ -187,9 +222,14 @@ int dalloc(HydistHandle* h, T** p, size_t n) {
         sz = o + bj;
       }
       void* q = nullptr;
-      CK(cudaMalloc(&q, sz));
+      const auto ta = Clock::now();
+      cudaMemPool_t pool = handle_pool(h->device);
+      if (!pool) return fail(HYDIST_ERR_CUDA, "no device memory pool");
+      CK(cudaMallocFromPoolAsync(&q, sz, pool, h->stream));
       h->allocs.push_back(q);
       CK(cudaMemsetAsync(q, 0, sz, h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+      h->create_ms[0] += ms_since(ta);
       h->chunk = static_cast<char*>(q);
       h->chunk_size = sz;
       off = 0;
@@ -200,7 +240,9 @@ int dalloc(HydistHandle* h, T** p, size_t n) {
     return HYDIST_OK;
   }
   void* q = nullptr;
-  CK(cudaMalloc(&q, raw));
+  cudaMemPool_t pool = handle_pool(h->device);
+  if (!pool) return fail(HYDIST_ERR_CUDA, "no device memory pool");
+  CK(cudaMallocFromPoolAsync(&q, raw, pool, h->stream));
   CK(cudaMemsetAsync(q, 0, raw, h->stream));
   h->allocs.push_back(q);
   *p = static_cast<T*>(q);
@@ -217,7 +259,9 @@ int check_device_err(HydistHandle* h) {
   int e = 0;
   CK(cudaMemcpyAsync(&e, h->S.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  if (e == DEV_SEG_OVERFLOW) return fail(HYDIST_ERR_SEGMENTS, "a line has more than 20 wet segments");
+  if (e & DEV_SEG_OVERFLOW) return fail(HYDIST_ERR_SEGMENTS, "a line has more than 20 wet segments");
+  if (e & DEV_NONFINITE)
+    return fail(HYDIST_ERR_NONFINITE, "a NaN or Inf was committed to u, v, z or the concentration");
   return HYDIST_OK;
 }
 
@@ -435,6 +479,9 @@ int check_params(const HydistParams* p, const HydistOptions* o) {
   if (o->precision != HYDIST_FP64 && o->precision != HYDIST_FP32_REFINE &&
       o->precision != HYDIST_FP32)
     return fail(HYDIST_ERR_ARG, "unknown precision");
+  for (int32_t f : {o->ketdinh, o->bed_change, o->kenhhepd, o->kenhhepng, o->channel_wave,
+                    o->reset_horizontal, o->bed_feedback})
+    if (f != 0 && f != 1) return fail(HYDIST_ERR_ARG, "option flags must be 0 or 1");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(HYDIST_ERR_NODEVICE, "no CUDA device");
@@ -465,6 +512,14 @@ int new_handle(const HydistParams* p, const HydistOptions* o, int device, int M,
   S.ketdinh = o->ketdinh ? 1 : 0;
   S.race_new = 1;
   S.refine = o->precision == HYDIST_FP32_REFINE ? 1 : 0;
+  // the reference's channel = kenhhepd xor kenhhepng (engine.h:33)
+  const bool channel = (o->kenhhepd != 0) != (o->kenhhepng != 0);
+  S.chan = channel ? (o->channel_wave ? 2 : 1) : 0;
+  S.x_lo = channel && o->kenhhepd ? 3 : 2;
+  S.x_hi = channel && o->kenhhepd ? M - 1 : M;
+  S.y_lo = channel && o->kenhhepng ? 3 : 2;
+  S.reset_h = o->reset_horizontal ? 1 : 0;
+  S.bed_fb = o->bed_change && o->bed_feedback ? 1 : 0;
   return HYDIST_OK;
 }
 
@@ -500,6 +555,7 @@ int private_arrays(HydistHandle* h) {
   TRY(dalloc(h, &S.hmax, 4));
   TRY(dalloc(h, &S.err, 4));
   TRY(dalloc(h, &S.colflag, S.W));
+  TRY(dalloc(h, &S.rowflag, S.H));
   TRY(dalloc(h, &S.segcnt, 2 * S.H + 2 * S.W));
   TRY(dalloc(h, &S.clock, 4));
   TRY(set_device_clock(h));
@@ -518,6 +574,12 @@ template <class R>
 int upload_new(HydistHandle* h, R** dst, const double* host, size_t n) {
   TRY(dalloc(h, dst, n));
   if (!host || h->planning) return HYDIST_OK;
+  const auto t0 = Clock::now();
+  struct Acc {
+    double& ms;
+    Clock::time_point t0;
+    ~Acc() { ms += ms_since(t0); }
+  } acc{h->create_ms[1], t0};
   if (sizeof(R) == 8) {
     CK(cudaMemcpyAsync(*dst, host, n * 8, cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -571,6 +633,14 @@ void mirror_common(HydistHandle* h) {
   F.ketdinh = S.ketdinh;
   F.race_new = S.race_new;
   F.refine = S.refine;
+  F.chan = S.chan;
+  F.x_lo = S.x_lo;
+  F.x_hi = S.x_hi;
+  F.y_lo = S.y_lo;
+  F.reset_h = S.reset_h;
+  F.bed_fb = S.bed_fb;
+  F.h0 = S.h0;
+  F.htaiz0 = S.htaiz0;
   F.h = S.h;
   F.hsnham = S.hsnham;
   F.htaiz = S.htaiz;
@@ -594,6 +664,7 @@ void mirror_common(HydistHandle* h) {
   F.mocj = S.mocj;
   F.err = S.err;
   F.colflag = S.colflag;
+  F.rowflag = S.rowflag;
   F.segcnt = S.segcnt;
   F.clock = S.clock;
 }
@@ -628,6 +699,7 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistO
   if (sc->n_boundary_type < 4 * SEG)
     return fail(HYDIST_ERR_ARG, "boundary_type needs 4 sides x 20 segments");
   TRY(check_params(p, o));
+  const auto t_create = Clock::now();
   HydistHandle* h = nullptr;
   int rc = new_handle(p, o, device, sc->M, sc->N, sc->total_time, sc->bienQ, &h);
   if (rc == HYDIST_OK) rc = with_arena(h, [&]() -> int {
@@ -656,8 +728,15 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistO
     S.htaiz = tmp;
     TRY(dalloc(h, &tmp, n));
     S.htaiz_bd = tmp;
-    TRY(dalloc(h, &S.z, n));
-    TRY(dalloc(h, &S.tz, n));
+    if (S.bed_fb) {
+      // the initial bed, copied after the set-up kernels
+      TRY(dalloc(h, &tmp, n));
+      S.h0 = tmp;
+      TRY(dalloc(h, &tmp, n));
+      S.htaiz0 = tmp;
+    }
+    TRY(upload_new(h, &S.z, sc->z0, n));
+    TRY(upload_new(h, &S.tz, sc->z0, n));
     TRY(dalloc(h, &S.dH, n));
     TRY(dalloc(h, &S.khouot, n));
     TRY(dalloc(h, &S.daui, S.H * SEG));
@@ -674,16 +753,32 @@ int hydist_create(const HydistScenario* sc, const HydistParams* p, const HydistO
     return HYDIST_OK;
   });
   if (rc == HYDIST_OK) rc = [&]() -> int {
+    const auto t_init = Clock::now();
     on_state(h, [&](auto& St, auto& Cf) { launch_init(St, Cf, h->stream); });
     CK(cudaGetLastError());
+    const size_t nb = (size_t)h->S.W * h->S.H * sizeof(double);
+    if (h->S.bed_fb) {
+      CK(cudaMemcpyAsync(const_cast<double*>(h->S.h0), h->S.h, nb, cudaMemcpyDeviceToDevice,
+                         h->stream));
+      CK(cudaMemcpyAsync(const_cast<double*>(h->S.htaiz0), h->S.htaiz, nb,
+                         cudaMemcpyDeviceToDevice, h->stream));
+    }
     TRY(check_device_err(h));
+    h->create_ms[2] = ms_since(t_init);
     return HYDIST_OK;
   }();
   if (rc != HYDIST_OK) {
     hydist_destroy(h);
     return rc;
   }
+  h->create_ms[3] = ms_since(t_create);
   *out = h;
+  return HYDIST_OK;
+}
+
+int hydist_create_phases(const HydistHandle* h, double* ms) {
+  if (!h || !ms) return fail(HYDIST_ERR_ARG, "null argument");
+  for (int k = 0; k < 4; ++k) ms[k] = h->create_ms[k];
   return HYDIST_OK;
 }
 
@@ -705,6 +800,9 @@ int hydist_create_external(const HydistExternal* e, const HydistParams* p, const
   TRY(check_params(p, o));
   if (o->precision != HYDIST_FP64)
     return fail(HYDIST_ERR_ARG, "caller-owned arrays are FP64: use HYDIST_FP64");
+  if (o->bed_change && o->bed_feedback)
+    return fail(HYDIST_ERR_ARG,
+                "bed_feedback rewrites h, htaiz, Kx1 and Ky1, which an external handle only reads");
   HydistHandle* h = nullptr;
   int rc = new_handle(p, o, device, e->M, e->N, e->total_time, e->bienQ, &h);
   if (rc == HYDIST_OK) rc = [&]() -> int {
@@ -809,7 +907,7 @@ int hydist_update_boundary(HydistHandle* h, double t) {
   h->t = t;
   int rc = set_device_clock(h);
   if (rc == HYDIST_OK) {
-    on_state(h, [&](auto& St, auto&) { launch_boundary(St, h->stream); });
+    on_state(h, [&](auto& St, auto& Cf) { launch_boundary(St, Cf, h->stream); });
     h->trace.launches += 1;
     rc = cudaGetLastError() == cudaSuccess ? HYDIST_OK : fail(HYDIST_ERR_CUDA, "boundary launch failed");
   }
@@ -826,7 +924,9 @@ int hydist_destroy(HydistHandle* h) {
     if (g) cudaGraphExecDestroy(g);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
-  for (void* p : h->allocs) cudaFree(p);
+  // back into the device's pool (see handle_pool)
+  for (void* p : h->allocs) cudaFreeAsync(p, h->stream);
+  if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->mass_host) cudaFreeHost(h->mass_host);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -1141,20 +1241,25 @@ int hydist_checkpoint_load(HydistHandle* h, const char* path) {
     std::fclose(f);
     return fail(HYDIST_ERR_ARG, "the checkpoint is of another mesh size");
   }
+  // the whole body is read and its size checked before anything is
+  // uploaded, so a truncated or oversized file leaves the handle unchanged
   const size_t n = (size_t)h->S.W * h->S.H;
-  std::vector<double> buf(n);
+  std::vector<double> body((size_t)nf * n);
   std::vector<int32_t> mask(n);
-  bool ok = true;
-  CK(cudaStreamSynchronize(h->stream));
-  for (int fid : kCheckpointFields) {
-    ok = std::fread(buf.data(), 8, n, f) == n &&
-         field_from_host(h, field_ref(h, fid), buf.data(), n) == HYDIST_OK;
-    if (!ok) break;
-  }
-  ok = ok && std::fread(mask.data(), 4, n, f) == n &&
-       cudaMemcpy(h->S.khouot, mask.data(), n * 4, cudaMemcpyHostToDevice) == cudaSuccess;
+  bool ok = std::fread(body.data(), 8, body.size(), f) == body.size() &&
+            std::fread(mask.data(), 4, n, f) == n;
+  char extra;
+  ok = ok && std::fread(&extra, 1, 1, f) == 0 && std::feof(f);
   std::fclose(f);
-  if (!ok) return fail(HYDIST_ERR_ARG, std::string("truncated or unreadable checkpoint: ") + path);
+  if (!ok)
+    return fail(HYDIST_ERR_ARG, std::string("checkpoint size does not match header + ") +
+                                    std::to_string(nf) + " fields + mask: " + path);
+  CK(cudaStreamSynchronize(h->stream));
+  for (int k = 0; k < nf; ++k)
+    TRY(field_from_host(h, field_ref(h, kCheckpointFields[k]), body.data() + (size_t)k * n, n));
+  CK(cudaMemcpy(h->S.khouot, mask.data(), n * 4, cudaMemcpyHostToDevice));
+  // with the bed feedback, the bed follows from the initial bed and dH
+  if (h->S.bed_fb) on_state(h, [&](auto& St, auto& Cf) { launch_bed_feedback(St, Cf, h->stream); });
   on_state(h, [&](auto& St, auto& Cf) { launch_scan_segments(St, Cf, false, h->stream); });
   CK(cudaGetLastError());
   h->t = hd.t;

@@ -135,10 +135,12 @@ __device__ __forceinline__ void run_flags(bool wm1, bool w, bool wp1, bool wm2_l
 }
 
 // With dry != 0 the drying pass of Reset_states_vertical
-// (support_funcs.cpp:177-186) is applied on the fly: a wet cell of rows
-// 2..N, columns 1..M whose depth is at most H_TINH reads as dried (1) and
-// is written so. Reading a neighbour's mask while its thread writes it is
-// safe: the write turns 0 into 1 exactly when this test gives 1.
+// (support_funcs.cpp:177-186; dry = 1) or of Reset_states_horizontal
+// (:125-137; dry = 2) is applied on the fly: a wet cell of its range (rows
+// 2..N, columns 1..M; rows 1..N, columns 2..M) whose depth is at most H_TINH
+// reads as dried (1) and is written so. Reading a neighbour's mask while
+// its thread writes it is safe: the write turns 0 into 1 exactly when this
+// test gives 1.
 template <class R>
 __global__ void k_runs_flags(StateT<R> S, CoefT<R> c, int* seg_cnt, int dry) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
@@ -157,18 +159,23 @@ __global__ void k_runs_flags(StateT<R> S, CoefT<R> c, int* seg_cnt, int dry) {
     kk[n] = K[qs[n]];
     hh[n] = dry ? S.Hmoi[qs[n]] : R(0);
   }
+  const int ilo = dry == 2 ? 1 : 2, jlo = dry == 2 ? 2 : 1;
   auto mask = [&](int n, int qi, int qj) -> int {
     const int k = kk[n];
-    if (dry && k == 0 && qi >= 2 && qi <= S.N && qj >= 1 && qj <= S.M && hh[n] <= c.H_TINH)
+    if (dry && k == 0 && qi >= ilo && qi <= S.N && qj >= jlo && qj <= S.M && hh[n] <= c.H_TINH)
       return 1;
     return k;
   };
   if (dry) {
     const int k0 = mask(0, i, j);
     if (k0 != kk[0]) K[g] = k0;
-    if (j == 2) {  // column 1 is outside this grid
+    if (dry == 1 && j == 2) {  // column 1 is outside this grid
       const int k1 = mask(1, i, 1);
       if (k1 != kk[1]) K[g - 1] = k1;
+    }
+    if (dry == 2 && i == 2) {  // and so is row 1
+      const int k4 = mask(4, 1, j);
+      if (k4 != kk[4]) K[g - W] = k4;
     }
   }
   const bool w = mask(0, i, j) == 0;
@@ -243,7 +250,7 @@ __global__ void k_runs_sort(StateT<R> S, int* seg_cnt) {
   }
   int n = *cs;
   if (n > SEG || *ce != n) {
-    atomicExch(S.err, DEV_SEG_OVERFLOW);
+    atomicOr(S.err, DEV_SEG_OVERFLOW);
     n = min(n, SEG);
   }
   sort_small(dau, n);
@@ -333,8 +340,51 @@ __global__ void k_preprocess_sides(StateT<R> S, CoefT<R> c, double* p53) {
 // parameter in the reference (engine.cpp:22), hence the rounding. With half
 // != 0 the last block to finish stores the advanced clock (clock[1] counts
 // the blocks), after every block has read the old one.
+//
+// In the narrow-channel mode (S.chan) the series are not applied
+// (update_boundary_at_t, engine.cpp:24-30); with S.chan == 2 the standing
+// wave of boundary_up / boundary_down / boundary_left / boundary_right
+// (support_funcs.cpp:366-478) is imposed instead: thread i takes row i of
+// the up and down sides and column i of the left and right ones, each side
+// over the first wet segment of its line (the right side from row 2's
+// first start to row N's first end, as written there).
 template <class R>
-__global__ void k_boundary(StateT<R> S, double half) {
+__device__ void channel_wave_cell(const StateT<R>& S, double dX, double dY, double t, int i) {
+  const int M = S.M, N = S.N, W = S.W;
+  const double PI_ = 3.14159265358979323846;
+  const double ct = cos(2 * PI_ / 27.75 * t);
+  if (S.mocj[M] > 0 && S.dauj[M * SEG] <= i && i <= S.cuoij[M * SEG]) {
+    S.tz[i * W + M] = 0.01 * ct * cos(2 * (PI_ / 100) * (100 - dY / 2));
+    S.tz[i * W + M + 1] = 0.01 * ct * cos(2 * (PI_ / 100) * (100 + dY / 2));
+  }
+  if (S.mocj[2] > 0 && S.dauj[2 * SEG] <= i && i <= S.cuoij[2 * SEG]) {
+    if (S.bienQ[1]) {
+      S.vbd[i] = 0;
+    } else {
+      S.tz[i * W + 2] = 0.01 * ct * cos(2 * (PI_ / 100) * dY / 2);
+      S.tz[i * W + 1] = 0.01 * ct * cos(2 * (PI_ / 100) * (-dY) / 2);
+    }
+  }
+  if (S.moci[2] > 0 && S.daui[2 * SEG] <= i && i <= S.cuoii[2 * SEG]) {
+    if (S.bienQ[2]) {
+      S.ubt[i] = 0;
+    } else {
+      S.tz[2 * W + i] = 0.01 * ct * cos(2 * (PI_ / 100) * dX / 2);
+      S.tz[1 * W + i] = 0.01 * ct * cos(2 * (PI_ / 100) * (-dX) / 2);
+    }
+  }
+  if (S.moci[2] > 0 && S.moci[N] > 0 && S.daui[2 * SEG] <= i && i <= S.cuoii[N * SEG]) {
+    if (S.bienQ[3]) {
+      S.ubp[i] = 0;
+    } else {
+      S.tz[N * W + i] = 0.01 * ct * cos(2 * (PI_ / 100) * (100 - dX / 2));
+      S.tz[(N + 1) * W + i] = 0.01 * ct * cos(2 * (PI_ / 100) * (100 + dX / 2));
+    }
+  }
+}
+
+template <class R>
+__global__ void k_boundary(StateT<R> S, double half, double dX, double dY) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int M = S.M, N = S.N, W = S.W;
   const double t_new = S.clock[0] + half;
@@ -347,6 +397,10 @@ __global__ void k_boundary(StateT<R> S, double half) {
   }
   if (i > M && i > N) return;
   const double t = (double)(float)t_new;
+  if (S.chan) {
+    if (S.chan == 2) channel_wave_cell(S, dX, dY, t, i);
+    return;
+  }
   // the host refuses steps past the series; the clamp keeps reads in bounds
   const int t1 = min(max((int)(t / 3600), 0), S.T - 2);
   const double t2h = (t - (double)(3600.0f * (float)t1)) / 3600.0f;
@@ -416,7 +470,8 @@ __global__ void k_boundary(StateT<R> S, double half) {
 // Readers of the smoothed velocity use it directly and the half-step commit
 // writes it back to t_u / t_v, u / v. hmoi != 0 (the last smoothing of
 // half-step B, after the explicit u update that reads H_moi) also does
-// update_h_moi and flags the columns the wetting pass must visit.
+// update_h_moi and flags the columns (hmoi = 1) or rows (hmoi = 2) the
+// wetting pass must visit.
 // One thread smooths SMOOTH_ROWS consecutive rows of a column: the column's
 // values and mask over those rows and the two around them are loaded once
 // and shared between the rows, every operand before any arithmetic.
@@ -470,7 +525,13 @@ __global__ void k_smooth_full(StateT<R> S, CoefT<R> c) {
     if (hmoi && i >= 1 && i <= N + 1 && j >= 1 && j <= M) {
       const int kh = kcol[r + 1];
       if (i <= N && kh == 0) S.Hmoi[g] = S.htaiz[g] + S.tz[g];
-      if (kh == 1) S.colflag[j] = 1;
+      if (kh == 1) {
+        if (hmoi == 2) {
+          if (i <= N) S.rowflag[i] = 1;
+        } else {
+          S.colflag[j] = 1;
+        }
+      }
     }
     const R vg = col[r + 1];
     R out = vg;
@@ -648,6 +709,7 @@ __global__ void k_commit_a(StateT<R> S, CoefT<R> c, int vth_hi) {
   S.z[g] = tz;
   S.u[g] = tu * (1 - c.kenhhepd);
   S.v[g] = tv * (1 - c.kenhhepng);
+  canary(S.err, (double)tu, (double)tv, tz);
   if (in) {
     const R Hu = (hl + hp + zd + tz) * 0.5;
     const R Hv = (hup + hp + zr + tz) * 0.5;
@@ -687,6 +749,37 @@ __global__ void k_wetting(StateT<R> S, CoefT<R> c, int* colflag) {
   }
 }
 
+// The wetting loop of Reset_states_horizontal (support_funcs.cpp:103-120),
+// sequential along j, on flagged rows 1..N only.
+template <class R>
+__global__ void k_wetting_rows(StateT<R> S, CoefT<R> c, int* rowflag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i > S.N) return;
+  if (!rowflag[i]) return;
+  rowflag[i] = 0;
+  const int M = S.M;
+  const size_t r = (size_t)i * S.W;
+  double* tz = S.tz;
+  R* Hm = S.Hmoi;
+  int* kh = S.khouot;
+  for (int j = 2; j <= M; ++j) {
+    if (tz[r + j] > S.z[r + j]) {
+      if (kh[r + j - 1] == 1) {
+        tz[r + j - 1] = tz[r + j];
+        Hm[r + j - 1] = S.htaiz[r + j - 1] + tz[r + j];
+        kh[r + j - 1] = 0;
+        S.FS[r + j - 1] = S.FS[r + j];
+      }
+      if (kh[r + j + 1] == 1) {
+        tz[r + j + 1] = tz[r + j];
+        Hm[r + j + 1] = S.htaiz[r + j + 1] + tz[r + j];
+        kh[r + j + 1] = 0;
+        S.FS[r + j + 1] = S.FS[r + j];
+      }
+    }
+  }
+}
+
 // Half-step B commit: the drying loop of Reset_states_vertical (:177-187,
 // independent per cell), update_uvz and Htuongdoi. A drying cell (i,j)
 // zeroes t_u at (i-1,j),(i,j) and t_v at (i,j-1),(i,j); each cell here reads
@@ -696,7 +789,10 @@ __global__ void k_wetting(StateT<R> S, CoefT<R> c, int* colflag) {
 // k_commit_a: the segment scan and the boundary interpolation that follow
 // change none of their operands. The committed t_u(i-1, j) and t_v(i, j-1)
 // are rebuilt here from the same drying tests their own threads make.
-template <class R>
+//
+// HORIZ: the drying loop of Reset_states_horizontal instead (:125-137,
+// rows 1..N, columns 2..M), in the first half-step.
+template <class R, int HORIZ>
 __global__ void k_commit_b(StateT<R> S, CoefT<R> c, int vth_hi) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
@@ -706,8 +802,12 @@ __global__ void k_commit_b(StateT<R> S, CoefT<R> c, int vth_hi) {
   const bool vth = in && i <= vth_hi;
   // every operand before the first store (one round of memory latency);
   // nothing this kernel stores is read by another of its threads. A cell
-  // dries when it is wet with H_moi at most H_TINH (rows 2..N, columns 1..M).
-  auto in_dry = [&](int ii, int jj) { return ii >= 2 && ii <= S.N && jj >= 1 && jj <= S.M; };
+  // dries when it is wet with H_moi at most H_TINH (rows 2..N, columns 1..M;
+  // rows 1..N, columns 2..M with HORIZ).
+  auto in_dry = [&](int ii, int jj) {
+    return HORIZ ? (ii >= 1 && ii <= S.N && jj >= 2 && jj <= S.M)
+                 : (ii >= 2 && ii <= S.N && jj >= 1 && jj <= S.M);
+  };
   const bool c0 = in_dry(i, j), cd = in_dry(i + 1, j), cr = in_dry(i, j + 1);
   const bool cu = vth && in_dry(i - 1, j), cl = vth && in_dry(i, j - 1);
   const int k0 = c0 ? S.khouot[g] : 1, kd = cd ? S.khouot[g + W] : 1, kr = cr ? S.khouot[g + 1] : 1;
@@ -736,6 +836,7 @@ __global__ void k_commit_b(StateT<R> S, CoefT<R> c, int vth_hi) {
   S.z[g] = tz;
   S.u[g] = tu * (1 - c.kenhhepd);
   S.v[g] = tv * (1 - c.kenhhepng);
+  canary(S.err, tu, tv, tz);
   if (in) {
     const R Hu = (hl + hp + zd + tz) * 0.5;
     const R Hv = (hup + hp + zr + tz) * 0.5;
@@ -773,8 +874,8 @@ void launch_preprocess(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
 }
 
 template <class R>
-void launch_boundary(const StateT<R>& S, cudaStream_t st) {
-  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, 0.0);
+void launch_boundary(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
+  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, 0.0, (double)c.dX, (double)c.dY);
 }
 
 template <class R>
@@ -794,7 +895,7 @@ void launch_find_limits(const StateT<R>& S, const CoefT<R>& c, bool dry, cudaStr
 
 template <class R>
 void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr) {
-  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, 0.5 * c.dT);
+  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, 0.5 * c.dT, (double)c.dX, (double)c.dY);
   if (tr) tr->mark(st, PH_BOUNDARY_X, 1);
   if (tr) tr->kbegin(st, KS_SWEEP_X);
   const int nx = launch_sweep(S, c, 0, st);
@@ -806,6 +907,23 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   k_smooth_full<R, 1, 0><<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c);
   k_solve_v<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c);
   k_margin_v<<<cdiv(S.N - 1, 128), 128, 0, st>>>(S, c);
+  if (S.reset_h) {
+    // wetting and drying along rows (Reset_states_horizontal after
+    // update_h_moi): the smoothing of t_v also does update_h_moi and flags
+    // the rows holding a dried cell, the rows' wetting runs on those, the
+    // drying per cell in the commit, the mask is written by the segment
+    // scan (the mask can change, so the tables are rescanned)
+    k_smooth_full<R, 0, 2><<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c);
+    if (tr) tr->mark(st, PH_EXPLICIT_V, 4);
+    k_wetting_rows<<<cdiv(S.N, 128), 128, 0, st>>>(S, c, S.rowflag);
+    k_commit_b<R, 1><<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c, sed ? S.N : 0);
+    k_interp_fs_rows<<<dim3(cdiv(S.M, 128), 2), 128, 0, st>>>(S, c);
+    k_interp_fs_col<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
+    k_runs_flags<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, S.segcnt, 2);
+    k_runs_sort<<<cdiv(S.N + S.M - 2, 128), 128, 0, st>>>(S, S.segcnt);
+    if (tr) tr->mark(st, PH_COMMIT_X, 6);
+    return;
+  }
   k_smooth_full<R, 0, 0><<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c);
   if (tr) tr->mark(st, PH_EXPLICIT_V, 4);
   // update_h_moi + update_uvz + Htuongdoi; the wet/dry mask does not change
@@ -820,7 +938,7 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
 
 template <class R>
 void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr) {
-  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, c.dT * 0.5);
+  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, c.dT * 0.5, (double)c.dX, (double)c.dY);
   if (tr) tr->mark(st, PH_BOUNDARY_Y, 1);
   if (tr) tr->kbegin(st, KS_SWEEP_Y);
   const int ny = launch_sweep(S, c, 1, st);
@@ -837,7 +955,7 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   k_wetting<<<cdiv(S.M, 128), 128, 0, st>>>(S, c, S.colflag);
   // with sed, also Find_VTH + hesoK (rows to N-1: the launch shape of
   // engine.cpp:259-260 never reaches row N)
-  k_commit_b<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c, sed ? S.N - 1 : 0);
+  k_commit_b<R, 0><<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c, sed ? S.N - 1 : 0);
   // the drying mask is written by the segment scan (k_runs_flags, dry)
   launch_find_limits(S, c, true, st, tr);
   if (tr) tr->mark(st, PH_COMMIT_Y, 2);
@@ -846,7 +964,7 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
 #define HYD_HYDRO_INST(R)                                                                  \
   template void launch_init<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t);         \
   template void launch_preprocess<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t);   \
-  template void launch_boundary<R>(const StateT<R>&, cudaStream_t);                      \
+  template void launch_boundary<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t);    \
   template void launch_scan_segments<R>(const StateT<R>&, const CoefT<R>&, bool,         \
                                         cudaStream_t);                                    \
   template void launch_find_limits<R>(const StateT<R>&, const CoefT<R>&, bool, cudaStream_t, \

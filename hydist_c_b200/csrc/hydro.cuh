@@ -20,7 +20,7 @@ template <class R>
 void launch_preprocess(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st);
 // Update_Boundary_Value (support_funcs.cpp:603-728) at the device clock's time
 template <class R>
-void launch_boundary(const StateT<R>& S, cudaStream_t st);
+void launch_boundary(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st);
 // segment tables only (from khouot; dry: with the drying pass of
 // Reset_states_vertical applied to the mask first)
 template <class R>
@@ -50,5 +50,9 @@ int launch_fs_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, double s_sta
 template <class R>
 void launch_sediment(const StateT<R>& S, const CoefT<R>& c, double s_start, bool xdir, bool bed,
                      cudaStream_t st, Trace* tr);
+
+// the bed change fed back into h, htaiz, Kx1, Ky1 (HydistOptions::bed_feedback)
+template <class R>
+void launch_bed_feedback(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st);
 
 }  // namespace hyd

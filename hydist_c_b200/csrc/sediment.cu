@@ -149,6 +149,50 @@ __global__ void k_bed_load(StateT<R> S, CoefT<R> c) {
   S.dH[pos] += double(c.dT / (1 - c.Dorong) * (src + tH));
 }
 
+// The bed feedback (HydistOptions::bed_feedback; the reference computes dH
+// but never applies it): dH > 0 deepens the bed (dH = dT/(1-porosity)
+// (source + divergence), sediment_transport.cpp:535), so htaiz = htaiz0 + dH
+// at z points, a wet node's depth h is its initial depth plus the mean dH
+// of the four cells around it (a node at NANGDAY or below stays), and Kx1,
+// Ky1 follow from the new depths as Onetime_init computes them
+// (support_funcs.cpp:63-67). Thread (i, j) writes node (i, j) for i <= N+1,
+// j <= M+1 and the z point (i, j) for 1 <= i <= N, 1 <= j <= M, computing
+// the neighbouring nodes it needs from h0 and dH itself (nothing it reads
+// is written by another thread).
+template <class R>
+__global__ void k_bed_feedback(StateT<R> S, CoefT<R> c) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (i > S.N + 1 || j > S.M + 1) return;
+  const int W = S.W, p = i * W + j;
+  const double* dH = S.dH;
+  const double ND = c.NANGDAY;
+  auto node = [&](int q) {
+    const double b0 = S.h0[q];
+    return b0 > ND ? b0 + 0.25 * (dH[q] + dH[q + W] + dH[q + 1] + dH[q + W + 1]) : b0;
+  };
+  const double hp = node(p);
+  double* h = const_cast<double*>(S.h);
+  h[p] = hp;
+  if (i < 1 || j < 1 || i > S.N || j > S.M) return;
+  const double hl = node(p - 1), hu = node(p - W);
+  const_cast<double*>(S.htaiz)[p] = S.htaiz0[p] + dH[p];
+  const double g = c.g, e = -2 * (double)c.mu_mn;
+  if (hl + hp != 0)
+    const_cast<R*>(S.Kx1)[p] =
+        (R)(g * pow((hl + hp) * 0.5, e) * pow((S.hsnham[p - 1] + S.hsnham[p]) * 0.5, 2.0));
+  if (hu + hp != 0)
+    const_cast<R*>(S.Ky1)[p] =
+        (R)(g * pow((hu + hp) * 0.5, e) * pow((S.hsnham[p - W] + S.hsnham[p]) * 0.5, 2.0));
+}
+
+template <class R>
+void launch_bed_feedback(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
+  k_bed_feedback<<<dim3(cdiv(S.M + 2, 128), S.N + 2), 128, 0, st>>>(S, c);
+}
+template void launch_bed_feedback<double>(const StateT<double>&, const CoefT<double>&, cudaStream_t);
+template void launch_bed_feedback<float>(const StateT<float>&, const CoefT<float>&, cudaStream_t);
+
 constexpr int FS_ROWS = 8;
 
 template <class R>
@@ -164,6 +208,10 @@ __global__ void k_update_fs(StateT<R> S) {
 #pragma unroll
   for (int r = 0; r < FS_ROWS; ++r)
     if (i0 + r <= S.N) S.FS[(i0 + r) * S.W + j] = v[r];
+  bool fin = true;
+#pragma unroll
+  for (int r = 0; r < FS_ROWS; ++r) fin &= (bool)isfinite(v[r]);
+  if (!fin) atomicOr(S.err, DEV_NONFINITE);
 }
 
 template <class R>
@@ -180,6 +228,10 @@ void launch_sediment(const StateT<R>& S, const CoefT<R>& c, double s_start, bool
     k_calc_qb<<<dim3(cdiv(S.M - 1, 128), S.N - 1), 128, 0, st>>>(S, c);
     k_bed_load<<<dim3(cdiv(S.M - 1, 128), S.N - 4), 128, 0, st>>>(S, c);
     launched += 2;
+    if (S.bed_fb) {
+      launch_bed_feedback(S, c, st);
+      ++launched;
+    }
   }
   if (tr) tr->mark(st, xdir ? PH_SEDIMENT_X : PH_SEDIMENT_Y, launched);
 }

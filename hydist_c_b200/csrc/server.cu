@@ -40,7 +40,7 @@ int sfail(int code, const char* m) {
 // host copy of a scenario's inputs (submit copies, create reads later)
 struct ScenarioCopy {
   HydistScenario sc{};
-  std::vector<double> h, hsnham, visco, Fw, bc[4], CC[4], FS0;
+  std::vector<double> h, hsnham, visco, Fw, bc[4], CC[4], FS0, z0;
   std::vector<int32_t> btype;
 
   explicit ScenarioCopy(const HydistScenario& in) : sc(in) {
@@ -59,6 +59,7 @@ struct ScenarioCopy {
       cp(CC[k], ccs[k], (size_t)in.total_time);
     }
     cp(FS0, in.FS0, n);
+    cp(z0, in.z0, n);
     btype.assign(in.boundary_type, in.boundary_type + in.n_boundary_type);
     sc.h = h.data();
     sc.hsnham = hsnham.data();
@@ -71,6 +72,7 @@ struct ScenarioCopy {
       *cdst[k] = CC[k].empty() ? nullptr : CC[k].data();
     }
     sc.FS0 = FS0.empty() ? nullptr : FS0.data();
+    sc.z0 = z0.empty() ? nullptr : z0.data();
     sc.boundary_type = btype.data();
   }
 };

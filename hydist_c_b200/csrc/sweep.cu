@@ -41,8 +41,11 @@ struct HydroGen {
   CoefT<R> c;
   R* scratch;
   R f4;
+  // lines lp0 .. lp0 + nl - 1: columns 2..M (x) / rows 2..N (y), or the
+  // narrow-channel ranges (StateT::x_lo, x_hi, y_lo)
+  int lp0, nl;
 
-  __device__ int lines() const { return DIR == 0 ? S.M - 1 : S.N - 1; }
+  __device__ int lines() const { return nl; }
   __device__ int cells_per_line() const { return DIR == 0 ? S.N - 1 : S.M - 1; }
   __device__ int unknowns_per_line() const { return 2 * cells_per_line(); }
   __device__ int end_pos() const { return DIR == 0 ? S.N : S.M; }
@@ -57,7 +60,7 @@ struct HydroGen {
 
   __device__ void load_segment(LineSeg& LS, int line, int s) const {
     const bool ok = line < lines();
-    const int lp = line + 2;
+    const int lp = line + lp0;
     if (s == SEG) {
       LS.nseg = ok ? (DIR == 0 ? S.mocj[lp] : S.moci[lp]) : 0;
       return;
@@ -108,7 +111,7 @@ struct HydroGen {
     PreT<R> Pc, Pn;
     MomT<R> Mi;
     __device__ void init(const HydroGen& G, const LineSeg& LS, int line, int c0) {
-      lp = line + 2;
+      lp = line + G.lp0;
       si = 0;
       prev = -10;
       in = false;
@@ -184,11 +187,11 @@ struct HydroGen {
   struct Emitter {
     int lp, si;
     __device__ void init(const HydroGen& G, const LineSeg& LS, int line) {
-      lp = line + 2;
+      lp = line + G.lp0;
       si = LS.nseg - 1;
     }
     __device__ void init_fwd(const HydroGen& G, const LineSeg& LS, int line) {
-      lp = line + 2;
+      lp = line + G.lp0;
       si = -1;
     }
     template <bool FWD = false>
@@ -227,7 +230,7 @@ struct HydroGen {
   // Segment ends (_uzSolver_extract_solution :558-601 / _vzSolver_ :488-536).
   __device__ void fixup(const LineSeg& LS, const double* xlast, int line, int s) const {
     const SegD& d = LS.s[s];
-    const int lp = line + 2, first = d.first, last = d.last;
+    const int lp = line + lp0, first = d.first, last = d.last;
     R* vel = vel_ptr();
     double* tz = S.tz;
     if (first < last && extract_ok(first)) {
@@ -333,13 +336,16 @@ static int launch_lines(const Gen& G, int P, int lines, int lslots, cudaStream_t
 }
 
 template <int DIR, class R, bool REF>
-static int launch_dir(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, int lines, int P) {
+static int launch_dir(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, int P) {
   HydroGen<DIR, R, REF> G;
   G.S = S;
   G.c = c;
   G.scratch = S.lscratch;
   G.f4 = DIR == 0 ? 2 * c.g * c.dTchia2dX : 2 * c.g * c.dTchia2dY;
-  return launch_lines(G, P, lines, S.lslots, st);
+  G.lp0 = DIR == 0 ? S.x_lo : S.y_lo;
+  G.nl = DIR == 0 ? S.x_hi - S.x_lo + 1 : S.N - S.y_lo + 1;
+  if (G.nl <= 0) return 0;
+  return launch_lines(G, P, G.nl, S.lslots, st);
 }
 
 // ---------------------------------------------------------------------
@@ -516,14 +522,13 @@ int launch_fs_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, double s_sta
 template <class R>
 int launch_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t st) {
   const int ncells = dir == 0 ? S.N - 1 : S.M - 1;
-  const int lines = dir == 0 ? S.M - 1 : S.N - 1;
   const int P = line_chunks(ncells, 4);
   if (S.refine) {
-    if (dir == 0) return launch_dir<0, R, true>(S, c, st, lines, P);
-    return launch_dir<1, R, true>(S, c, st, lines, P);
+    if (dir == 0) return launch_dir<0, R, true>(S, c, st, P);
+    return launch_dir<1, R, true>(S, c, st, P);
   }
-  if (dir == 0) return launch_dir<0, R, false>(S, c, st, lines, P);
-  return launch_dir<1, R, false>(S, c, st, lines, P);
+  if (dir == 0) return launch_dir<0, R, false>(S, c, st, P);
+  return launch_dir<1, R, false>(S, c, st, P);
 }
 
 template int launch_sweep<double>(const StateT<double>&, const CoefT<double>&, int, cudaStream_t);

@@ -238,6 +238,19 @@ __global__ void __launch_bounds__(NT) k_gtsv_bulk(const T* __restrict__ dl, cons
     // wait for the rows (bounded)
     bool ok = false;
     for (long t = 0; t < GT_WAIT_TRIES && !ok; ++t) ok = mbar_try_wait(&bar[k], (phase >> k) & 1u);
+    if (!__syncthreads_and(ok)) {
+      // a copy that never completed: record it, give the copy in flight
+      // (the only one: the next system's is issued after this test) one
+      // more bounded wait, and leave the CTA's remaining systems unsolved;
+      // the call reports HYDIST_ERR_TIMEOUT for this batch
+      if (tid == 0) {
+        atomicExch(stalled, 1);
+        bool done = false;
+        for (long t = 0; t < GT_WAIT_TRIES && !done; ++t) done = mbar_try_wait(&bar[k], (phase >> k) & 1u);
+      }
+      __syncthreads();
+      return;
+    }
     phase ^= 1u << k;
     const int inext = i + gridDim.x;
     if (NBUF == 2 && tid == 0 && inext < cnt) {
@@ -259,11 +272,6 @@ __global__ void __launch_bounds__(NT) k_gtsv_bulk(const T* __restrict__ dl, cons
       rD[r] = b[o + r];
     }
     __syncthreads();
-    if (!__syncthreads_and(ok)) {
-      // a copy that never completed: record it and leave the system
-      if (tid == 0) atomicExch(stalled, 1);
-      continue;
-    }
     // ---- partition solve in place: forward per chunk, separators by PCR
     const int S = bulk_chunk(n, NT), P = max(1, n / S);
     const int q0 = tid * S;
@@ -646,16 +654,11 @@ int solve_batch(const T* dl, const T* d, const T* du, const T* b, T* x, const in
   if (cudaMemsetAsync(D.scr.counts, 0, (GT_NB + 2) * sizeof(int), st) != cudaSuccess)
     return HYDIST_ERR_CUDA;
   hyd::k_gt_classify<<<(nsys + 255) / 256, 256, 0, st>>>(off, len, nsys, D.scr.lists, D.scr.counts);
-  // band sizes, packed extent, the offset check and the stall flag in one
-  // synchronisation
+  // band sizes, packed extent and the offset check in one synchronisation
   int counts[GT_NB + 3];
   if (cudaMemcpyAsync(counts, D.scr.counts, sizeof(counts), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return HYDIST_ERR_CUDA;
-  if (counts[GT_NB + 2]) {
-    cudaMemsetAsync(D.scr.counts + GT_NB + 2, 0, sizeof(int), st);
-    return HYDIST_ERR_TIMEOUT;
-  }
   if (counts[GT_NB + 1]) return HYDIST_ERR_ARG;
   // the CTA solvers stage rows with bulk copies, which need 16-byte aligned
   // arrays; misaligned ones go to Thomas
@@ -675,11 +678,28 @@ int solve_batch(const T* dl, const T* d, const T* du, const T* b, T* x, const in
     rc = ensure_scratch(D.scr, (size_t)counts[GT_NB] * sizeof(T), (size_t)nsys);
     if (rc != HYDIST_OK) return rc;
   }
+  bool staged = false;  // a bulk-staged CTA solver ran
   for (int bnd = 0; bnd < GT_NB; ++bnd) {
     rc = launch_band<T>(table[bnd], bnd, dl, d, du, b, x, (T*)D.scr.w, off, len,
                         D.scr.lists + (size_t)bnd * nsys, D.scr.counts + bnd,
                         D.scr.counts + GT_NB + 2, counts[bnd], D, st);
     if (rc != HYDIST_OK) return rc;
+    staged |= counts[bnd] > 0 && (table[bnd] == HYDIST_GTSV_PARTITION ||
+                                  table[bnd] == HYDIST_GTSV_PARTITION_512 ||
+                                  table[bnd] == HYDIST_GTSV_PARTITION_128);
+  }
+  if (staged) {
+    // a CTA whose staging copy never completed left systems unsolved: read
+    // its flag now, so that this batch, not a later one, reports it
+    int flag = 0;
+    if (cudaMemcpyAsync(&flag, D.scr.counts + GT_NB + 2, sizeof(int), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      return HYDIST_ERR_CUDA;
+    if (flag) {
+      cudaMemsetAsync(D.scr.counts + GT_NB + 2, 0, sizeof(int), st);
+      return HYDIST_ERR_TIMEOUT;
+    }
   }
   return HYDIST_OK;
 }
@@ -834,8 +854,8 @@ extern "C" int hydist_gtsv_batched(const void* dl, const void* d, const void* du
   }
   if (rc == HYDIST_ERR_ARG) hyd::set_last_error("hydist_gtsv_batched: a system has a negative offset");
   else if (rc == HYDIST_ERR_TIMEOUT)
-    hyd::set_last_error("hydist_gtsv_batched: a previous batch gave a system up (its rows never "
-                        "arrived in shared memory); this batch was not solved");
+    hyd::set_last_error("hydist_gtsv_batched: a CTA solver gave up waiting for a system's rows "
+                        "in shared memory; some systems of this batch are unsolved");
   else if (rc != HYDIST_OK) hyd::set_last_error("hydist_gtsv_batched: a CUDA call failed");
   return rc;
 }
@@ -877,7 +897,37 @@ __global__ void k_thomas_noalloc(const T* __restrict__ dl, const T* __restrict__
 namespace {
 constexpr int kNoallocDevices = 64;
 std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[kNoallocDevices] = {};  // scratch address per device, set once
+// scratch address per device, with the context it was looked up in: a
+// device reset gives the device a new context (and the array a new
+// address), which the next call notices and looks the address up again
+struct NoallocSlot {
+  void* ctx = nullptr;
+  void* ptr = nullptr;
+};
+NoallocSlot g_noalloc[kNoallocDevices];
+
+// the driver's cuCtxGetCurrent through the runtime's entry-point query (the
+// library links only the runtime); null if the driver does not offer it
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn ctx_get_current() {
+  static const CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return (CtxGetCurrentFn)p;
+  }();
+  return fn;
+}
+
+void* current_ctx() {
+  void* c = nullptr;
+  const CtxGetCurrentFn f = ctx_get_current();
+  if (!f || f(&c) != 0) return nullptr;
+  return c;
+}
 }  // namespace
 
 extern "C" int hydist_gtsv_batched_noalloc(const void* dl, const void* d, const void* du,
@@ -910,16 +960,20 @@ extern "C" int hydist_gtsv_batched_noalloc(const void* dl, const void* d, const 
   void* w = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    NoallocSlot& slot = g_noalloc[dev];
+    void* ctx = current_ctx();
+    if (!slot.ptr || !ctx || ctx != slot.ctx) {
+      // set-up on this device (and again after a reset of its context)
       void* p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, hyd::g_noalloc_w);
       if (e != cudaSuccess || !p) {
         hyd::set_last_error("hydist_gtsv_batched_noalloc: cudaGetSymbolAddress failed");
         return HYDIST_ERR_CUDA;
       }
-      g_noalloc_ptr[dev] = p;
+      slot.ptr = p;
+      slot.ctx = current_ctx();  // current now that the runtime has set the device up
     }
-    w = g_noalloc_ptr[dev];
+    w = slot.ptr;
   }
   if (nsys == 0 || rows == 0) return HYDIST_OK;
   cudaStream_t st = (cudaStream_t)stream;

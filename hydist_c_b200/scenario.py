@@ -104,10 +104,14 @@ def config0(seed=20260000):
 
 def config1(seed=20260001):
     """Hydraulics + sediment, 2048x1024, dx=dy=5 m, dt=2 s, sediment from
-    600 s, 1 h. Fw ~ U(0.5,1.5) is used as the reference's tau_b = ro*Fw*V^2
+    600 s, 1 h, with the bed change (Calculate_Qb + BedLoad,
+    sediment_transport.cpp:352-537) accumulated once per step from then on.
+    Fw ~ U(0.5,1.5) is used as the reference's tau_b = ro*Fw*V^2
     coefficient (sediment_transport.cpp:17) literally."""
-    return make_channel(N=2048, M=1024, seed=seed, dx=5.0, dt=2.0, hours=1.0,
-                        sediment=True, sediment_start=600.0)
+    b = make_channel(N=2048, M=1024, seed=seed, dx=5.0, dt=2.0, hours=1.0,
+                     sediment=True, sediment_start=600.0)
+    b["options"]["bed_change"] = 1
+    return b
 
 
 def config3_member(k, seed=20263000):

@@ -116,6 +116,28 @@ typedef struct HydistOptions {
                               sediment_transport.cpp:352-537, which the
                               reference never launches)                     */
   int32_t precision;       /* enum HydistPrecision                          */
+  /* narrow-channel mode (Options::kenhhepd / kenhhepng, engine.h:19-33;
+     main.cpp flags -kd / -kn). With exactly one of the two set (the
+     reference's `channel`), the boundary series are not applied
+     (update_boundary_at_t does nothing, engine.cpp:24-30), and the x sweep
+     takes columns 3..M-1 (kenhhepd, engine.cpp:77-80) or the y sweep rows
+     3..N (kenhhepng, :190-193) instead of 2..M / 2..N. */
+  int32_t kenhhepd, kenhhepng;
+  /* 1: in channel mode, impose the standing-wave water levels of
+     boundary_up / boundary_down / boundary_left / boundary_right
+     (support_funcs.cpp:366-478) at every half-step, as the calls the
+     reference keeps commented out at engine.cpp:25-28 would */
+  int32_t channel_wave;
+  /* 1: wetting and drying along rows as well: Reset_states_horizontal
+     (support_funcs.cpp:88-138, which the reference never launches) after
+     update_h_moi in the first half-step, the place Reset_states_vertical
+     takes in the second (engine.cpp:238-240) */
+  int32_t reset_horizontal;
+  /* 1 (with bed_change): the accumulated bed change feeds back into the
+     bed: htaiz = htaiz0 + dH at z points, the node depths h and the
+     friction coefficients Kx1, Ky1 (support_funcs.cpp:21-69) follow
+     once per step */
+  int32_t bed_feedback;
   int32_t reserved;
 } HydistOptions;
 
@@ -143,6 +165,10 @@ typedef struct HydistScenario {
   int32_t bienQ[4];           /* discharge flag per side (up,down,left,right)
                                  as loader.cpp:157-164 derives it            */
   const double* FS0;          /* optional initial concentration, or NULL      */
+  const double* z0;           /* optional initial water level (z and t_z
+                                 before the set-up kernels; the reference
+                                 starts from the zeroed allocation,
+                                 loader.cpp:269-271), or NULL               */
 } HydistScenario;
 
 typedef struct HydistHandle HydistHandle;
@@ -303,6 +329,12 @@ int hydist_step_traced(HydistHandle* h, float* phase_ms);
  * not run). */
 #define HYDIST_SWEEPS 4
 int hydist_step_traced_sweeps(HydistHandle* h, float* phase_ms, float* sweep_ms);
+/* Host time of the handle's hydist_create by part, in ms (the reference
+ * has no counterpart): ms[0] device allocation and zeroing (the arrays come
+ * from a per-device memory pool that keeps what destroyed handles release),
+ * ms[1] copies of the host inputs, ms[2] set-up kernels (Onetime_init,
+ * segment tables, Htuongdoi, preprocess_data), ms[3] the whole call. */
+int hydist_create_phases(const HydistHandle* h, double* ms);
 /* Number of kernels the handle has enqueued since creation (set-up
  * excluded). */
 int hydist_kernel_launches(HydistHandle* h, int64_t* count);
@@ -335,9 +367,13 @@ int hydist_kernel_launches(HydistHandle* h, int64_t* count);
  * No pivoting: the systems are expected to be diagonally dominant, as the
  * ADI sweeps' are.
  * stream is a cudaStream_t (NULL = default stream). Scratch is allocated by
- * the library on first use and grown as needed; the call synchronises the
- * stream once, to read the band sizes and the packed extent. A batch with a
- * negative offset is refused with HYDIST_ERR_ARG. */
+ * the library on first use and grown as needed. The call synchronises the
+ * stream once to read the band sizes and the packed extent, and, when a
+ * shared-memory CTA solver (PARTITION*) ran, once more at the end: every
+ * wait of those solvers for a system's rows is bounded, and a CTA that gave
+ * up leaves its remaining systems unsolved, which this call (not a later
+ * one) reports as HYDIST_ERR_TIMEOUT. A batch with a negative offset is
+ * refused with HYDIST_ERR_ARG. */
 enum HydistGtsvAlgo {
   HYDIST_GTSV_AUTO = 0,
   HYDIST_GTSV_THOMAS = 1,
@@ -375,7 +411,9 @@ int hydist_gtsv_autotune(int32_t dtype, void* stream, int32_t* algo_per_band);
  *          a system outside is left unsolved. rows above the limit return
  *          HYDIST_ERR_BUDGET without launching anything.
  * The first call on each device (with that device current) looks up the
- * scratch address; make that call before capturing a stream. Nothing needs
+ * scratch address; make that call before capturing a stream. A call that
+ * finds the device's context changed since (cudaDeviceReset) looks the
+ * address up again, as a first call does. Nothing needs
  * zeroing beforehand. The scratch is shared by all calls on a device, so
  * calls that overlap in time on one device (two streams or host threads)
  * race and must be serialised by the caller. */

@@ -1,5 +1,9 @@
 """TEST INFRASTRUCTURE: builds the CPU oracle and, where the reference source
-tree is present, the reference driver.
+tree is given, the reference driver.
+
+The reference source tree is named by the caller (the ``src`` argument) or by
+the environment variable HYDIST_REFERENCE_SRC (``reference_src()``); nothing
+here assumes where it lies.
 
 * ``build_oracle()`` compiles hydist_oracle.cpp into
   ``oracle/_build/libhydist_oracle.so`` (g++, FP64, no fused multiply-add).
@@ -70,7 +74,13 @@ def build_oracle(force=False) -> Path:
     return ORACLE_SO
 
 
-def build_reference(src="/root/reference", force=False):
+def reference_src():
+    """The reference source tree named by HYDIST_REFERENCE_SRC, or None."""
+    p = os.environ.get("HYDIST_REFERENCE_SRC")
+    return Path(p) if p else None
+
+
+def build_reference(src, force=False):
     """Compile the reference CUDA sources from ``src`` into oracle/_ref."""
     src = Path(src)
     if not (src / "engine.cpp").exists():
@@ -109,7 +119,7 @@ def build_reference(src="/root/reference", force=False):
     return REF_DRIVER
 
 
-def build_reference_engine_on_library_kernels(src="/root/reference"):
+def build_reference_engine_on_library_kernels(src):
     """Link ref_driver.cu and the reference's engine.cpp, support_funcs.cpp,
     loader.cpp and sediment_transport.cpp (objects from build_reference) with
     libhydist_b200.so for the UVZSolver kernels (include/hydist_uvz_compat.h):
@@ -129,7 +139,7 @@ def build_reference_engine_on_library_kernels(src="/root/reference"):
     return REF_DRIVER_UVZ
 
 
-def build_reference_main_on_library(src="/root/reference"):
+def build_reference_main_on_library(src):
     """Link the reference's main.cpp, loader.cpp and support_funcs.cpp (its
     set-up kernels) with libhydist_b200.so instead of engine.cpp: the
     library's Hydraulic_Calculation / update_boundary_at_t / synch_and_check
@@ -156,4 +166,7 @@ def build_reference_main_on_library(src="/root/reference"):
 if __name__ == "__main__":
     print(build_oracle(force="--force" in sys.argv))
     if "--ref" in sys.argv:
-        print(build_reference(force="--force" in sys.argv))
+        src = reference_src()
+        if src is None:
+            sys.exit("set HYDIST_REFERENCE_SRC to the reference source tree")
+        print(build_reference(src, force="--force" in sys.argv))

@@ -184,6 +184,38 @@ struct Sim {
       }
   }
 
+  // The bed feedback (HydistOptions::bed_feedback; the reference computes
+  // dH but never applies it): dH > 0 deepens the bed (the Exner balance of
+  // sediment_transport.cpp:535, dH = dT/(1-porosity) (source + divergence)),
+  // so htaiz = htaiz0 + dH at z points, a wet node's depth is its initial
+  // depth plus the mean dH of the four cells around it (a node at NANGDAY
+  // or below stays as it is), and Kx1, Ky1 follow from the new depths as in
+  // Onetime_init (support_funcs.cpp:63-67). Once per step, after BedLoad.
+  std::vector<double> h0, htaiz0;
+  void keep_initial_bed() {
+    h0 = h;
+    htaiz0 = htaiz;
+  }
+  void bed_feedback() {
+    for (int i = 0; i <= N + 1; ++i)
+      for (int j = 0; j <= M + 1; ++j) {
+        const int p = id(i, j);
+        if (h0[p] > c.NANGDAY)
+          h[p] = h0[p] + 0.25 * (dH[p] + dH[id(i + 1, j)] + dH[id(i, j + 1)] + dH[id(i + 1, j + 1)]);
+      }
+    for (int i = 1; i <= N; ++i)
+      for (int j = 1; j <= M; ++j) {
+        const int p = id(i, j);
+        htaiz[p] = htaiz0[p] + dH[p];
+        if (h[id(i, j - 1)] + h[p] != 0)
+          Kx1[p] = c.g * std::pow((h[id(i, j - 1)] + h[p]) * 0.5, -2 * c.mu_mn) *
+                   std::pow((hsnham[id(i, j - 1)] + hsnham[p]) * 0.5, 2);
+        if (h[id(i - 1, j)] + h[p] != 0)
+          Ky1[p] = c.g * std::pow((h[id(i - 1, j)] + h[p]) * 0.5, -2 * c.mu_mn) *
+                   std::pow((hsnham[id(i - 1, j)] + hsnham[p]) * 0.5, 2);
+      }
+  }
+
   // preprocess_data, support_funcs.cpp:482-601 (one thread).
   void preprocess_data() {
     double* hu = hi.data();
@@ -313,6 +345,15 @@ struct Sim {
     return nseg;
   }
 
+  // the segment tables alone, from the mask as it stands (used after a
+  // state is loaded from elsewhere)
+  void rescan_segments() {
+    for (int i = 2; i <= N; ++i)
+      moci[i] = scan_line(&khouot[id(i, 0)], 1, M, &daui[i * SEG], &cuoii[i * SEG]);
+    for (int j = 2; j <= M; ++j)
+      mocj[j] = scan_line(&khouot[j], W, N, &dauj[j * SEG], &cuoij[j * SEG]);
+  }
+
   void find_limits() {
     // Find_Calculation_limits_Horizontal, support_funcs.cpp:238-290
     interpolate_fs_ng(N, N - 1, -1);
@@ -393,6 +434,58 @@ struct Sim {
         FS[id(ii, jj)] = cv * htaiz_bd[id(ii, jj)] * S.hmax;
       }
     }
+  }
+
+  // The narrow-channel standing wave: boundary_up / boundary_down /
+  // boundary_left / boundary_right (support_funcs.cpp:366-478), whose calls
+  // the reference keeps commented out in update_boundary_at_t
+  // (engine.cpp:25-28). Each walks the first wet segment of its side's line
+  // (boundary_right from row 2's first start to row N's first end, as
+  // written); a side without a wet segment is skipped.
+  void channel_wave(double t_in) {
+    const double t = (double)(float)t_in;
+    const double PI_ = 3.14159265358979323846;
+    const double ct = std::cos(2 * PI_ / 27.75 * t);
+    if (mocj[M] > 0)  // up: column M, bienQ[0] not consulted
+      for (int i = dauj[M * SEG]; i <= cuoij[M * SEG]; ++i) {
+        tz[id(i, M)] = 0.01 * ct * std::cos(2 * (PI_ / 100) * (100 - c.dY / 2));
+        tz[id(i, M + 1)] = 0.01 * ct * std::cos(2 * (PI_ / 100) * (100 + c.dY / 2));
+      }
+    if (mocj[2] > 0)  // down: column 2
+      for (int i = dauj[2 * SEG]; i <= cuoij[2 * SEG]; ++i) {
+        if (bienQ[1]) {
+          vbd[i] = 0;
+        } else {
+          tz[id(i, 2)] = 0.01 * ct * std::cos(2 * (PI_ / 100) * c.dY / 2);
+          tz[id(i, 1)] = 0.01 * ct * std::cos(2 * (PI_ / 100) * (-c.dY) / 2);
+        }
+      }
+    if (moci[2] > 0)  // left: row 2
+      for (int j = daui[2 * SEG]; j <= cuoii[2 * SEG]; ++j) {
+        if (bienQ[2]) {
+          ubt[j] = 0;
+        } else {
+          tz[id(2, j)] = 0.01 * ct * std::cos(2 * (PI_ / 100) * c.dX / 2);
+          tz[id(1, j)] = 0.01 * ct * std::cos(2 * (PI_ / 100) * (-c.dX) / 2);
+        }
+      }
+    if (moci[2] > 0 && moci[N] > 0)  // right: row N
+      for (int j = daui[2 * SEG]; j <= cuoii[N * SEG]; ++j) {
+        if (bienQ[3]) {
+          ubp[j] = 0;
+        } else {
+          tz[id(N, j)] = 0.01 * ct * std::cos(2 * (PI_ / 100) * (100 - c.dX / 2));
+          tz[id(N + 1, j)] = 0.01 * ct * std::cos(2 * (PI_ / 100) * (100 + c.dX / 2));
+        }
+      }
+  }
+
+  // update_boundary_at_t (engine.cpp:22-36): the series outside channel
+  // mode; in channel mode nothing, or the standing wave when asked for
+  bool channel() const { return (o.kenhhepd != 0) != (o.kenhhepng != 0); }
+  void update_boundary(double t_in) {
+    if (!channel()) boundary(t_in);
+    else if (o.channel_wave) channel_wave(t_in);
   }
 
   // -------------------------------------------------- segment end flags
@@ -1000,6 +1093,43 @@ struct Sim {
     }
   }
 
+  // Reset_states_horizontal (support_funcs.cpp:88-138): per row i = 1..N
+  // the wetting loop along j, then the drying loop along j. The reference
+  // runs one thread per row; rows are independent (a row's loops read and
+  // write the mask, depths and levels of its own cells only), so they are
+  // taken one after another here.
+  void reset_states_horizontal() {
+    const int off = W;
+    for (int i = 1; i <= N; ++i) {
+      for (int j = 2; j <= M; ++j) {
+        if (tz[i * off + j] > z[i * off + j]) {
+          if (khouot[i * off + j - 1] == 1) {
+            tz[i * off + j - 1] = tz[i * off + j];
+            Hmoi[i * off + j - 1] = htaiz[i * off + j - 1] + tz[i * off + j];
+            khouot[i * off + j - 1] = 0;
+            FS[i * off + j - 1] = FS[i * off + j];
+          }
+          if (khouot[i * off + j + 1] == 1) {
+            tz[i * off + j + 1] = tz[i * off + j];
+            Hmoi[i * off + j + 1] = htaiz[i * off + j + 1] + tz[i * off + j];
+            khouot[i * off + j + 1] = 0;
+            FS[i * off + j + 1] = FS[i * off + j];
+          }
+        }
+      }
+      for (int j = 2; j <= M; ++j) {
+        if ((khouot[i * off + j] == 0) && (Hmoi[i * off + j] <= c.H_TINH)) {
+          tu[(i - 1) * off + j] = 0;
+          tu[i * off + j] = 0;
+          tv[i * off + j - 1] = 0;
+          tv[i * off + j] = 0;
+          khouot[i * off + j] = 1;
+          FS[i * off + j] = 0;
+        }
+      }
+    }
+  }
+
   // --------------------------------------------------------- sediment
   // Find_VTH, sediment_transport.cpp:575-602.
   void find_vth(int i_hi) {
@@ -1374,15 +1504,20 @@ struct Sim {
   // One full step: the body of the while-loop of Hydraulic_Calculation,
   // engine.cpp:65-295.
   void step() {
-    // ---- first half: UZ sweep, explicit v (engine.cpp:66-170)
+    // ---- first half: UZ sweep, explicit v (engine.cpp:66-170); in channel
+    // mode with kenhhepd the sweep takes columns 3..M-1 (engine.cpp:77-80)
     t += 0.5 * c.dT;
-    boundary(t);
-    for_lines(2, M, [&](LineBuf& L, int j) { uz_column(L, j); });
+    update_boundary(t);
+    const bool narrow_x = channel() && o.kenhhepd;
+    for_lines(narrow_x ? 3 : 2, narrow_x ? M - 1 : M, [&](LineBuf& L, int j) { uz_column(L, j); });
     normalize(true, tmpbuf);
     solve_v();
     margin_v();
     normalize(false, tmpbuf);
     update_h_moi();
+    // wetting/drying along rows, where Reset_states_vertical has its place
+    // in the second half (the reference never launches it)
+    if (o.reset_horizontal) reset_states_horizontal();
     update_uvz();
     find_limits();
     htuongdoi();
@@ -1393,10 +1528,12 @@ struct Sim {
       for_lines(3, M - 1, [&](LineBuf& L, int j) { fsj_column(L, j, tt); });
       update_fs();
     }
-    // ---- second half: VZ sweep, explicit u, wet/dry (engine.cpp:176-282)
+    // ---- second half: VZ sweep, explicit u, wet/dry (engine.cpp:176-282);
+    // rows 3..N with kenhhepng in channel mode (engine.cpp:190-193)
     t += c.dT * 0.5;
-    boundary(t);
-    for_lines(2, N, [&](LineBuf& L, int i) { vz_row(L, i); });
+    update_boundary(t);
+    const bool narrow_y = channel() && o.kenhhepng;
+    for_lines(narrow_y ? 3 : 2, N, [&](LineBuf& L, int i) { vz_row(L, i); });
     normalize(false, tmpbuf);
     solve_u();
     margin_u();
@@ -1416,6 +1553,7 @@ struct Sim {
       if (o.bed_change && t >= o.bed_change_start) {
         calc_qb();
         bed_load();
+        if (o.bed_feedback) bed_feedback();
       }
     }
   }
@@ -1490,12 +1628,17 @@ OracleSim* oracle_create(const HydistScenario* sc, const HydistParams* p,
     s.FS.assign(sc->FS0, sc->FS0 + n);
     s.tFS = s.FS;
   }
+  if (sc->z0) {
+    s.z.assign(sc->z0, sc->z0 + n);
+    s.tz = s.z;
+  }
   s.alloc_bufs();
   // set-up sequence of main.cpp:262-298
   s.onetime_init();
   s.find_limits();
   s.htuongdoi();
   s.preprocess_data();
+  if (o->bed_feedback) s.keep_initial_bed();
   if (s.seg_overflow) {
     set_err("more than 20 wet segments in a line");
     delete os;
@@ -1520,6 +1663,20 @@ int oracle_step(OracleSim* os, int nsteps) {
 }
 
 double oracle_time(OracleSim* os) { return os->s.t; }
+
+void oracle_set_time(OracleSim* os, double t) { os->s.t = t; }
+
+// Rebuild the wet-segment tables from the mask (after oracle_set of the
+// mask); HYDIST_ERR_SEGMENTS if a line has more than 20 wet segments.
+int oracle_rescan_segments(OracleSim* os) {
+  os->s.seg_overflow = false;
+  os->s.rescan_segments();
+  if (os->s.seg_overflow) {
+    set_err("more than 20 wet segments in a line");
+    return HYDIST_ERR_SEGMENTS;
+  }
+  return HYDIST_OK;
+}
 
 // Debug: run the first nops operations of one hydraulic step (no sediment).
 int oracle_step_ops(OracleSim* os, int nops) { return os->s.step_ops(nops); }

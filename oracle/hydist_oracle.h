@@ -18,6 +18,8 @@ void oracle_destroy(OracleSim* s);
 void oracle_set_race_mode(OracleSim* s, int race_new);
 int oracle_step(OracleSim* s, int nsteps);
 double oracle_time(OracleSim* s);
+void oracle_set_time(OracleSim* s, double t);
+int oracle_rescan_segments(OracleSim* s);
 int oracle_get(OracleSim* s, int field, void* out);
 int oracle_set(OracleSim* s, int field, const void* in);
 int oracle_get_segments(OracleSim* s, int kind, int* dau, int* cuoi, int* moc);

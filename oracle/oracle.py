@@ -33,6 +33,8 @@ def lib():
         L.oracle_step.argtypes = [vp, C.c_int]
         L.oracle_time.argtypes = [vp]
         L.oracle_time.restype = C.c_double
+        L.oracle_set_time.argtypes = [vp, C.c_double]
+        L.oracle_rescan_segments.argtypes = [vp]
         L.oracle_get.argtypes = [vp, C.c_int, vp]
         L.oracle_set.argtypes = [vp, C.c_int, vp]
         L.oracle_get_segments.argtypes = [vp, C.c_int, ip, ip, ip]
@@ -76,6 +78,19 @@ class OracleSim:
     @property
     def t(self):
         return lib().oracle_time(self._h)
+
+    @t.setter
+    def t(self, value):
+        lib().oracle_set_time(self._h, float(value))
+
+    def load_state(self, fields: dict):
+        """Set the given fields (name -> array; the mask as "khouot") and
+        rebuild the segment tables from the mask."""
+        for name, arr in fields.items():
+            self.set(name, arr)
+        st = lib().oracle_rescan_segments(self._h)
+        if st != 0:
+            raise RuntimeError("oracle_rescan_segments: " + lib().oracle_last_error().decode())
 
     def get(self, name):
         f = capi.FIELDS[name]

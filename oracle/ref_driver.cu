@@ -10,13 +10,20 @@
 //
 // usage: hydist_ref_driver <input_dir/> <out_dir> <steps_csv> [key=value ...]
 //   keys: sediment_start, bed_change_start, dX, dT, Toe, Tod, Mbochat, wss,
-//         fs0 (binary float64 file of (N+3)*(M+3) initial concentration)
+//         fs0 (binary float64 file of (N+3)*(M+3) initial concentration),
+//         z0 (the same for the initial water level, loaded into z and t_z
+//         before the set-up kernels, as a warm start would be),
+//         ketdinh (0: non-cohesive source), kenhhepd / kenhhepng (the
+//         narrow-channel options of main.cpp's -kd / -kn), Wind, huonggio,
+//         CORIOLIS (Constant_Coeffs members; Windx / Windy derived as
+//         Load_coeffs derives them, loader.cpp:81-82)
 // Output: <out_dir>/state_<steps>.bin = int32 {N, M, steps, nfields},
 //         double t, then nfields float64 arrays of (N+3)*(M+3):
 //         u v z FS H_moi t_u t_v t_z Htdu Htdv khouot tFS VTH Kx Ky
 //         (plus ubt, ubp padded... not written)
 // stdout of the reference (it prints t every half-step) should be
 // redirected by the caller.
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -163,6 +170,14 @@ int main(int argc, char** argv) {
     for (DOUBLE* p : a2) ck(cudaMemset(p, 0, s2), "memset");
     ck(cudaMemset(h_arr.SN, 0, sizeof(int) * segment_limit * (std::max(M, N) + 8)), "memset");
   }
+  if (kv.count("z0")) {
+    std::vector<double> z0(n);
+    FILE* f = fopen(kv["z0"].c_str(), "rb");
+    if (!f || fread(z0.data(), sizeof(double), n, f) != n) die("cannot read z0");
+    fclose(f);
+    ck(cudaMemcpy(h_arg.z, z0.data(), nb, cudaMemcpyHostToDevice), "z0");
+    ck(cudaMemcpy(h_arg.t_z, z0.data(), nb, cudaMemcpyHostToDevice), "z0");
+  }
   if (kv.count("fs0")) {
     std::vector<double> fs0(n);
     FILE* f = fopen(kv["fs0"].c_str(), "rb");
@@ -183,6 +198,14 @@ int main(int argc, char** argv) {
   if (kv.count("Tod")) hc.Tod = getd("Tod", hc.Tod);
   if (kv.count("Mbochat")) hc.Mbochat = getd("Mbochat", hc.Mbochat);
   if (kv.count("wss")) hc.wss = getd("wss", hc.wss);
+  if (kv.count("CORIOLIS")) hc.CORIOLIS_FORCE = getd("CORIOLIS", hc.CORIOLIS_FORCE);
+  if (kv.count("Wind") || kv.count("huonggio")) {
+    hc.Wind = getd("Wind", hc.Wind);
+    hc.huonggio = getd("huonggio", hc.huonggio);
+    const double W = hc.Wind, aW = W < 0 ? -W : W;
+    hc.Windx = 0.0013 * (0.00075 + 0.000067 * aW) * aW * W * cos(hc.huonggio * (PI / 180));
+    hc.Windy = 0.0013 * (0.00075 + 0.000067 * aW) * aW * W * sin(hc.huonggio * (PI / 180));
+  }
   ck(cudaMalloc((void**)&dc, sizeof(Constant_Coeffs)), "malloc coeffs");
   ck(cudaMemcpy(dc, &hc, sizeof(Constant_Coeffs), cudaMemcpyHostToDevice), "coeffs");
 
@@ -200,7 +223,11 @@ int main(int argc, char** argv) {
 
   const double sed = getd("sediment_start", 1e12);
   const double bcs = getd("bed_change_start", 1e12);
-  Options ops(0.0, 0.0, 1 << 30, sed, bcs, true, false, false, false, false);
+  const bool cohesive = getd("ketdinh", 1) != 0;
+  const bool kd = getd("kenhhepd", 0) != 0, kn = getd("kenhhepng", 0) != 0;
+  // Options(Tmax, t_start, interval, sediment_start, bed_change_start,
+  // cohesive, kenhng, kenhd, debug, plot), engine.h:25-35
+  Options ops(0.0, 0.0, 1 << 30, sed, bcs, cohesive, kn, kd, false, false);
   ops.M = M;
   ops.N = N;
   ops.total_time = total_time;
@@ -213,8 +240,20 @@ int main(int argc, char** argv) {
     if (target > done) {
       ops.t_start = t;
       ops.Tmax = t + (target - done) * hc.dT;
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      cudaEventRecord(e0);
       Hydraulic_Calculation(hc.dT, hc.NANGDAY, d_arg, d_arr, dc, h_arg, ops);
+      cudaEventRecord(e1);
       synch_and_check();
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      // the reference's own time step, device-timed (it synchronises after
+      // every kernel, so this is also its wall time)
+      fprintf(stderr, "ref_driver: Hydraulic_Calculation steps %d..%d: %.3f ms\n", done, target, ms);
       t = ops.Tmax;
       done = target;
     }

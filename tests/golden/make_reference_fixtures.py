@@ -36,7 +36,10 @@ sys.path.insert(0, str(ROOT))
 
 from hydist_c_b200 import scenario as S  # noqa: E402
 
-REF_INPUTS = Path("/root/reference/Inputs")
+# the reference's Inputs/ directory, under the source tree named by
+# HYDIST_REFERENCE_SRC (the cases that need it are skipped without it)
+_SRC = os.environ.get("HYDIST_REFERENCE_SRC")
+REF_INPUTS = Path(_SRC) / "Inputs" if _SRC else Path("HYDIST_REFERENCE_SRC-unset")
 CASES = {
     "channel": dict(steps=[1, 2, 10, 100, 1800], stride=3, fields=["u", "v", "z"],
                     args=[]),
@@ -50,7 +53,26 @@ CASES = {
     # differences at still-water cells into visible ones. Steps 1 and 700
     # are the pinned ones.
     "wetdry": dict(steps=[1, 700], stride=1, fields=["u", "v", "z"], args=[]),
+    # wind stress and Coriolis force on (Constant_Coeffs Windx/Windy and
+    # CORIOLIS_FORCE, loader.cpp:75,81-82; zero in the shipped Load_coeffs)
+    "windcor": dict(steps=[1, 10, 100, 300], stride=2, fields=["u", "v", "z"],
+                    args=["Wind=10", "huonggio=30", "CORIOLIS=0.0001"]),
+    # non-cohesive sediment source (source_nchs, sediment_transport.cpp:41-49)
+    "noncoh": dict(steps=[1, 10, 100, 300], stride=3, fields=["u", "v", "z", "FS"],
+                   args=["sediment_start=0", "bed_change_start=0", "dX=5", "Toe=0.2",
+                         "Tod=0.1", "Mbochat=0.0001", "wss=0.0005", "fs0=fs0.bin",
+                         "ketdinh=0"]),
+    # the narrow-channel modes (-kd, -kn): no boundary update, the sweeps'
+    # ranges of engine.cpp:77-80 / 190-193; a sloshing initial level
+    "narrow_d": dict(steps=[1, 10, 100, 300], stride=2, fields=["u", "v", "z"],
+                     args=["z0=z0.bin", "kenhhepd=1"]),
+    "narrow_n": dict(steps=[1, 10, 100, 300], stride=2, fields=["u", "v", "z"],
+                     args=["z0=z0.bin", "kenhhepng=1"]),
 }
+# the cases a command runs: all, or those named in HYDIST_FIXTURE_CASES
+# (comma-separated)
+_SEL = os.environ.get("HYDIST_FIXTURE_CASES")
+SELECTED = [c for c in CASES if not _SEL or c in _SEL.split(",")]
 
 
 def sediment_bundle():
@@ -106,7 +128,39 @@ def wetdry_bundle():
     return b
 
 
+def windcor_bundle():
+    b = S.make_channel(N=128, M=64, seed=20265100, dx=10.0, dt=2.0, hours=1.0)
+    b["params"] = dict(b["params"], Wind=10.0, huonggio=30.0, CORIOLIS_FORCE=1e-4)
+    return b
+
+
+def noncoh_bundle():
+    b = sediment_bundle()
+    b["options"] = dict(b["options"], ketdinh=0)
+    return b
+
+
+def narrow_bundle(kind):
+    """A 96x48 channel at rest with a sloshing water level (0.05 m times a
+    half cosine along x and a quarter along y), in the narrow-channel mode
+    -kd (kind "d") or -kn ("n")."""
+    b = S.make_channel(N=96, M=48, seed=20265200, dx=10.0, dt=2.0, hours=1.0)
+    sc = b["scenario"]
+    H, W = sc["h"].shape
+    ii = np.arange(H, dtype=np.float64)[:, None]
+    jj = np.arange(W, dtype=np.float64)[None, :]
+    sc["z0"] = 0.05 * np.cos(np.pi * (ii - 2) / (H - 5)) * (1 + 0.25 * np.cos(0.5 * np.pi * jj / W))
+    b["options"] = dict(b["options"], kenhhepd=int(kind == "d"), kenhhepng=int(kind == "n"))
+    return b
+
+
 def bundle(case):
+    if case == "windcor":
+        return windcor_bundle()
+    if case == "noncoh":
+        return noncoh_bundle()
+    if case in ("narrow_d", "narrow_n"):
+        return narrow_bundle(case[-1])
     if case == "channel":
         return S.config0()
     if case == "wetdry":
@@ -131,25 +185,28 @@ def write_luy_inputs(d: Path):
 
 def cmd_inputs(root):
     root = Path(root)
-    for case in CASES:
+    for case in SELECTED:
         d = root / case
         if case == "luy":
             write_luy_inputs(d)
         else:
             b = bundle(case)
             S.write_reference_inputs(b["scenario"], d)
-            if b["scenario"].get("FS0") is not None:
-                np.ascontiguousarray(b["scenario"]["FS0"], dtype="<f8").tofile(d / "fs0.bin")
+            for key, name in (("FS0", "fs0.bin"), ("z0", "z0.bin")):
+                if b["scenario"].get(key) is not None:
+                    np.ascontiguousarray(b["scenario"][key], dtype="<f8").tofile(d / name)
     print("inputs written under", root)
 
 
 def cmd_run(root, out):
     root, out = Path(root), Path(out)
     drv = ROOT / "oracle" / "_ref" / "hydist_ref_driver"
-    for case, spec in CASES.items():
+    for case in SELECTED:
+        spec = CASES[case]
         o = out / case
         o.mkdir(parents=True, exist_ok=True)
-        args = [a.replace("fs0=fs0.bin", f"fs0={root / case / 'fs0.bin'}") for a in spec["args"]]
+        args = [a.replace("fs0=fs0.bin", f"fs0={root / case / 'fs0.bin'}")
+                 .replace("z0=z0.bin", f"z0={root / case / 'z0.bin'}") for a in spec["args"]]
         cmd = [str(drv), str(root / case) + "/", str(o), ",".join(map(str, spec["steps"]))] + args
         # the reference prints t every half-step (engine.cpp:67) and, on an
         # open water-level first end, one line per thread per half-step
@@ -164,7 +221,11 @@ def cmd_run(root, out):
 PACK_FIELDS = {"channel": ["u", "v", "z", "FS", "H_moi", "t_u", "t_v", "t_z", "khouot"],
                "luy": ["u", "v", "z", "khouot"],
                "wetdry": ["u", "v", "z", "H_moi", "t_u", "t_v", "t_z", "Htdu", "Htdv", "khouot"],
-               "sediment": ["u", "v", "z", "FS", "tFS", "H_moi", "VTH", "Kx", "Ky", "khouot"]}
+               "sediment": ["u", "v", "z", "FS", "tFS", "H_moi", "VTH", "Kx", "Ky", "khouot"],
+               "windcor": ["u", "v", "z", "khouot"],
+               "noncoh": ["u", "v", "z", "FS", "khouot"],
+               "narrow_d": ["u", "v", "z", "khouot"],
+               "narrow_n": ["u", "v", "z", "khouot"]}
 
 
 def cmd_pack(out):
@@ -172,7 +233,8 @@ def cmd_pack(out):
     raw files are removed so that the results fit the return channel)."""
     from oracle.oracle import read_ref_state
     out = Path(out)
-    for case, spec in CASES.items():
+    for case in SELECTED:
+        spec = CASES[case]
         arrs = {}
         for st in spec["steps"]:
             p = out / case / f"state_{st}.bin"
@@ -188,7 +250,8 @@ def cmd_pack(out):
 
 def cmd_collect(out):
     out = Path(out)
-    for case, spec in CASES.items():
+    for case in SELECTED:
+        spec = CASES[case]
         arrs = {}
         meta = dict(case=case, steps=spec["steps"], stride=spec["stride"], fields=spec["fields"])
         s = spec["stride"]

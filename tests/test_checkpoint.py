@@ -36,4 +36,18 @@ def test_resume_is_bit_identical(hyd, tmp_path):
     bad.write_bytes(b"not a checkpoint" * 8)
     with pytest.raises(hyd.HydistError, match="format"):
         b.load(bad)
+    # a truncated file (valid header, body cut short) and one with trailing
+    # bytes are refused before anything is uploaded: the handle's state and
+    # time stay as they were
+    raw = ck.read_bytes()
+    before = {f: b.download(f) for f in ("u", "z", "khouot")}
+    t_before = b.t
+    for name, data in (("cut.ck", raw[:len(raw) - 1000]), ("long.ck", raw + b"\0" * 8)):
+        p = tmp_path / name
+        p.write_bytes(data)
+        with pytest.raises(hyd.HydistError, match="size"):
+            b.load(p)
+        assert b.t == t_before
+        for f, w in before.items():
+            np.testing.assert_array_equal(b.download(f), w, err_msg=f)
     b.close()

@@ -293,6 +293,36 @@ def test_bed_change(hyd, oracle_mod):
     assert not bad, bad
 
 
+def test_noncohesive_sediment_case(hyd, oracle_mod):
+    """Non-cohesive sediment (ketdinh = 0): the source of source_nchs
+    (sediment_transport.cpp:41-49) in the concentration sweeps and in the bed
+    change, against the oracle: 1e-10 after the first steps with the source
+    on, 1e-8 after 30 more. The concentration differs from the cohesive
+    run's, so the other branch was taken."""
+    def bundle(ketdinh):
+        b = S.make_channel(N=96, M=48, seed=20269100, dx=10.0, dt=2.0, hours=1.0, sediment=True,
+                           sediment_start=10.0)
+        b["options"] = dict(b["options"], ketdinh=ketdinh, bed_change=1, bed_change_start=10.0)
+        return b
+    b = bundle(0)
+    sim = hyd.Simulation(b)
+    orc = oracle_mod.OracleSim(b, nthreads=4)
+    sim.step(10)
+    orc.step(10)
+    sim.sync()
+    bad = _compare(sim, orc, ["u", "v", "z", "FS", "tFS", "VTH", "Qbx", "Qby", "dH"], 1e-10)
+    assert not bad, bad
+    sim.step(30)
+    orc.step(30)
+    sim.sync()
+    bad = _compare(sim, orc, ["u", "v", "z", "FS", "dH"], 1e-8)
+    assert not bad, bad
+    coh = hyd.Simulation(bundle(1))
+    coh.step(40)
+    coh.sync()
+    assert _max_rel(coh.download("FS"), sim.download("FS")) > 1e-6
+
+
 @pytest.mark.parametrize("N,M,inflow", [(8, 8, 5.0), (10, 9, 5.0), (20, 12, 50.0), (40, 24, 200.0)])
 def test_short_lines_match_oracle(hyd, oracle_mod, N, M, inflow):
     """Meshes whose lines are shorter than 64 cells take fewer chunks per

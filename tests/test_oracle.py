@@ -54,7 +54,8 @@ def _fixture_bundle(case):
     return F.bundle(case)
 
 
-@pytest.mark.parametrize("case", ["channel", "sediment", "luy", "wetdry"])
+@pytest.mark.parametrize("case", ["channel", "sediment", "luy", "wetdry", "windcor", "noncoh",
+                                  "narrow_d", "narrow_n"])
 def test_oracle_matches_reference_run(oracle_mod, case):
     """The oracle against the reference's own time step, run on a B200 from
     its sources (tests/golden/make_reference_fixtures.py): u, v, z (FS) on a

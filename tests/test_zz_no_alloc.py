@@ -1,8 +1,9 @@
 """hydist_gtsv_batched_noalloc: the allocation-free batched Thomas solve.
 
-Its results are compared with hydist_gtsv_batched (algo 1, the same Thomas
-recurrence) on two consecutive calls; the second call must leave the
-device's free memory unchanged. The file name sorts last so that the GPU
+Its results are compared with the FP64 CPU oracle's batched Thomas and with
+hydist_gtsv_batched (the allocating entry point, autotuned solver choice) on
+two consecutive calls; the second call must leave the device's free memory
+unchanged. The file name sorts last so that the GPU
 tests also run it after every other test has used the device.
 """
 import ctypes as C
@@ -50,8 +51,8 @@ def test_noalloc_rejects_rows_beyond_limit(hyd):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("dtype,rtol", [("float64", 1e-12), ("float32", 1e-5)])
-def test_noalloc_matches_gtsv_batched(hyd, dtype, rtol):
+@pytest.mark.parametrize("dtype,rtol", [("float64", 1e-12), ("float32", 2e-5)])
+def test_noalloc_matches_oracle_and_gtsv_batched(hyd, oracle_mod, dtype, rtol):
     import torch
     from hydist_c_b200 import capi
     lib = hyd.library()
@@ -59,10 +60,17 @@ def test_noalloc_matches_gtsv_batched(hyd, dtype, rtol):
     tdt = getattr(torch, dtype)
     a, d, c, b, offs, lens, rows = _packed_batch(7, 3000, 300)
     assert rows <= MAX_ROWS
+    # the oracle solves the systems as the device sees them (rounded to the
+    # call's type first)
     t = [torch.from_numpy(v).to(dev, tdt).contiguous() for v in (a, d, c, b)]
+    host = [v.double().cpu().numpy() for v in t]
+    ref = torch.from_numpy(oracle_mod.thomas_batched(*host, offs, lens)).to(dev, tdt)
     o = torch.from_numpy(offs).to(dev)
     n = torch.from_numpy(lens).to(dev)
-    ref = hyd.gtsv_batched(*t, o, n, algo=1)
+    alloc = hyd.gtsv_batched(*t, o, n, algo=capi.GTSV_AUTO)
+    torch.cuda.synchronize()
+    scale0 = torch.clamp(ref.abs(), min=1.0)
+    assert ((alloc - ref).abs() / scale0).max().item() <= rtol
     stream = torch.cuda.current_stream(dev).cuda_stream
     outs = [torch.zeros(rows, dtype=tdt, device=dev) for _ in range(2)]
     scale = torch.clamp(ref.abs(), min=1.0)
@@ -76,6 +84,9 @@ def test_noalloc_matches_gtsv_batched(hyd, dtype, rtol):
         free.append((before, torch.cuda.mem_get_info(dev)[0]))
         err = ((x - ref).abs() / scale).max().item()
         assert err <= rtol, err
+        # both are within rtol of the FP64 solution
+        err = ((x - alloc).abs() / scale).max().item()
+        assert err <= 2 * rtol, err
     # the second call allocated nothing on the device (the first one may
     # load the library's kernels and their fixed scratch)
     assert free[1][0] == free[1][1]
@@ -93,7 +104,7 @@ def test_noalloc_matches_gtsv_batched(hyd, dtype, rtol):
 
 
 @pytest.mark.gpu
-def test_noalloc_leaves_systems_outside_rows_unsolved(hyd):
+def test_noalloc_leaves_systems_outside_rows_unsolved(hyd, oracle_mod):
     import torch
     from hydist_c_b200 import capi
     lib = hyd.library()
@@ -102,7 +113,7 @@ def test_noalloc_leaves_systems_outside_rows_unsolved(hyd):
     t = [torch.from_numpy(v).to(dev).contiguous() for v in (a, d, c, b)]
     o = torch.from_numpy(offs).to(dev)
     n = torch.from_numpy(lens).to(dev)
-    ref = hyd.gtsv_batched(*t, o, n, algo=1)
+    ref = torch.from_numpy(oracle_mod.thomas_batched(a, d, c, b, offs, lens)).to(dev)
     cut = int(offs[-1]) + 1  # the last system crosses the declared rows
     x = torch.zeros(rows, dtype=torch.float64, device=dev)
     st = _call(lib, t, o, n, x, cut, torch.cuda.current_stream(dev).cuda_stream)
