@@ -268,6 +268,17 @@ def run_ensemble(args):
     step_bytes = BYTES_PER_CELL_STEP[("fp64" if args.precision == "fp64" else "fp32", True)] * cells
     ach = step_bytes / (ms / args.steps * 1e-3) / 1e9
     mass = [m.mass() for m in sims[:4]]
+    # the same steps with every member on its own launches (one graph of
+    # the members' kernels on their streams), for comparison
+    ens.batched(False)
+    ens.step(max(args.warmup, 3))
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    ens.step(args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    per_member_ms = ev0.elapsed_time(ev1) / args.steps
     ens.close()
     for m in sims:
         m.close()
@@ -320,10 +331,14 @@ def run_ensemble(args):
             "data": "synthetic (seeded per member)",
             "config": {"workload": ENSEMBLE, "members": nmem, "N": 1024, "M": 512, "cells": cells,
                        "precision": args.precision,
-                       "sediment": True, "cuda_graph": "one graph launch per step for all members",
+                       "sediment": True,
+                       "cuda_graph": "one graph launch per step; each kernel one launch over all "
+                                     "members (batched)",
                        "l2": "inputs larger than L2", "parallelism": f"replicas x{ws}"},
             "p50_step_ms": float(np.percentile(per, 50)), "p99_step_ms": float(np.percentile(per, 99)),
             "member_mass": mass,
+            "per_member_launches_ms_per_step": per_member_ms,
+            "batched_speedup": per_member_ms / (ms / args.steps),
             "roofline": {"bound": "hbm", "kernel": "ensemble step (all members' kernels)",
                          "bytes_per_launch": step_bytes, "achieved": ach, "peak": hbm,
                          "unit": "GB/s", "frac": ach / hbm, "traffic": None,
@@ -383,6 +398,20 @@ def run_serving(args):
             srv.release(rid)
     makespan = time.perf_counter() - t0
     srv.close()
+    # the baseline: the plain FP64 form, one request at a time in arrival
+    # order (each request created, stepped through its step graph, its
+    # result read back, released, before the next starts; the device is
+    # idle while no request has arrived), the same requests and inputs
+    base_lat, vt = [], 0.0
+    for r in sorted(reqs, key=lambda r: r["arrival"]):
+        vt = max(vt, r["arrival"])
+        t1 = time.perf_counter()
+        sim = H.Simulation(r["bundle"], device=dev.index, precision=H.FP64)
+        sim.step_graph(r["nsteps"])
+        sim.download("z")
+        sim.close()
+        vt += time.perf_counter() - t1
+        base_lat.append(vt - r["arrival"])
     R.barrier(ws)
     span = R.max_over_ranks(makespan, ws)
     value = R.sum_over_ranks(work, ws) / span
@@ -400,6 +429,15 @@ def run_serving(args):
                           "max": float(np.max(lat))},
             "makespan_s": makespan, "cell_steps": work,
             "offered_cell_steps_per_s": work / (reqs[-1]["arrival"] + 1e-9),
+            "one_at_a_time_fp64": {
+                "makespan_s": vt, "value": work / vt,
+                "latency_s": {"p50": float(np.percentile(base_lat, 50)),
+                              "p99": float(np.percentile(base_lat, 99)),
+                              "max": float(np.max(base_lat))},
+                "note": "the same requests run one after another in arrival order, each "
+                        "created, stepped and read back alone; idle time until an arrival "
+                        "counted, not slept"},
+            "speedup_vs_one_at_a_time": vt / makespan,
             "e2e": {"value": value, "unit": "cell-steps/s",
                     "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                     "note": "wall clock from the first arrival, host inputs copied at submit"},
@@ -434,6 +472,25 @@ def run_tridiag_reference(args):
         "e2e": {"value": v, "unit": "unknowns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def rel_residual(a, d, c, b, off, ln, x):
+    """max over rows of |b - A x| / (|a x_{-1}| + |d x| + |c x_{+1}| + |b|):
+    the componentwise backward error of a packed batch's solution (dl of a
+    system's first row and du of its last row ignored)."""
+    n = len(d)
+    first = np.zeros(n, bool)
+    last = np.zeros(n, bool)
+    nz = ln > 0
+    first[off[nz]] = True
+    last[off[nz] + ln[nz] - 1] = True
+    xm = np.where(first, 0.0, np.roll(x, 1))
+    xp = np.where(last, 0.0, np.roll(x, -1))
+    am = np.where(first, 0.0, a)
+    cp = np.where(last, 0.0, c)
+    r = np.abs(b - am * xm - d * x - cp * xp)
+    den = np.abs(am * xm) + np.abs(d * x) + np.abs(cp * xp) + np.abs(b)
+    return float(np.max(r / np.maximum(den, 1e-300)))
 
 
 def run_tridiag(args):
@@ -532,6 +589,34 @@ def run_tridiag(args):
         cpu = {"value": n / tc, "unit": "unknowns/s", "cores": threads, "kind": "port",
                "sample": f"one solve of the whole batch ({tc:.2f} s), FP64 serial Thomas per "
                          "system, OpenMP over systems"}
+    refined = None
+    if rank == 0 and args.dtype == "f64":
+        # the same FP64 systems solved in FP32 with one FP64-residual
+        # refinement (hydist_gtsv_batched_refine), timed the same way
+        xr = torch.empty_like(t[1])
+
+        def solve_ref():
+            st = lib.hydist_gtsv_batched_refine(
+                t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), t[3].data_ptr(),
+                xr.data_ptr(), o_d.data_ptr(), l_d.data_ptr(), len(ln),
+                args.gtsv_algo or capi.GTSV_AUTO, C.c_void_p(stream.cuda_stream))
+            capi.check(lib, st, "hydist_gtsv_batched_refine")
+
+        for _ in range(3):
+            solve_ref()
+        torch.cuda.synchronize(dev)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            solve_ref()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        rms = ev0.elapsed_time(ev1) / args.steps
+        xrs = xr.cpu().numpy()
+        refined = {"ms_per_step": rms, "value": n / (rms * 1e-3),
+                   "max_rel_err_vs_fp64_oracle":
+                       float(np.max(np.abs(xrs - ref) / np.maximum(np.abs(ref), 1.0))),
+                   "max_rel_residual": rel_residual(a, d, c, b, off, ln, xrs)}
     if rank == 0:
         hbm, peak_kind = _peaks()
         alg = TRIDIAG_BYTES[args.dtype] * n
@@ -548,12 +633,15 @@ def run_tridiag(args):
                        "l2": "inputs larger than L2", "parallelism": f"replicas x{ws}"},
             "p50_step_ms": float(np.percentile(per, 50)), "p99_step_ms": float(np.percentile(per, 99)),
             "max_rel_err_vs_fp64_oracle": err,
+            "max_rel_residual": rel_residual(a, d, c, b, off, ln, xs),
             "roofline": {"bound": "hbm", "kernel": "batched solve (classify + per-band solvers)",
                          "bytes_per_launch": alg, "achieved": ach, "peak": hbm, "unit": "GB/s",
                          "frac": ach / hbm, "traffic": None, "peak_source": peak_kind},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps * (1 + nonempty),
             "clocks": clk,
         }
+        if refined is not None:
+            line["fp32_refined"] = refined
         print(json.dumps(line), flush=True)
     R.finish(ws)
 

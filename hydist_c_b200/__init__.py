@@ -198,6 +198,12 @@ class Ensemble:
     def step(self, n: int = 1):
         capi.check(self._lib, self._lib.hydist_ensemble_step(self._e, int(n)), "hydist_ensemble_step")
 
+    def batched(self, enable: bool = True):
+        """Batch the members' launches (the default where they allow it) or
+        step them by their own launches (hydist_ensemble_batched)."""
+        capi.check(self._lib, self._lib.hydist_ensemble_batched(self._e, int(bool(enable))),
+                   "hydist_ensemble_batched")
+
     def sync(self):
         capi.check(self._lib, self._lib.hydist_ensemble_sync(self._e), "hydist_ensemble_sync")
 
@@ -296,12 +302,18 @@ class Server:
             pass
 
 
-def gtsv_batched(dl, d, du, b, offsets, lengths, algo: int = 0, x=None, stream=None):
+def gtsv_batched(dl, d, du, b, offsets, lengths, algo: int = 0, x=None, stream=None,
+                 refine: bool = False):
     """Solve a packed batch of tridiagonal systems on the GPU.
 
     Arguments are CUDA tensors (torch) of one dtype (float64 or float32);
-    offsets/lengths are int32 CUDA tensors. Returns x. algo: 0 autotuned,
-    1 Thomas, 2 partitioned Thomas/SPIKE with diagonal pivoting, 3 PCR-Thomas.
+    offsets/lengths are int32 tensors. Returns x. algo (enum HydistGtsvAlgo):
+    0 autotuned per length band, 1 Thomas, 2 / 4 / 5 the CTA partition
+    solver on 256 / 512 / 128 threads, 3 the warp partition solver, 6
+    Gaussian elimination with diagonal pivoting (for systems that are not
+    diagonally dominant; the others do not pivot). refine (float64 only):
+    solve in FP32 and refine once with the FP64 residual
+    (hydist_gtsv_batched_refine).
     """
     import torch
 
@@ -321,6 +333,15 @@ def gtsv_batched(dl, d, du, b, offsets, lengths, algo: int = 0, x=None, stream=N
     lengths = lengths.to(device=d.device, dtype=torch.int32).contiguous()
     if stream is None:
         stream = torch.cuda.current_stream(d.device).cuda_stream
+    if refine:
+        if dt != 0:
+            raise TypeError("refine takes float64 systems")
+        st = lib.hydist_gtsv_batched_refine(dl.data_ptr(), d.data_ptr(), du.data_ptr(),
+                                            b.data_ptr(), x.data_ptr(), offsets.data_ptr(),
+                                            lengths.data_ptr(), int(offsets.numel()), int(algo),
+                                            C.c_void_p(stream))
+        capi.check(lib, st, "hydist_gtsv_batched_refine")
+        return x
     st = lib.hydist_gtsv_batched(dl.data_ptr(), d.data_ptr(), du.data_ptr(), b.data_ptr(),
                                  x.data_ptr(), offsets.data_ptr(), lengths.data_ptr(),
                                  int(offsets.numel()), dt, int(algo), C.c_void_p(stream))

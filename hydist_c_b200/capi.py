@@ -206,12 +206,15 @@ def _declare(lib):
                                         C.c_int32, vp]
     lib.hydist_gtsv_batched_noalloc.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int32,
                                                 C.c_int32, C.c_int32, vp]
+    lib.hydist_gtsv_batched_refine.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32,
+                                               vp]
     lib.hydist_gtsv_autotune.argtypes = [C.c_int32, vp, _ip]
     lib.hydist_create_external.argtypes = [C.POINTER(HydistExternal), C.POINTER(HydistParams),
                                            C.POINTER(HydistOptions), C.c_int, C.POINTER(vp)]
     lib.hydist_half_step.argtypes = [vp, C.c_int32]
     lib.hydist_ensemble_create.argtypes = [C.POINTER(vp), C.c_int32, C.POINTER(vp)]
     lib.hydist_ensemble_step.argtypes = [vp, C.c_int32]
+    lib.hydist_ensemble_batched.argtypes = [vp, C.c_int32]
     lib.hydist_ensemble_sync.argtypes = [vp]
     lib.hydist_ensemble_destroy.argtypes = [vp]
     lib.hydist_ensemble_stream.argtypes = [vp]
@@ -258,10 +261,10 @@ EXPORTED_SYMBOLS = [
     "hydist_server_destroy", "hydist_server_submit", "hydist_server_round",
     "hydist_server_status", "hydist_server_counts", "hydist_server_handle",
     "hydist_server_release", "hydist_checkpoint_save", "hydist_checkpoint_load",
-    "hydist_create_phases",
+    "hydist_create_phases", "hydist_gtsv_batched_refine", "hydist_ensemble_batched",
 ]
-GTSV_AUTO, GTSV_THOMAS, GTSV_PARTITION, GTSV_WARP, GTSV_PARTITION_512, GTSV_PARTITION_128 = \
-    0, 1, 2, 3, 4, 5
+GTSV_AUTO, GTSV_THOMAS, GTSV_PARTITION, GTSV_WARP, GTSV_PARTITION_512, GTSV_PARTITION_128, \
+    GTSV_PIVOT = 0, 1, 2, 3, 4, 5, 6
 GTSV_BANDS = 7
 
 PHASES = ["boundary_x", "sweep_x", "explicit_v", "commit_x", "sediment_x",

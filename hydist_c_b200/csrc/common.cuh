@@ -76,6 +76,7 @@ struct StateT {
   int x_lo, x_hi, y_lo;
   int reset_h;     // Reset_states_horizontal in the first half-step
   int bed_fb;      // the bed change feeds back into h, htaiz, Kx1, Ky1
+  double src_start;  // the concentration sweeps' erosion source from this time
   const double *h0, *htaiz0;  // the initial bed (with bed_fb)
   // static fields
   const double *h, *hsnham, *htaiz, *htaiz_bd;
@@ -96,6 +97,9 @@ struct StateT {
   R *su, *sv;    // t_u / t_v after the smoothing of the current half-step
   int* err;      // [0]: DevErr
   R* lscratch;   // partitioned line solver: one slot per resident CTA
+  // the preindex values of every cell for the next hydraulic sweep (f1, f2,
+  // f3, f5, a2, c2, d2: seven arrays of (N+3)*(M+3), array k at pre + k*W*H)
+  R* pre;
   int lslots;    // number of slots (CTAs of the persistent sweep grid)
   int* colflag;  // per column: holds a cell dried during the run
   int* rowflag;  // per row: the same (wetting along rows)
@@ -103,6 +107,34 @@ struct StateT {
   double* clock; // [0]: simulated time, advanced on the device by k_tick
 };
 using State = StateT<double>;
+
+// Many scenarios of one mesh size stepped by the same launches: the states
+// and coefficients of the members in device arrays; a kernel launched for
+// the batch takes member blockIdx.z (the line solvers: the member of the
+// line group). n = 0: one scenario, passed by value.
+template <class R>
+struct Batch {
+  const StateT<R>* S = nullptr;
+  const CoefT<R>* c = nullptr;
+  int n = 0;
+};
+
+// The state and coefficients a kernel works on: its by-value arguments, or
+// with BATCH those of member blockIdx.z.
+template <int BATCH, class R>
+__device__ __forceinline__ StateT<R> member_state(const StateT<R>& S0, const Batch<R>& b) {
+  if constexpr (BATCH != 0) return b.S[blockIdx.z];
+  else return S0;
+}
+template <int BATCH, class R>
+__device__ __forceinline__ CoefT<R> member_coef(const CoefT<R>& c0, const Batch<R>& b) {
+  if constexpr (BATCH != 0) return b.c[blockIdx.z];
+  else return c0;
+}
+
+// grid z of a launch: one slice per member of a batch
+template <class R>
+inline unsigned grid_z(const Batch<R>& b) { return b.n > 0 ? (unsigned)b.n : 1u; }
 
 __host__ __device__ inline int cdiv(int a, int b) { return (a + b - 1) / b; }
 

@@ -279,10 +279,10 @@ int check_horizon(HydistHandle* h, int nsteps) {
 void enqueue_step(HydistHandle* h, bool sed_x, bool sed_y, bool bed, Trace* tr) {
   on_state(h, [&](auto& St, auto& Cf) {
     launch_half_x(St, Cf, sed_x, h->stream, tr);
-    if (sed_x) launch_sediment(St, Cf, h->o.bed_change_start, true, false, h->stream, tr);
+    if (sed_x) launch_sediment(St, Cf, true, false, h->stream, tr);
     else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_X + 1], h->stream);
     launch_half_y(St, Cf, sed_y, h->stream, tr);
-    if (sed_y) launch_sediment(St, Cf, h->o.bed_change_start, false, bed, h->stream, tr);
+    if (sed_y) launch_sediment(St, Cf, false, bed, h->stream, tr);
     else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_Y + 1], h->stream);
   });
 }
@@ -520,6 +520,7 @@ int new_handle(const HydistParams* p, const HydistOptions* o, int device, int M,
   S.y_lo = channel && o->kenhhepng ? 3 : 2;
   S.reset_h = o->reset_horizontal ? 1 : 0;
   S.bed_fb = o->bed_change && o->bed_feedback ? 1 : 0;
+  S.src_start = o->bed_change_start;
   return HYDIST_OK;
 }
 
@@ -534,6 +535,7 @@ int bulk_private(HydistHandle* h, StateT<R>& B) {
   const size_t n = (size_t)S.W * S.H;
   TRY(dalloc(h, &B.tmp, n));
   TRY(dalloc(h, &B.sv, n));
+  TRY(dalloc(h, &B.pre, 7 * n));
   B.su = B.tmp;
   int nsm = 0;
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
@@ -639,6 +641,7 @@ void mirror_common(HydistHandle* h) {
   F.y_lo = S.y_lo;
   F.reset_h = S.reset_h;
   F.bed_fb = S.bed_fb;
+  F.src_start = S.src_start;
   F.h0 = S.h0;
   F.htaiz0 = S.htaiz0;
   F.h = S.h;
@@ -884,13 +887,13 @@ int hydist_half_step(HydistHandle* h, int32_t half) {
   if (half == 0) {
     on_state(h, [&](auto& St, auto& Cf) {
       launch_half_x(St, Cf, sed, h->stream, &h->trace);
-      if (sed) launch_sediment(St, Cf, h->o.bed_change_start, true, false, h->stream, &h->trace);
+      if (sed) launch_sediment(St, Cf, true, false, h->stream, &h->trace);
     });
   } else {
     on_state(h, [&](auto& St, auto& Cf) {
       launch_half_y(St, Cf, sed, h->stream, &h->trace);
       if (sed)
-        launch_sediment(St, Cf, h->o.bed_change_start, false, bed_on(h, t), h->stream,
+        launch_sediment(St, Cf, false, bed_on(h, t), h->stream,
                         &h->trace);
     });
   }
@@ -1050,7 +1053,56 @@ struct HydistEnsemble {
   std::vector<cudaEvent_t> join;
   // one graph per pattern of the members' sediment phases
   std::map<std::vector<unsigned char>, std::pair<cudaGraphExec_t, long long>> graphs;
+  // batched stepping: members of one mesh size and form, whose states and
+  // coefficients are copied to the device once, so that each kernel of a
+  // step is one launch over all members (uniform: they allow it; batched:
+  // it is used when the members' sediment phases agree)
+  bool uniform = false, batched = false;
+  void *bS = nullptr, *bC = nullptr;  // StateT<R>[n], CoefT<R>[n]
 };
+
+}  // extern "C"
+
+namespace {
+
+// members that can share launches: same mesh, form and launch-shaping
+// options
+bool same_launches(const HydistHandle* a, const HydistHandle* b) {
+  return a->S.M == b->S.M && a->S.N == b->S.N && a->fp32 == b->fp32 && a->S.refine == b->S.refine &&
+         a->S.x_lo == b->S.x_lo && a->S.x_hi == b->S.x_hi && a->S.y_lo == b->S.y_lo &&
+         a->S.reset_h == b->S.reset_h && a->S.bed_fb == b->S.bed_fb &&
+         a->S.lslots == b->S.lslots && a->Sf.lslots == b->Sf.lslots;
+}
+
+// one step of every member of a batch, on stream st
+template <class R>
+void enqueue_step_batch(const StateT<R>& S0, const CoefT<R>& c0, const Batch<R>& b, bool sx,
+                        bool sy, bool bed, cudaStream_t st, Trace* tr) {
+  launch_half_x(S0, c0, sx, st, tr, b);
+  if (sx) launch_sediment(S0, c0, true, false, st, tr, b);
+  launch_half_y(S0, c0, sy, st, tr, b);
+  if (sy) launch_sediment(S0, c0, false, bed, st, tr, b);
+}
+
+template <class R>
+int upload_batch(HydistEnsemble* e, StateT<R> HydistHandle::*sm, CoefT<R> HydistHandle::*cm) {
+  const int n = (int)e->m.size();
+  std::vector<StateT<R>> S(n);
+  std::vector<CoefT<R>> C(n);
+  for (int i = 0; i < n; ++i) {
+    S[i] = e->m[i]->*sm;
+    C[i] = e->m[i]->*cm;
+  }
+  CK(cudaMalloc(&e->bS, n * sizeof(StateT<R>)));
+  CK(cudaMalloc(&e->bC, n * sizeof(CoefT<R>)));
+  CK(cudaMemcpy(e->bS, S.data(), n * sizeof(StateT<R>), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(e->bC, C.data(), n * sizeof(CoefT<R>), cudaMemcpyHostToDevice));
+  return HYDIST_OK;
+}
+
+}  // namespace
+
+extern "C" {
 
 int hydist_ensemble_create(HydistHandle* const* members, int32_t n, HydistEnsemble** out) {
   if (!members || !out || n < 1) return fail(HYDIST_ERR_ARG, "null argument or empty ensemble");
@@ -1073,6 +1125,13 @@ int hydist_ensemble_create(HydistHandle* const* members, int32_t n, HydistEnsemb
     CK(cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming));
     e->join.resize(n);
     for (auto& ev : e->join) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    e->uniform = true;
+    for (int i = 1; i < n; ++i) e->uniform = e->uniform && same_launches(members[0], members[i]);
+    if (e->uniform) {
+      if (members[0]->fp32) TRY(upload_batch<float>(e, &HydistHandle::Sf, &HydistHandle::cf));
+      else TRY(upload_batch<double>(e, &HydistHandle::S, &HydistHandle::c));
+      e->batched = true;
+    }
     return HYDIST_OK;
   }();
   if (rc != HYDIST_OK) {
@@ -1091,6 +1150,8 @@ int hydist_ensemble_destroy(HydistEnsemble* e) {
     if (kv.second.first) cudaGraphExecDestroy(kv.second.first);
   for (auto& ev : e->join)
     if (ev) cudaEventDestroy(ev);
+  if (e->bS) cudaFree(e->bS);
+  if (e->bC) cudaFree(e->bC);
   if (e->fork) cudaEventDestroy(e->fork);
   if (e->done) cudaEventDestroy(e->done);
   if (e->origin) cudaStreamDestroy(e->origin);
@@ -1122,29 +1183,51 @@ int hydist_ensemble_step(HydistEnsemble* e, int32_t nsteps) {
       key[3 * i + 1] = t2 >= h->o.sediment_start;
       key[3 * i + 2] = bed_on(h, t2);
     }
-    auto it = e->graphs.find(key);
+    // all members in the same sediment phase: one launch per kernel for the
+    // batch (the graph's key is that phase alone)
+    bool same = e->batched;
+    for (int i = 1; same && i < n; ++i)
+      same = key[3 * i] == key[0] && key[3 * i + 1] == key[1] && key[3 * i + 2] == key[2];
+    std::vector<unsigned char> gkey = same ? std::vector<unsigned char>{2, key[0], key[1], key[2]}
+                                           : key;
+    auto it = e->graphs.find(gkey);
     if (it == e->graphs.end()) {
-      // one step of every member: fork from the origin stream onto the
-      // members' streams, join back
       cudaGraph_t g = nullptr;
       long long launches = 0;
       CK(cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal));
-      CK(cudaEventRecord(e->fork, e->origin));
-      for (int i = 0; i < n; ++i) {
-        HydistHandle* h = e->m[i];
-        CK(cudaStreamWaitEvent(h->stream, e->fork, 0));
+      if (same) {
+        HydistHandle* h0 = e->m[0];
         Trace tr;
-        enqueue_step(h, key[3 * i], key[3 * i + 1], key[3 * i + 2], &tr);
-        launches += tr.launches;
-        CK(cudaEventRecord(e->join[i], h->stream));
-        CK(cudaStreamWaitEvent(e->origin, e->join[i], 0));
+        if (h0->fp32) {
+          const Batch<float> b{static_cast<const StateT<float>*>(e->bS),
+                               static_cast<const CoefT<float>*>(e->bC), n};
+          enqueue_step_batch(h0->Sf, h0->cf, b, key[0], key[1], key[2], e->origin, &tr);
+        } else {
+          const Batch<double> b{static_cast<const State*>(e->bS),
+                                static_cast<const Coef*>(e->bC), n};
+          enqueue_step_batch(h0->S, h0->c, b, key[0], key[1], key[2], e->origin, &tr);
+        }
+        launches = tr.launches;
+      } else {
+        // one step of every member: fork from the origin stream onto the
+        // members' streams, join back
+        CK(cudaEventRecord(e->fork, e->origin));
+        for (int i = 0; i < n; ++i) {
+          HydistHandle* h = e->m[i];
+          CK(cudaStreamWaitEvent(h->stream, e->fork, 0));
+          Trace tr;
+          enqueue_step(h, key[3 * i], key[3 * i + 1], key[3 * i + 2], &tr);
+          launches += tr.launches;
+          CK(cudaEventRecord(e->join[i], h->stream));
+          CK(cudaStreamWaitEvent(e->origin, e->join[i], 0));
+        }
       }
       CK(cudaStreamEndCapture(e->origin, &g));
       cudaGraphExec_t ex = nullptr;
       const cudaError_t err = cudaGraphInstantiate(&ex, g, 0);
       cudaGraphDestroy(g);
       CK(err);
-      it = e->graphs.emplace(key, std::make_pair(ex, launches)).first;
+      it = e->graphs.emplace(gkey, std::make_pair(ex, launches)).first;
     }
     CK(cudaGraphLaunch(it->second.first, e->origin));
     for (int i = 0; i < n; ++i) {
@@ -1161,6 +1244,14 @@ int hydist_ensemble_step(HydistEnsemble* e, int32_t nsteps) {
 }
 
 void* hydist_ensemble_stream(HydistEnsemble* e) { return e ? (void*)e->origin : nullptr; }
+
+int hydist_ensemble_batched(HydistEnsemble* e, int32_t enable) {
+  if (!e) return fail(HYDIST_ERR_ARG, "null ensemble");
+  if (enable && !e->uniform)
+    return fail(HYDIST_ERR_ARG, "the members differ in mesh size, form or launch options");
+  e->batched = enable != 0;
+  return HYDIST_OK;
+}
 
 int hydist_ensemble_sync(HydistEnsemble* e) {
   if (!e) return fail(HYDIST_ERR_ARG, "null ensemble");

@@ -73,8 +73,10 @@ __global__ void k_onetime_init(StateT<R> S, CoefT<R> c) {
 }
 
 // ------------------------------------------------------- segment tables
-template <class R>
-__global__ void k_interp_fs_rows(StateT<R> S, CoefT<R> c) {
+template <class R, int BATCH = 0>
+__global__ void k_interp_fs_rows(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   // Interpolate_FS_ng at row N (offset N-1, sign -1) and row 2 (offset 2, +1)
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int which = blockIdx.y;
@@ -97,8 +99,10 @@ __global__ void k_interp_fs_rows(StateT<R> S, CoefT<R> c) {
   }
 }
 
-template <class R>
-__global__ void k_interp_fs_col(StateT<R> S, CoefT<R> c) {
+template <class R, int BATCH = 0>
+__global__ void k_interp_fs_col(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   // Interpolate_FS_d at column M (offset M-1, sign -1); rows 1..M-1 as the
   // reference loops them (support_funcs.cpp:227)
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -141,8 +145,11 @@ __device__ __forceinline__ void run_flags(bool wm1, bool w, bool wp1, bool wm2_l
 // reads as dried (1) and is written so. Reading a neighbour's mask while
 // its thread writes it is safe: the write turns 0 into 1 exactly when this
 // test gives 1.
-template <class R>
-__global__ void k_runs_flags(StateT<R> S, CoefT<R> c, int* seg_cnt, int dry) {
+template <class R, int BATCH = 0>
+__global__ void k_runs_flags(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int dry) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
+  int* seg_cnt = S.segcnt;
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int i = blockIdx.y + 2;
   if (i > S.N || j > S.M) return;
@@ -226,8 +233,10 @@ __device__ __forceinline__ void sort_small(int* a, int n) {
 
 // One thread per line: order the claimed slots, set the counts, clear the
 // counters for the next scan.
-template <class R>
-__global__ void k_runs_sort(StateT<R> S, int* seg_cnt) {
+template <class R, int BATCH = 0>
+__global__ void k_runs_sort(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  int* seg_cnt = S.segcnt;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int H = S.H, W = S.W;
   const int nrow = S.N - 1, ncol = S.M - 1;
@@ -383,8 +392,11 @@ __device__ void channel_wave_cell(const StateT<R>& S, double dX, double dY, doub
   }
 }
 
-template <class R>
-__global__ void k_boundary(StateT<R> S, double half, double dX, double dY) {
+template <class R, int BATCH = 0>
+__global__ void k_boundary(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, double half) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
+  const double dX = (double)c.dX, dY = (double)c.dY;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int M = S.M, N = S.N, W = S.W;
   const double t_new = S.clock[0] + half;
@@ -463,6 +475,23 @@ __global__ void k_boundary(StateT<R> S, double half, double dX, double dY) {
   }
 }
 
+// ------------------------------------------------------------- preindex
+// _uzSolver_calculate_preindex (DIR 0) / _vzSolver_calculate_preindex
+// (DIR 1) of every cell of rows 2..N, columns 2..M into StateT::pre, ahead
+// of the sweep that reads them: one thread per cell, adjacent threads on
+// adjacent cells, so the stencils' loads are shared through L1 instead of
+// each line walker fetching its own.
+template <class R, int DIR, int BATCH = 0>
+__global__ void k_pre(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int i = blockIdx.y + 2;
+  if (i > S.N || j > S.M) return;
+  const PreT<R> P = DIR == 0 ? pre_x(S, c, i, j) : pre_y(S, c, i, j);
+  store_pre(S, (size_t)S.W * S.H, i * S.W + j, P);
+}
+
 // ------------------------------------------------------------ smoothing
 // _normalize / update_buffer (support_funcs.cpp:761-808) into a complete
 // array (su / sv): smoothed on the interior [2,N]x[2,M], the unsmoothed
@@ -479,8 +508,10 @@ constexpr int SMOOTH_ROWS = 4;
 
 // isU: t_u (else t_v); hmoi: with update_h_moi and the column flags. Both
 // are template parameters: each launch compiles to its own variant.
-template <class R, int isU, int hmoi>
-__global__ void k_smooth_full(StateT<R> S, CoefT<R> c) {
+template <class R, int isU, int hmoi, int BATCH = 0>
+__global__ void k_smooth_full(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   constexpr int RB = SMOOTH_ROWS;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i0 = blockIdx.y * RB;
@@ -572,8 +603,10 @@ __device__ __forceinline__ bool find_seg(const int* dau, const int* cuoi, int n,
 
 // vSolver driven by solveV (UVZSolver_multithread.cpp:607-663, 961-978);
 // the cell's arithmetic is v_new (explicit.cuh).
-template <class R>
-__global__ void k_solve_v(StateT<R> S, CoefT<R> c) {
+template <class R, int BATCH = 0>
+__global__ void k_solve_v(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   // the block's cells share one row: its segment table goes to shared memory
   __shared__ int s_first[SEG], s_last[SEG];
   __shared__ int s_n;
@@ -601,8 +634,10 @@ __global__ void k_solve_v(StateT<R> S, CoefT<R> c) {
 
 // uSolver driven by solveU (UVZSolver_multithread.cpp:724-795, 938-959);
 // the cell's arithmetic is u_new (explicit.cuh).
-template <class R>
-__global__ void k_solve_u(StateT<R> S, CoefT<R> c) {
+template <class R, int BATCH = 0>
+__global__ void k_solve_u(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int col = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int row = blockIdx.y + 1;
   if (row > S.N || col > S.M) return;
@@ -618,8 +653,10 @@ __global__ void k_solve_u(StateT<R> S, CoefT<R> c) {
 
 // update_margin_elem_V (UVZSolver_multithread.cpp:1018-1060), one row per
 // thread.
-template <class R>
-__global__ void k_margin_v(StateT<R> S, CoefT<R> c) {
+template <class R, int BATCH = 0>
+__global__ void k_margin_v(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
   if (i > S.N) return;
   margin_v(S, (double)c.NANGDAY, i);
@@ -627,8 +664,10 @@ __global__ void k_margin_v(StateT<R> S, CoefT<R> c) {
 
 // update_margin_elem_U (UVZSolver_multithread.cpp:980-1016), one column per
 // thread.
-template <class R>
-__global__ void k_margin_u(StateT<R> S, CoefT<R> c) {
+template <class R, int BATCH = 0>
+__global__ void k_margin_u(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
   if (j > S.M) return;
   margin_u(S, (double)c.NANGDAY, j);
@@ -674,8 +713,10 @@ __device__ __forceinline__ void vth_heso_cell(const StateT<R>& S, const CoefT<R>
 // column M+1). With vth_hi > 0 (the concentration step follows) also
 // Find_VTH + hesoK on rows 1..vth_hi: nothing between this commit and the
 // concentration sweep changes what they read.
-template <class R>
-__global__ void k_commit_a(StateT<R> S, CoefT<R> c, int vth_hi) {
+template <class R, int BATCH = 0>
+__global__ void k_commit_a(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   if (i > S.N || j > S.M) return;
@@ -721,8 +762,11 @@ __global__ void k_commit_a(StateT<R> S, CoefT<R> c, int vth_hi) {
 
 // The wetting loop of Reset_states_vertical (support_funcs.cpp:160-175),
 // sequential along i, on flagged columns only.
-template <class R>
-__global__ void k_wetting(StateT<R> S, CoefT<R> c, int* colflag) {
+template <class R, int BATCH = 0>
+__global__ void k_wetting(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
+  int* colflag = S.colflag;
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (j > S.M) return;
   if (!colflag[j]) return;
@@ -751,8 +795,11 @@ __global__ void k_wetting(StateT<R> S, CoefT<R> c, int* colflag) {
 
 // The wetting loop of Reset_states_horizontal (support_funcs.cpp:103-120),
 // sequential along j, on flagged rows 1..N only.
-template <class R>
-__global__ void k_wetting_rows(StateT<R> S, CoefT<R> c, int* rowflag) {
+template <class R, int BATCH = 0>
+__global__ void k_wetting_rows(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
+  int* rowflag = S.rowflag;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i > S.N) return;
   if (!rowflag[i]) return;
@@ -792,8 +839,10 @@ __global__ void k_wetting_rows(StateT<R> S, CoefT<R> c, int* rowflag) {
 //
 // HORIZ: the drying loop of Reset_states_horizontal instead (:125-137,
 // rows 1..N, columns 2..M), in the first half-step.
-template <class R, int HORIZ>
-__global__ void k_commit_b(StateT<R> S, CoefT<R> c, int vth_hi) {
+template <class R, int HORIZ, int BATCH = 0>
+__global__ void k_commit_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   if (i > S.N || j > S.M) return;
@@ -859,6 +908,20 @@ __global__ void k_commit_b(StateT<R> S, CoefT<R> c, int vth_hi) {
 // ------------------------------------------------------------- launchers
 static inline dim3 grid2(int nx, int ny, int bx) { return dim3(cdiv(nx, bx), ny); }
 
+// Launches a step kernel for one scenario (ks, b.n == 0) or for every
+// member of a batch (kb, grid z = members).
+template <class R, class KS, class KB, class... A>
+static void launch2(KS ks, KB kb, dim3 g, int bs, cudaStream_t st, const StateT<R>& S,
+                    const CoefT<R>& c, const Batch<R>& b, A... a) {
+  if (b.n > 0) {
+    g.z = (unsigned)b.n;
+    kb<<<g, bs, 0, st>>>(S, c, b, a...);
+  } else {
+    ks<<<g, bs, 0, st>>>(S, c, b, a...);
+  }
+}
+#define HYD_K2(name, ...) name<__VA_ARGS__, 0>, name<__VA_ARGS__, 1>
+
 template <class R>
 void launch_init(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
   k_onetime_init<<<dim3(cdiv(S.W, 128), S.H), 128, 0, st>>>(S, c);
@@ -875,89 +938,99 @@ void launch_preprocess(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
 
 template <class R>
 void launch_boundary(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
-  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, 0.0, (double)c.dX, (double)c.dY);
+  launch2(HYD_K2(k_boundary, R), dim3(cdiv(max(S.M, S.N), 128)), 128, st, S, c, Batch<R>{}, 0.0);
 }
 
 template <class R>
-void launch_scan_segments(const StateT<R>& S, const CoefT<R>& c, bool dry, cudaStream_t st) {
-  k_runs_flags<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, S.segcnt, dry ? 1 : 0);
-  k_runs_sort<<<cdiv(S.N + S.M - 2, 128), 128, 0, st>>>(S, S.segcnt);
+void launch_scan_segments(const StateT<R>& S, const CoefT<R>& c, bool dry, cudaStream_t st,
+                          const Batch<R>& b) {
+  launch2(HYD_K2(k_runs_flags, R), grid2(S.M - 1, S.N - 1, 128), 128, st, S, c, b, dry ? 1 : 0);
+  launch2(HYD_K2(k_runs_sort, R), dim3(cdiv(S.N + S.M - 2, 128)), 128, st, S, c, b);
 }
 
 template <class R>
 void launch_find_limits(const StateT<R>& S, const CoefT<R>& c, bool dry, cudaStream_t st,
-                        Trace* tr) {
-  k_interp_fs_rows<<<dim3(cdiv(S.M, 128), 2), 128, 0, st>>>(S, c);
-  k_interp_fs_col<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
-  launch_scan_segments(S, c, dry, st);
+                        Trace* tr, const Batch<R>& b) {
+  launch2(HYD_K2(k_interp_fs_rows, R), dim3(cdiv(S.M, 128), 2), 128, st, S, c, b);
+  launch2(HYD_K2(k_interp_fs_col, R), dim3(cdiv(S.M, 128)), 128, st, S, c, b);
+  launch_scan_segments(S, c, dry, st, b);
   if (tr) tr->launches += 4;
 }
 
 template <class R>
-void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr) {
-  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, 0.5 * c.dT, (double)c.dX, (double)c.dY);
+void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr,
+                   const Batch<R>& b) {
+  const dim3 cells(cdiv(S.M - 1, 128), S.N - 1);
+  const dim3 smooth(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS));
+  const dim3 commit(cdiv(S.M + 1, 128), S.N + 1);
+  launch2(HYD_K2(k_boundary, R), dim3(cdiv(max(S.M, S.N), 128)), 128, st, S, c, b, 0.5 * (double)c.dT);
   if (tr) tr->mark(st, PH_BOUNDARY_X, 1);
   if (tr) tr->kbegin(st, KS_SWEEP_X);
-  const int nx = launch_sweep(S, c, 0, st);
+  launch2(HYD_K2(k_pre, R, 0), cells, 128, st, S, c, b);
+  const int nx = 1 + launch_sweep(S, c, 0, st, b);
   if (tr) tr->kend(st, KS_SWEEP_X);
   if (tr) tr->mark(st, PH_SWEEP_X, nx);
   // smoothing of t_u into su, explicit v from it, margins, smoothing of t_v
   // into sv; k_commit_a writes both back (Normalize/update_buffer pairs,
   // engine.cpp:109-124)
-  k_smooth_full<R, 1, 0><<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c);
-  k_solve_v<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c);
-  k_margin_v<<<cdiv(S.N - 1, 128), 128, 0, st>>>(S, c);
+  launch2(HYD_K2(k_smooth_full, R, 1, 0), smooth, 128, st, S, c, b);
+  launch2(HYD_K2(k_solve_v, R), cells, 128, st, S, c, b);
+  launch2(HYD_K2(k_margin_v, R), dim3(cdiv(S.N - 1, 128)), 128, st, S, c, b);
   if (S.reset_h) {
     // wetting and drying along rows (Reset_states_horizontal after
     // update_h_moi): the smoothing of t_v also does update_h_moi and flags
     // the rows holding a dried cell, the rows' wetting runs on those, the
     // drying per cell in the commit, the mask is written by the segment
     // scan (the mask can change, so the tables are rescanned)
-    k_smooth_full<R, 0, 2><<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c);
+    launch2(HYD_K2(k_smooth_full, R, 0, 2), smooth, 128, st, S, c, b);
     if (tr) tr->mark(st, PH_EXPLICIT_V, 4);
-    k_wetting_rows<<<cdiv(S.N, 128), 128, 0, st>>>(S, c, S.rowflag);
-    k_commit_b<R, 1><<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c, sed ? S.N : 0);
-    k_interp_fs_rows<<<dim3(cdiv(S.M, 128), 2), 128, 0, st>>>(S, c);
-    k_interp_fs_col<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
-    k_runs_flags<<<grid2(S.M - 1, S.N - 1, 128), 128, 0, st>>>(S, c, S.segcnt, 2);
-    k_runs_sort<<<cdiv(S.N + S.M - 2, 128), 128, 0, st>>>(S, S.segcnt);
+    launch2(HYD_K2(k_wetting_rows, R), dim3(cdiv(S.N, 128)), 128, st, S, c, b);
+    launch2(HYD_K2(k_commit_b, R, 1), commit, 128, st, S, c, b, sed ? S.N : 0);
+    launch2(HYD_K2(k_interp_fs_rows, R), dim3(cdiv(S.M, 128), 2), 128, st, S, c, b);
+    launch2(HYD_K2(k_interp_fs_col, R), dim3(cdiv(S.M, 128)), 128, st, S, c, b);
+    launch2(HYD_K2(k_runs_flags, R), grid2(S.M - 1, S.N - 1, 128), 128, st, S, c, b, 2);
+    launch2(HYD_K2(k_runs_sort, R), dim3(cdiv(S.N + S.M - 2, 128)), 128, st, S, c, b);
     if (tr) tr->mark(st, PH_COMMIT_X, 6);
     return;
   }
-  k_smooth_full<R, 0, 0><<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c);
+  launch2(HYD_K2(k_smooth_full, R, 0, 0), smooth, 128, st, S, c, b);
   if (tr) tr->mark(st, PH_EXPLICIT_V, 4);
   // update_h_moi + update_uvz + Htuongdoi; the wet/dry mask does not change
   // in this half-step, so the segment tables are not rescanned, only the
   // boundary concentration is interpolated (support_funcs.cpp:255-258, 311)
   // with sed, also Find_VTH + hesoK of the concentration step (rows to N)
-  k_commit_a<<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c, sed ? S.N : 0);
-  k_interp_fs_rows<<<dim3(cdiv(S.M, 128), 2), 128, 0, st>>>(S, c);
-  k_interp_fs_col<<<cdiv(S.M, 128), 128, 0, st>>>(S, c);
+  launch2(HYD_K2(k_commit_a, R), commit, 128, st, S, c, b, sed ? S.N : 0);
+  launch2(HYD_K2(k_interp_fs_rows, R), dim3(cdiv(S.M, 128), 2), 128, st, S, c, b);
+  launch2(HYD_K2(k_interp_fs_col, R), dim3(cdiv(S.M, 128)), 128, st, S, c, b);
   if (tr) tr->mark(st, PH_COMMIT_X, 3);
 }
 
 template <class R>
-void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr) {
-  k_boundary<<<cdiv(max(S.M, S.N), 128), 128, 0, st>>>(S, c.dT * 0.5, (double)c.dX, (double)c.dY);
+void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr,
+                   const Batch<R>& b) {
+  const dim3 smooth(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS));
+  const dim3 commit(cdiv(S.M + 1, 128), S.N + 1);
+  launch2(HYD_K2(k_boundary, R), dim3(cdiv(max(S.M, S.N), 128)), 128, st, S, c, b, (double)c.dT * 0.5);
   if (tr) tr->mark(st, PH_BOUNDARY_Y, 1);
   if (tr) tr->kbegin(st, KS_SWEEP_Y);
-  const int ny = launch_sweep(S, c, 1, st);
+  launch2(HYD_K2(k_pre, R, 1), dim3(cdiv(S.M - 1, 128), S.N - 1), 128, st, S, c, b);
+  const int ny = 1 + launch_sweep(S, c, 1, st, b);
   if (tr) tr->kend(st, KS_SWEEP_Y);
   if (tr) tr->mark(st, PH_SWEEP_Y, ny);
-  k_smooth_full<R, 0, 0><<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c);
-  k_solve_u<<<grid2(S.M - 1, S.N, 128), 128, 0, st>>>(S, c);
-  k_margin_u<<<cdiv(S.M - 1, 128), 128, 0, st>>>(S, c);
+  launch2(HYD_K2(k_smooth_full, R, 0, 0), smooth, 128, st, S, c, b);
+  launch2(HYD_K2(k_solve_u, R), dim3(cdiv(S.M - 1, 128), S.N), 128, st, S, c, b);
+  launch2(HYD_K2(k_margin_u, R), dim3(cdiv(S.M - 1, 128)), 128, st, S, c, b);
   // with update_h_moi and the wetting pass's column flags
-  k_smooth_full<R, 1, 1><<<dim3(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS)), 128, 0, st>>>(S, c);
+  launch2(HYD_K2(k_smooth_full, R, 1, 1), smooth, 128, st, S, c, b);
   if (tr) tr->mark(st, PH_EXPLICIT_U, 4);
   // update_h_moi, Reset_states_vertical (wetting on flagged columns, drying
   // per cell), update_uvz, Htuongdoi, then the segment tables
-  k_wetting<<<cdiv(S.M, 128), 128, 0, st>>>(S, c, S.colflag);
+  launch2(HYD_K2(k_wetting, R), dim3(cdiv(S.M, 128)), 128, st, S, c, b);
   // with sed, also Find_VTH + hesoK (rows to N-1: the launch shape of
   // engine.cpp:259-260 never reaches row N)
-  k_commit_b<R, 0><<<grid2(S.M + 1, S.N + 1, 128), 128, 0, st>>>(S, c, sed ? S.N - 1 : 0);
+  launch2(HYD_K2(k_commit_b, R, 0), commit, 128, st, S, c, b, sed ? S.N - 1 : 0);
   // the drying mask is written by the segment scan (k_runs_flags, dry)
-  launch_find_limits(S, c, true, st, tr);
+  launch_find_limits(S, c, true, st, tr, b);
   if (tr) tr->mark(st, PH_COMMIT_Y, 2);
 }
 
@@ -966,11 +1039,13 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   template void launch_preprocess<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t);   \
   template void launch_boundary<R>(const StateT<R>&, const CoefT<R>&, cudaStream_t);    \
   template void launch_scan_segments<R>(const StateT<R>&, const CoefT<R>&, bool,         \
-                                        cudaStream_t);                                    \
+                                        cudaStream_t, const Batch<R>&);                   \
   template void launch_find_limits<R>(const StateT<R>&, const CoefT<R>&, bool, cudaStream_t, \
-                                      Trace*);                                            \
-  template void launch_half_x<R>(const StateT<R>&, const CoefT<R>&, bool, cudaStream_t, Trace*); \
-  template void launch_half_y<R>(const StateT<R>&, const CoefT<R>&, bool, cudaStream_t, Trace*);
+                                      Trace*, const Batch<R>&);                           \
+  template void launch_half_x<R>(const StateT<R>&, const CoefT<R>&, bool, cudaStream_t, Trace*, \
+                                 const Batch<R>&);                                        \
+  template void launch_half_y<R>(const StateT<R>&, const CoefT<R>&, bool, cudaStream_t, Trace*, \
+                                 const Batch<R>&);
 HYD_HYDRO_INST(double)
 HYD_HYDRO_INST(float)
 

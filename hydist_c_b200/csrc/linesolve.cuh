@@ -74,10 +74,15 @@ constexpr size_t line_smem(bool refine) {
 // Gen::MIN_BLOCKS: resident CTAs per SM the P = 128 solver is compiled for
 // (2 caps registers at 64 per thread).
 // The launch solves line groups 0 .. ngroups-1 of L lines from line0 on.
-template <class Gen, int P, int L = LPB>
+// BATCH: the groups of every member of a batch, gpm groups per member (the
+// member of group g is g / gpm, its state and coefficients bound into a
+// copy of G0 for that group); the persistent grid walks them all, each CTA
+// with its own scratch slot of G0's scratch.
+template <class Gen, int P, int L = LPB, int BATCH = 0>
 __global__ void __launch_bounds__(L * P, (P == 128 && L == LPB) ? Gen::MIN_BLOCKS : 1)
-    k_line_solve(Gen G, int line0, int ngroups) {
+    k_line_solve(Gen G0, int line0, int ngroups, Batch<typename Gen::Real> bt, int gpm) {
   using R = typename Gen::Real;
+  // sizes and scratch from G0: the same for every member of a batch
   extern __shared__ __align__(16) unsigned char smem_raw[];
   LSShared<R, P, L>& sh = *reinterpret_cast<LSShared<R, P, L>*>(smem_raw);
   // with refinement: the PCR multipliers, 2 per level per thread
@@ -86,23 +91,24 @@ __global__ void __launch_bounds__(L * P, (P == 128 && L == LPB) ? Gen::MIN_BLOCK
   const int tid = threadIdx.x;
   const int l = tid % L, k = tid / L;
   const int cidx = k * L + l;
-  const int U = G.unknowns_per_line();
+  const int U = G0.unknowns_per_line();
   // scratch slot of this CTA: c', y', v' per unknown, and with refinement
   // also the rows A, B, C, D (Gen::SCRATCH_ARRAYS arrays of U x L)
   const size_t UL = (size_t)U * L;
-  R* scr = G.scratch + (size_t)blockIdx.x * Gen::SCRATCH_ARRAYS * UL;
+  R* scr = G0.scratch + (size_t)blockIdx.x * Gen::SCRATCH_ARRAYS * UL;
   R* sc_c = scr;
   R* sc_y = scr + UL;
   R* sc_v = scr + 2 * UL;
-  const int ncells = G.cells_per_line();
+  const int ncells = G0.cells_per_line();
   const int upc = Gen::UPC;
 
-  for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
-    const int line = line0 + grp * L + l;
+  // one group of L lines: gg-th of its scenario, with that scenario's G
+  auto solve_group = [&](const Gen& G, int gg) {
+    const int line = line0 + gg * L + l;
     // ---- segment descriptors of the group's lines
     for (int e = tid; e < L * (SEG + 1); e += blockDim.x) {
       const int ll = e / (SEG + 1), s = e % (SEG + 1);
-      G.load_segment(sh.seg[ll], line0 + grp * L + ll, s);
+      G.load_segment(sh.seg[ll], line0 + gg * L + ll, s);
     }
     __syncthreads();
     const LineSeg& LS = sh.seg[l];
@@ -344,9 +350,19 @@ __global__ void __launch_bounds__(L * P, (P == 128 && L == LPB) ? Gen::MIN_BLOCK
     // ---- per-segment end fix-ups
     for (int e = tid; e < L * SEG; e += blockDim.x) {
       const int ll = e / SEG, s = e % SEG;
-      if (s < sh.seg[ll].nseg) G.fixup(sh.seg[ll], sh.xlast[ll], line0 + grp * L + ll, s);
+      if (s < sh.seg[ll].nseg) G.fixup(sh.seg[ll], sh.xlast[ll], line0 + gg * L + ll, s);
     }
     __syncthreads();
+  };
+  for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    if constexpr (BATCH != 0) {
+      const int m = grp / gpm;
+      Gen Gm = G0;
+      Gm.bind(bt.S[m], bt.c[m]);
+      solve_group(Gm, grp - m * gpm);
+    } else {
+      solve_group(G0, grp);
+    }
   }
 }
 

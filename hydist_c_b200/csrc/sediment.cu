@@ -22,8 +22,10 @@ namespace hyd {
 // the VTH it tests to be zero), Toee starting from the coefficient Toe
 // (:359), both components in the corner copies (:410-419), t_u[pos] > 0 in
 // the downwind test (:479).
-template <class R>
-__global__ void k_calc_qb(StateT<R> S, CoefT<R> c) {
+template <class R, int BATCH = 0>
+__global__ void k_calc_qb(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int i = blockIdx.y + 2;
   if (i > S.N || j > S.M) return;
@@ -81,8 +83,10 @@ __global__ void k_calc_qb(StateT<R> S, CoefT<R> c) {
 
 // _bed_load on rows 3..N-2 (BedLoad with the j-sweep's range,
 // engine.cpp:292), cells of the row's wet segments of at least 3 cells.
-template <class R>
-__global__ void k_bed_load(StateT<R> S, CoefT<R> c) {
+template <class R, int BATCH = 0>
+__global__ void k_bed_load(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   __shared__ int s_first[SEG], s_last[SEG];
   __shared__ int s_n;
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
@@ -159,8 +163,10 @@ __global__ void k_bed_load(StateT<R> S, CoefT<R> c) {
 // j <= M+1 and the z point (i, j) for 1 <= i <= N, 1 <= j <= M, computing
 // the neighbouring nodes it needs from h0 and dH itself (nothing it reads
 // is written by another thread).
-template <class R>
-__global__ void k_bed_feedback(StateT<R> S, CoefT<R> c) {
+template <class R, int BATCH = 0>
+__global__ void k_bed_feedback(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   if (i > S.N + 1 || j > S.M + 1) return;
@@ -187,16 +193,23 @@ __global__ void k_bed_feedback(StateT<R> S, CoefT<R> c) {
 }
 
 template <class R>
-void launch_bed_feedback(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
-  k_bed_feedback<<<dim3(cdiv(S.M + 2, 128), S.N + 2), 128, 0, st>>>(S, c);
+void launch_bed_feedback(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st,
+                         const Batch<R>& b) {
+  const dim3 g(cdiv(S.M + 2, 128), S.N + 2, grid_z(b));
+  if (b.n > 0) k_bed_feedback<R, 1><<<g, 128, 0, st>>>(S, c, b);
+  else k_bed_feedback<R, 0><<<g, 128, 0, st>>>(S, c, b);
 }
-template void launch_bed_feedback<double>(const StateT<double>&, const CoefT<double>&, cudaStream_t);
-template void launch_bed_feedback<float>(const StateT<float>&, const CoefT<float>&, cudaStream_t);
+template void launch_bed_feedback<double>(const StateT<double>&, const CoefT<double>&, cudaStream_t,
+                                          const Batch<double>&);
+template void launch_bed_feedback<float>(const StateT<float>&, const CoefT<float>&, cudaStream_t,
+                                         const Batch<float>&);
 
 constexpr int FS_ROWS = 8;
 
-template <class R>
-__global__ void k_update_fs(StateT<R> S) {
+template <class R, int BATCH = 0>
+__global__ void k_update_fs(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   // FS = tFS on rows 1..N, columns 1..M; FS_ROWS rows per thread, every
   // load before the first store
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -215,30 +228,39 @@ __global__ void k_update_fs(StateT<R> S) {
 }
 
 template <class R>
-void launch_sediment(const StateT<R>& S, const CoefT<R>& c, double s_start, bool xdir, bool bed,
-                     cudaStream_t st, Trace* tr) {
+void launch_sediment(const StateT<R>& S, const CoefT<R>& c, bool xdir, bool bed, cudaStream_t st,
+                     Trace* tr, const Batch<R>& b) {
   // Find_VTH + hesoK ran in the half-step's commit (k_commit_a/k_commit_b)
   if (tr) tr->kbegin(st, xdir ? KS_FS_X : KS_FS_Y);
-  const int nfs = launch_fs_sweep(S, c, xdir ? 0 : 1, s_start, st);
+  const int nfs = launch_fs_sweep(S, c, xdir ? 0 : 1, st, b);
   if (tr) tr->kend(st, xdir ? KS_FS_X : KS_FS_Y);
-  k_update_fs<<<dim3(cdiv(S.M, 128), cdiv(S.N, FS_ROWS)), 128, 0, st>>>(S);
+  const unsigned z = grid_z(b);
+  const dim3 gfs(cdiv(S.M, 128), cdiv(S.N, FS_ROWS), z);
+  if (b.n > 0) k_update_fs<R, 1><<<gfs, 128, 0, st>>>(S, c, b);
+  else k_update_fs<R, 0><<<gfs, 128, 0, st>>>(S, c, b);
   int launched = nfs + 1;
   if (bed && S.N >= 5) {
     // the bed change once per step, after the j-sweep (engine.cpp:290-293)
-    k_calc_qb<<<dim3(cdiv(S.M - 1, 128), S.N - 1), 128, 0, st>>>(S, c);
-    k_bed_load<<<dim3(cdiv(S.M - 1, 128), S.N - 4), 128, 0, st>>>(S, c);
+    const dim3 gq(cdiv(S.M - 1, 128), S.N - 1, z), gl(cdiv(S.M - 1, 128), S.N - 4, z);
+    if (b.n > 0) {
+      k_calc_qb<R, 1><<<gq, 128, 0, st>>>(S, c, b);
+      k_bed_load<R, 1><<<gl, 128, 0, st>>>(S, c, b);
+    } else {
+      k_calc_qb<R, 0><<<gq, 128, 0, st>>>(S, c, b);
+      k_bed_load<R, 0><<<gl, 128, 0, st>>>(S, c, b);
+    }
     launched += 2;
     if (S.bed_fb) {
-      launch_bed_feedback(S, c, st);
+      launch_bed_feedback(S, c, st, b);
       ++launched;
     }
   }
   if (tr) tr->mark(st, xdir ? PH_SEDIMENT_X : PH_SEDIMENT_Y, launched);
 }
 
-template void launch_sediment<double>(const StateT<double>&, const CoefT<double>&, double, bool,
-                                      bool, cudaStream_t, Trace*);
-template void launch_sediment<float>(const StateT<float>&, const CoefT<float>&, double, bool, bool,
-                                     cudaStream_t, Trace*);
+template void launch_sediment<double>(const StateT<double>&, const CoefT<double>&, bool, bool,
+                                      cudaStream_t, Trace*, const Batch<double>&);
+template void launch_sediment<float>(const StateT<float>&, const CoefT<float>&, bool, bool,
+                                     cudaStream_t, Trace*, const Batch<float>&);
 
 }  // namespace hyd

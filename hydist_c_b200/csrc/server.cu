@@ -7,9 +7,15 @@
 //   1. queued requests are admitted in arrival order while their device
 //      footprint (hydist_scenario_bytes) fits in the budget left by the
 //      active ones; a request is created on the device when admitted;
-//   2. every active request is advanced by up to steps_per_round steps, each
-//      on its own stream through its replayed step graph, so the requests'
-//      kernels overlap on the device;
+//   2. every active request is advanced by up to steps_per_round steps.
+//      Active requests of one mesh size and form that advance the same
+//      number of steps are stepped as one ensemble (hydist_ensemble_*): each
+//      kernel of a step is one launch over all of them while they are in the
+//      same sediment phase (their sweeps batched together). The ensemble of
+//      a group is kept while the group's membership stays the same (its step
+//      graphs are reused) and released when it changes. A request alone in
+//      its group steps through its own replayed step graph. Groups and lone
+//      requests run on their own streams, so their kernels overlap;
 //   3. the round waits for the device, and requests that reached their
 //      horizon are retired: their state stays on the device (and counts
 //      against the budget) until released, so results can be downloaded.
@@ -102,7 +108,22 @@ struct HydistServer {
   int64_t next_id = 1;
   std::deque<Request*> queue;        // arrival order
   std::map<int64_t, Request*> reqs;  // every request not yet released
+  // the ensembles of the current groups, by their members' ids
+  std::map<std::vector<int64_t>, HydistEnsemble*> groups;
 };
+
+namespace {
+
+// requests that can share launches: mesh size, form and the options that
+// shape the launches (the ensemble checks the rest), and the round's steps
+struct GroupKey {
+  int32_t M, N, precision, kenhhepd, kenhhepng, reset_horizontal, bed_feedback, steps;
+  bool operator<(const GroupKey& o) const {
+    return std::memcmp(this, &o, sizeof(GroupKey)) < 0;
+  }
+};
+
+}  // namespace
 
 extern "C" {
 
@@ -139,6 +160,7 @@ int hydist_server_create(int device, uint64_t budget_bytes, int32_t steps_per_ro
 
 int hydist_server_destroy(HydistServer* s) {
   if (!s) return HYDIST_OK;
+  for (auto& g : s->groups) hydist_ensemble_destroy(g.second);
   for (auto& kv : s->reqs) {
     if (kv.second->h) hydist_destroy(kv.second->h);
     delete kv.second;
@@ -181,17 +203,62 @@ int hydist_server_round(HydistServer* s, int64_t* done, int32_t cap, int32_t* nd
     r->state = RQ_ACTIVE;
     s->held += r->bytes;
   }
-  // 2. every active request advances on its own stream
+  // 2. the active requests advance: grouped by mesh size, form and steps
+  std::map<GroupKey, std::vector<Request*>> byKey;
   for (auto& kv : s->reqs) {
     Request* r = kv.second;
     if (r->state != RQ_ACTIVE) continue;
     const int k = std::min(s->steps_per_round, r->nsteps - r->done_steps);
-    if (k > 0) {
-      const int rc = hydist_step_graph(r->h, k);
-      if (rc != HYDIST_OK) return rc;
-      r->done_steps += k;
-    }
+    if (k <= 0) continue;
+    GroupKey g;
+    std::memset(&g, 0, sizeof(g));
+    g.M = r->input.sc.M;
+    g.N = r->input.sc.N;
+    g.precision = r->o.precision;
+    g.kenhhepd = r->o.kenhhepd;
+    g.kenhhepng = r->o.kenhhepng;
+    g.reset_horizontal = r->o.reset_horizontal;
+    g.bed_feedback = r->o.bed_change && r->o.bed_feedback;
+    g.steps = k;
+    byKey[g].push_back(r);
   }
+  std::map<std::vector<int64_t>, HydistEnsemble*> keep;
+  for (auto& kv : byKey) {
+    std::vector<Request*>& rs = kv.second;
+    const int k = kv.first.steps;
+    int rc = HYDIST_OK;
+    if (rs.size() == 1) {
+      rc = hydist_step_graph(rs[0]->h, k);
+    } else {
+      std::vector<int64_t> ids;
+      std::vector<HydistHandle*> hs;
+      for (Request* r : rs) {
+        ids.push_back(r->id);
+        hs.push_back(r->h);
+      }
+      HydistEnsemble* e = nullptr;
+      auto it = s->groups.find(ids);
+      if (it != s->groups.end()) {
+        e = it->second;
+        s->groups.erase(it);
+      } else {
+        rc = hydist_ensemble_create(hs.data(), (int32_t)hs.size(), &e);
+      }
+      if (rc == HYDIST_OK) {
+        keep[ids] = e;
+        rc = hydist_ensemble_step(e, k);
+      }
+    }
+    if (rc != HYDIST_OK) {
+      for (auto& g : keep) s->groups[g.first] = g.second;
+      return rc;
+    }
+    for (Request* r : rs) r->done_steps += k;
+  }
+  // the ensembles of groups that no longer exist (their work is ordered
+  // before any later work of their members)
+  for (auto& g : s->groups) hydist_ensemble_destroy(g.second);
+  s->groups.swap(keep);
   // 3. wait, then retire the requests that reached their horizon
   for (auto& kv : s->reqs) {
     Request* r = kv.second;
@@ -241,6 +308,17 @@ int hydist_server_release(HydistServer* s, int64_t id) {
   if (it == s->reqs.end()) return sfail(HYDIST_ERR_ARG, "unknown request");
   Request* r = it->second;
   if (r->state == RQ_ACTIVE) return sfail(HYDIST_ERR_STATE, "the request is still running");
+  // an ensemble holding the request goes first
+  for (auto g = s->groups.begin(); g != s->groups.end();) {
+    bool has = false;
+    for (int64_t x : g->first) has |= x == id;
+    if (has) {
+      hydist_ensemble_destroy(g->second);
+      g = s->groups.erase(g);
+    } else {
+      ++g;
+    }
+  }
   if (r->state == RQ_QUEUED) {
     for (auto q = s->queue.begin(); q != s->queue.end(); ++q)
       if (*q == r) {

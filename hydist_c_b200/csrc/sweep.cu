@@ -45,14 +45,21 @@ struct HydroGen {
   // narrow-channel ranges (StateT::x_lo, x_hi, y_lo)
   int lp0, nl;
 
+  __host__ __device__ void bind(const StateT<R>& s, const CoefT<R>& cc) {
+    S = s;
+    c = cc;
+    f4 = DIR == 0 ? 2 * cc.g * cc.dTchia2dX : 2 * cc.g * cc.dTchia2dY;
+  }
   __device__ int lines() const { return nl; }
   __device__ int cells_per_line() const { return DIR == 0 ? S.N - 1 : S.M - 1; }
   __device__ int unknowns_per_line() const { return 2 * cells_per_line(); }
   __device__ int end_pos() const { return DIR == 0 ? S.N : S.M; }
   // field index of position p on line position lp
   __device__ int at(int lp, int p) const { return DIR == 0 ? p * S.W + lp : lp * S.W + p; }
+  // the preindex values of a cell, computed for every cell by k_pre before
+  // the sweep (a coalesced per-cell pass over the stencils)
   __device__ PreT<R> pre(int lp, int p) const {
-    return DIR == 0 ? pre_x(S, c, p, lp) : pre_y(S, c, lp, p);
+    return load_pre(S, (size_t)S.W * S.H, at(lp, p));
   }
   __device__ R* vel() const { return DIR == 0 ? S.tu : S.tv; }
   // the VZ extraction reaches columns j <= N only (UVZSolver_multithread.cpp:851)
@@ -273,21 +280,33 @@ static size_t prepare(int dev) {
 }
 
 template <class Gen, int P, int L = LPB>
-static void launch_gen(const Gen& G, cudaStream_t st, int grid, int line0, int ngroups) {
+static void launch_gen(const Gen& G, cudaStream_t st, int grid, int line0, int ngroups,
+                       const Batch<typename Gen::Real>& b = {}, int gpm = 0) {
   int dev = 0;
   cudaGetDevice(&dev);
   const size_t smem = prepare<Gen, P, L>(dev);
-  k_line_solve<Gen, P, L><<<grid, L * P, smem, st>>>(G, line0, ngroups);
+  if (b.n > 0) {
+    static bool attr[64] = {};
+    if (dev < 64 && !attr[dev]) {
+      cudaFuncSetAttribute(k_line_solve<Gen, P, L, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      attr[dev] = true;
+    }
+    k_line_solve<Gen, P, L, 1><<<grid, L * P, smem, st>>>(G, line0, ngroups, b, gpm);
+  } else {
+    k_line_solve<Gen, P, L><<<grid, L * P, smem, st>>>(G, line0, ngroups, b, 0);
+  }
 }
 
 template <class Gen>
-static void launch_any(const Gen& G, int P, cudaStream_t st, int grid, int line0, int ngroups) {
-  if (P == 128) launch_gen<Gen, 128>(G, st, grid, line0, ngroups);
-  else if (P == 64) launch_gen<Gen, 64>(G, st, grid, line0, ngroups);
-  else if (P == 32) launch_gen<Gen, 32>(G, st, grid, line0, ngroups);
-  else if (P == 16) launch_gen<Gen, 16>(G, st, grid, line0, ngroups);
-  else if (P == 4) launch_gen<Gen, 4>(G, st, grid, line0, ngroups);
-  else launch_gen<Gen, 1>(G, st, grid, line0, ngroups);
+static void launch_any(const Gen& G, int P, cudaStream_t st, int grid, int line0, int ngroups,
+                       const Batch<typename Gen::Real>& b = {}, int gpm = 0) {
+  if (P == 128) launch_gen<Gen, 128>(G, st, grid, line0, ngroups, b, gpm);
+  else if (P == 64) launch_gen<Gen, 64>(G, st, grid, line0, ngroups, b, gpm);
+  else if (P == 32) launch_gen<Gen, 32>(G, st, grid, line0, ngroups, b, gpm);
+  else if (P == 16) launch_gen<Gen, 16>(G, st, grid, line0, ngroups, b, gpm);
+  else if (P == 4) launch_gen<Gen, 4>(G, st, grid, line0, ngroups, b, gpm);
+  else launch_gen<Gen, 1>(G, st, grid, line0, ngroups, b, gpm);
 }
 
 // CTAs of the 128-chunk solver resident on the device at once (queried once
@@ -314,9 +333,18 @@ static int resident_slots() {
 // half of the resident CTAs idle (2047 rows on 148 one-CTA SMs: 68 of 512
 // groups), that remainder runs as a second launch of 2-line groups with 256
 // chunks per line, half the chain per thread, on every SM.
+//
+// With a batch, one launch walks the line groups of every member (the
+// persistent grid takes them in member order).
 template <class Gen>
-static int launch_lines(const Gen& G, int P, int lines, int lslots, cudaStream_t st) {
+static int launch_lines(const Gen& G, int P, int lines, int lslots, cudaStream_t st,
+                        const Batch<typename Gen::Real>& b = {}) {
   const int groups = cdiv(lines, LPB);
+  if (b.n > 0) {
+    const long long total = (long long)groups * b.n;
+    launch_any(G, P, st, (int)std::min<long long>(total, lslots), 0, (int)total, b, groups);
+    return 1;
+  }
   if constexpr (Gen::DIRECTION == 1) {
     if (P == 128) {
       const int slots = std::min(resident_slots<Gen>(), lslots);
@@ -336,16 +364,15 @@ static int launch_lines(const Gen& G, int P, int lines, int lslots, cudaStream_t
 }
 
 template <int DIR, class R, bool REF>
-static int launch_dir(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, int P) {
+static int launch_dir(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, int P,
+                      const Batch<R>& b) {
   HydroGen<DIR, R, REF> G;
-  G.S = S;
-  G.c = c;
+  G.bind(S, c);
   G.scratch = S.lscratch;
-  G.f4 = DIR == 0 ? 2 * c.g * c.dTchia2dX : 2 * c.g * c.dTchia2dY;
   G.lp0 = DIR == 0 ? S.x_lo : S.y_lo;
   G.nl = DIR == 0 ? S.x_hi - S.x_lo + 1 : S.N - S.y_lo + 1;
   if (G.nl <= 0) return 0;
-  return launch_lines(G, P, G.nl, S.lslots, st);
+  return launch_lines(G, P, G.nl, S.lslots, st, b);
 }
 
 // ---------------------------------------------------------------------
@@ -365,8 +392,11 @@ struct FSGen {
   StateT<R> S;
   CoefT<R> c;
   R* scratch;
-  double s_start;
 
+  __host__ __device__ void bind(const StateT<R>& s, const CoefT<R>& cc) {
+    S = s;
+    c = cc;
+  }
   __device__ int lines() const { return DIR == 0 ? S.M - 3 : S.N - 3; }
   __device__ int cells_per_line() const { return DIR == 0 ? S.N - 1 : S.M - 1; }
   __device__ int unknowns_per_line() const { return cells_per_line(); }
@@ -447,7 +477,7 @@ struct FSGen {
       }
       const SegD& d = LS.s[si];
       const int i = DIR == 0 ? pos : lp, j = DIR == 0 ? lp : pos;
-      fs_cell(G.S, G.c, DIR == 0, i, j, vel_c, hk_c, vel_p, hk_p, tt, G.s_start, A, B, C, D);
+      fs_cell(G.S, G.c, DIR == 0, i, j, vel_c, hk_c, vel_p, hk_p, tt, G.S.src_start, A, B, C, D);
       const R* vel = G.vel();
       if (pos == d.first + 1) {
         // the velocity at the segment's first cell is the previous cell's
@@ -505,37 +535,40 @@ struct FSGen {
 };
 
 template <class R>
-int launch_fs_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, double s_start,
-                    cudaStream_t st) {
+int launch_fs_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t st,
+                    const Batch<R>& b) {
   const int ncells = dir == 0 ? S.N - 1 : S.M - 1;
   const int lines = dir == 0 ? S.M - 3 : S.N - 3;
   if (lines <= 0) return 0;
   const int P = line_chunks(ncells, 4);
   if (dir == 0) {
-    if (S.refine) return launch_lines(FSGen<0, R, true>{S, c, S.lscratch, s_start}, P, lines, S.lslots, st);
-    return launch_lines(FSGen<0, R, false>{S, c, S.lscratch, s_start}, P, lines, S.lslots, st);
+    if (S.refine) return launch_lines(FSGen<0, R, true>{S, c, S.lscratch}, P, lines, S.lslots, st, b);
+    return launch_lines(FSGen<0, R, false>{S, c, S.lscratch}, P, lines, S.lslots, st, b);
   }
-  if (S.refine) return launch_lines(FSGen<1, R, true>{S, c, S.lscratch, s_start}, P, lines, S.lslots, st);
-  return launch_lines(FSGen<1, R, false>{S, c, S.lscratch, s_start}, P, lines, S.lslots, st);
+  if (S.refine) return launch_lines(FSGen<1, R, true>{S, c, S.lscratch}, P, lines, S.lslots, st, b);
+  return launch_lines(FSGen<1, R, false>{S, c, S.lscratch}, P, lines, S.lslots, st, b);
 }
 
 template <class R>
-int launch_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t st) {
+int launch_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t st,
+                 const Batch<R>& b) {
   const int ncells = dir == 0 ? S.N - 1 : S.M - 1;
   const int P = line_chunks(ncells, 4);
   if (S.refine) {
-    if (dir == 0) return launch_dir<0, R, true>(S, c, st, P);
-    return launch_dir<1, R, true>(S, c, st, P);
+    if (dir == 0) return launch_dir<0, R, true>(S, c, st, P, b);
+    return launch_dir<1, R, true>(S, c, st, P, b);
   }
-  if (dir == 0) return launch_dir<0, R, false>(S, c, st, P);
-  return launch_dir<1, R, false>(S, c, st, P);
+  if (dir == 0) return launch_dir<0, R, false>(S, c, st, P, b);
+  return launch_dir<1, R, false>(S, c, st, P, b);
 }
 
-template int launch_sweep<double>(const StateT<double>&, const CoefT<double>&, int, cudaStream_t);
-template int launch_sweep<float>(const StateT<float>&, const CoefT<float>&, int, cudaStream_t);
-template int launch_fs_sweep<double>(const StateT<double>&, const CoefT<double>&, int, double,
-                                     cudaStream_t);
-template int launch_fs_sweep<float>(const StateT<float>&, const CoefT<float>&, int, double,
-                                    cudaStream_t);
+template int launch_sweep<double>(const StateT<double>&, const CoefT<double>&, int, cudaStream_t,
+                                  const Batch<double>&);
+template int launch_sweep<float>(const StateT<float>&, const CoefT<float>&, int, cudaStream_t,
+                                 const Batch<float>&);
+template int launch_fs_sweep<double>(const StateT<double>&, const CoefT<double>&, int, cudaStream_t,
+                                     const Batch<double>&);
+template int launch_fs_sweep<float>(const StateT<float>&, const CoefT<float>&, int, cudaStream_t,
+                                    const Batch<float>&);
 
 }  // namespace hyd

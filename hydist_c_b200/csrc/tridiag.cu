@@ -102,6 +102,142 @@ __global__ void k_thomas_list(const T* __restrict__ dl, const T* __restrict__ d,
   }
 }
 
+// ---------------------------------------------------- diagonal pivoting
+// Gaussian elimination with diagonal pivoting for systems that are not
+// diagonally dominant: at each step the current diagonal (1x1 pivot) or the
+// 2x2 block of the current and the next row is eliminated, by the
+// Bunch-Kaufman criterion with kappa = (sqrt(5)-1)/2 (Bunch and Kaufman,
+// Math. Comp. 31, 1977; the tridiagonal form of Erway and Marcia and of Chang
+// et al., SC'12, which the reference's SPIKE tile solver,
+// spike_kernel.hxx:119-376, also follows): the 1x1 pivot d' is taken when
+// |d'| sigma >= kappa |c_k a_{k+1}|, sigma the largest magnitude of the
+// entries coupling the next two rows. P holds the modified pivot of a row
+// (for a 2x2 block: its first row's modified diagonal, its second row's
+// determinant), F marks the second rows of 2x2 blocks, X the modified
+// right-hand side and then the solution.
+template <class T>
+__device__ __forceinline__ void pivot_system(const T* A, const T* B, const T* C, const T* D, T* X,
+                                             T* P, unsigned char* F, int n) {
+  const T kappa = T(0.6180339887498949);
+  T dk = B[0], rk = D[0];
+  int k = 0;
+  while (k < n) {
+    F[k] = 0;
+    if (k == n - 1) {
+      P[k] = dk;
+      X[k] = rk;
+      break;
+    }
+    T sigma = fmax(fmax(fabs(C[k]), fabs(A[k + 1])), fabs(B[k + 1]));
+    if (k + 2 < n) sigma = fmax(sigma, fmax(fabs(C[k + 1]), fabs(A[k + 2])));
+    if (fabs(dk) * sigma >= kappa * fabs(C[k] * A[k + 1])) {
+      P[k] = dk;
+      X[k] = rk;
+      const T l = A[k + 1] / dk;
+      dk = B[k + 1] - l * C[k];
+      rk = D[k + 1] - l * rk;
+      k += 1;
+    } else {
+      const T det = dk * B[k + 1] - C[k] * A[k + 1];
+      P[k] = dk;
+      P[k + 1] = det;
+      F[k + 1] = 1;
+      X[k] = rk;
+      X[k + 1] = D[k + 1];
+      if (k + 2 < n) {
+        // row k+2 minus A[k+2] times the block inverse's second row applied
+        // to the block's right-hand sides ((B^-1)_22 = dk / det)
+        const T l = A[k + 2] / det;
+        rk = D[k + 2] - l * (dk * D[k + 1] - A[k + 1] * rk);
+        dk = B[k + 2] - l * dk * C[k + 1];
+      }
+      k += 2;
+    }
+  }
+  T xn = 0;  // x_{i+1}
+  int i = n - 1;
+  while (i >= 0) {
+    if (F[i]) {
+      // rows i-1, i: [[p, C[i-1]], [A[i], B[i]]] [x_{i-1}; x_i] = [r0; r1]
+      const T p = P[i - 1], det = P[i];
+      const T r0 = X[i - 1];
+      const T r1 = X[i] - (i + 1 < n ? C[i] * xn : T(0));
+      const T xi = (p * r1 - A[i] * r0) / det;
+      const T xi1 = (B[i] * r0 - C[i - 1] * r1) / det;
+      X[i] = xi;
+      X[i - 1] = xi1;
+      xn = xi1;
+      i -= 2;
+    } else {
+      const T xi = (X[i] - (i + 1 < n ? C[i] * xn : T(0))) / P[i];
+      X[i] = xi;
+      xn = xi;
+      i -= 1;
+    }
+  }
+}
+
+// the systems of one band's list, one thread each, with diagonal pivoting
+// (P in the value scratch, F in the byte scratch, both at the system's rows)
+template <class T>
+__global__ void k_pivot_list(const T* __restrict__ dl, const T* __restrict__ d,
+                             const T* __restrict__ du, const T* __restrict__ b, T* __restrict__ x,
+                             T* __restrict__ w, unsigned char* __restrict__ flags,
+                             const int* __restrict__ off, const int* __restrict__ len,
+                             const int* __restrict__ list, const int* __restrict__ count) {
+  const int cnt = *count;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    const int s = list[i];
+    const int o = off[s];
+    pivot_system(dl + o, d + o, du + o, b + o, x + o, w + o, flags + o, len[s]);
+  }
+}
+
+// ------------------------------------------------ refinement (FP64 systems)
+// x32 -> x64 and the FP64 residual r = b - A x of the FP32 solution, rounded
+// to FP32 as the right-hand side of the correction solve.
+__global__ void k_gt_residual(const double* __restrict__ dl, const double* __restrict__ d,
+                              const double* __restrict__ du, const double* __restrict__ b,
+                              const float* __restrict__ x32, double* __restrict__ x,
+                              float* __restrict__ r32, const int* __restrict__ off,
+                              const int* __restrict__ len, int nsys) {
+  const int s = blockIdx.x;
+  if (s >= nsys) return;
+  const int o = off[s], n = len[s];
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    const int g = o + q;
+    const double xq = x32[g];
+    double r = b[g] - d[g] * xq;
+    if (q > 0) r -= dl[g] * (double)x32[g - 1];
+    if (q + 1 < n) r -= du[g] * (double)x32[g + 1];
+    x[g] = xq;
+    r32[g] = (float)r;
+  }
+}
+
+// x += the FP32 correction, in FP64
+__global__ void k_gt_correct(double* __restrict__ x, const float* __restrict__ c32,
+                             const int* __restrict__ off, const int* __restrict__ len, int nsys) {
+  const int s = blockIdx.x;
+  if (s >= nsys) return;
+  const int o = off[s], n = len[s];
+  for (int q = threadIdx.x; q < n; q += blockDim.x) x[o + q] += (double)c32[o + q];
+}
+
+// FP64 -> FP32 copies of a system's four arrays
+// (array k at f + k * ld)
+__global__ void k_gt_to_f32(const double* __restrict__ dl, const double* __restrict__ d,
+                            const double* __restrict__ du, const double* __restrict__ b,
+                            float* __restrict__ f, size_t rows, size_t ld) {
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < rows;
+       r += (size_t)gridDim.x * blockDim.x) {
+    f[r] = (float)dl[r];
+    f[ld + r] = (float)d[r];
+    f[2 * ld + r] = (float)du[r];
+    f[3 * ld + r] = (float)b[r];
+  }
+}
+
 // ------------------------------------------------- staged partition solvers
 // Stages a system's rows into shared memory with asynchronous copies
 // (cp.async): every thread's copies are in flight at once instead of one
@@ -453,8 +589,12 @@ namespace {
 using hyd::GT_NB;
 
 struct DevScratch {
-  void* w = nullptr;  // Thomas forward-sweep scratch (rows x 8 B)
+  void* w = nullptr;  // Thomas forward-sweep / pivoting scratch (rows x 8 B)
   size_t w_bytes = 0;
+  unsigned char* flags = nullptr;  // pivoting: 2x2 block marks (rows x 1 B)
+  size_t flags_bytes = 0;
+  float* f32 = nullptr;  // refinement: FP32 copies of the systems and x (rows x 5 x 4 B)
+  size_t f32_bytes = 0;
   int* lists = nullptr;  // GT_NB x nsys
   size_t lists_cap = 0;  // systems
   int* counts = nullptr;  // GT_NB
@@ -517,7 +657,7 @@ Caps caps_of(const DevInfo& D) {
 
 bool feasible(int algo, int band, const Caps& c) {
   const int hi = hyd::gt_band_hi(band);
-  if (algo == HYDIST_GTSV_THOMAS) return true;
+  if (algo == HYDIST_GTSV_THOMAS || algo == HYDIST_GTSV_PIVOT) return true;
   if (algo == HYDIST_GTSV_WARP) return hi <= hyd::GT_WARP_MAX;
   if (algo == HYDIST_GTSV_PARTITION) return hi <= c.cta256;
   if (algo == HYDIST_GTSV_PARTITION_512) return hi <= c.cta512;
@@ -592,12 +732,16 @@ int launch_cta(int nmax, const T* dl, const T* d, const T* du, const T* b, T* x,
 
 template <class T>
 int launch_band(int algo, int band, const T* dl, const T* d, const T* du, const T* b, T* x, T* w,
-                const int* off, const int* len, const int* list, const int* count, int* stalled,
-                int nsys_band, const DevInfo& D, cudaStream_t st) {
+                unsigned char* flags, const int* off, const int* len, const int* list,
+                const int* count, int* stalled, int nsys_band, const DevInfo& D, cudaStream_t st) {
   if (nsys_band <= 0) return HYDIST_OK;
   const int hi = hyd::gt_band_hi(band);
   int rc = HYDIST_OK;
-  if (algo == HYDIST_GTSV_PARTITION_128) {
+  if (algo == HYDIST_GTSV_PIVOT) {
+    const int bs = 128;
+    const int grid = std::min((nsys_band + bs - 1) / bs, 8 * D.nsm);
+    hyd::k_pivot_list<T><<<grid, bs, 0, st>>>(dl, d, du, b, x, w, flags, off, len, list, count);
+  } else if (algo == HYDIST_GTSV_PARTITION_128) {
     rc = launch_cta<T, 128>(hi, dl, d, du, b, x, off, len, list, count, stalled, nsys_band, D, st);
   } else if (algo == HYDIST_GTSV_PARTITION) {
     rc = launch_cta<T, 256>(hi, dl, d, du, b, x, off, len, list, count, stalled, nsys_band, D, st);
@@ -621,13 +765,20 @@ int launch_band(int algo, int band, const T* dl, const T* d, const T* du, const 
   return cudaGetLastError() == cudaSuccess ? HYDIST_OK : HYDIST_ERR_CUDA;
 }
 
-int ensure_scratch(DevScratch& s, size_t w_bytes, size_t nsys) {
+int ensure_scratch(DevScratch& s, size_t w_bytes, size_t nsys, size_t flag_bytes = 0) {
   if (w_bytes > 0 && s.w_bytes < w_bytes) {
     if (s.w) cudaFree(s.w);
     s.w = nullptr;
     s.w_bytes = 0;
     if (cudaMalloc(&s.w, w_bytes + 256) != cudaSuccess) return HYDIST_ERR_OOM;
     s.w_bytes = w_bytes;
+  }
+  if (flag_bytes > 0 && s.flags_bytes < flag_bytes) {
+    if (s.flags) cudaFree(s.flags);
+    s.flags = nullptr;
+    s.flags_bytes = 0;
+    if (cudaMalloc(&s.flags, flag_bytes + 256) != cudaSuccess) return HYDIST_ERR_OOM;
+    s.flags_bytes = flag_bytes;
   }
   if (s.lists_cap < nsys) {
     if (s.lists) cudaFree(s.lists);
@@ -672,15 +823,19 @@ int solve_batch(const T* dl, const T* d, const T* du, const T* b, T* x, const in
                    ? HYDIST_GTSV_THOMAS
                    : table[bnd];
   table = tab;
-  bool thomas = false;
-  for (int bnd = 0; bnd < GT_NB; ++bnd) thomas |= counts[bnd] > 0 && table[bnd] == HYDIST_GTSV_THOMAS;
-  if (thomas) {
-    rc = ensure_scratch(D.scr, (size_t)counts[GT_NB] * sizeof(T), (size_t)nsys);
+  bool thomas = false, pivot = false;
+  for (int bnd = 0; bnd < GT_NB; ++bnd) {
+    thomas |= counts[bnd] > 0 && table[bnd] == HYDIST_GTSV_THOMAS;
+    pivot |= counts[bnd] > 0 && table[bnd] == HYDIST_GTSV_PIVOT;
+  }
+  if (thomas || pivot) {
+    rc = ensure_scratch(D.scr, (size_t)counts[GT_NB] * sizeof(T), (size_t)nsys,
+                        pivot ? (size_t)counts[GT_NB] : 0);
     if (rc != HYDIST_OK) return rc;
   }
   bool staged = false;  // a bulk-staged CTA solver ran
   for (int bnd = 0; bnd < GT_NB; ++bnd) {
-    rc = launch_band<T>(table[bnd], bnd, dl, d, du, b, x, (T*)D.scr.w, off, len,
+    rc = launch_band<T>(table[bnd], bnd, dl, d, du, b, x, (T*)D.scr.w, D.scr.flags, off, len,
                         D.scr.lists + (size_t)bnd * nsys, D.scr.counts + bnd,
                         D.scr.counts + GT_NB + 2, counts[bnd], D, st);
     if (rc != HYDIST_OK) return rc;
@@ -820,7 +975,7 @@ extern "C" int hydist_gtsv_batched(const void* dl, const void* d, const void* du
     hyd::set_last_error("hydist_gtsv_batched: dtype must be 0 (FP64) or 1 (FP32)");
     return HYDIST_ERR_ARG;
   }
-  if (algo < HYDIST_GTSV_AUTO || algo > HYDIST_GTSV_PARTITION_128) {
+  if (algo < HYDIST_GTSV_AUTO || algo > HYDIST_GTSV_PIVOT) {
     hyd::set_last_error("hydist_gtsv_batched: unknown algo");
     return HYDIST_ERR_ARG;
   }
@@ -858,6 +1013,81 @@ extern "C" int hydist_gtsv_batched(const void* dl, const void* d, const void* du
                         "in shared memory; some systems of this batch are unsolved");
   else if (rc != HYDIST_OK) hyd::set_last_error("hydist_gtsv_batched: a CUDA call failed");
   return rc;
+}
+
+// ---- FP32 solve refined once with an FP64 residual -------------------------
+extern "C" int hydist_gtsv_batched_refine(const double* dl, const double* d, const double* du,
+                                          const double* b, double* x, const int32_t* offsets,
+                                          const int32_t* lengths, int32_t nsys, int32_t algo,
+                                          void* stream) {
+  if (!dl || !d || !du || !b || !x || !offsets || !lengths || nsys < 0) {
+    hyd::set_last_error("hydist_gtsv_batched_refine: null pointer or negative count");
+    return HYDIST_ERR_ARG;
+  }
+  if (algo < HYDIST_GTSV_AUTO || algo > HYDIST_GTSV_PIVOT) {
+    hyd::set_last_error("hydist_gtsv_batched_refine: unknown algo");
+    return HYDIST_ERR_ARG;
+  }
+  if (nsys == 0) return HYDIST_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return HYDIST_ERR_CUDA;
+  // the packed extent, for the FP32 copies (a device reduction of off+len)
+  size_t rows = 0;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevInfo* D = dev_info(dev);
+    if (!D) return HYDIST_ERR_ARG;
+    int rc = ensure_scratch(D->scr, 0, (size_t)nsys);
+    if (rc != HYDIST_OK) return rc;
+    if (cudaMemsetAsync(D->scr.counts, 0, (GT_NB + 2) * sizeof(int), st) != cudaSuccess)
+      return HYDIST_ERR_CUDA;
+    hyd::k_gt_classify<<<(nsys + 255) / 256, 256, 0, st>>>(offsets, lengths, nsys, D->scr.lists,
+                                                           D->scr.counts);
+    int counts[GT_NB + 2];
+    if (cudaMemcpyAsync(counts, D->scr.counts, sizeof(counts), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      return HYDIST_ERR_CUDA;
+    if (counts[GT_NB + 1]) {
+      hyd::set_last_error("hydist_gtsv_batched_refine: a system has a negative offset");
+      return HYDIST_ERR_ARG;
+    }
+    rows = (size_t)counts[GT_NB];
+    // each FP32 array starts 16-byte aligned (the CTA solvers stage rows
+    // with bulk copies)
+    const size_t need = (rows + 3) / 4 * 4 * 5 * sizeof(float);
+    if (D->scr.f32_bytes < need) {
+      if (D->scr.f32) cudaFree(D->scr.f32);
+      D->scr.f32 = nullptr;
+      D->scr.f32_bytes = 0;
+      if (cudaMalloc(&D->scr.f32, need + 256) != cudaSuccess) return HYDIST_ERR_OOM;
+      D->scr.f32_bytes = need;
+    }
+  }
+  if (rows == 0) return HYDIST_OK;
+  float* f = nullptr;
+  int nsm = 1;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    f = dev_info(dev)->scr.f32;
+    nsm = dev_info(dev)->nsm;
+  }
+  const size_t ld = (rows + 3) / 4 * 4;
+  float *fl = f, *fd = f + ld, *fu = f + 2 * ld, *fb = f + 3 * ld, *fx = f + 4 * ld;
+  hyd::k_gt_to_f32<<<4 * nsm, 256, 0, st>>>(dl, d, du, b, f, rows, ld);
+  int rc = hydist_gtsv_batched(fl, fd, fu, fb, fx, offsets, lengths, nsys, 1, algo, stream);
+  if (rc != HYDIST_OK) return rc;
+  // x = x32, r = b - A x32 in FP64, into fb as the correction's right-hand side
+  hyd::k_gt_residual<<<nsys, 128, 0, st>>>(dl, d, du, b, fx, x, fb, offsets, lengths, nsys);
+  rc = hydist_gtsv_batched(fl, fd, fu, fb, fx, offsets, lengths, nsys, 1, algo, stream);
+  if (rc != HYDIST_OK) return rc;
+  hyd::k_gt_correct<<<nsys, 128, 0, st>>>(x, fx, offsets, lengths, nsys);
+  if (cudaGetLastError() != cudaSuccess) {
+    hyd::set_last_error("hydist_gtsv_batched_refine: a kernel launch failed");
+    return HYDIST_ERR_CUDA;
+  }
+  return HYDIST_OK;
 }
 
 // ---- allocation-free variant --------------------------------------------

@@ -115,13 +115,15 @@ def config1(seed=20260001):
 
 
 def config3_member(k, seed=20263000):
-    """One of the 64 ensemble scenarios of 1024x512, 30 min, sediment from
-    300 s; per-member bumps, Manning U(0.018,0.040), inflow U(200,1200),
-    tidal amplitude U(0.2,1.0)."""
+    """One of the 64 ensemble scenarios of 1024x512, 30 min, sediment (and
+    the bed change) from 300 s; per-member bumps, Manning U(0.018,0.040),
+    inflow U(200,1200), tidal amplitude U(0.2,1.0)."""
     rng = np.random.default_rng(seed + 7919 * k)
-    return make_channel(N=1024, M=512, seed=seed + k, dx=5.0, dt=2.0, hours=0.5,
-                        inflow=rng.uniform(200, 1200), tide_amp=rng.uniform(0.2, 1.0),
-                        manning=(0.018, 0.040), sediment=True, sediment_start=300.0)
+    b = make_channel(N=1024, M=512, seed=seed + k, dx=5.0, dt=2.0, hours=0.5,
+                     inflow=rng.uniform(200, 1200), tide_amp=rng.uniform(0.2, 1.0),
+                     manning=(0.018, 0.040), sediment=True, sediment_start=300.0)
+    b["options"]["bed_change"] = 1
+    return b
 
 
 SERVING_MESHES = ((256, 128), (512, 256), (1024, 512), (2048, 1024))

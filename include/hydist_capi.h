@@ -271,13 +271,19 @@ int hydist_checkpoint_save(HydistHandle* h, const char* path);
 int hydist_checkpoint_load(HydistHandle* h, const char* path);
 
 /* ---- ensembles (the reference has none) ---------------------------------
- * Many scenarios on one device stepped together: one step of every member is
- * captured into one CUDA graph (forked from the ensemble's stream onto the
- * members' streams and joined back), replayed once per step, so the members'
- * kernels overlap on the device. A graph is captured per pattern of the
- * members' sediment phases. Members keep their own handles (download,
- * mass, ...); their own stream work before and after an ensemble step is
- * ordered with it. The ensemble does not own the members. */
+ * Many scenarios on one device stepped together, one CUDA graph replay per
+ * step. Members of one mesh size, form and launch-shaping options
+ * (narrow-channel ranges, horizontal wetting, bed feedback) are batched:
+ * each kernel of the step is one launch over all members (the per-cell
+ * kernels take member blockIdx.z, the persistent line solvers walk the
+ * line groups of every member), whenever the members are in the same
+ * sediment phase. Otherwise one step of every member is captured with the
+ * members' launches on their own streams, forked from the ensemble's stream
+ * and joined back, so that they overlap on the device. A graph is captured
+ * per pattern of the members' sediment phases. Members keep their own
+ * handles (download, mass, ...); their own stream work before and after an
+ * ensemble step is ordered with it. The ensemble does not own the members.
+ * Results are the same as stepping each member alone. */
 typedef struct HydistEnsemble HydistEnsemble;
 int hydist_ensemble_create(HydistHandle* const* members, int32_t n,
                            HydistEnsemble** out);
@@ -285,6 +291,10 @@ int hydist_ensemble_step(HydistEnsemble* e, int32_t nsteps);
 int hydist_ensemble_sync(HydistEnsemble* e);
 /* The stream the ensemble's graphs are launched on (a cudaStream_t). */
 void* hydist_ensemble_stream(HydistEnsemble* e);
+/* enable = 0: step the members by their own launches even where they could
+ * be batched; 1: batch them again (HYDIST_ERR_ARG if they differ in mesh
+ * size, form or launch options). Batching is on after create where allowed. */
+int hydist_ensemble_batched(HydistEnsemble* e, int32_t enable);
 int hydist_ensemble_destroy(HydistEnsemble* e);
 
 /* ---- serving (the reference has none) ------------------------------------
@@ -292,9 +302,11 @@ int hydist_ensemble_destroy(HydistEnsemble* e);
  * scenario (host inputs copied at submit; the pointers are not kept) and a
  * horizon in steps. hydist_server_round: admits queued requests in arrival
  * order while their device footprint fits the budget; advances every active
- * request by up to steps_per_round steps, each on its own stream (their
- * kernels overlap on the device); waits; retires those at their horizon and
- * returns their ids. A retired request keeps its device state (and its share
+ * request by up to steps_per_round steps, the requests of one mesh size and
+ * form that advance alike stepped as an ensemble (their kernels launched
+ * together for all of them, see hydist_ensemble_*), each group and each lone
+ * request on its own stream (their kernels overlap on the device); waits;
+ * retires those at their horizon and returns their ids. A retired request keeps its device state (and its share
  * of the budget) until hydist_server_release; hydist_server_handle gives its
  * handle for hydist_download / hydist_mass. Each request is computed by its
  * own handle, so its result is the same alone and in the mix. */
@@ -364,8 +376,13 @@ int hydist_kernel_launches(HydistHandle* h, int64_t* count);
  * PARTITION_128, PARTITION and PARTITION_512 are the same CTA partition
  * solver on 128, 256 or 512 threads per system: fewer threads give each
  * thread a longer chunk and the separators a shorter reduction. Systems of length 0 are skipped.
- * No pivoting: the systems are expected to be diagonally dominant, as the
- * ADI sweeps' are.
+ *   PIVOT      one thread per system, Gaussian elimination with diagonal
+ *              pivoting (1x1 or 2x2 pivots by the Bunch-Kaufman criterion,
+ *              kappa = (sqrt(5)-1)/2: the pivoting of the reference's SPIKE
+ *              tile solver, spike_kernel.hxx:119-376), for systems that are
+ *              not diagonally dominant; never chosen by AUTO.
+ * The other solvers do not pivot: they expect diagonally dominant systems,
+ * as the ADI sweeps' are.
  * stream is a cudaStream_t (NULL = default stream). Scratch is allocated by
  * the library on first use and grown as needed. The call synchronises the
  * stream once to read the band sizes and the packed extent, and, when a
@@ -380,12 +397,26 @@ enum HydistGtsvAlgo {
   HYDIST_GTSV_PARTITION = 2,
   HYDIST_GTSV_WARP = 3,
   HYDIST_GTSV_PARTITION_512 = 4,
-  HYDIST_GTSV_PARTITION_128 = 5
+  HYDIST_GTSV_PARTITION_128 = 5,
+  HYDIST_GTSV_PIVOT = 6
 };
 int hydist_gtsv_batched(const void* dl, const void* d, const void* du,
                         const void* b, void* x, const int32_t* offsets,
                         const int32_t* lengths, int32_t nsys, int32_t dtype,
                         int32_t algo, void* stream);
+
+/* The same solve for FP64 systems computed in FP32 with one refinement
+ * whose residual is computed in FP64 (the refine option of the batched
+ * solve; the reference has no counterpart): the systems are rounded to
+ * FP32 and solved by `algo`'s FP32 solvers, r = b - A x is formed in FP64
+ * from the FP64 arrays, the correction A d = r is solved in FP32 by the same
+ * solvers and x + d is returned in FP64. Arrays as for
+ * hydist_gtsv_batched with dtype 0; the library's scratch holds the FP32
+ * copies (20 bytes per row). */
+int hydist_gtsv_batched_refine(const double* dl, const double* d, const double* du,
+                               const double* b, double* x, const int32_t* offsets,
+                               const int32_t* lengths, int32_t nsys, int32_t algo,
+                               void* stream);
 
 /* Length bands of the batched solver: band b holds the systems with
  * hi[b-1] < length <= hi[b] (hi[-1] = 0), HYDIST_GTSV_BANDS entries. */
