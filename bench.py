@@ -190,6 +190,10 @@ def workload(name: str, rank: int = 0):
         return S.config1(seed=replica_seed(20260001, rank)), 300
     if name == "channel-256x128":
         return S.config0(seed=replica_seed(20260000, rank)), 0
+    if name == "sediment-1024x512":
+        # one ensemble member's scenario alone (a state of ~30 fields of
+        # 4.2 MB, still larger than L2: the size for per-kernel profiles)
+        return S.config3_member(0, seed=replica_seed(20263000, rank)), 150
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -963,7 +967,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "fp32-refine"])
     ap.add_argument("--workload", default="sediment-2048x1024",
-                    help="sediment-2048x1024 | channel-256x128 | " + TRIDIAG + " | " + ENSEMBLE +
+                    help="sediment-2048x1024 | sediment-1024x512 | channel-256x128 | " + TRIDIAG +
+                         " | " + ENSEMBLE +
                          " | " + SERVING)
     ap.add_argument("--budget-gb", type=float, default=120.0,
                     help="HBM budget of the " + SERVING + " workload")

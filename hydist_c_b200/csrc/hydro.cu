@@ -33,6 +33,10 @@
 #include "explicit.cuh"
 #include "hydro.cuh"
 
+#ifndef HYDIST_PRE
+#define HYDIST_PRE 1
+#endif
+
 namespace hyd {
 
 // ----------------------------------------------------------------- init
@@ -966,8 +970,12 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   launch2(HYD_K2(k_boundary, R), dim3(cdiv(max(S.M, S.N), 128)), 128, st, S, c, b, 0.5 * (double)c.dT);
   if (tr) tr->mark(st, PH_BOUNDARY_X, 1);
   if (tr) tr->kbegin(st, KS_SWEEP_X);
+  int nx = 0;
+#if HYDIST_PRE
   launch2(HYD_K2(k_pre, R, 0), cells, 128, st, S, c, b);
-  const int nx = 1 + launch_sweep(S, c, 0, st, b);
+  nx = 1;
+#endif
+  nx += launch_sweep(S, c, 0, st, b);
   if (tr) tr->kend(st, KS_SWEEP_X);
   if (tr) tr->mark(st, PH_SWEEP_X, nx);
   // smoothing of t_u into su, explicit v from it, margins, smoothing of t_v
@@ -1013,8 +1021,12 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   launch2(HYD_K2(k_boundary, R), dim3(cdiv(max(S.M, S.N), 128)), 128, st, S, c, b, (double)c.dT * 0.5);
   if (tr) tr->mark(st, PH_BOUNDARY_Y, 1);
   if (tr) tr->kbegin(st, KS_SWEEP_Y);
+  int ny = 0;
+#if HYDIST_PRE
   launch2(HYD_K2(k_pre, R, 1), dim3(cdiv(S.M - 1, 128), S.N - 1), 128, st, S, c, b);
-  const int ny = 1 + launch_sweep(S, c, 1, st, b);
+  ny = 1;
+#endif
+  ny += launch_sweep(S, c, 1, st, b);
   if (tr) tr->kend(st, KS_SWEEP_Y);
   if (tr) tr->mark(st, PH_SWEEP_Y, ny);
   launch2(HYD_K2(k_smooth_full, R, 0, 0), smooth, 128, st, S, c, b);

@@ -204,6 +204,37 @@ template void launch_bed_feedback<double>(const StateT<double>&, const CoefT<dou
 template void launch_bed_feedback<float>(const StateT<float>&, const CoefT<float>&, cudaStream_t,
                                          const Batch<float>&);
 
+#ifndef HYDIST_FS_ROWS_PRE
+#define HYDIST_FS_ROWS_PRE 1
+#endif
+
+// The rows of a concentration sweep (_FSj / _FSi_calculate__mactrix_coeff,
+// sediment_transport.cpp:204-313, 51-164, without the segment-end
+// conditions, which the sweep applies) of every cell of rows 2..N, columns
+// 2..M into the first four arrays of StateT::pre (A, B, C, D), ahead of the
+// sweep: one thread per cell, adjacent threads on adjacent cells. DIR 0:
+// the i-sweep (along i, the cell before is (i-1, j)), 1: the j-sweep.
+template <class R, int DIR, int BATCH = 0>
+__global__ void k_fs_rows(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
+  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int i = blockIdx.y + 2;
+  if (i > S.N || j > S.M) return;
+  const int W = S.W, g = i * W + j, gp = DIR == 0 ? g - W : g - 1;
+  const R* vel = DIR == 0 ? S.tu : S.tv;
+  const R hk_c = DIR == 0 ? S.Htdu[g] * S.Kx[g] : S.Htdv[g] * S.Ky[g];
+  const R hk_p = DIR == 0 ? S.Htdu[gp] * S.Kx[gp] : S.Htdv[gp] * S.Ky[gp];
+  R A, B, C, D;
+  fs_cell(S, c, DIR == 0, i, j, vel[g], hk_c, vel[gp], hk_p, S.clock[0], S.src_start, A, B, C, D);
+  const size_t n = (size_t)W * S.H;
+  R* q = S.pre + g;
+  q[0] = A;
+  q[n] = B;
+  q[2 * n] = C;
+  q[3 * n] = D;
+}
+
 constexpr int FS_ROWS = 8;
 
 template <class R, int BATCH = 0>
@@ -232,9 +263,23 @@ void launch_sediment(const StateT<R>& S, const CoefT<R>& c, bool xdir, bool bed,
                      Trace* tr, const Batch<R>& b) {
   // Find_VTH + hesoK ran in the half-step's commit (k_commit_a/k_commit_b)
   if (tr) tr->kbegin(st, xdir ? KS_FS_X : KS_FS_Y);
-  const int nfs = launch_fs_sweep(S, c, xdir ? 0 : 1, st, b);
-  if (tr) tr->kend(st, xdir ? KS_FS_X : KS_FS_Y);
   const unsigned z = grid_z(b);
+  int nrows = 0;
+#if HYDIST_FS_ROWS_PRE
+  {
+    const dim3 gr(cdiv(S.M - 1, 128), S.N - 1, z);
+    if (b.n > 0) {
+      if (xdir) k_fs_rows<R, 0, 1><<<gr, 128, 0, st>>>(S, c, b);
+      else k_fs_rows<R, 1, 1><<<gr, 128, 0, st>>>(S, c, b);
+    } else {
+      if (xdir) k_fs_rows<R, 0, 0><<<gr, 128, 0, st>>>(S, c, b);
+      else k_fs_rows<R, 1, 0><<<gr, 128, 0, st>>>(S, c, b);
+    }
+    nrows = 1;
+  }
+#endif
+  const int nfs = nrows + launch_fs_sweep(S, c, xdir ? 0 : 1, st, b);
+  if (tr) tr->kend(st, xdir ? KS_FS_X : KS_FS_Y);
   const dim3 gfs(cdiv(S.M, 128), cdiv(S.N, FS_ROWS), z);
   if (b.n > 0) k_update_fs<R, 1><<<gfs, 128, 0, st>>>(S, c, b);
   else k_update_fs<R, 0><<<gfs, 128, 0, st>>>(S, c, b);

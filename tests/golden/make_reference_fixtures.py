@@ -17,6 +17,9 @@ Three steps, run where each can run:
    tests/golden/ref_<case>.npz: a strided subsample of u, v, z (and FS for the
    sediment case) at each saved step, plus the full wet/dry mask.
 
+``luy-inputs`` (here) writes tests/golden/luy_inputs.npz, the reference's river
+inputs in the scenario layout (for the pinned river case without the tree).
+
 ``kat`` (here) writes tests/golden/khouot_kat.npz: the reference's shipped
 Inputs/bandodosau.txt and the wet/dry mask its Onetime_init produced from it
 (Outputs/khouot.txt, written by main.cpp:268-280).
@@ -82,8 +85,20 @@ def sediment_bundle():
     return b
 
 
+LUY_NPZ = Path(__file__).resolve().parent / "luy_inputs.npz"
+
+
 def luy_bundle():
-    """The reference's river inputs as a scenario dict."""
+    """The reference's river inputs as a scenario dict (from its Inputs/, or
+    from tests/golden/luy_inputs.npz, the copy `luy-inputs` writes)."""
+    if not REF_INPUTS.exists() and LUY_NPZ.exists():
+        z = np.load(LUY_NPZ)
+        sc = {k: z[k] for k in z.files if k not in ("M", "N", "total_time", "bienQ")}
+        sc.update(M=int(z["M"]), N=int(z["N"]), total_time=int(z["total_time"]),
+                  bienQ=[int(v) for v in z["bienQ"]], FS0=None)
+        return dict(scenario=sc, params={},
+                    options=dict(sediment_start=1e12, bed_change_start=1e12),
+                    meta=dict(name="luy"))
     h = np.loadtxt(REF_INPUTS / "bandodosau.txt")
     n = h.size
     hs = np.loadtxt(REF_INPUTS / "hsnham.txt").ravel()[:n].reshape(h.shape)
@@ -266,6 +281,16 @@ def cmd_collect(out):
         print("wrote", case)
 
 
+def cmd_luy_inputs():
+    """tests/golden/luy_inputs.npz: the reference's river inputs (Inputs/) in
+    the scenario layout, so that the pinned river case runs without the
+    reference tree."""
+    sc = luy_bundle()["scenario"]
+    arrs = {k: np.asarray(v) for k, v in sc.items() if isinstance(v, np.ndarray)}
+    np.savez_compressed(LUY_NPZ, **arrs, M=sc["M"], N=sc["N"], total_time=sc["total_time"],
+                        bienQ=np.asarray(sc["bienQ"], dtype=np.int32))
+
+
 def cmd_kat():
     h = np.loadtxt(REF_INPUTS / "bandodosau.txt")
     k = np.loadtxt(REF_INPUTS.parent / "Outputs" / "khouot.txt").astype(np.int8)
@@ -284,3 +309,5 @@ if __name__ == "__main__":
         cmd_pack(sys.argv[2])
     elif cmd == "collect":
         cmd_collect(sys.argv[2])
+    elif cmd == "luy-inputs":
+        cmd_luy_inputs()

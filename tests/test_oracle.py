@@ -49,7 +49,7 @@ def _fixture_bundle(case):
     sys.path.insert(0, str(GOLDEN))
     import make_reference_fixtures as F
     if case == "luy":
-        if not F.REF_INPUTS.exists():
+        if not F.REF_INPUTS.exists() and not F.LUY_NPZ.exists():
             pytest.skip("reference inputs not present")
     return F.bundle(case)
 
@@ -68,6 +68,14 @@ def test_oracle_matches_reference_run(oracle_mod, case):
     for st in meta["steps"]:
         if st > 300 and case == "luy":
             break  # the 600-step river check is in the slow test below
+        if st > 100 and case == "narrow_n":
+            # with the y sweep off row 2 (-kn), row 2 is never solved
+            # implicitly and its velocities grow without bound (3.6 m/s from a
+            # 5 cm slosh by step 300); the growth amplifies the rounding
+            # difference between the reference's fused multiply-adds and the
+            # oracle's separate ones (1e-16 at step 10, 1e-12 at 100, 1e-6 at
+            # 300, all on row 2), as in the wet/dry case
+            break
         o.step(st - done)
         done = st
         assert o.t == pytest.approx(float(z[f"t_{st}"]))
