@@ -111,34 +111,6 @@ __device__ __forceinline__ PreT<R> pre_y(const StateT<R>& S, const CoefT<R>& c, 
   return P;
 }
 
-// The preindex values of cell g in the seven arrays of StateT::pre
-// (array stride n = W*H), written by k_pre ahead of a sweep.
-template <class R>
-__device__ __forceinline__ void store_pre(const StateT<R>& S, size_t n, int g, const PreT<R>& P) {
-  R* q = S.pre + g;
-  q[0] = P.f1;
-  q[n] = P.f2;
-  q[2 * n] = P.f3;
-  q[3 * n] = P.f5;
-  q[4 * n] = P.a2;
-  q[5 * n] = P.c2;
-  q[6 * n] = P.d2;
-}
-
-template <class R>
-__device__ __forceinline__ PreT<R> load_pre(const StateT<R>& S, size_t n, int g) {
-  const R* q = S.pre + g;
-  PreT<R> P;
-  P.f1 = q[0];
-  P.f2 = q[n];
-  P.f3 = q[2 * n];
-  P.f5 = q[3 * n];
-  P.a2 = q[4 * n];
-  P.c2 = q[5 * n];
-  P.d2 = q[6 * n];
-  return P;
-}
-
 template <class R>
 struct MomT {
   R a1, b1, c1, d1;

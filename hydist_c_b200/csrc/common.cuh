@@ -97,8 +97,8 @@ struct StateT {
   R *su, *sv;    // t_u / t_v after the smoothing of the current half-step
   int* err;      // [0]: DevErr
   R* lscratch;   // partitioned line solver: one slot per resident CTA
-  // the preindex values of every cell for the next hydraulic sweep (f1, f2,
-  // f3, f5, a2, c2, d2: seven arrays of (N+3)*(M+3), array k at pre + k*W*H)
+  // the rows of the next concentration sweep (A, B, C, D of every cell:
+  // four arrays of (N+3)*(M+3), array k at pre + k*W*H)
   R* pre;
   int lslots;    // number of slots (CTAs of the persistent sweep grid)
   int* colflag;  // per column: holds a cell dried during the run

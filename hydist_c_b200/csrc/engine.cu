@@ -281,7 +281,7 @@ void enqueue_step(HydistHandle* h, bool sed_x, bool sed_y, bool bed, Trace* tr) 
     launch_half_x(St, Cf, sed_x, h->stream, tr);
     if (sed_x) launch_sediment(St, Cf, true, false, h->stream, tr);
     else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_X + 1], h->stream);
-    launch_half_y(St, Cf, sed_y, h->stream, tr);
+    launch_half_y(St, Cf, sed_y, h->stream, tr, {}, sed_y && bed);
     if (sed_y) launch_sediment(St, Cf, false, bed, h->stream, tr);
     else if (tr && tr->ev) cudaEventRecord(tr->ev[PH_SEDIMENT_Y + 1], h->stream);
   });
@@ -535,7 +535,7 @@ int bulk_private(HydistHandle* h, StateT<R>& B) {
   const size_t n = (size_t)S.W * S.H;
   TRY(dalloc(h, &B.tmp, n));
   TRY(dalloc(h, &B.sv, n));
-  TRY(dalloc(h, &B.pre, 7 * n));
+  TRY(dalloc(h, &B.pre, 4 * n));
   B.su = B.tmp;
   int nsm = 0;
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
@@ -891,10 +891,9 @@ int hydist_half_step(HydistHandle* h, int32_t half) {
     });
   } else {
     on_state(h, [&](auto& St, auto& Cf) {
-      launch_half_y(St, Cf, sed, h->stream, &h->trace);
-      if (sed)
-        launch_sediment(St, Cf, false, bed_on(h, t), h->stream,
-                        &h->trace);
+      const bool bed = sed && bed_on(h, t);
+      launch_half_y(St, Cf, sed, h->stream, &h->trace, {}, bed);
+      if (sed) launch_sediment(St, Cf, false, bed, h->stream, &h->trace);
     });
   }
   h->t = t;
@@ -1080,7 +1079,7 @@ void enqueue_step_batch(const StateT<R>& S0, const CoefT<R>& c0, const Batch<R>&
                         bool sy, bool bed, cudaStream_t st, Trace* tr) {
   launch_half_x(S0, c0, sx, st, tr, b);
   if (sx) launch_sediment(S0, c0, true, false, st, tr, b);
-  launch_half_y(S0, c0, sy, st, tr, b);
+  launch_half_y(S0, c0, sy, st, tr, b, sy && bed);
   if (sy) launch_sediment(S0, c0, false, bed, st, tr, b);
 }
 

@@ -32,10 +32,7 @@
 #include "common.cuh"
 #include "explicit.cuh"
 #include "hydro.cuh"
-
-#ifndef HYDIST_PRE
-#define HYDIST_PRE 1
-#endif
+#include "sediment_cell.cuh"
 
 namespace hyd {
 
@@ -479,23 +476,6 @@ __global__ void k_boundary(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, doub
   }
 }
 
-// ------------------------------------------------------------- preindex
-// _uzSolver_calculate_preindex (DIR 0) / _vzSolver_calculate_preindex
-// (DIR 1) of every cell of rows 2..N, columns 2..M into StateT::pre, ahead
-// of the sweep that reads them: one thread per cell, adjacent threads on
-// adjacent cells, so the stencils' loads are shared through L1 instead of
-// each line walker fetching its own.
-template <class R, int DIR, int BATCH = 0>
-__global__ void k_pre(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
-  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
-  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
-  const int i = blockIdx.y + 2;
-  if (i > S.N || j > S.M) return;
-  const PreT<R> P = DIR == 0 ? pre_x(S, c, i, j) : pre_y(S, c, i, j);
-  store_pre(S, (size_t)S.W * S.H, i * S.W + j, P);
-}
-
 // ------------------------------------------------------------ smoothing
 // _normalize / update_buffer (support_funcs.cpp:761-808) into a complete
 // array (su / sv): smoothed on the interior [2,N]x[2,M], the unsmoothed
@@ -684,19 +664,20 @@ __global__ void k_margin_u(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
 // cell, of (i, j-1) and of (i-1, j), and the new Htdu, Htdv. Rows 1..vth_hi
 // (the sediment launch shape: N after half-step A, N-1 after B), VTH from
 // row and column 2.
+// Returns the speed stored at (i, j) (0 where none is, i or j below 2).
 template <class R>
-__device__ __forceinline__ void vth_heso_cell(const StateT<R>& S, const CoefT<R>& c, int i, int j,
-                                              int g, R tu, R tv, R tu_up, R tv_left, R Hm,
-                                              double ht, double hp, double hl, double hup, R Hu,
-                                              R Hv) {
+__device__ __forceinline__ R vth_heso_cell(const StateT<R>& S, const CoefT<R>& c, int i, int j,
+                                           int g, R tu, R tv, R tu_up, R tv_left, R Hm,
+                                           double ht, double hp, double hl, double hup, R Hu,
+                                           R Hv) {
+  R vthv = 0;
   if (i >= 2 && j >= 2) {
     if ((ht > c.NANGDAY) && (Hm > c.H_TINH)) {
       const R ut = (tu + tu_up) * R(0.5);
       const R vt = (tv + tv_left) * R(0.5);
-      S.VTH[g] = sqrt(ut * ut + vt * vt);
-    } else {
-      S.VTH[g] = 0;
+      vthv = sqrt(ut * ut + vt * vt);
     }
+    S.VTH[g] = vthv;
   }
   if (Hu > 0) {
     const R Cz = 18 * log(12 * Hu / c.Ks);
@@ -708,6 +689,7 @@ __device__ __forceinline__ void vth_heso_cell(const StateT<R>& S, const CoefT<R>
     const R k = R(5.93) * c.sqrt_g * R(hup + hp) * R(0.25) * fabs(tv) / Cz;
     S.Ky[g] = fmin(R(100), fmax(R(5), k));
   }
+  return vthv;
 }
 
 // Half-step A commit: update_h_moi (support_funcs.cpp:71-86) on [1,N]x[1,M],
@@ -843,8 +825,14 @@ __global__ void k_wetting_rows(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) 
 //
 // HORIZ: the drying loop of Reset_states_horizontal instead (:125-137,
 // rows 1..N, columns 2..M), in the first half-step.
+//
+// qb != 0 (the bed change follows this step's concentration j-sweep): also
+// Calculate_Qb (qb_cell) on rows 2..N, columns 2..M, from the committed
+// velocities, the speed, the mask after the drying pass and H_moi; nothing
+// between this pass and BedLoad changes them. On row N the speed is the
+// first half-step's (its hesoK launch shape never reaches row N).
 template <class R, int HORIZ, int BATCH = 0>
-__global__ void k_commit_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi) {
+__global__ void k_commit_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi, int qb) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -853,6 +841,8 @@ __global__ void k_commit_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int 
   const int W = S.W, g = i * W + j;
   const bool in = i >= 1 && j >= 1;
   const bool vth = in && i <= vth_hi;
+  const bool qbc = qb && i >= 2 && j >= 2;
+  const bool nbr = vth || qbc;  // the committed t_u(i-1, j), t_v(i, j-1) are needed
   // every operand before the first store (one round of memory latency);
   // nothing this kernel stores is read by another of its threads. A cell
   // dries when it is wet with H_moi at most H_TINH (rows 2..N, columns 1..M;
@@ -862,7 +852,7 @@ __global__ void k_commit_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int 
                  : (ii >= 2 && ii <= S.N && jj >= 1 && jj <= S.M);
   };
   const bool c0 = in_dry(i, j), cd = in_dry(i + 1, j), cr = in_dry(i, j + 1);
-  const bool cu = vth && in_dry(i - 1, j), cl = vth && in_dry(i, j - 1);
+  const bool cu = nbr && in_dry(i - 1, j), cl = nbr && in_dry(i, j - 1);
   const int k0 = c0 ? S.khouot[g] : 1, kd = cd ? S.khouot[g + W] : 1, kr = cr ? S.khouot[g + 1] : 1;
   const int ku = cu ? S.khouot[g - W] : 1, kl = cl ? S.khouot[g - 1] : 1;
   const R h0 = c0 ? S.Hmoi[g] : R(0), hd = cd ? S.Hmoi[g + W] : R(0), hr = cr ? S.Hmoi[g + 1] : R(0);
@@ -874,8 +864,10 @@ __global__ void k_commit_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int 
   const double hp = S.h[g];
   const double hl = in ? S.h[g - 1] : 0.0, hup = in ? S.h[g - W] : 0.0;
   const double ht = vth ? S.htaiz[g] : 0.0;
-  const R hm = vth ? S.Hmoi[g] : R(0);
-  const R su_up = vth ? S.su[g - W] : R(0), sv_left = vth ? S.sv[g - 1] : R(0);
+  const R hm = (vth || qbc) ? S.Hmoi[g] : R(0);
+  const R su_up = nbr ? S.su[g - W] : R(0), sv_left = nbr ? S.sv[g - 1] : R(0);
+  const R fw = qbc ? S.Fw[g] : R(0);
+  const R vth_old = (qbc && !vth) ? S.VTH[g] : R(0);
   const bool d0 = c0 && k0 == 0 && h0 <= c.H_TINH;
   const bool ddown = cd && kd == 0 && hd <= c.H_TINH;
   const bool dright = cr && kr == 0 && hr <= c.H_TINH;
@@ -895,14 +887,17 @@ __global__ void k_commit_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int 
     const R Hv = (hup + hp + zr + tz) * 0.5;
     S.Htdu[g] = Hu;
     S.Htdv[g] = Hv;
-    if (vth) {
+    if (nbr) {
       // t_u(i-1, j) is zeroed when (i-1, j) or (i, j) dries, t_v(i, j-1)
       // when (i, j-1) or (i, j) does
       const bool dup = cu && ku == 0 && hu <= c.H_TINH;
       const bool dleft = cl && kl == 0 && hl_ <= c.H_TINH;
       const R tu_up = (dup || d0) ? R(0) : su_up;
       const R tv_left = (dleft || d0) ? R(0) : sv_left;
-      vth_heso_cell(S, c, i, j, g, R(tu), R(tv), tu_up, tv_left, hm, ht, hp, hl, hup, Hu, Hv);
+      R vthv = vth_old;
+      if (vth) vthv = vth_heso_cell(S, c, i, j, g, R(tu), R(tv), tu_up, tv_left, hm, ht, hp, hl, hup, Hu, Hv);
+      // the mask after this pass's drying (the segment scan writes it)
+      if (qbc) qb_cell(S, c, i, j, vthv, d0 ? 1 : k0, hm, fw, R(tu), tu_up, R(tv), tv_left);
     }
   }
 }
@@ -970,12 +965,7 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   launch2(HYD_K2(k_boundary, R), dim3(cdiv(max(S.M, S.N), 128)), 128, st, S, c, b, 0.5 * (double)c.dT);
   if (tr) tr->mark(st, PH_BOUNDARY_X, 1);
   if (tr) tr->kbegin(st, KS_SWEEP_X);
-  int nx = 0;
-#if HYDIST_PRE
-  launch2(HYD_K2(k_pre, R, 0), cells, 128, st, S, c, b);
-  nx = 1;
-#endif
-  nx += launch_sweep(S, c, 0, st, b);
+  const int nx = launch_sweep(S, c, 0, st, b);
   if (tr) tr->kend(st, KS_SWEEP_X);
   if (tr) tr->mark(st, PH_SWEEP_X, nx);
   // smoothing of t_u into su, explicit v from it, margins, smoothing of t_v
@@ -993,7 +983,7 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
     launch2(HYD_K2(k_smooth_full, R, 0, 2), smooth, 128, st, S, c, b);
     if (tr) tr->mark(st, PH_EXPLICIT_V, 4);
     launch2(HYD_K2(k_wetting_rows, R), dim3(cdiv(S.N, 128)), 128, st, S, c, b);
-    launch2(HYD_K2(k_commit_b, R, 1), commit, 128, st, S, c, b, sed ? S.N : 0);
+    launch2(HYD_K2(k_commit_b, R, 1), commit, 128, st, S, c, b, sed ? S.N : 0, 0);
     launch2(HYD_K2(k_interp_fs_rows, R), dim3(cdiv(S.M, 128), 2), 128, st, S, c, b);
     launch2(HYD_K2(k_interp_fs_col, R), dim3(cdiv(S.M, 128)), 128, st, S, c, b);
     launch2(HYD_K2(k_runs_flags, R), grid2(S.M - 1, S.N - 1, 128), 128, st, S, c, b, 2);
@@ -1015,18 +1005,13 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
 
 template <class R>
 void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr,
-                   const Batch<R>& b) {
+                   const Batch<R>& b, bool qb) {
   const dim3 smooth(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS));
   const dim3 commit(cdiv(S.M + 1, 128), S.N + 1);
   launch2(HYD_K2(k_boundary, R), dim3(cdiv(max(S.M, S.N), 128)), 128, st, S, c, b, (double)c.dT * 0.5);
   if (tr) tr->mark(st, PH_BOUNDARY_Y, 1);
   if (tr) tr->kbegin(st, KS_SWEEP_Y);
-  int ny = 0;
-#if HYDIST_PRE
-  launch2(HYD_K2(k_pre, R, 1), dim3(cdiv(S.M - 1, 128), S.N - 1), 128, st, S, c, b);
-  ny = 1;
-#endif
-  ny += launch_sweep(S, c, 1, st, b);
+  const int ny = launch_sweep(S, c, 1, st, b);
   if (tr) tr->kend(st, KS_SWEEP_Y);
   if (tr) tr->mark(st, PH_SWEEP_Y, ny);
   launch2(HYD_K2(k_smooth_full, R, 0, 0), smooth, 128, st, S, c, b);
@@ -1040,7 +1025,10 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   launch2(HYD_K2(k_wetting, R), dim3(cdiv(S.M, 128)), 128, st, S, c, b);
   // with sed, also Find_VTH + hesoK (rows to N-1: the launch shape of
   // engine.cpp:259-260 never reaches row N)
-  launch2(HYD_K2(k_commit_b, R, 0), commit, 128, st, S, c, b, sed ? S.N - 1 : 0);
+  // with qb, also Calculate_Qb of the bed change that follows this step's
+  // concentration j-sweep
+  launch2(HYD_K2(k_commit_b, R, 0), commit, 128, st, S, c, b, sed ? S.N - 1 : 0,
+          qb && S.N >= 5 ? 1 : 0);
   // the drying mask is written by the segment scan (k_runs_flags, dry)
   launch_find_limits(S, c, true, st, tr, b);
   if (tr) tr->mark(st, PH_COMMIT_Y, 2);
@@ -1057,7 +1045,7 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   template void launch_half_x<R>(const StateT<R>&, const CoefT<R>&, bool, cudaStream_t, Trace*, \
                                  const Batch<R>&);                                        \
   template void launch_half_y<R>(const StateT<R>&, const CoefT<R>&, bool, cudaStream_t, Trace*, \
-                                 const Batch<R>&);
+                                 const Batch<R>&, bool);
 HYD_HYDRO_INST(double)
 HYD_HYDRO_INST(float)
 

@@ -39,10 +39,11 @@ template <class R>
 void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr,
                    const Batch<R>& b = {});
 // hydraulic half-step B: t += dT/2, boundary, y sweep, explicit u, wet/dry,
-// commit; sed as above
+// commit; sed as above; qb: the bed change follows the step's concentration
+// j-sweep (the commit computes its flux, Calculate_Qb)
 template <class R>
 void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t st, Trace* tr,
-                   const Batch<R>& b = {});
+                   const Batch<R>& b = {}, bool qb = false);
 // partitioned hydraulic line sweep: dir 0 = x (columns), 1 = y (rows)
 template <class R>
 int launch_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t st,

@@ -7,7 +7,7 @@
 //                   solution, :51-349, 604-651]: the partitioned line solver
 //                   with FSGen (sweep.cu), cell rows in sediment_cell.cuh
 //   k_update_fs    [Update_FS, :654-663]
-//   k_calc_qb      [Calculate_Qb, :352-434]
+//   Calculate_Qb   [:352-434] runs in the second commit (hydro.cu k_commit_b)
 //   k_bed_load     [_bed_load / BedLoad, :436-537, :664-673]
 #include "common.cuh"
 #include "hydro.cuh"
@@ -15,72 +15,12 @@
 
 namespace hyd {
 
-// ---- bed change: Calculate_Qb (sediment_transport.cpp:352-434) and
-// _bed_load / BedLoad (:436-537, :664-673), which the reference never
-// launches (engine.cpp:290-293). Read as intended where the code cannot be
-// meant literally: the flux where the speed is not zero (:385 divides by
-// the VTH it tests to be zero), Toee starting from the coefficient Toe
-// (:359), both components in the corner copies (:410-419), t_u[pos] > 0 in
-// the downwind test (:479).
-template <class R, int BATCH = 0>
-__global__ void k_calc_qb(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
-  const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
-  const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
-  const int i = blockIdx.y + 2;
-  if (i > S.N || j > S.M) return;
-  const int w = S.W, pos = i * w + j, N = S.N, M = S.M;
-  R qx = 0, qy = 0;
-  const R vth = S.VTH[pos];
-  if (vth != 0 && S.khouot[pos] == 0) {
-    R Toee = c.Toe, Tx = 0;
-    const R Hm = S.Hmoi[pos];
-    const R Tob = c.ro * S.Fw[pos] * (vth * vth);
-    if (Hm > c.ghtoe) Toee = c.Toe * (1 + c.hstoe * ((Hm - c.ghtoe)));
-    if (Tob > Toee) Tx = Tob / Toee - 1;
-    const R base = c.qb_k * pow(Tx, R(2.1)) * c.Dxr_m03;
-    qx = base * (S.tu[pos] + S.tu[pos - w]) * R(0.5) / vth;
-    qy = base * (S.tv[pos] + S.tv[pos - 1]) * R(0.5) / vth;
-  }
-  R* Qbx = S.Qbx;
-  R* Qby = S.Qby;
-  Qbx[pos] = qx;
-  Qby[pos] = qy;
-  // margins and corners copy the nearest interior value (:402-431)
-  if (i == 2) {
-    Qbx[pos - w] = qx;
-    Qby[pos - w] = qy;
-  }
-  if (i == N) {
-    Qbx[pos + w] = qx;
-    Qby[pos + w] = qy;
-  }
-  if (j == 2) {
-    Qbx[pos - 1] = qx;
-    Qby[pos - 1] = qy;
-    if (i == 2) {
-      Qbx[1 * w + 1] = qx;
-      Qby[1 * w + 1] = qy;
-    }
-    if (i == N) {
-      Qbx[(N + 1) * w + 1] = qx;
-      Qby[(N + 1) * w + 1] = qy;
-    }
-  }
-  if (j == M) {
-    Qbx[pos + 1] = qx;
-    Qby[pos + 1] = qy;
-    if (i == 2) {
-      Qbx[1 * w + M + 1] = qx;
-      Qby[1 * w + M + 1] = qy;
-    }
-    if (i == N) {
-      Qbx[(N + 1) * w + M + 1] = qx;
-      Qby[(N + 1) * w + M + 1] = qy;
-    }
-  }
-}
-
+// ---- bed change: Calculate_Qb (sediment_transport.cpp:352-434, qb_cell in
+// sediment_cell.cuh) runs in the second half-step's commit (k_commit_b, with
+// the values that pass holds), _bed_load / BedLoad (:436-537, :664-673) here;
+// the reference never launches either (engine.cpp:290-293). Read as intended
+// where the code cannot be meant literally: t_u[pos] > 0 in the downwind test
+// (:479).
 // _bed_load on rows 3..N-2 (BedLoad with the j-sweep's range,
 // engine.cpp:292), cells of the row's wet segments of at least 3 cells.
 template <class R, int BATCH = 0>
@@ -204,10 +144,6 @@ template void launch_bed_feedback<double>(const StateT<double>&, const CoefT<dou
 template void launch_bed_feedback<float>(const StateT<float>&, const CoefT<float>&, cudaStream_t,
                                          const Batch<float>&);
 
-#ifndef HYDIST_FS_ROWS_PRE
-#define HYDIST_FS_ROWS_PRE 1
-#endif
-
 // The rows of a concentration sweep (_FSj / _FSi_calculate__mactrix_coeff,
 // sediment_transport.cpp:204-313, 51-164, without the segment-end
 // conditions, which the sweep applies) of every cell of rows 2..N, columns
@@ -264,8 +200,6 @@ void launch_sediment(const StateT<R>& S, const CoefT<R>& c, bool xdir, bool bed,
   // Find_VTH + hesoK ran in the half-step's commit (k_commit_a/k_commit_b)
   if (tr) tr->kbegin(st, xdir ? KS_FS_X : KS_FS_Y);
   const unsigned z = grid_z(b);
-  int nrows = 0;
-#if HYDIST_FS_ROWS_PRE
   {
     const dim3 gr(cdiv(S.M - 1, 128), S.N - 1, z);
     if (b.n > 0) {
@@ -275,10 +209,8 @@ void launch_sediment(const StateT<R>& S, const CoefT<R>& c, bool xdir, bool bed,
       if (xdir) k_fs_rows<R, 0, 0><<<gr, 128, 0, st>>>(S, c, b);
       else k_fs_rows<R, 1, 0><<<gr, 128, 0, st>>>(S, c, b);
     }
-    nrows = 1;
   }
-#endif
-  const int nfs = nrows + launch_fs_sweep(S, c, xdir ? 0 : 1, st, b);
+  const int nfs = 1 + launch_fs_sweep(S, c, xdir ? 0 : 1, st, b);
   if (tr) tr->kend(st, xdir ? KS_FS_X : KS_FS_Y);
   const dim3 gfs(cdiv(S.M, 128), cdiv(S.N, FS_ROWS), z);
   if (b.n > 0) k_update_fs<R, 1><<<gfs, 128, 0, st>>>(S, c, b);
@@ -286,15 +218,11 @@ void launch_sediment(const StateT<R>& S, const CoefT<R>& c, bool xdir, bool bed,
   int launched = nfs + 1;
   if (bed && S.N >= 5) {
     // the bed change once per step, after the j-sweep (engine.cpp:290-293)
-    const dim3 gq(cdiv(S.M - 1, 128), S.N - 1, z), gl(cdiv(S.M - 1, 128), S.N - 4, z);
-    if (b.n > 0) {
-      k_calc_qb<R, 1><<<gq, 128, 0, st>>>(S, c, b);
-      k_bed_load<R, 1><<<gl, 128, 0, st>>>(S, c, b);
-    } else {
-      k_calc_qb<R, 0><<<gq, 128, 0, st>>>(S, c, b);
-      k_bed_load<R, 0><<<gl, 128, 0, st>>>(S, c, b);
-    }
-    launched += 2;
+    // the flux Qb was computed by this step's second commit (k_commit_b)
+    const dim3 gl(cdiv(S.M - 1, 128), S.N - 4, z);
+    if (b.n > 0) k_bed_load<R, 1><<<gl, 128, 0, st>>>(S, c, b);
+    else k_bed_load<R, 0><<<gl, 128, 0, st>>>(S, c, b);
+    launched += 1;
     if (S.bed_fb) {
       launch_bed_feedback(S, c, st, b);
       ++launched;

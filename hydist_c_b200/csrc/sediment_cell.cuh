@@ -39,6 +39,67 @@ __device__ __forceinline__ R source_nchs(const CoefT<R>& c, R wsm, R Zf, R Uf, R
   return wsm * (Cac - gamac * fs);
 }
 
+// Calculate_Qb (sediment_transport.cpp:352-434) at cell (i, j) of rows
+// 2..N, columns 2..M, read as intended where the code cannot be meant
+// literally: the flux where the speed is not zero (:385 divides by the VTH
+// it tests to be zero), Toee starting from the coefficient Toe (:359), both
+// components in the corner copies (:410-419). vth, kh, Hm, fw are the cell's
+// speed, mask, H_moi and Fw; tu, tu_up = t_u(i, j), t_u(i-1, j); tv,
+// tv_left = t_v(i, j), t_v(i, j-1). The margins and corners copy the
+// nearest interior value (:402-431).
+template <class R>
+__device__ __forceinline__ void qb_cell(const StateT<R>& S, const CoefT<R>& c, int i, int j,
+                                        R vth, int kh, R Hm, R fw, R tu, R tu_up, R tv,
+                                        R tv_left) {
+  const int w = S.W, pos = i * w + j, N = S.N, M = S.M;
+  R qx = 0, qy = 0;
+  if (vth != 0 && kh == 0) {
+    R Toee = c.Toe, Tx = 0;
+    const R Tob = c.ro * fw * (vth * vth);
+    if (Hm > c.ghtoe) Toee = c.Toe * (1 + c.hstoe * ((Hm - c.ghtoe)));
+    if (Tob > Toee) Tx = Tob / Toee - 1;
+    const R base = c.qb_k * pow(Tx, R(2.1)) * c.Dxr_m03;
+    qx = base * (tu + tu_up) * R(0.5) / vth;
+    qy = base * (tv + tv_left) * R(0.5) / vth;
+  }
+  R* Qbx = S.Qbx;
+  R* Qby = S.Qby;
+  Qbx[pos] = qx;
+  Qby[pos] = qy;
+  if (i == 2) {
+    Qbx[pos - w] = qx;
+    Qby[pos - w] = qy;
+  }
+  if (i == N) {
+    Qbx[pos + w] = qx;
+    Qby[pos + w] = qy;
+  }
+  if (j == 2) {
+    Qbx[pos - 1] = qx;
+    Qby[pos - 1] = qy;
+    if (i == 2) {
+      Qbx[1 * w + 1] = qx;
+      Qby[1 * w + 1] = qy;
+    }
+    if (i == N) {
+      Qbx[(N + 1) * w + 1] = qx;
+      Qby[(N + 1) * w + 1] = qy;
+    }
+  }
+  if (j == M) {
+    Qbx[pos + 1] = qx;
+    Qby[pos + 1] = qy;
+    if (i == 2) {
+      Qbx[1 * w + M + 1] = qx;
+      Qby[1 * w + M + 1] = qy;
+    }
+    if (i == N) {
+      Qbx[(N + 1) * w + M + 1] = qx;
+      Qby[(N + 1) * w + M + 1] = qy;
+    }
+  }
+}
+
 // One cell's row of a concentration sweep: xdir = _FSj (:204-313), else
 // _FSi (:51-164). The along-line values are passed in by the caller, which
 // carries them from cell to cell: vel_c / hk_c are the sweep-direction

@@ -136,6 +136,7 @@ int64_t hydist_scenario_bytes(int32_t M, int32_t N) {
   uint64_t t = 0;
   t += 29 * r(n * 8 + 64);  // 4 inputs, 6 derived, 17 state, 2 smoothing buffers
   t += r(n * 4 + 64);       // mask
+  t += r(4 * n * 8 + 64);   // the concentration sweep's rows (StateT::pre)
   int nsm = 148;
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

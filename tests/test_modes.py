@@ -116,7 +116,10 @@ def test_reset_states_horizontal(hyd, oracle_mod):
     sim = hyd.Simulation(b)
     done = 0
     seen_dry = seen_rewet = False
-    for target in (700, 1000, 2300, 2500):
+    # windows that see rows and columns dry (from step 288) and re-wet (from
+    # step 637); this basin with the horizontal reset stays finite in the
+    # oracle to about step 1560 and diverges after it, so targets stay below
+    for target in (285, 634, 735, 1400):
         orc.step(target - done)
         done = target
         for f in STATE:
