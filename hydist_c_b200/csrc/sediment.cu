@@ -38,6 +38,24 @@ __global__ void k_bed_load(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
   if (threadIdx.x == 0) s_n = S.moci[i];
   __syncthreads();
   if (i >= S.N - 1 || j > S.M) return;
+  const int w = S.W, pos = i * w + j, M = S.M, N = S.N;
+  const int* kh = S.khouot;
+  const R *Qbx = S.Qbx, *Qby = S.Qby, *FS = S.FS;
+  // every operand (all in bounds for rows 3..N-2, columns 2..M) before the
+  // segment lookup and the upwind tests that choose among them: one round
+  // of memory latency
+  const int kN = kh[pos - w], kS = kh[pos + w], kN2 = kh[pos - 2 * w], kS2 = kh[pos + 2 * w];
+  const int kW = kh[pos - 1], kE = kh[pos + 1], kW2 = kh[pos - 2], kE2 = kh[pos + 2];
+  const R tu = S.tu[pos], tv = S.tv[pos];
+  const R qx0 = Qbx[pos], qxN = Qbx[pos - w], qxS = Qbx[pos + w], qxN2 = Qbx[pos - 2 * w],
+          qxS2 = Qbx[pos + 2 * w];
+  const R qy0 = Qby[pos], qyW = Qby[pos - 1], qyE = Qby[pos + 1], qyW2 = Qby[pos - 2],
+          qyE2 = Qby[pos + 2];
+  const R fs = FS[pos], fN = FS[pos - w], fS = FS[pos + w], fW = FS[pos - 1], fE = FS[pos + 1];
+  const R hu0 = S.Htdu[pos], huN = S.Htdu[pos - w], kx0 = S.Kx[pos], kxN = S.Kx[pos - w];
+  const R hv0 = S.Htdv[pos], hvW = S.Htdv[pos - 1], ky0 = S.Ky[pos], kyW = S.Ky[pos - 1];
+  const R Hm = S.Hmoi[pos], vth = S.VTH[pos];
+  const R fw = S.ketdinh ? S.Fw[pos] : R(0);
   int first = 0, last = 0;
   for (int k = 0; k < s_n; ++k)
     if (s_first[k] <= j && j <= s_last[k]) {
@@ -46,49 +64,45 @@ __global__ void k_bed_load(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
       break;
     }
   if (last - first < 2 || j < first || j > last) return;
-  const int w = S.W, pos = i * w + j, M = S.M, N = S.N;
-  const int* kh = S.khouot;
-  const R *Qbx = S.Qbx, *Qby = S.Qby, *FS = S.FS, *tu = S.tu, *tv = S.tv;
   R p = 0, q = 0;
-  if (kh[pos - w] == 1) {
-    if (tu[pos] < 0) p = (-3 * Qbx[pos] + 4 * Qbx[pos + w] - Qbx[pos + 2 * w]) * c.r_dX2;
+  if (kN == 1) {
+    if (tu < 0) p = (-3 * qx0 + 4 * qxS - qxS2) * c.r_dX2;
   } else {
-    if (kh[pos + w] == 1) {
-      if (tu[pos] > 0) p = (3 * Qbx[pos] - 4 * Qbx[pos - w] + Qbx[pos - 2 * w]) * c.r_dX2;
+    if (kS == 1) {
+      if (tu > 0) p = (3 * qx0 - 4 * qxN + qxN2) * c.r_dX2;
     } else {
-      p = (Qbx[pos + w] - Qbx[pos - w]) * c.r_dX2;
+      p = (qxS - qxN) * c.r_dX2;
     }
   }
-  if (kh[pos - 1] == 1) {
-    if (tv[pos] < 0) q = (-3 * Qby[pos] + 4 * Qby[pos + 1] - Qby[pos + 2]) * c.r_dY2;
+  if (kW == 1) {
+    if (tv < 0) q = (-3 * qy0 + 4 * qyE - qyE2) * c.r_dY2;
   } else {
-    if (kh[pos + 1] == 1) {
-      if (tv[pos] > 0) q = (3 * Qby[pos] - 4 * Qby[pos - 1] + Qby[pos - 2]) * c.r_dY2;
+    if (kE == 1) {
+      if (tv > 0) q = (3 * qy0 - 4 * qyW + qyW2) * c.r_dY2;
     } else {
-      q = (Qby[pos + 1] - Qby[pos - 1]) * c.r_dY2;
+      q = (qyE - qyW) * c.r_dY2;
     }
   }
   R tH = p + q;
-  p = FS[pos + w] - FS[pos];
-  if ((kh[pos + 2 * w] == 1 || kh[pos - w] == 1) && (i < N)) p = 0;
-  q = FS[pos] - FS[pos - w];
-  if ((i > 2) && (kh[pos - 2 * w] == 1 || kh[pos + w] == 1)) q = 0;
-  p = c.r_dXbp * (S.Htdu[pos] * S.Kx[pos] * p - S.Htdu[pos - w] * S.Kx[pos - w] * q);
+  p = fS - fs;
+  if ((kS2 == 1 || kN == 1) && (i < N)) p = 0;
+  q = fs - fN;
+  if ((i > 2) && (kN2 == 1 || kS == 1)) q = 0;
+  p = c.r_dXbp * (hu0 * kx0 * p - huN * kxN * q);
   tH = tH + p;
-  p = FS[pos + 1] - FS[pos];
-  if (((last < M) && (kh[pos - 1] == 1 || kh[pos + 2] == 1)) || (last == M && (kh[pos - 1] == 1))) p = 0;
-  q = FS[pos] - FS[pos - 1];
-  if (((first > 2) && (kh[pos - 2] == 1 || kh[pos + 1] == 1)) || (first == 2 && kh[pos + 1] == 1)) q = 0;
-  p = c.r_dYbp * (S.Htdv[pos] * S.Ky[pos] * p - S.Htdv[pos - 1] * S.Ky[pos - 1] * q);
+  p = fE - fs;
+  if (((last < M) && (kW == 1 || kE2 == 1)) || (last == M && (kW == 1))) p = 0;
+  q = fs - fW;
+  if (((first > 2) && (kW2 == 1 || kE == 1)) || (first == 2 && kE == 1)) q = 0;
+  p = c.r_dYbp * (hv0 * ky0 * p - hvW * kyW * q);
   tH = tH + p;
-  const R Hm = S.Hmoi[pos], fs = FS[pos], vth = S.VTH[pos];
   const R cc = 18 * log(12 * Hm / c.Ks);
   const R Uf = c.sqrt_g * fabs(vth) / cc;
   const R om = 1 - fs, om2 = om * om;
   const R wsm = c.wss * (om2 * om2);
   R Zf = 0;
   if (fs > R(0)) Zf = wsm / (R(0.4) * (Uf + 2 * wsm));
-  const R src = S.ketdinh ? source_chs(c, wsm, Zf, fs, S.Fw[pos], vth, Hm)
+  const R src = S.ketdinh ? source_chs(c, wsm, Zf, fs, fw, vth, Hm)
                           : source_nchs(c, wsm, Zf, Uf, R(1) / Hm, fs);
   S.dH[pos] += double(c.dT / (1 - c.Dorong) * (src + tH));
 }

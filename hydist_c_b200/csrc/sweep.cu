@@ -144,52 +144,59 @@ struct HydroGen {
     }
     __device__ void row(const HydroGen& G, const LineSeg& LS, int e, R& A, R& B, R& C,
                         R& D) const {
-      const int r = 2 * pos + e;
       if (!in) {
         A = 0; B = 1; C = 0; D = 0;
         return;
       }
-      const SegD& d = LS.s[si];
-      if (r < d.off || r > d.rend) {
-        A = 0; B = 1; C = 0; D = 0;
-        return;
-      }
-      const bool even = (r & 1) == 0;
-      if ((bool)d.ran == even) {
-        const PreT<R>& P = d.ran ? Pc : Pn;
-        A = P.a2; B = 1; C = P.c2; D = P.d2;
-      } else {
-        A = Mi.a1; B = Mi.b1; C = Mi.c1; D = Mi.d1;
-      }
-      if (r == d.off) {
-        if (d.ran) {
-          if (d.qfirst) {
-            const R ub = DIR == 0 ? G.S.ubt[lp] : G.S.vbd[lp];
-            D = Pc.d2 - Pc.a2 * ub;
-          } else {
-            D = Pc.d2;
-          }
-        } else {
-          const R TZ_l = R(G.S.tz[G.at(lp, d.first)]);
-          D = Mi.d1 - Mi.a1 * TZ_l;
-        }
-        A = 0;  // the system starts here
-      }
-      if (r == d.rend) {
-        const PreT<R>& PL = (pos == d.last) ? Pc : Pn;
-        if (d.last_kind == 1) {
-          const R ub = DIR == 0 ? G.S.ubp[lp] : G.S.vbt[lp];
-          A = PL.a2; B = 1; D = PL.d2 - PL.c2 * ub;
-        } else if (d.last_kind == 2) {
-          const R TZ_r = R(G.S.tz[G.at(lp, d.last)]);
-          A = Mi.a1; B = Mi.b1; D = Mi.d1 - Mi.c1 * TZ_r;
-        } else {
-          A = PL.a2; B = 1; D = PL.d2;
-        }
-        C = 0;  // and ends here
-      }
+      G.rows_in(LS.s[si], lp, pos, Pc, Pn, Mi, e, A, B, C, D);
     }
   };
+
+  // Row 2*pos + e of the line system at line position lp, for a cell pos of
+  // segment d with its preindex values Pc, those of the next cell Pn (Pc at
+  // the segment's last cell) and its momentum coefficients Mi.
+  __device__ void rows_in(const SegD& d, int lp, int pos, const PreT<R>& Pc, const PreT<R>& Pn,
+                          const MomT<R>& Mi, int e, R& A, R& B, R& C, R& D) const {
+    const int r = 2 * pos + e;
+    if (r < d.off || r > d.rend) {
+      A = 0; B = 1; C = 0; D = 0;
+      return;
+    }
+    const bool even = (r & 1) == 0;
+    if ((bool)d.ran == even) {
+      const PreT<R>& P = d.ran ? Pc : Pn;
+      A = P.a2; B = 1; C = P.c2; D = P.d2;
+    } else {
+      A = Mi.a1; B = Mi.b1; C = Mi.c1; D = Mi.d1;
+    }
+    if (r == d.off) {
+      if (d.ran) {
+        if (d.qfirst) {
+          const R ub = DIR == 0 ? S.ubt[lp] : S.vbd[lp];
+          D = Pc.d2 - Pc.a2 * ub;
+        } else {
+          D = Pc.d2;
+        }
+      } else {
+        const R TZ_l = R(S.tz[at(lp, d.first)]);
+        D = Mi.d1 - Mi.a1 * TZ_l;
+      }
+      A = 0;  // the system starts here
+    }
+    if (r == d.rend) {
+      const PreT<R>& PL = (pos == d.last) ? Pc : Pn;
+      if (d.last_kind == 1) {
+        const R ub = DIR == 0 ? S.ubp[lp] : S.vbt[lp];
+        A = PL.a2; B = 1; D = PL.d2 - PL.c2 * ub;
+      } else if (d.last_kind == 2) {
+        const R TZ_r = R(S.tz[at(lp, d.last)]);
+        A = Mi.a1; B = Mi.b1; D = Mi.d1 - Mi.c1 * TZ_r;
+      } else {
+        A = PL.a2; B = 1; D = PL.d2;
+      }
+      C = 0;  // and ends here
+    }
+  }
 
   // Writes each solved unknown to t_z / t_u (t_v) as the extraction does.
   // FWD: the unknowns come in increasing order (init_fwd), else decreasing.
@@ -212,29 +219,35 @@ struct HydroGen {
         while (si >= 0 && LS.s[si].first > pos) --si;
       }
       if (si < 0) return;
-      const SegD& d = LS.s[si];
-      if (pos > d.last || r < d.off || r > d.rend) return;
-      if (r == d.rend) xlast[si] = x;
-      R* vel = G.vel();
-      if (d.ran) {
-        const int i = r >> 1;
-        if (i < d.last && G.extract_ok(i)) {
-          if (r & 1) vel[G.at(lp, i)] = x;
-          else G.S.tz[G.at(lp, i)] = x;
-        }
+      G.store_in(LS.s[si], xlast + si, lp, q, x);
+    }
+  };
+
+  // The extraction of unknown q (row q + 4) of segment d on line position
+  // lp; the segment's last row also goes to *xl for the end fix-up.
+  __device__ void store_in(const SegD& d, double* xl, int lp, int q, double x) const {
+    const int r = q + 4, pos = r >> 1;
+    if (pos > d.last || r < d.off || r > d.rend) return;
+    if (r == d.rend) *xl = x;
+    R* v = vel_ptr();
+    if (d.ran) {
+      const int i = r >> 1;
+      if (i < d.last && extract_ok(i)) {
+        if (r & 1) v[at(lp, i)] = x;
+        else S.tz[at(lp, i)] = x;
+      }
+    } else {
+      if (r == 2 * d.first) {
+        if (extract_ok(d.first)) v[at(lp, d.first)] = x;
       } else {
-        if (r == 2 * d.first) {
-          if (G.extract_ok(d.first)) vel[G.at(lp, d.first)] = x;
-        } else {
-          const int i = (r + 1) >> 1;
-          if (i > d.first && i < d.last && G.extract_ok(i)) {
-            if (r & 1) G.S.tz[G.at(lp, i)] = x;
-            else vel[G.at(lp, i)] = x;
-          }
+        const int i = (r + 1) >> 1;
+        if (i > d.first && i < d.last && extract_ok(i)) {
+          if (r & 1) S.tz[at(lp, i)] = x;
+          else v[at(lp, i)] = x;
         }
       }
     }
-  };
+  }
 
   // Segment ends (_uzSolver_extract_solution :558-601 / _vzSolver_ :488-536).
   __device__ void fixup(const LineSeg& LS, const double* xlast, int line, int s) const {
@@ -460,33 +473,40 @@ struct FSGen {
         A = 0; B = 1; C = 0; D = 0;
         return;
       }
-      const SegD& d = LS.s[si];
-      // the row as k_fs_rows wrote it, then the segment's end conditions
-      {
-        const size_t n = (size_t)G.S.W * G.S.H;
-        const R* q = G.S.pre + G.at(lp, pos);
-        A = q[0];
-        B = q[n];
-        C = q[2 * n];
-        D = q[3 * n];
-      }
-      const R vel_p = pos == d.first + 1 ? G.vel()[G.at(lp, d.first)] : R(1);
-      const R* vel = G.vel();
-      if (pos == d.first + 1) {
-        // the velocity at the segment's first cell is the previous cell's
-        if (d.br1 || vel_p == 0) B = B + A;
-        else D = D - A * G.S.FS[G.at(lp, d.first)];
-        A = 0;
-      }
-      if (pos == d.last - 1) {
-        // '&&' in the i-sweep (sediment_transport.cpp:304), '||' in the j-sweep (:153)
-        const bool zero = vel[G.at(lp, d.last)] == 0;
-        if (DIR == 0 ? (d.br2 && zero) : (d.br2 || zero)) B = B + C;
-        else D = D - C * G.S.FS[G.at(lp, d.last)];
-        C = 0;
-      }
+      G.row_in(LS.s[si], lp, pos, A, B, C, D);
     }
   };
+
+  // The row of cell pos of line position lp inside segment d: as k_fs_rows
+  // wrote it, then the segment's end conditions.
+  __device__ void row_in(const SegD& d, int lp, int pos, R& A, R& B, R& C, R& D) const {
+    load_row(lp, pos, A, B, C, D);
+    end_rows(d, lp, pos, A, B, C, D);
+  }
+  __device__ void load_row(int lp, int pos, R& A, R& B, R& C, R& D) const {
+    const size_t n = (size_t)S.W * S.H;
+    const R* q = S.pre + at(lp, pos);
+    A = q[0];
+    B = q[n];
+    C = q[2 * n];
+    D = q[3 * n];
+  }
+  __device__ void end_rows(const SegD& d, int lp, int pos, R& A, R& B, R& C, R& D) const {
+    const R* v = vel();
+    if (pos == d.first + 1) {
+      // the velocity at the segment's first cell is the previous cell's
+      if (d.br1 || v[at(lp, d.first)] == 0) B = B + A;
+      else D = D - A * S.FS[at(lp, d.first)];
+      A = 0;
+    }
+    if (pos == d.last - 1) {
+      // '&&' in the i-sweep (sediment_transport.cpp:304), '||' in the j-sweep (:153)
+      const bool zero = v[at(lp, d.last)] == 0;
+      if (DIR == 0 ? (d.br2 && zero) : (d.br2 || zero)) B = B + C;
+      else D = D - C * S.FS[at(lp, d.last)];
+      C = 0;
+    }
+  }
 
   // FWD: the unknowns come in increasing order (init_fwd), else decreasing.
   struct Emitter {
