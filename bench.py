@@ -50,7 +50,10 @@ BYTES_PER_CELL_STEP = {  # algorithmic bytes per interior cell and full step
 #     Tsxw (Tsyw) = 9 x 8 B; write t_z and t_u (t_v) = 2 x 8 B  -> 88 B
 #   concentration sweeps: read FS, H_moi, VTH, Fw, t_u, t_v, Htdu, Htdv, Kx,
 #     Ky = 10 x 8 B; write tFS = 8 B                             -> 88 B
-# The line-solver scratch (3 doubles per unknown, L2-resident) is not counted.
+#     (a concentration sweep is timed over its two launches: the per-cell
+#     row kernel k_fs_rows and the line solve)
+# The line-solver scratch (3 doubles per unknown) and the concentration rows
+# passed between the two launches (4 doubles per cell) are not counted.
 # In the FP32 form z is read (8 B) and t_z written (8 B) in FP64, the other
 # fields are 4 B: hydraulic 8 + 8 x 4 + 8 + 4 = 52 B, concentration 11 x 4 = 44 B.
 SWEEP_BYTES_PER_CELL = {
@@ -890,6 +893,50 @@ def measure_forms(H, sim, bundle, dev, args, fp64_ms, window=10):
             entry["ms_per_step"] = fp64_ms
         out[name] = entry
         f.close()
+    try:
+        out["batched"] = measure_batched_forms(H, dev, args,
+                                               bundle["meta"]["cells"] / (fp64_ms * 1e-3))
+    except Exception as e:  # reported, not fatal to the benchmark line
+        out["batched"] = {"error": str(e)[:300]}
+    return out
+
+
+def measure_batched_forms(H, dev, args, fp64_plain_value, nmem=64, steps=10):
+    """The batched forms of the ensemble workload (64 scenarios of 1024x512,
+    per-member bathymetry, Manning, inflow and tide; sediment sweeps and the
+    bed change from t = 300 s), each form one graph launch per step over
+    every member: the members spun up to t = 300 s untimed, then the device
+    time per step (CUDA events over `steps` steps after 3 warm-up steps),
+    cell-steps/s, and the ratio of each to the plain FP64 form of the
+    benchmarked workload (fp64_plain_value, cell-steps/s). The errors of the
+    FP32 forms against the oracle are those of the single-scenario forms
+    above (the same kernels, batched)."""
+    import torch
+    from hydist_c_b200 import scenario as S
+    out = {"workload": ENSEMBLE, "members": nmem, "steps": steps}
+    for name, prec in (("fp64", H.FP64), ("fp32", H.FP32), ("fp32-refine", H.FP32_REFINE)):
+        bundles = [S.config3_member(k, seed=20263000) for k in range(nmem)]
+        cells = sum(b["meta"]["cells"] for b in bundles)
+        sims = [H.Simulation(b, device=dev, precision=prec) for b in bundles]
+        ens = H.Ensemble(sims)
+        ens.step(150 + 3)  # to the sediment start, then warm-up
+        ens.sync()
+        stream = torch.cuda.ExternalStream(ens.stream, device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        ens.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ens.sync()
+        ms = e0.elapsed_time(e1) / steps
+        v = cells * steps / (e0.elapsed_time(e1) * 1e-3)
+        out[name] = {"ms_per_step": ms, "value": v, "vs_fp64_plain": v / fp64_plain_value}
+        ens.close()
+        for m in sims:
+            m.close()
+    out["fp32-refine"]["vs_fp64_batched"] = out["fp32-refine"]["value"] / out["fp64"]["value"]
+    out["fp32"]["vs_fp64_batched"] = out["fp32"]["value"] / out["fp64"]["value"]
     return out
 
 
