@@ -72,14 +72,25 @@ constexpr size_t line_smem(bool refine) {
 }
 
 // Gen::MIN_BLOCKS: resident CTAs per SM the P = 128 solver is compiled for
-// (2 caps registers at 64 per thread).
+// (2 caps registers at 64 per thread). The solvers for shorter lines (fewer
+// chunks, smaller CTAs) are compiled for at least 512 threads per SM, the
+// row sweeps' for as many as their P = 128 solver (at most 32 CTAs): left
+// uncapped, the row sweeps' short-line solvers took up to 198 registers and
+// ran 8 warps per SM; the column sweeps' spill under the 64-register cap.
+template <class Gen, int P, int L>
+constexpr int line_min_blocks() {
+  constexpr int k = (L * P >= 512) ? 1 : 512 / (L * P);
+  constexpr int b = Gen::DIRECTION == 1 ? k * Gen::MIN_BLOCKS : k;
+  return (P == 128 && L == LPB) ? Gen::MIN_BLOCKS : (b > 32 ? 32 : b);
+}
+
 // The launch solves line groups 0 .. ngroups-1 of L lines from line0 on.
 // BATCH: the groups of every member of a batch, gpm groups per member (the
 // member of group g is g / gpm, its state and coefficients bound into a
 // copy of G0 for that group); the persistent grid walks them all, each CTA
 // with its own scratch slot of G0's scratch.
 template <class Gen, int P, int L = LPB, int BATCH = 0>
-__global__ void __launch_bounds__(L * P, (P == 128 && L == LPB) ? Gen::MIN_BLOCKS : 1)
+__global__ void __launch_bounds__(L * P, line_min_blocks<Gen, P, L>())
     k_line_solve(Gen G0, int line0, int ngroups, Batch<typename Gen::Real> bt, int gpm) {
   using R = typename Gen::Real;
   // sizes and scratch from G0: the same for every member of a batch

@@ -378,6 +378,20 @@ static int launch_lines(const Gen& G, int P, int lines, int lslots, cudaStream_t
   return 1;
 }
 
+// Scratch slots for a sweep of lines of `unknowns` unknowns in P chunks:
+// the scratch holds StateT::lslots slots of lines of 2*max(M, N) unknowns,
+// so a sweep of shorter lines has proportionally more. Only the solvers of
+// fewer than 128 chunks (smaller CTAs, more of them resident per SM) use
+// them: their grid may then exceed the CTAs resident at once, the extra
+// CTAs starting as earlier ones finish. (For the 128-chunk solvers the
+// persistent grid of lslots CTAs measured as fast or faster.)
+template <class R>
+static int sweep_slots(const StateT<R>& S, int unknowns, int P) {
+  if (P >= 128) return S.lslots;
+  const int umax = 2 * std::max(S.M, S.N);
+  return S.lslots * std::max(1, umax / std::max(unknowns, 1));
+}
+
 template <int DIR, class R, bool REF>
 static int launch_dir(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, int P,
                       const Batch<R>& b) {
@@ -387,7 +401,8 @@ static int launch_dir(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st, in
   G.lp0 = DIR == 0 ? S.x_lo : S.y_lo;
   G.nl = DIR == 0 ? S.x_hi - S.x_lo + 1 : S.N - S.y_lo + 1;
   if (G.nl <= 0) return 0;
-  return launch_lines(G, P, G.nl, S.lslots, st, b);
+  const int ncells = DIR == 0 ? S.N - 1 : S.M - 1;
+  return launch_lines(G, P, G.nl, sweep_slots(S, 2 * ncells, P), st, b);
 }
 
 // ---------------------------------------------------------------------
@@ -554,12 +569,13 @@ int launch_fs_sweep(const StateT<R>& S, const CoefT<R>& c, int dir, cudaStream_t
   const int lines = dir == 0 ? S.M - 3 : S.N - 3;
   if (lines <= 0) return 0;
   const int P = line_chunks(ncells, 4);
+  const int slots = sweep_slots(S, ncells, P);
   if (dir == 0) {
-    if (S.refine) return launch_lines(FSGen<0, R, true>{S, c, S.lscratch}, P, lines, S.lslots, st, b);
-    return launch_lines(FSGen<0, R, false>{S, c, S.lscratch}, P, lines, S.lslots, st, b);
+    if (S.refine) return launch_lines(FSGen<0, R, true>{S, c, S.lscratch}, P, lines, slots, st, b);
+    return launch_lines(FSGen<0, R, false>{S, c, S.lscratch}, P, lines, slots, st, b);
   }
-  if (S.refine) return launch_lines(FSGen<1, R, true>{S, c, S.lscratch}, P, lines, S.lslots, st, b);
-  return launch_lines(FSGen<1, R, false>{S, c, S.lscratch}, P, lines, S.lslots, st, b);
+  if (S.refine) return launch_lines(FSGen<1, R, true>{S, c, S.lscratch}, P, lines, slots, st, b);
+  return launch_lines(FSGen<1, R, false>{S, c, S.lscratch}, P, lines, slots, st, b);
 }
 
 template <class R>
