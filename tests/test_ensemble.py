@@ -61,7 +61,7 @@ def test_ensemble_equals_members_alone(hyd):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", ["FP64", "FP32_REFINE"])
+@pytest.mark.parametrize("precision", ["FP64", "FP32", "FP32_REFINE"])
 def test_batched_ensemble_launches_once_per_kernel(hyd, precision):
     """Members of one mesh size in the same phase share every launch (one
     launch per kernel of the step for the whole batch), with each member's
