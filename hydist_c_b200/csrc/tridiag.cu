@@ -517,7 +517,7 @@ __global__ void __launch_bounds__(GT_WARPS * 32) k_gtsv_warp(
     const T* __restrict__ b, T* __restrict__ x, const int* __restrict__ off,
     const int* __restrict__ len, const int* __restrict__ list, const int* __restrict__ count,
     int slice) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* base = reinterpret_cast<T*>(smem_raw) + (size_t)warp * 4 * slice;
   const int cnt = *count;
