@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(L * P, line_min_blocks<Gen, P, L>())
               cp = C * m;
             }
             const size_t o = (size_t)(q0 + s) * L + l;
-            if constexpr (Gen::REFINE) {
+            if constexpr (Gen::REFINE && !Gen::ROWS_AGAIN) {
               // the interior rows, for the residual
               scr[3 * UL + o] = A;
               scr[4 * UL + o] = B;
@@ -270,18 +270,33 @@ __global__ void __launch_bounds__(L * P, line_min_blocks<Gen, P, L>())
       // the same Schur complement as pass A, so the reduction reuses pass
       // A's PCR multipliers; the chunk interiors are then substituted
       // forward and x + d is emitted in FP64.
-      R* sA = scr + 3 * UL;
+      // Gen::ROWS_AGAIN: the rows are read again from where the generator
+      // read them in pass A (the same values), not from the scratch, and
+      // (a, h, w) go over the c', v' of the row they belong to (consumed by
+      // then) and a fourth scratch array; else the stored rows' A, D, C.
+      R* sA = Gen::ROWS_AGAIN ? sc_c : scr + 3 * UL;
       R* sB = scr + 4 * UL;
-      R* sC = scr + 5 * UL;
-      R* sD = scr + 6 * UL;
+      R* sC = Gen::ROWS_AGAIN ? sc_v : scr + 5 * UL;
+      R* sD = Gen::ROWS_AGAIN ? scr + 3 * UL : scr + 6 * UL;
+      typename Gen::RowCursor cur;
+      cur.init(G, LS, line);
       const R xr = sh.xsep[cidx];
       const R xl = (k > 0) ? sh.xsep[cidx - L] : R(0);
       R x_before_sep = 0;  // x of the chunk's last interior unknown
       R ha = 0, hy = 0, hw = -1;  // (a, h, w) of the row below the one eliminated
       R gy = 0, gw = 0, Q = 1;    // d of the last interior unknown: gy - gw d_R + Q d_L
-      auto eliminate = [&](size_t o, R xm, R x, R xp) {
-        const R A = sA[o], B = sB[o], C = sC[o];
-        const R r = (R)((double)sD[o] - (double)A * (double)xm - (double)B * (double)x -
+      // row q (slot o), q decreasing from call to call
+      auto eliminate = [&](size_t o, int q, R xm, R x, R xp) {
+        R A, B, C, D;
+        if constexpr (Gen::ROWS_AGAIN) {
+          cur.row(G, LS, q, A, B, C, D);
+        } else {
+          A = sA[o];
+          B = sB[o];
+          C = sC[o];
+          D = sD[o];
+        }
+        const R r = (R)((double)D - (double)A * (double)xm - (double)B * (double)x -
                         (double)C * (double)xp);
         const R m = rcp(B - C * ha);
         ha = A * m;
@@ -301,13 +316,13 @@ __global__ void __launch_bounds__(L * P, line_min_blocks<Gen, P, L>())
           const R x = sc_y[o] + sc_v[o] * xl - sc_c[o] * x1;
           sc_y[o] = x;
           if (t == nu - 2) x_before_sep = x;
-          else eliminate(o + L, x, x1, x2);
+          else eliminate(o + L, q0 + t + 1, x, x1, x2);
           x2 = x1;
           x1 = x;
         }
         // the first unknown: its left neighbour is the previous separator
         // (none at the line's start)
-        if (nu >= 2) eliminate((size_t)q0 * L + l, q0 > 0 ? xl : R(0), x1, x2);
+        if (nu >= 2) eliminate((size_t)q0 * L + l, q0, q0 > 0 ? xl : R(0), x1, x2);
       }
       // the first interior unknown's constant term, for the previous chunk
       sh.tri[0][cidx] = hy;
@@ -318,8 +333,13 @@ __global__ void __launch_bounds__(L * P, line_min_blocks<Gen, P, L>())
         // unknown (none at the line's end)
         const int q = q0 + nu - 1;
         const size_t o = (size_t)q * L + l;
-        const R xm = nu >= 2 ? x_before_sep : (q > 0 ? sc_y[o - L] : R(0));
-        const R xp = q + 1 < U ? sc_y[o + L] : R(0);
+        // the unknown left of the separator: the chunk's last interior one,
+        // or the previous chunk's separator; right of it: the next chunk's
+        // first unknown, its separator where that chunk holds nothing else
+        const int nu_next = (k + 1 < P)
+            ? ((int)(((long long)(k + 2) * ncells) / P) - c1) * upc : 0;
+        const R xm = nu >= 2 ? x_before_sep : (q > 0 ? xl : R(0));
+        const R xp = q + 1 < U ? (nu_next >= 2 ? sc_y[o + L] : sh.xsep[cidx + L]) : R(0);
         const R as = sh.sep[0][cidx], bs = sh.sep[1][cidx], cs = sh.sep[2][cidx],
                 ds = sh.sep[3][cidx];
         const R rs = (R)((double)ds - (double)as * (double)xm - (double)bs * (double)xr -

@@ -31,6 +31,8 @@ template <int DIR, class R, bool REF = false>
 struct HydroGen {
   using Real = R;
   static constexpr bool REFINE = REF;
+  // the rows are generated from the stencils: the refinement keeps them
+  static constexpr bool ROWS_AGAIN = false;
   static constexpr int SCRATCH_ARRAYS = REFINE ? 7 : 3;
   static constexpr int UPC = 2;
   static constexpr int DIRECTION = DIR;
@@ -197,6 +199,12 @@ struct HydroGen {
       C = 0;  // and ends here
     }
   }
+
+  // (the refinement reads the stored rows: no cursor over them)
+  struct RowCursor {
+    __device__ void init(const HydroGen&, const LineSeg&, int) {}
+    __device__ void row(const HydroGen&, const LineSeg&, int, R&, R&, R&, R&) {}
+  };
 
   // Writes each solved unknown to t_z / t_u (t_v) as the extraction does.
   // FWD: the unknowns come in increasing order (init_fwd), else decreasing.
@@ -414,7 +422,9 @@ template <int DIR, class R, bool REF = false>
 struct FSGen {
   using Real = R;
   static constexpr bool REFINE = REF;
-  static constexpr int SCRATCH_ARRAYS = REFINE ? 7 : 3;
+  // the rows are in StateT::pre (k_fs_rows): the refinement reads them again
+  static constexpr bool ROWS_AGAIN = true;
+  static constexpr int SCRATCH_ARRAYS = REFINE ? 4 : 3;
   static constexpr int UPC = 1;
   static constexpr int DIRECTION = DIR;
   // two CTAs per SM in both directions and precisions
@@ -522,6 +532,25 @@ struct FSGen {
       C = 0;
     }
   }
+
+  // The rows of a line again, unknown by unknown in decreasing order (the
+  // refinement's residuals): the same values the Walker gave pass A.
+  struct RowCursor {
+    int lp, si;
+    __device__ void init(const FSGen& G, const LineSeg& LS, int line) {
+      lp = line + 3;
+      si = LS.nseg - 1;
+    }
+    __device__ void row(const FSGen& G, const LineSeg& LS, int q, R& A, R& B, R& C, R& D) {
+      const int pos = q + 2;
+      while (si >= 0 && LS.s[si].first > pos) --si;
+      if (si < 0 || pos < LS.s[si].off || pos > LS.s[si].rend) {
+        A = 0; B = 1; C = 0; D = 0;
+        return;
+      }
+      G.row_in(LS.s[si], lp, pos, A, B, C, D);
+    }
+  };
 
   // FWD: the unknowns come in increasing order (init_fwd), else decreasing.
   struct Emitter {
