@@ -20,8 +20,9 @@
 //      horizon are retired: their state stays on the device (and counts
 //      against the budget) until released, so results can be downloaded.
 // Requests arriving between rounds join at the next round (continuous
-// batching). Each request's arithmetic is that of its own handle, so its
-// result does not depend on what runs beside it.
+// batching). A request stepped alone gives bit for bit what its scenario
+// gives alone; one stepped in a batch gives it to rounding (the batched
+// kernels are separately compiled variants of the same arithmetic).
 #include <cuda_runtime.h>
 
 #include <cstring>

@@ -312,7 +312,9 @@ int hydist_ensemble_destroy(HydistEnsemble* e);
  * retires those at their horizon and returns their ids. A retired request keeps its device state (and its share
  * of the budget) until hydist_server_release; hydist_server_handle gives its
  * handle for hydist_download / hydist_mass. Each request is computed by its
- * own handle, so its result is the same alone and in the mix. */
+ * own handle: its result is the same alone and in the mix, bit for bit where
+ * it steps alone, to rounding where its group steps as a batch (as for
+ * ensembles). */
 typedef struct HydistServer HydistServer;
 enum HydistRequestState { HYDIST_RQ_QUEUED = 0, HYDIST_RQ_ACTIVE = 1, HYDIST_RQ_DONE = 2 };
 /* Device bytes hydist_create allocates for an M x N scenario (upper bound). */
