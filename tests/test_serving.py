@@ -60,3 +60,47 @@ def test_results_same_alone_and_in_the_mix(hyd):
     with pytest.raises(hyd.HydistError, match="BUDGET"):
         tiny.submit(_req(3, 64, 32), 10)
     tiny.close()
+
+
+@pytest.mark.gpu
+def test_same_size_requests_step_as_one_batch(hyd):
+    """Requests of one mesh size admitted together and advancing alike are
+    stepped as one batch (one launch per kernel for all of them: the batch's
+    launches are counted once, on its first member); each result agrees with
+    its scenario solved alone to rounding (the batched kernels are separately
+    compiled variants of the same arithmetic)."""
+    import ctypes as C
+    from hydist_c_b200 import Server, capi
+    n = 40
+    alone = {}
+    for k in range(3):
+        sim = hyd.Simulation(_req(10 + k, 64, 32))
+        sim.step(n)
+        alone[k] = {f: sim.download(f) for f in ("u", "v", "z", "FS")}
+        solo_launches = sim.kernel_launches
+        sim.close()
+    srv = Server(8 * Server.scenario_bytes(32, 64), steps_per_round=20)
+    ids = {srv.submit(_req(10 + k, 64, 32), n): k for k in range(3)}
+    results, launches = {}, {}
+    lib = capi.load_library()
+    for _ in range(10):
+        for rid in srv.round():
+            k = ids[rid]
+            results[k] = {f: srv.download(rid, f) for f in ("u", "v", "z", "FS")}
+            v = C.c_int64()
+            capi.check(lib, lib.hydist_kernel_launches(C.c_void_p(lib.hydist_server_handle(srv._s, rid)),
+                                                       C.byref(v)), "hydist_kernel_launches")
+            launches[k] = v.value
+        if len(results) == 3:
+            break
+    assert sorted(results) == [0, 1, 2]
+    for k, res in results.items():
+        for f, ref in alone[k].items():
+            scale = max(float(np.abs(ref).max()), 1e-30)
+            d = float(np.abs(res[f] - ref).max()) / scale
+            assert d <= 1e-11, (k, f, d)
+    # the three requests' steps launched about as many kernels as one
+    # request's alone (each handle's own set-up launches aside), not three
+    # times as many
+    assert sum(launches.values()) < 2 * solo_launches, (launches, solo_launches)
+    srv.close()
