@@ -605,6 +605,11 @@ struct DevInfo {
   bool init = false;
   int table[2][GT_NB] = {};  // autotuned solver per dtype and band (0: not tuned)
   DevScratch scr;
+  // the bands of a batch run side by side: one stream per band, forked from
+  // the caller's stream and joined back (created on first use, kept)
+  cudaStream_t band_st[GT_NB] = {};
+  cudaEvent_t fork = nullptr, join[GT_NB] = {};
+  bool streams = false;
 };
 
 std::mutex g_mu;
@@ -796,6 +801,21 @@ int ensure_scratch(DevScratch& s, size_t w_bytes, size_t nsys, size_t flag_bytes
   return HYDIST_OK;
 }
 
+// the per-band streams and events of a device (false if they cannot be made:
+// the bands then run one after another on the caller's stream)
+bool band_streams(DevInfo& D) {
+  if (D.streams) return true;
+  for (int k = 0; k < GT_NB; ++k) {
+    if (!D.band_st[k] && cudaStreamCreateWithFlags(&D.band_st[k], cudaStreamNonBlocking) != cudaSuccess)
+      return false;
+    if (!D.join[k] && cudaEventCreateWithFlags(&D.join[k], cudaEventDisableTiming) != cudaSuccess)
+      return false;
+  }
+  if (!D.fork && cudaEventCreateWithFlags(&D.fork, cudaEventDisableTiming) != cudaSuccess) return false;
+  D.streams = true;
+  return true;
+}
+
 // one batched solve with a given solver per band (table[b])
 template <class T>
 int solve_batch(const T* dl, const T* d, const T* du, const T* b, T* x, const int* off,
@@ -834,14 +854,29 @@ int solve_batch(const T* dl, const T* d, const T* du, const T* b, T* x, const in
     if (rc != HYDIST_OK) return rc;
   }
   bool staged = false;  // a bulk-staged CTA solver ran
+  // the bands' solves are independent (disjoint systems, per-band lists,
+  // per-system scratch): each non-empty band on its own stream, so that the
+  // short bands' launches and the long bands' tails overlap
+  int nonempty = 0;
+  for (int bnd = 0; bnd < GT_NB; ++bnd) nonempty += counts[bnd] > 0;
+  const bool side = nonempty > 1 && band_streams(D);
+  if (side && cudaEventRecord(D.fork, st) != cudaSuccess) return HYDIST_ERR_CUDA;
   for (int bnd = 0; bnd < GT_NB; ++bnd) {
+    if (counts[bnd] == 0) continue;
+    cudaStream_t bs = st;
+    if (side) {
+      bs = D.band_st[bnd];
+      if (cudaStreamWaitEvent(bs, D.fork, 0) != cudaSuccess) return HYDIST_ERR_CUDA;
+    }
     rc = launch_band<T>(table[bnd], bnd, dl, d, du, b, x, (T*)D.scr.w, D.scr.flags, off, len,
                         D.scr.lists + (size_t)bnd * nsys, D.scr.counts + bnd,
-                        D.scr.counts + GT_NB + 2, counts[bnd], D, st);
+                        D.scr.counts + GT_NB + 2, counts[bnd], D, bs);
+    if (side && (cudaEventRecord(D.join[bnd], bs) != cudaSuccess ||
+                 cudaStreamWaitEvent(st, D.join[bnd], 0) != cudaSuccess))
+      return HYDIST_ERR_CUDA;
     if (rc != HYDIST_OK) return rc;
-    staged |= counts[bnd] > 0 && (table[bnd] == HYDIST_GTSV_PARTITION ||
-                                  table[bnd] == HYDIST_GTSV_PARTITION_512 ||
-                                  table[bnd] == HYDIST_GTSV_PARTITION_128);
+    staged |= table[bnd] == HYDIST_GTSV_PARTITION || table[bnd] == HYDIST_GTSV_PARTITION_512 ||
+              table[bnd] == HYDIST_GTSV_PARTITION_128;
   }
   if (staged) {
     // a CTA whose staging copy never completed left systems unsolved: read

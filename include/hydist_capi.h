@@ -388,8 +388,11 @@ int hydist_kernel_launches(HydistHandle* h, int64_t* count);
  *              not diagonally dominant; never chosen by AUTO.
  * The other solvers do not pivot: they expect diagonally dominant systems,
  * as the ADI sweeps' are.
- * stream is a cudaStream_t (NULL = default stream). Scratch is allocated by
- * the library on first use and grown as needed. The call synchronises the
+ * stream is a cudaStream_t (NULL = default stream). The bands' solves run
+ * side by side on the library's own streams, forked from `stream` and joined
+ * back into it, so work queued on `stream` after the call waits for all of
+ * them. Scratch is allocated by the library on first use and grown as
+ * needed. The call synchronises the
  * stream once to read the band sizes and the packed extent, and, when a
  * shared-memory CTA solver (PARTITION*) ran, once more at the end: every
  * wait of those solvers for a system's rows is bounded, and a CTA that gave
