@@ -1,10 +1,11 @@
 // linesolve.cuh -- partitioned tridiagonal line solver for the ADI sweeps.
 //
-// One CTA solves L adjacent lines at a time (LPB = 4; a persistent loop
-// walks the line groups). Each line is split into P chunks of consecutive
-// cells; thread (chunk k, line l) = threadIdx.x = k*L + l, so with L = 4 a
-// warp covers 8 chunks x 4 adjacent lines and every global access of the x
-// sweep reads 4 adjacent columns (one 32-byte sector).
+// One CTA solves L adjacent lines at a time (LPB = 4; XPB = 8 for the
+// 128-chunk column sweeps; a persistent loop walks the line groups). Each
+// line is split into P chunks of consecutive cells; thread (chunk k, line l)
+// = threadIdx.x = k*L + l, so with L = 4 a warp covers 8 chunks x 4 adjacent
+// lines and every global access of a column sweep reads 4 adjacent columns
+// (one 32-byte sector), with L = 8 4 chunks x 8 columns (64 bytes).
 //
 // The line's tridiagonal system (all wet segments of the line, identity rows
 // between them) is solved by the partition method:
@@ -32,6 +33,7 @@
 namespace hyd {
 
 constexpr int LPB = 4;  // lines per CTA
+constexpr int XPB = 8;  // lines per CTA of the 128-chunk column sweeps
 
 // One wet segment of a line, with its system layout.
 struct SegD {
