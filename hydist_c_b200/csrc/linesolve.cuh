@@ -83,6 +83,7 @@ template <class Gen, int P, int L>
 constexpr int line_min_blocks() {
   constexpr int k = (L * P >= 512) ? 1 : 512 / (L * P);
   constexpr int b = Gen::DIRECTION == 1 ? k * Gen::MIN_BLOCKS : k;
+  if (L * P >= 1024) return 1;  // one CTA per SM, 64 registers per thread
   return (P == 128 && L == LPB) ? Gen::MIN_BLOCKS : (b > 32 ? 32 : b);
 }
 
