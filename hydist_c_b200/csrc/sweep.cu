@@ -363,20 +363,21 @@ template <class Gen>
 static int launch_lines(const Gen& G, int P, int lines, int lslots, cudaStream_t st,
                         const Batch<typename Gen::Real>& b = {}) {
   if constexpr (Gen::DIRECTION == 1) {
-    if (P == 64 || (P == 128 && Gen::UPC == 1 && Gen::REFINE)) {
-      // row sweeps of 64 chunks (rows of 256 to 511 cells), and the refined
-      // concentration row sweep of 128: groups of 8 adjacent rows (their
+    if (P == 64 || (P == 128 && Gen::UPC == 1 && sizeof(typename Gen::Real) == 4)) {
+      // row sweeps of 64 chunks (rows of 256 to 511 cells), and the FP32
+      // concentration row sweeps of 128: groups of 8 adjacent rows (their
       // stencil rows shared through L1 by twice as many lines). The
       // 64-member ensemble of 1024x512 in FP32 with refinement: 13.64 ->
-      // 12.63 ms per step (FP64 unchanged); the refined concentration y
-      // sweep of 2048x1024 0.122 -> 0.108 ms (the FP64 one 3 us slower, so
-      // it keeps 4-row groups). A group's scratch slot is two 4-line slots.
+      // 12.63 ms per step (FP64 unchanged); the concentration y sweep of
+      // 2048x1024 0.122 -> 0.108 ms refined, 0.087 -> 0.079 ms in FP32 (the
+      // FP64 one 3 us slower, so it keeps 4-row groups). A group's scratch
+      // slot is two 4-line slots.
       const int g8 = cdiv(lines, XPB);
       const long long total = (long long)g8 * std::max(b.n, 1);
       const int grid = (int)std::min<long long>(total, lslots / 2);
       if (P == 64) {
         launch_gen<Gen, 64, XPB>(G, st, grid, 0, (int)total, b, b.n > 0 ? g8 : 0);
-      } else if constexpr (Gen::UPC == 1 && Gen::REFINE) {
+      } else if constexpr (Gen::UPC == 1 && sizeof(typename Gen::Real) == 4) {
         launch_gen<Gen, 128, XPB>(G, st, grid, 0, (int)total, b, b.n > 0 ? g8 : 0);
       }
       return 1;
