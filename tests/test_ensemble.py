@@ -100,3 +100,32 @@ def test_batched_ensemble_launches_once_per_kernel(hyd, precision):
     ens.close()
     for sim in mix + [solo]:
         sim.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["FP64", "FP32_REFINE"])
+def test_batched_eight_line_groups(hyd, precision):
+    """Members whose columns take the 128-chunk solver (512 cells or more)
+    and whose rows take the 64-chunk one (256 to 511 cells), both run in
+    groups of 8 lines: stepped as one batch they agree with each scenario
+    alone to rounding."""
+    from hydist_c_b200 import scenario as S
+    prec = getattr(hyd, precision)
+    members = [S.make_channel(N=600, M=300, seed=SEEDS[k], dx=10.0, dt=2.0, hours=1.0,
+                              sediment=True, sediment_start=0.0) for k in range(3)]
+    alone = []
+    for b in members:
+        sim = hyd.Simulation(b, precision=prec)
+        sim.step(6)
+        alone.append({f: sim.download(f) for f in ("u", "v", "z", "FS")})
+        sim.close()
+    mix = [hyd.Simulation(b, precision=prec) for b in members]
+    ens = hyd.Ensemble(mix)
+    ens.step(6)
+    ens.sync()
+    for k, sim in enumerate(mix):
+        for f, ref in alone[k].items():
+            _close(sim.download(f), ref, BATCH_RTOL[precision], f"member {k} {f}")
+    ens.close()
+    for sim in mix:
+        sim.close()
