@@ -362,6 +362,16 @@ static int resident_slots() {
 template <class Gen>
 static int launch_lines(const Gen& G, int P, int lines, int lslots, cudaStream_t st,
                         const Batch<typename Gen::Real>& b = {}) {
+  if constexpr (Gen::DIRECTION == 1 && Gen::UPC == 2 && Gen::REFINE) {
+    if (P == 128 && b.n == 0) {
+      // the refined hydraulic row sweep: groups of 8 rows of 64 chunks (one
+      // 512-thread CTA per SM): 0.210 -> 0.204 ms on 2048x1024 (the FP64 and
+      // FP32 ones slower that way: 0.231 / 0.153 against 0.173 / 0.131 ms)
+      const int g8 = cdiv(lines, XPB);
+      launch_gen<Gen, 64, XPB>(G, st, std::min(g8, lslots / 2), 0, g8);
+      return 1;
+    }
+  }
   if constexpr (Gen::DIRECTION == 1) {
     if (P == 64 || (P == 128 && Gen::UPC == 1 && sizeof(typename Gen::Real) == 4)) {
       // row sweeps of 64 chunks (rows of 256 to 511 cells), and the FP32
