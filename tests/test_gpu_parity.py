@@ -375,15 +375,17 @@ def test_row_sweep_tail_launch_matches_oracle(hyd, oracle_mod):
 
 
 @pytest.mark.parametrize("form", ["FP64", "FP32_REFINE"])
-def test_mid_length_rows_match_oracle(hyd, oracle_mod, form):
+@pytest.mark.parametrize("mesh", [(600, 400), (400, 300)])
+def test_mid_length_rows_match_oracle(hyd, oracle_mod, form, mesh):
     """Rows of 256 to 511 cells (the row sweeps' 64-chunk solvers, run in
-    groups of 8 adjacent rows) and columns of 512 or more (the column
-    sweeps' 128-chunk solvers, groups of 8 adjacent columns): from the
-    oracle's state after 12 steps with the concentration sweeps on, one step
-    on each agrees to 1e-10 in FP64 and to 1e-4 of each field's magnitude in
-    FP32 with refinement."""
-    b = S.make_channel(N=600, M=400, seed=20268100, dx=10.0, dt=2.0, hours=1.0, sediment=True,
-                       sediment_start=0.0)
+    groups of 8 adjacent rows) with columns of 512 or more (the column
+    sweeps' 128-chunk solvers, groups of 8 adjacent columns) or of 256 to
+    511 (64-chunk solvers, in groups of 8 when refined): from the oracle's
+    state after 12 steps with the concentration sweeps on, one step on each
+    agrees to 1e-10 in FP64 and to 1e-4 of each field's magnitude in FP32
+    with refinement."""
+    b = S.make_channel(N=mesh[0], M=mesh[1], seed=20268100, dx=10.0, dt=2.0, hours=1.0,
+                       sediment=True, sediment_start=0.0)
     orc = oracle_mod.OracleSim(b, nthreads=8)
     orc.step(12)
     sim = hyd.Simulation(b, precision=getattr(hyd, form))
