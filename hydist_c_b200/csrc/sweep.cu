@@ -362,6 +362,20 @@ static int resident_slots() {
 template <class Gen>
 static int launch_lines(const Gen& G, int P, int lines, int lslots, cudaStream_t st,
                         const Batch<typename Gen::Real>& b = {}) {
+  if constexpr (Gen::DIRECTION == 1 && Gen::UPC == 2 && !Gen::REFINE &&
+                sizeof(typename Gen::Real) == 4) {
+    if (P == 128) {
+      // the FP32 hydraulic row sweep: groups of 8 rows, one 1024-thread CTA
+      // per SM (its 64 registers as at two 512-thread CTAs): 0.130 -> 0.121
+      // ms on 2048x1024 (the FP64 one, capped from 102 registers, 0.247
+      // against 0.172: it keeps 4-row groups)
+      const int g8 = cdiv(lines, XPB);
+      const long long total = (long long)g8 * std::max(b.n, 1);
+      launch_gen<Gen, 128, XPB>(G, st, (int)std::min<long long>(total, lslots / 2), 0, (int)total,
+                                b, b.n > 0 ? g8 : 0);
+      return 1;
+    }
+  }
   if constexpr (Gen::DIRECTION == 1 && Gen::UPC == 2 && Gen::REFINE) {
     if (P == 128 && b.n == 0) {
       // the refined hydraulic row sweep: groups of 8 rows of 64 chunks (one
