@@ -394,7 +394,7 @@ __device__ void channel_wave_cell(const StateT<R>& S, double dX, double dY, doub
 }
 
 template <class R, int BATCH = 0>
-__global__ void k_boundary(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, double half) {
+__global__ void HYD_CELL_BOUNDS(BATCH) k_boundary(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, double half) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const double dX = (double)c.dX, dY = (double)c.dY;
@@ -588,7 +588,7 @@ __device__ __forceinline__ bool find_seg(const int* dau, const int* cuoi, int n,
 // vSolver driven by solveV (UVZSolver_multithread.cpp:607-663, 961-978);
 // the cell's arithmetic is v_new (explicit.cuh).
 template <class R, int BATCH = 0>
-__global__ void k_solve_v(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+__global__ void HYD_CELL_BOUNDS(BATCH) k_solve_v(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   // the block's cells share one row: its segment table goes to shared memory
@@ -619,7 +619,7 @@ __global__ void k_solve_v(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
 // uSolver driven by solveU (UVZSolver_multithread.cpp:724-795, 938-959);
 // the cell's arithmetic is u_new (explicit.cuh).
 template <class R, int BATCH = 0>
-__global__ void k_solve_u(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+__global__ void HYD_CELL_BOUNDS(BATCH) k_solve_u(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int col = blockIdx.x * blockDim.x + threadIdx.x + 2;
@@ -700,7 +700,7 @@ __device__ __forceinline__ R vth_heso_cell(const StateT<R>& S, const CoefT<R>& c
 // Find_VTH + hesoK on rows 1..vth_hi: nothing between this commit and the
 // concentration sweep changes what they read.
 template <class R, int BATCH = 0>
-__global__ void k_commit_a(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi) {
+__global__ void HYD_CELL_BOUNDS(BATCH) k_commit_a(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -832,7 +832,7 @@ __global__ void k_wetting_rows(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) 
 // between this pass and BedLoad changes them. On row N the speed is the
 // first half-step's (its hesoK launch shape never reaches row N).
 template <class R, int HORIZ, int BATCH = 0>
-__global__ void k_commit_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi, int qb) {
+__global__ void HYD_CELL_BOUNDS(BATCH) k_commit_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi, int qb) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int j = blockIdx.x * blockDim.x + threadIdx.x;

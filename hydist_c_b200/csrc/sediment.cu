@@ -24,7 +24,7 @@ namespace hyd {
 // _bed_load on rows 3..N-2 (BedLoad with the j-sweep's range,
 // engine.cpp:292), cells of the row's wet segments of at least 3 cells.
 template <class R, int BATCH = 0>
-__global__ void k_bed_load(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+__global__ void HYD_CELL_BOUNDS(BATCH) k_bed_load(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   __shared__ int s_first[SEG], s_last[SEG];
@@ -165,7 +165,7 @@ template void launch_bed_feedback<float>(const StateT<float>&, const CoefT<float
 // sweep: one thread per cell, adjacent threads on adjacent cells. DIR 0:
 // the i-sweep (along i, the cell before is (i-1, j)), 1: the j-sweep.
 template <class R, int DIR, int BATCH = 0>
-__global__ void k_fs_rows(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+__global__ void HYD_CELL_BOUNDS(BATCH) k_fs_rows(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
