@@ -125,8 +125,8 @@ struct Batch {
 // of them in FP64); capped at 64, eight CTAs per SM: the 64-member ensemble
 // of 1024x512 steps in 14.9 against 16.9 ms (FP64), 10.35 against 10.69
 // (FP32), 12.28 against 12.63 (FP32 refined), their few spills in L1. The
-// single-scenario variants keep their occupancy (one CTA per SM is no bound).
-#define HYD_CELL_BOUNDS(BATCH) __launch_bounds__(128, (BATCH) ? 8 : 1)
+// single-scenario kernels are separate entry points without the bound.
+#define HYD_CELL_BOUNDS __launch_bounds__(128, 8)
 
 // The state and coefficients a kernel works on: its by-value arguments, or
 // with BATCH those of member blockIdx.z.

@@ -394,7 +394,7 @@ __device__ void channel_wave_cell(const StateT<R>& S, double dX, double dY, doub
 }
 
 template <class R, int BATCH = 0>
-__global__ void HYD_CELL_BOUNDS(BATCH) k_boundary(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, double half) {
+__device__ __forceinline__ void boundary_cells(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, double half) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const double dX = (double)c.dX, dY = (double)c.dY;
@@ -588,7 +588,7 @@ __device__ __forceinline__ bool find_seg(const int* dau, const int* cuoi, int n,
 // vSolver driven by solveV (UVZSolver_multithread.cpp:607-663, 961-978);
 // the cell's arithmetic is v_new (explicit.cuh).
 template <class R, int BATCH = 0>
-__global__ void HYD_CELL_BOUNDS(BATCH) k_solve_v(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+__device__ __forceinline__ void solve_v_cells(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   // the block's cells share one row: its segment table goes to shared memory
@@ -619,7 +619,7 @@ __global__ void HYD_CELL_BOUNDS(BATCH) k_solve_v(StateT<R> S_arg, CoefT<R> c_arg
 // uSolver driven by solveU (UVZSolver_multithread.cpp:724-795, 938-959);
 // the cell's arithmetic is u_new (explicit.cuh).
 template <class R, int BATCH = 0>
-__global__ void HYD_CELL_BOUNDS(BATCH) k_solve_u(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+__device__ __forceinline__ void solve_u_cells(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int col = blockIdx.x * blockDim.x + threadIdx.x + 2;
@@ -700,7 +700,7 @@ __device__ __forceinline__ R vth_heso_cell(const StateT<R>& S, const CoefT<R>& c
 // Find_VTH + hesoK on rows 1..vth_hi: nothing between this commit and the
 // concentration sweep changes what they read.
 template <class R, int BATCH = 0>
-__global__ void HYD_CELL_BOUNDS(BATCH) k_commit_a(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi) {
+__device__ __forceinline__ void commit_a_cells(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -832,7 +832,7 @@ __global__ void k_wetting_rows(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) 
 // between this pass and BedLoad changes them. On row N the speed is the
 // first half-step's (its hesoK launch shape never reaches row N).
 template <class R, int HORIZ, int BATCH = 0>
-__global__ void HYD_CELL_BOUNDS(BATCH) k_commit_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi, int qb) {
+__device__ __forceinline__ void commit_b_cells(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi, int qb) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -909,6 +909,55 @@ static inline dim3 grid2(int nx, int ny, int bx) { return dim3(cdiv(nx, bx), ny)
 
 // Launches a step kernel for one scenario (ks, b.n == 0) or for every
 // member of a batch (kb, grid z = members).
+// Entry points of the passes above: the single-scenario kernels unbounded,
+// the batch ones (suffix _b) under HYD_CELL_BOUNDS. A bound changes ptxas's
+// register choice even where it does not bind, so the two are separate
+// kernels.
+template <class R, int BATCH = 0>
+__global__ void k_boundary(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, double half) {
+  boundary_cells<R, BATCH>(S_arg, c_arg, b_arg, half);
+}
+template <class R>
+__global__ void HYD_CELL_BOUNDS k_boundary_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, double half) {
+  boundary_cells<R, 1>(S_arg, c_arg, b_arg, half);
+}
+
+template <class R, int BATCH = 0>
+__global__ void k_solve_v(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  solve_v_cells<R, BATCH>(S_arg, c_arg, b_arg);
+}
+template <class R>
+__global__ void HYD_CELL_BOUNDS k_solve_v_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  solve_v_cells<R, 1>(S_arg, c_arg, b_arg);
+}
+
+template <class R, int BATCH = 0>
+__global__ void k_solve_u(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  solve_u_cells<R, BATCH>(S_arg, c_arg, b_arg);
+}
+template <class R>
+__global__ void HYD_CELL_BOUNDS k_solve_u_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  solve_u_cells<R, 1>(S_arg, c_arg, b_arg);
+}
+
+template <class R, int BATCH = 0>
+__global__ void k_commit_a(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi) {
+  commit_a_cells<R, BATCH>(S_arg, c_arg, b_arg, vth_hi);
+}
+template <class R>
+__global__ void HYD_CELL_BOUNDS k_commit_a_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi) {
+  commit_a_cells<R, 1>(S_arg, c_arg, b_arg, vth_hi);
+}
+
+template <class R, int HORIZ, int BATCH = 0>
+__global__ void k_commit_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi, int qb) {
+  commit_b_cells<R, HORIZ, BATCH>(S_arg, c_arg, b_arg, vth_hi, qb);
+}
+template <class R, int HORIZ>
+__global__ void HYD_CELL_BOUNDS k_commit_b_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg, int vth_hi, int qb) {
+  commit_b_cells<R, HORIZ, 1>(S_arg, c_arg, b_arg, vth_hi, qb);
+}
+
 template <class R, class KS, class KB, class... A>
 static void launch2(KS ks, KB kb, dim3 g, int bs, cudaStream_t st, const StateT<R>& S,
                     const CoefT<R>& c, const Batch<R>& b, A... a) {
@@ -920,6 +969,8 @@ static void launch2(KS ks, KB kb, dim3 g, int bs, cudaStream_t st, const StateT<
   }
 }
 #define HYD_K2(name, ...) name<__VA_ARGS__, 0>, name<__VA_ARGS__, 1>
+// the same for the passes with separate batch entry points (name_b)
+#define HYD_K2B(name, ...) name<__VA_ARGS__, 0>, name##_b<__VA_ARGS__>
 
 template <class R>
 void launch_init(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
@@ -937,7 +988,7 @@ void launch_preprocess(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
 
 template <class R>
 void launch_boundary(const StateT<R>& S, const CoefT<R>& c, cudaStream_t st) {
-  launch2(HYD_K2(k_boundary, R), dim3(cdiv(max(S.M, S.N), 128)), 128, st, S, c, Batch<R>{}, 0.0);
+  launch2(HYD_K2B(k_boundary, R), dim3(cdiv(max(S.M, S.N), 128)), 128, st, S, c, Batch<R>{}, 0.0);
 }
 
 template <class R>
@@ -962,7 +1013,7 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   const dim3 cells(cdiv(S.M - 1, 128), S.N - 1);
   const dim3 smooth(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS));
   const dim3 commit(cdiv(S.M + 1, 128), S.N + 1);
-  launch2(HYD_K2(k_boundary, R), dim3(cdiv(max(S.M, S.N), 128)), 128, st, S, c, b, 0.5 * (double)c.dT);
+  launch2(HYD_K2B(k_boundary, R), dim3(cdiv(max(S.M, S.N), 128)), 128, st, S, c, b, 0.5 * (double)c.dT);
   if (tr) tr->mark(st, PH_BOUNDARY_X, 1);
   if (tr) tr->kbegin(st, KS_SWEEP_X);
   const int nx = launch_sweep(S, c, 0, st, b);
@@ -972,7 +1023,7 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   // into sv; k_commit_a writes both back (Normalize/update_buffer pairs,
   // engine.cpp:109-124)
   launch2(HYD_K2(k_smooth_full, R, 1, 0), smooth, 128, st, S, c, b);
-  launch2(HYD_K2(k_solve_v, R), cells, 128, st, S, c, b);
+  launch2(HYD_K2B(k_solve_v, R), cells, 128, st, S, c, b);
   launch2(HYD_K2(k_margin_v, R), dim3(cdiv(S.N - 1, 128)), 128, st, S, c, b);
   if (S.reset_h) {
     // wetting and drying along rows (Reset_states_horizontal after
@@ -983,7 +1034,7 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
     launch2(HYD_K2(k_smooth_full, R, 0, 2), smooth, 128, st, S, c, b);
     if (tr) tr->mark(st, PH_EXPLICIT_V, 4);
     launch2(HYD_K2(k_wetting_rows, R), dim3(cdiv(S.N, 128)), 128, st, S, c, b);
-    launch2(HYD_K2(k_commit_b, R, 1), commit, 128, st, S, c, b, sed ? S.N : 0, 0);
+    launch2(HYD_K2B(k_commit_b, R, 1), commit, 128, st, S, c, b, sed ? S.N : 0, 0);
     launch2(HYD_K2(k_interp_fs_rows, R), dim3(cdiv(S.M, 128), 2), 128, st, S, c, b);
     launch2(HYD_K2(k_interp_fs_col, R), dim3(cdiv(S.M, 128)), 128, st, S, c, b);
     launch2(HYD_K2(k_runs_flags, R), grid2(S.M - 1, S.N - 1, 128), 128, st, S, c, b, 2);
@@ -997,7 +1048,7 @@ void launch_half_x(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   // in this half-step, so the segment tables are not rescanned, only the
   // boundary concentration is interpolated (support_funcs.cpp:255-258, 311)
   // with sed, also Find_VTH + hesoK of the concentration step (rows to N)
-  launch2(HYD_K2(k_commit_a, R), commit, 128, st, S, c, b, sed ? S.N : 0);
+  launch2(HYD_K2B(k_commit_a, R), commit, 128, st, S, c, b, sed ? S.N : 0);
   launch2(HYD_K2(k_interp_fs_rows, R), dim3(cdiv(S.M, 128), 2), 128, st, S, c, b);
   launch2(HYD_K2(k_interp_fs_col, R), dim3(cdiv(S.M, 128)), 128, st, S, c, b);
   if (tr) tr->mark(st, PH_COMMIT_X, 3);
@@ -1008,14 +1059,14 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
                    const Batch<R>& b, bool qb) {
   const dim3 smooth(cdiv(S.W, 128), cdiv(S.H, SMOOTH_ROWS));
   const dim3 commit(cdiv(S.M + 1, 128), S.N + 1);
-  launch2(HYD_K2(k_boundary, R), dim3(cdiv(max(S.M, S.N), 128)), 128, st, S, c, b, (double)c.dT * 0.5);
+  launch2(HYD_K2B(k_boundary, R), dim3(cdiv(max(S.M, S.N), 128)), 128, st, S, c, b, (double)c.dT * 0.5);
   if (tr) tr->mark(st, PH_BOUNDARY_Y, 1);
   if (tr) tr->kbegin(st, KS_SWEEP_Y);
   const int ny = launch_sweep(S, c, 1, st, b);
   if (tr) tr->kend(st, KS_SWEEP_Y);
   if (tr) tr->mark(st, PH_SWEEP_Y, ny);
   launch2(HYD_K2(k_smooth_full, R, 0, 0), smooth, 128, st, S, c, b);
-  launch2(HYD_K2(k_solve_u, R), dim3(cdiv(S.M - 1, 128), S.N), 128, st, S, c, b);
+  launch2(HYD_K2B(k_solve_u, R), dim3(cdiv(S.M - 1, 128), S.N), 128, st, S, c, b);
   launch2(HYD_K2(k_margin_u, R), dim3(cdiv(S.M - 1, 128)), 128, st, S, c, b);
   // with update_h_moi and the wetting pass's column flags
   launch2(HYD_K2(k_smooth_full, R, 1, 1), smooth, 128, st, S, c, b);
@@ -1027,7 +1078,7 @@ void launch_half_y(const StateT<R>& S, const CoefT<R>& c, bool sed, cudaStream_t
   // engine.cpp:259-260 never reaches row N)
   // with qb, also Calculate_Qb of the bed change that follows this step's
   // concentration j-sweep
-  launch2(HYD_K2(k_commit_b, R, 0), commit, 128, st, S, c, b, sed ? S.N - 1 : 0,
+  launch2(HYD_K2B(k_commit_b, R, 0), commit, 128, st, S, c, b, sed ? S.N - 1 : 0,
           qb && S.N >= 5 ? 1 : 0);
   // the drying mask is written by the segment scan (k_runs_flags, dry)
   launch_find_limits(S, c, true, st, tr, b);

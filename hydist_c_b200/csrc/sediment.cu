@@ -24,7 +24,7 @@ namespace hyd {
 // _bed_load on rows 3..N-2 (BedLoad with the j-sweep's range,
 // engine.cpp:292), cells of the row's wet segments of at least 3 cells.
 template <class R, int BATCH = 0>
-__global__ void HYD_CELL_BOUNDS(BATCH) k_bed_load(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+__device__ __forceinline__ void bed_load_cells(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   __shared__ int s_first[SEG], s_last[SEG];
@@ -165,7 +165,7 @@ template void launch_bed_feedback<float>(const StateT<float>&, const CoefT<float
 // sweep: one thread per cell, adjacent threads on adjacent cells. DIR 0:
 // the i-sweep (along i, the cell before is (i-1, j)), 1: the j-sweep.
 template <class R, int DIR, int BATCH = 0>
-__global__ void HYD_CELL_BOUNDS(BATCH) k_fs_rows(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+__device__ __forceinline__ void fs_rows_cells(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
@@ -208,6 +208,28 @@ __global__ void k_update_fs(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
   if (!fin) atomicOr(S.err, DEV_NONFINITE);
 }
 
+// Entry points of the passes above: the single-scenario kernels unbounded,
+// the batch ones (suffix _b) under HYD_CELL_BOUNDS. A bound changes ptxas's
+// register choice even where it does not bind, so the two are separate
+// kernels.
+template <class R, int BATCH = 0>
+__global__ void k_bed_load(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  bed_load_cells<R, BATCH>(S_arg, c_arg, b_arg);
+}
+template <class R>
+__global__ void HYD_CELL_BOUNDS k_bed_load_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  bed_load_cells<R, 1>(S_arg, c_arg, b_arg);
+}
+
+template <class R, int DIR, int BATCH = 0>
+__global__ void k_fs_rows(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  fs_rows_cells<R, DIR, BATCH>(S_arg, c_arg, b_arg);
+}
+template <class R, int DIR>
+__global__ void HYD_CELL_BOUNDS k_fs_rows_b(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+  fs_rows_cells<R, DIR, 1>(S_arg, c_arg, b_arg);
+}
+
 template <class R>
 void launch_sediment(const StateT<R>& S, const CoefT<R>& c, bool xdir, bool bed, cudaStream_t st,
                      Trace* tr, const Batch<R>& b) {
@@ -217,8 +239,8 @@ void launch_sediment(const StateT<R>& S, const CoefT<R>& c, bool xdir, bool bed,
   {
     const dim3 gr(cdiv(S.M - 1, 128), S.N - 1, z);
     if (b.n > 0) {
-      if (xdir) k_fs_rows<R, 0, 1><<<gr, 128, 0, st>>>(S, c, b);
-      else k_fs_rows<R, 1, 1><<<gr, 128, 0, st>>>(S, c, b);
+      if (xdir) k_fs_rows_b<R, 0><<<gr, 128, 0, st>>>(S, c, b);
+      else k_fs_rows_b<R, 1><<<gr, 128, 0, st>>>(S, c, b);
     } else {
       if (xdir) k_fs_rows<R, 0, 0><<<gr, 128, 0, st>>>(S, c, b);
       else k_fs_rows<R, 1, 0><<<gr, 128, 0, st>>>(S, c, b);
@@ -234,7 +256,7 @@ void launch_sediment(const StateT<R>& S, const CoefT<R>& c, bool xdir, bool bed,
     // the bed change once per step, after the j-sweep (engine.cpp:290-293)
     // the flux Qb was computed by this step's second commit (k_commit_b)
     const dim3 gl(cdiv(S.M - 1, 128), S.N - 4, z);
-    if (b.n > 0) k_bed_load<R, 1><<<gl, 128, 0, st>>>(S, c, b);
+    if (b.n > 0) k_bed_load_b<R><<<gl, 128, 0, st>>>(S, c, b);
     else k_bed_load<R, 0><<<gl, 128, 0, st>>>(S, c, b);
     launched += 1;
     if (S.bed_fb) {
