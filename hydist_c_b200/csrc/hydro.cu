@@ -492,8 +492,10 @@ constexpr int SMOOTH_ROWS = 4;
 
 // isU: t_u (else t_v); hmoi: with update_h_moi and the column flags. Both
 // are template parameters: each launch compiles to its own variant.
+// (ten CTAs per SM, eight for a batch: 3 us less per FP32 step on 2048x1024)
 template <class R, int isU, int hmoi, int BATCH = 0>
-__global__ void k_smooth_full(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+__global__ void __launch_bounds__(128, BATCH ? 8 : 10)
+    k_smooth_full(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
   const StateT<R> S = member_state<BATCH>(S_arg, b_arg);
   const CoefT<R> c = member_coef<BATCH>(c_arg, b_arg);
   constexpr int RB = SMOOTH_ROWS;

@@ -212,8 +212,13 @@ __global__ void k_update_fs(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
 // the batch ones (suffix _b) under HYD_CELL_BOUNDS. A bound changes ptxas's
 // register choice even where it does not bind, so the two are separate
 // kernels.
+// (the single-scenario ones bounded as well where that measured faster: in FP64
+// the bed load at seven CTAs per SM and the concentration rows at ten, 7 us
+// less per step on 2048x1024; in FP32 the bounds keep ptxas's own choice,
+// 48 and 32 registers, a looser bound having cost 4 us)
 template <class R, int BATCH = 0>
-__global__ void k_bed_load(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+__global__ void __launch_bounds__(128, sizeof(R) == 8 ? 7 : 10)
+    k_bed_load(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
   bed_load_cells<R, BATCH>(S_arg, c_arg, b_arg);
 }
 template <class R>
@@ -222,7 +227,8 @@ __global__ void HYD_CELL_BOUNDS k_bed_load_b(StateT<R> S_arg, CoefT<R> c_arg, Ba
 }
 
 template <class R, int DIR, int BATCH = 0>
-__global__ void k_fs_rows(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
+__global__ void __launch_bounds__(128, sizeof(R) == 8 ? 10 : 16)
+    k_fs_rows(StateT<R> S_arg, CoefT<R> c_arg, Batch<R> b_arg) {
   fs_rows_cells<R, DIR, BATCH>(S_arg, c_arg, b_arg);
 }
 template <class R, int DIR>
